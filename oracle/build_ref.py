@@ -1,0 +1,123 @@
+#!/usr/bin/env python3
+"""Build the reference's own sources into oracle/_ref/ (test infrastructure).
+
+The reference (alexanderchasteen/Staggered_Fermions_HMC) fixes the lattice
+size, the fermion mass and the CG tolerance as compile-time constants in its
+Parameters.h (Parameters.h:9-24) and needs Eigen, which is absent here.  This
+recipe therefore builds one binary per (L, T, mass, tol) in a directory of
+symbolic links to the unmodified reference files, next to:
+
+  * a generated Parameters.h with the same constant names, and
+  * the project's Eigen-API subset header (oracle/eigen_subset).
+
+Only Lattice.cpp, Fermions.cpp, SU3_Sampling.cpp and rng.cpp are compiled,
+together with oracle/ref_harness.cpp.  Outputs go to oracle/_ref/<tag>/ only.
+Nothing here runs the reference's own build (submit_roar.slurm).
+
+usage: python oracle/build_ref.py [L T mass tol] ...   (default: the fixture set)
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("SFH_REFERENCE_DIR", "/root/reference")
+OUT = os.path.join(HERE, "_ref")
+SOURCES = ["Lattice.cpp", "Fermions.cpp", "SU3_Sampling.cpp", "rng.cpp"]
+HEADERS = ["Lattice.h", "Fermions.h", "SU3_Sampling.h", "rng.h"]
+
+# (L, T, mass, tol): the golden-fixture lattices and the timing lattices
+DEFAULT_CONFIGS = [
+    (4, 4, 0.1, 1e-12),
+    (4, 6, 0.5, 1e-12),
+    (8, 8, 0.1, 1e-10),
+    (16, 16, 0.1, 1e-10),
+]
+
+
+def tag(L, T, mass, tol):
+    return f"L{L}T{T}_m{mass:g}_tol{tol:g}"
+
+
+def parameters_h(L, T, mass, tol, maxit=50000, eps=1e-2, nsteps=100):
+    """Generated stand-in for the reference Parameters.h (same names)."""
+    V = L * L * L * T
+    return f"""// generated by oracle/build_ref.py: lattice {L}^3x{T}, mass {mass!r}, tol {tol!r}
+#pragma once
+#include <vector>
+#include <array>
+#include <cmath>
+#include <random>
+constexpr int Spatial_Size = {L};
+constexpr int temporal_size = {T};
+constexpr int array_size = 4*Spatial_Size*Spatial_Size*Spatial_Size*18*temporal_size;
+constexpr int Nplaq = Spatial_Size*Spatial_Size*Spatial_Size*temporal_size*6;
+const int maxdistance = std::floor(Spatial_Size/2)-1;
+const double fermion_mass = {mass!r};
+const int Staggered_Fermion_field_indices = {6 * V};
+const int conjugate_field_array_size = {72 * V};
+const double epsilon = {eps!r};
+const int number_of_steps_fermion = {nsteps};
+const double tol = {tol!r};
+const int max_iter = {maxit};
+constexpr double dbeta = 0.5;
+constexpr double beta_min = 4.1;
+constexpr int CONFIG = 1;
+constexpr double beta_max = beta_min + CONFIG * dbeta;
+constexpr std::array<double, CONFIG> make_couplings() {{
+    std::array<double, CONFIG> a{{}};
+    for (int i = 0; i < CONFIG; ++i) a[i] = beta_min + i * dbeta;
+    return a;
+}}
+inline std::array<double, CONFIG> coupling_constants = make_couplings();
+constexpr int thermal_sweeps = 1000;
+constexpr int autocorrelation_sweeps = 100;
+constexpr int measurment_sweeps = 1000;
+constexpr int maxlag = 10;
+constexpr double c_11 = 5.0/3.0;
+constexpr double c_12 = -1.0/12.0;
+"""
+
+
+def build(L, T, mass, tol, verbose=True):
+    d = os.path.join(OUT, tag(L, T, mass, tol))
+    exe = os.path.join(d, "ref_harness")
+    os.makedirs(d, exist_ok=True)
+    for f in SOURCES + HEADERS:
+        link = os.path.join(d, f)
+        if not os.path.lexists(link):
+            os.symlink(os.path.join(REF, f), link)
+    with open(os.path.join(d, "Parameters.h"), "w") as fh:
+        fh.write(parameters_h(L, T, mass, tol))
+    harness = os.path.join(d, "ref_harness.cpp")
+    if not os.path.lexists(harness):
+        os.symlink(os.path.join(HERE, "ref_harness.cpp"), harness)
+    cmd = ["g++", "-std=c++17", "-O3", "-fopenmp", "-w",
+           "-I" + os.path.join(HERE, "eigen_subset"), "-I" + d, "-o", exe]
+    cmd += [os.path.join(d, f) for f in SOURCES] + [harness]
+    if verbose:
+        print("build", tag(L, T, mass, tol), flush=True)
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def exe_path(L, T, mass, tol):
+    return os.path.join(OUT, tag(L, T, mass, tol), "ref_harness")
+
+
+def main(argv):
+    if not os.path.isdir(REF):
+        print(f"reference sources not found at {REF}; nothing to build")
+        return 0
+    configs = DEFAULT_CONFIGS
+    if len(argv) >= 4:
+        configs = []
+        for i in range(0, len(argv) - 3, 4):
+            configs.append((int(argv[i]), int(argv[i + 1]), float(argv[i + 2]), float(argv[i + 3])))
+    for c in configs:
+        build(*c)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

@@ -1,0 +1,941 @@
+/*
+ * sfh_oracle.c — CPU oracle (plain C restatement) of the reference's
+ * staggered-fermion HMC hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  It is loaded by
+ * tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, and
+ * by nothing else.  Every function cites the reference file:line it restates
+ * (alexanderchasteen/Staggered_Fermions_HMC).  Parity of this restatement is
+ * pinned against outputs of the unmodified reference sources (tests/golden)
+ * and the reference's analytic known-answer tests.
+ *
+ * Layouts are the reference's AoS layouts (see sfh_oracle.h).  Dimensions are
+ * runtime values; the reference uses compile-time constants with
+ * Lx = Ly = Lz = Spatial_Size and Lt = temporal_size (Parameters.h:9-10).
+ */
+#include "sfh_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cx;
+
+/* ------------------------------------------------------------------------ */
+/* geometry                                                                  */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int L[4];
+    long V;
+    int* up;    /* [s*4+mu] neighbour s+mu                     */
+    int* dn;    /* [s*4+mu] neighbour s-mu                     */
+    int* bcup;  /* fermion boundary sign of the +mu hop        */
+    int* bcdn;  /* fermion boundary sign of the -mu hop        */
+    int* eta;   /* staggered phase eta_mu(x)                   */
+} tab_t;
+
+static long site_of(const int L[4], const int c[4])
+{
+    return (((long)c[0] * L[1] + c[1]) * L[2] + c[2]) * L[3] + c[3];
+}
+
+static void coords_of(const int L[4], long s, int c[4])
+{
+    c[3] = (int)(s % L[3]); s /= L[3];
+    c[2] = (int)(s % L[2]); s /= L[2];
+    c[1] = (int)(s % L[1]); s /= L[1];
+    c[0] = (int)s;
+}
+
+/* Fermions.cpp:20-96.  eta_mu(x) = prod_{nu<mu} (-1)^{x_nu}; the +t hop that
+ * wraps and the -t hop that wraps carry a -1 (anti-periodic in time); spatial
+ * directions are periodic. */
+static void tab_fill(const int L[4], int* up, int* dn, int* bcup, int* bcdn,
+                     int* eta)
+{
+    long V = (long)L[0] * L[1] * L[2] * L[3];
+    for (long s = 0; s < V; ++s) {
+        int c[4];
+        coords_of(L, s, c);
+        for (int mu = 0; mu < 4; ++mu) {
+            int e = 1;
+            for (int nu = 0; nu < mu; ++nu)
+                if (c[nu] & 1) e = -e;
+            eta[s * 4 + mu] = e;
+
+            int cu[4] = {c[0], c[1], c[2], c[3]};
+            int bu = 1;
+            cu[mu] += 1;
+            if (cu[mu] >= L[mu]) {
+                cu[mu] -= L[mu];
+                if (mu == 3) bu = -1;
+            }
+            up[s * 4 + mu] = (int)site_of(L, cu);
+            bcup[s * 4 + mu] = bu;
+
+            int cd[4] = {c[0], c[1], c[2], c[3]};
+            int bd = 1;
+            if (cd[mu] == 0) {
+                cd[mu] = L[mu] - 1;
+                if (mu == 3) bd = -1;
+            } else {
+                cd[mu] -= 1;
+            }
+            dn[s * 4 + mu] = (int)site_of(L, cd);
+            bcdn[s * 4 + mu] = bd;
+        }
+    }
+}
+
+static void tab_build(tab_t* t, const int dims[4])
+{
+    memcpy(t->L, dims, sizeof(int) * 4);
+    t->V = (long)dims[0] * dims[1] * dims[2] * dims[3];
+    size_t n = (size_t)t->V * 4;
+    t->up = (int*)malloc(n * sizeof(int));
+    t->dn = (int*)malloc(n * sizeof(int));
+    t->bcup = (int*)malloc(n * sizeof(int));
+    t->bcdn = (int*)malloc(n * sizeof(int));
+    t->eta = (int*)malloc(n * sizeof(int));
+    tab_fill(dims, t->up, t->dn, t->bcup, t->bcdn, t->eta);
+}
+
+static void tab_free(tab_t* t)
+{
+    free(t->up); free(t->dn); free(t->bcup); free(t->bcdn); free(t->eta);
+}
+
+void orc_tables(const int dims[4], int* up, int* dn, int* bc_up, int* bc_dn,
+                int* eta)
+{
+    tab_fill(dims, up, dn, bc_up, bc_dn, eta);
+}
+
+/* ------------------------------------------------------------------------ */
+/* 3x3 complex helpers (row-major, matching the [row][col][re,im] storage)   */
+/* ------------------------------------------------------------------------ */
+
+static const cx* link_at(const double* U, long s, int mu)
+{
+    return (const cx*)(U + (s * 4 + mu) * 18);
+}
+
+static void m_id(cx* a)
+{
+    for (int i = 0; i < 9; ++i) a[i] = 0;
+    a[0] = a[4] = a[8] = 1;
+}
+
+static void m_mul(const cx* a, const cx* b, cx* out)   /* out = a b */
+{
+    cx t[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            cx s = 0;
+            for (int k = 0; k < 3; ++k) s += a[i * 3 + k] * b[k * 3 + j];
+            t[i * 3 + j] = s;
+        }
+    memcpy(out, t, sizeof(t));
+}
+
+static void m_mul_adj(const cx* a, const cx* b, cx* out)  /* out = a b^dag */
+{
+    cx t[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            cx s = 0;
+            for (int k = 0; k < 3; ++k) s += a[i * 3 + k] * conj(b[j * 3 + k]);
+            t[i * 3 + j] = s;
+        }
+    memcpy(out, t, sizeof(t));
+}
+
+static void m_adj(const cx* a, cx* out)
+{
+    cx t[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i * 3 + j] = conj(a[j * 3 + i]);
+    memcpy(out, t, sizeof(t));
+}
+
+static cx m_tr(const cx* a) { return a[0] + a[4] + a[8]; }
+
+static void mv(const cx* a, const cx* v, cx* out)   /* out = a v */
+{
+    for (int i = 0; i < 3; ++i)
+        out[i] = a[i * 3 + 0] * v[0] + a[i * 3 + 1] * v[1] + a[i * 3 + 2] * v[2];
+}
+
+static void mdv(const cx* a, const cx* v, cx* out)  /* out = a^dag v */
+{
+    for (int i = 0; i < 3; ++i)
+        out[i] = conj(a[0 * 3 + i]) * v[0] + conj(a[1 * 3 + i]) * v[1] +
+                 conj(a[2 * 3 + i]) * v[2];
+}
+
+/* ------------------------------------------------------------------------ */
+/* staggered operator                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Fermions.cpp:218-247 (sign=+1) and 254-283 (sign=-1). */
+static void dirac_tab(const tab_t* t, double mass, int sign, const double* U,
+                      const double* in, double* out)
+{
+    const cx* psi = (const cx*)in;
+    cx* res = (cx*)out;
+    long V = t->V;
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s) {
+        cx r[3], tmp[3];
+        for (int c = 0; c < 3; ++c) r[c] = mass * psi[s * 3 + c];
+        for (int mu = 0; mu < 4; ++mu) {
+            long k = s * 4 + mu;
+            double cf = 0.5 * t->eta[k] * t->bcup[k] * sign;
+            mv(link_at(U, s, mu), psi + (long)t->up[k] * 3, tmp);
+            for (int c = 0; c < 3; ++c) r[c] += cf * tmp[c];
+            long d = t->dn[k];
+            double cb = 0.5 * t->eta[k] * t->bcdn[k] * sign;
+            mdv(link_at(U, d, mu), psi + d * 3, tmp);
+            for (int c = 0; c < 3; ++c) r[c] -= cb * tmp[c];
+        }
+        for (int c = 0; c < 3; ++c) res[s * 3 + c] = r[c];
+    }
+}
+
+void orc_dirac(const int dims[4], double mass, int sign, const double* U,
+               const double* in, double* out)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    dirac_tab(&t, mass, sign >= 0 ? 1 : -1, U, in, out);
+    tab_free(&t);
+}
+
+/* Fermions.cpp:530-547: temp = D^dag in; out = D temp. */
+static void ddag_tab(const tab_t* t, double mass, const double* U,
+                     const double* in, double* out, double* tmp)
+{
+    dirac_tab(t, mass, -1, U, in, tmp);
+    dirac_tab(t, mass, +1, U, tmp, out);
+}
+
+void orc_ddag(const int dims[4], double mass, const double* U,
+              const double* in, double* out)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    double* tmp = (double*)malloc(sizeof(double) * 6 * t.V);
+    ddag_tab(&t, mass, U, in, out, tmp);
+    free(tmp);
+    tab_free(&t);
+}
+
+/* Fermions.cpp:521-528 */
+double orc_dot(long n, const double* a, const double* b)
+{
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (long i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* Fermions.cpp:553-617: plain CG with X0 = 0, stop when r^2 < tol^2 |phi|^2
+ * (recursive residual), breakdown / non-finite checks as in the reference. */
+static int cg_tab(const tab_t* t, double mass, const double* U,
+                  const double* phi, double tol, int maxit, double* X,
+                  int* iters, double* final_rsq)
+{
+    long n = 6 * t->V;
+    double* r = (double*)malloc(sizeof(double) * n);
+    double* p = (double*)malloc(sizeof(double) * n);
+    double* v = (double*)malloc(sizeof(double) * n);
+    double* tmp = (double*)malloc(sizeof(double) * n);
+    int status = ORC_OK, it = 0;
+    memset(X, 0, sizeof(double) * n);
+    memcpy(r, phi, sizeof(double) * n);
+    memcpy(p, phi, sizeof(double) * n);
+    double rsq = orc_dot(n, r, r);
+    double phisq = orc_dot(n, phi, phi);
+    if (phisq < 1e-28) goto done;
+    double target = tol * tol * phisq;
+    for (it = 0; it < maxit; ++it) {
+        if (rsq < target) break;
+        ddag_tab(t, mass, U, p, v, tmp);
+        double pv = orc_dot(n, p, v);
+        if (!isfinite(pv) || fabs(pv) < 1e-30) { status = ORC_ERR_BREAKDOWN; goto done; }
+        double alpha = rsq / pv;
+        if (!isfinite(alpha)) { status = ORC_ERR_BREAKDOWN; goto done; }
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; ++i) {
+            X[i] += alpha * p[i];
+            r[i] -= alpha * v[i];
+        }
+        double rnew = orc_dot(n, r, r);
+        double beta = rnew / rsq;
+        if (!isfinite(beta)) { status = ORC_ERR_BREAKDOWN; goto done; }
+        rsq = rnew;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n; ++i) p[i] = r[i] + beta * p[i];
+    }
+    if (rsq >= target) status = ORC_ERR_NOCONV;
+done:
+    if (iters) *iters = it;
+    if (final_rsq) *final_rsq = rsq;
+    free(r); free(p); free(v); free(tmp);
+    return status;
+}
+
+int orc_cg(const int dims[4], double mass, const double* U, const double* phi,
+           double tol, int maxit, double* X, int* iters, double* final_rsq)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    int st = cg_tab(&t, mass, U, phi, tol, maxit, X, iters, final_rsq);
+    tab_free(&t);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* staples and gauge force                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Product of links along a lattice path.  step = +(mu+1) walks forward in mu
+ * (multiplies U_mu(pos)), step = -(mu+1) walks backward (multiplies
+ * U_mu(pos-mu)^dag).  Gauge links are periodic in every direction
+ * (Lattice.cpp:213-235). */
+static void path_product(const tab_t* t, const double* U, long start,
+                         const int* steps, int nsteps, cx* out)
+{
+    cx m[9];
+    m_id(m);
+    long pos = start;
+    for (int i = 0; i < nsteps; ++i) {
+        int st = steps[i];
+        int mu = (st > 0 ? st : -st) - 1;
+        if (st > 0) {
+            m_mul(m, link_at(U, pos, mu), m);
+            pos = t->up[pos * 4 + mu];
+        } else {
+            pos = t->dn[pos * 4 + mu];
+            m_mul_adj(m, link_at(U, pos, mu), m);
+        }
+    }
+    memcpy(out, m, sizeof(m));
+}
+
+/* Plaquette staple sum A1 for link (s, mu), Lattice.cpp:249-313: the paths
+ * from x+mu back to x, so that U_mu(x) A1 is a sum of closed plaquettes. */
+static void staple_plaq(const tab_t* t, const double* U, long s, int mu,
+                        cx* A1)
+{
+    long xp = t->up[s * 4 + mu];
+    int M = mu + 1;
+    for (int i = 0; i < 9; ++i) A1[i] = 0;
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        int N = nu + 1;
+        const int top[3] = {+N, -M, -N};
+        const int bot[3] = {-N, -M, +N};
+        cx m[9];
+        path_product(t, U, xp, top, 3, m);
+        for (int i = 0; i < 9; ++i) A1[i] += m[i];
+        path_product(t, U, xp, bot, 3, m);
+        for (int i = 0; i < 9; ++i) A1[i] += m[i];
+    }
+}
+
+/* Rectangle staple sum A2 for link (s, mu), Lattice.cpp:315-499: the six
+ * 1x2 / 2x1 rectangles per orthogonal direction nu that contain the link,
+ * each as the path from x+mu back to x (types 1..6 of the reference). */
+static void staple_rect(const tab_t* t, const double* U, long s, int mu,
+                        cx* A2)
+{
+    long xp = t->up[s * 4 + mu];
+    int M = mu + 1;
+    for (int i = 0; i < 9; ++i) A2[i] = 0;
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        int N = nu + 1;
+        const int paths[6][5] = {
+            {-N, -N, -M, +N, +N},  /* type 1: short side, below  */
+            {+N, +N, -M, -N, -N},  /* type 2: short side, above  */
+            {+M, -N, -M, -M, +N},  /* type 3: long side, below, link first */
+            {+N, -M, -M, -N, +M},  /* type 4: long side, above, link second */
+            {-N, -M, -M, +N, +M},  /* type 5: long side, below, link second */
+            {+M, +N, -M, -M, -N},  /* type 6: long side, above, link first */
+        };
+        for (int k = 0; k < 6; ++k) {
+            cx m[9];
+            path_product(t, U, xp, paths[k], 5, m);
+            for (int i = 0; i < 9; ++i) A2[i] += m[i];
+        }
+    }
+}
+
+void orc_staples(const int dims[4], const double* U, double* A1, double* A2)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    long V = t.V;
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < 4 * V; ++l) {
+        long s = l / 4;
+        int mu = (int)(l % 4);
+        staple_plaq(&t, U, s, mu, (cx*)(A1 + l * 18));
+        staple_rect(&t, U, s, mu, (cx*)(A2 + l * 18));
+    }
+    tab_free(&t);
+}
+
+/* make a 3x3 traceless: a -= tr(a)/3 I */
+static void m_traceless(cx* a)
+{
+    cx tr3 = m_tr(a) / 3.0;
+    a[0] -= tr3; a[4] -= tr3; a[8] -= tr3;
+}
+
+/* Fermions.cpp:372-384: F = -i (beta/12) (Q - Q^dag), Q = U V,
+ * V = c11 A1 + c12 A2 (Lattice.cpp:502-507); trace removed. */
+static void gauge_force_link(const tab_t* t, double beta, double c11,
+                             double c12, const double* U, long s, int mu,
+                             cx* F)
+{
+    cx A1[9], A2[9], Vs[9], Q[9];
+    staple_plaq(t, U, s, mu, A1);
+    staple_rect(t, U, s, mu, A2);
+    for (int i = 0; i < 9; ++i) Vs[i] = c11 * A1[i] + c12 * A2[i];
+    m_mul(link_at(U, s, mu), Vs, Q);
+    cx f = -I * (beta / 12.0);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            F[i * 3 + j] = f * (Q[i * 3 + j] - conj(Q[j * 3 + i]));
+    m_traceless(F);
+}
+
+void orc_gauge_force(const int dims[4], double beta, double c11, double c12,
+                     const double* U, double* F)
+{
+    tab_t t;
+    tab_build(&t, dims);
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < 4 * t.V; ++l)
+        gauge_force_link(&t, beta, c11, c12, U, l / 4, (int)(l % 4),
+                         (cx*)(F + l * 18));
+    tab_free(&t);
+}
+
+/* Fermions.cpp:443-515: c = eta bc / 4;
+ * A_f = (U Y(x+mu)) X(x)^dag, A_b = Y(x) X(x+mu)^dag U^dag,
+ * F = -i c [(A_f - A_f^dag) + (A_b - A_b^dag)], trace removed. */
+static void fermion_force_link(const tab_t* t, const double* U,
+                               const double* X, const double* Y, long s,
+                               int mu, cx* F)
+{
+    long k = s * 4 + mu;
+    long up = t->up[k];
+    double c = 0.25 * t->eta[k] * t->bcup[k];
+    const cx* Ux = link_at(U, s, mu);
+    const cx* Xx = (const cx*)X + s * 3;
+    const cx* Xu = (const cx*)X + up * 3;
+    const cx* Yx = (const cx*)Y + s * 3;
+    const cx* Yu = (const cx*)Y + up * 3;
+    cx uy[3], Af[9], T[9], Ab[9];
+    mv(Ux, Yu, uy);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            Af[i * 3 + j] = uy[i] * conj(Xx[j]);
+            T[i * 3 + j] = Yx[i] * conj(Xu[j]);
+        }
+    m_mul_adj(T, Ux, Ab);
+    cx f = -I * c;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            cx a = (Af[i * 3 + j] - conj(Af[j * 3 + i])) +
+                   (Ab[i * 3 + j] - conj(Ab[j * 3 + i]));
+            F[i * 3 + j] = f * a;
+        }
+    m_traceless(F);
+}
+
+void orc_fermion_force(const int dims[4], const double* U, const double* X,
+                       const double* Y, double* F)
+{
+    tab_t t;
+    tab_build(&t, dims);
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < 4 * t.V; ++l)
+        fermion_force_link(&t, U, X, Y, l / 4, (int)(l % 4),
+                           (cx*)(F + l * 18));
+    tab_free(&t);
+}
+
+static void full_force_tab(const tab_t* t, double beta, double c11, double c12,
+                           const double* U, const double* X, const double* Y,
+                           double* F)
+{
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < 4 * t->V; ++l) {
+        cx fg[9], ff[9];
+        gauge_force_link(t, beta, c11, c12, U, l / 4, (int)(l % 4), fg);
+        fermion_force_link(t, U, X, Y, l / 4, (int)(l % 4), ff);
+        cx* o = (cx*)(F + l * 18);
+        for (int i = 0; i < 9; ++i) o[i] = fg[i] + ff[i];
+    }
+}
+
+/* Fermions.cpp:640-659 */
+void orc_full_force(const int dims[4], double beta, double c11, double c12,
+                    const double* U, const double* X, const double* Y,
+                    double* F)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    full_force_tab(&t, beta, c11, c12, U, X, Y, F);
+    tab_free(&t);
+}
+
+/* ------------------------------------------------------------------------ */
+/* exp(iQ) by Cayley-Hamilton (Morningstar & Peardon, hep-lat/0311018)       */
+/* ------------------------------------------------------------------------ */
+
+/* Fermions.cpp:834-841 */
+static double sinc_stable(double x)
+{
+    if (fabs(x) <= 0.05) {
+        double x2 = x * x;
+        return 1.0 - (x2 / 6.0) * (1.0 - (x2 / 20.0) * (1.0 - x2 / 42.0));
+    }
+    return sin(x) / x;
+}
+
+/* Fermions.cpp:843-902 */
+static int expiq_cx(const cx* Q, cx* out)
+{
+    cx Q2[9], Q3[9];
+    m_mul(Q, Q, Q2);
+    m_mul(Q2, Q, Q3);
+    cx t3 = m_tr(Q3);
+    if (fabs(cimag(t3)) > 1e-10) return ORC_ERR_DOMAIN;
+    double c0 = creal(t3) / 3.0;
+    double c1 = 0.5 * creal(m_tr(Q2));
+    if (c1 < 0.0) return ORC_ERR_DOMAIN;
+    if (c1 < 1e-12) {
+        for (int i = 0; i < 9; ++i) out[i] = I * Q[i] - 0.5 * Q2[i];
+        out[0] += 1; out[4] += 1; out[8] += 1;
+        return ORC_OK;
+    }
+    int neg = c0 < 0.0;
+    c0 = fabs(c0);
+    double c0max = 2.0 * sqrt(c1 * c1 * c1 / 27.0);
+    double ratio = 1.0;
+    if (c0max > 0.0) {
+        ratio = c0 / c0max;
+        if (ratio > 1.0) ratio = 1.0;
+        if (ratio < -1.0) ratio = -1.0;
+    }
+    double theta = acos(ratio);
+    double w = sqrt(c1) * sin(theta / 3.0);
+    double u = sqrt(c1 / 3.0) * cos(theta / 3.0);
+    double xi = sinc_stable(w), cw = cos(w);
+    cx e2u = cexp(2.0 * I * u), emu = cexp(-I * u);
+    cx h0 = (u * u - w * w) * e2u +
+            emu * (8.0 * u * u * cw + 2.0 * I * u * (3.0 * u * u + w * w) * xi);
+    cx h1 = 2.0 * u * e2u - emu * (2.0 * u * cw - I * (3.0 * u * u - w * w) * xi);
+    cx h2 = e2u - emu * (cw + 3.0 * I * u * xi);
+    double den = 9.0 * u * u - w * w;
+    cx f0 = h0 / den, f1 = h1 / den, f2 = h2 / den;
+    if (neg) {
+        f0 = conj(f0);
+        f1 = -conj(f1);
+        f2 = conj(f2);
+    }
+    for (int i = 0; i < 9; ++i) out[i] = f1 * Q[i] + f2 * Q2[i];
+    out[0] += f0; out[4] += f0; out[8] += f0;
+    return ORC_OK;
+}
+
+int orc_expiq(const double* Q, double* out)
+{
+    cx o[9];
+    int st = expiq_cx((const cx*)Q, o);
+    if (st == ORC_OK) memcpy(out, o, sizeof(o));
+    return st;
+}
+
+int orc_exp_field(long n, double eps, const double* H, double* U)
+{
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long i = 0; i < n; ++i) {
+        cx q[9];
+        const cx* h = (const cx*)(H + i * 18);
+        for (int k = 0; k < 9; ++k) q[k] = eps * h[k];
+        if (expiq_cx(q, (cx*)(U + i * 18)) != ORC_OK) bad = 1;
+    }
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
+/* Fermions.cpp:984-994: U <- exp(i eps P) U for every link. */
+static int link_update_V(long V, double eps, const double* P, double* U)
+{
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long l = 0; l < 4 * V; ++l) {
+        cx q[9], e[9];
+        const cx* p = (const cx*)(P + l * 18);
+        cx* u = (cx*)(U + l * 18);
+        for (int k = 0; k < 9; ++k) q[k] = eps * p[k];
+        if (expiq_cx(q, e) != ORC_OK) { bad = 1; continue; }
+        m_mul(e, u, u);
+    }
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
+int orc_link_update(const int dims[4], double eps, const double* P, double* U)
+{
+    long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
+    return link_update_V(V, eps, P, U);
+}
+
+/* Fermions.cpp:662-678 */
+double orc_trp2(const int dims[4], const double* P)
+{
+    long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
+    double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+    for (long l = 0; l < 4 * V; ++l) {
+        const cx* p = (const cx*)(P + l * 18);
+        cx p2[9];
+        m_mul(p, p, p2);
+        acc += creal(m_tr(p2));
+    }
+    return acc;
+}
+
+/* Lattice.cpp:759-781 */
+double orc_action(const int dims[4], double beta, double c11, double c12,
+                  const double* U)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+    for (long l = 0; l < 4 * t.V; ++l) {
+        cx A1[9], A2[9], m[9];
+        long s = l / 4;
+        int mu = (int)(l % 4);
+        staple_plaq(&t, U, s, mu, A1);
+        staple_rect(&t, U, s, mu, A2);
+        m_mul(link_at(U, s, mu), A1, m);
+        double ap = creal(m_tr(m)) / 4.0;
+        m_mul(link_at(U, s, mu), A2, m);
+        double ar = creal(m_tr(m)) / 6.0;
+        acc += -(beta / 3.0) * (c11 * ap + c12 * ar);
+    }
+    tab_free(&t);
+    return acc;
+}
+
+/* Lattice.cpp:784-804 (sum over links of ReTr(U A1)/3, divided by 4V) */
+double orc_avg_plaq(const int dims[4], const double* U)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    double acc = 0.0;
+#pragma omp parallel for reduction(+ : acc) schedule(static)
+    for (long l = 0; l < 4 * t.V; ++l) {
+        cx A1[9], m[9];
+        staple_plaq(&t, U, l / 4, (int)(l % 4), A1);
+        m_mul(link_at(U, l / 4, (int)(l % 4)), A1, m);
+        acc += creal(m_tr(m)) / 3.0;
+    }
+    double V = (double)t.V;
+    tab_free(&t);
+    return acc / (4.0 * V);
+}
+
+/* ------------------------------------------------------------------------ */
+/* leapfrog: local_initial_half_step / local_leapfrog_steps /                */
+/* local_final_step, Fermions.cpp:967-1028                                   */
+/* ------------------------------------------------------------------------ */
+
+static int force_and_kick(const tab_t* t, double mass, double beta, double c11,
+                          double c12, double kick, double tol, int maxit,
+                          const double* phi, double* P, const double* U,
+                          double* X, double* Y, double* F, long* iters_total)
+{
+    int it = 0;
+    int st = cg_tab(t, mass, U, phi, tol, maxit, X, &it, NULL);
+    if (iters_total) *iters_total += it;
+    if (st != ORC_OK) return st;
+    dirac_tab(t, mass, -1, U, X, Y);                      /* Fermions.cpp:623-633 */
+    full_force_tab(t, beta, c11, c12, U, X, Y, F);
+    long n = 72 * t->V;
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) P[i] -= kick * F[i];
+    return ORC_OK;
+}
+
+int orc_leapfrog(const int dims[4], double mass, double beta, double c11,
+                 double c12, double eps, int n_steps, double tol, int maxit,
+                 const double* phi, double* P, double* U, double* X,
+                 long* cg_iters_total)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    double* Y = (double*)malloc(sizeof(double) * 6 * t.V);
+    double* F = (double*)malloc(sizeof(double) * 72 * t.V);
+    if (cg_iters_total) *cg_iters_total = 0;
+    int st = force_and_kick(&t, mass, beta, c11, c12, eps * 0.5, tol, maxit,
+                            phi, P, U, X, Y, F, cg_iters_total);
+    for (int n = 1; st == ORC_OK && n < n_steps; ++n) {
+        st = link_update_V(t.V, eps, P, U);
+        if (st != ORC_OK) break;
+        st = force_and_kick(&t, mass, beta, c11, c12, eps, tol, maxit, phi, P,
+                            U, X, Y, F, cg_iters_total);
+    }
+    if (st == ORC_OK) st = link_update_V(t.V, eps, P, U);
+    if (st == ORC_OK)
+        st = force_and_kick(&t, mass, beta, c11, c12, eps * 0.5, tol, maxit,
+                            phi, P, U, X, Y, F, cg_iters_total);
+    free(Y); free(F);
+    tab_free(&t);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Polyakov loop                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Lattice.cpp:849-882 */
+void orc_polyakov_grid(const int dims[4], const double* U, double* out)
+{
+    int Lx = dims[0], Ly = dims[1], Lz = dims[2], Lt = dims[3];
+#pragma omp parallel for schedule(static)
+    for (long g = 0; g < (long)Lx * Ly * Lz; ++g) {
+        int c[4] = {(int)(g / ((long)Ly * Lz)), (int)((g / Lz) % Ly),
+                    (int)(g % Lz), 0};
+        cx w[9];
+        m_id(w);
+        for (int tt = 0; tt < Lt; ++tt) {
+            c[3] = tt;
+            m_mul(w, link_at(U, site_of(dims, c), 3), w);
+        }
+        cx tr = m_tr(w);
+        out[2 * g] = creal(tr);
+        out[2 * g + 1] = cimag(tr);
+    }
+}
+
+/* Lattice.cpp:886-948: average of P(m) conj(P(m+d)) over m and over the
+ * displacement vectors d with |d|^2 = r2 (|d_i| <= L/2, d_i != L/2 for even L).
+ * Assumes a cubic spatial volume as the reference does. */
+void orc_polyakov_corr(const int dims[4], const double* grid, int r2,
+                       double* out2)
+{
+    int L = dims[0];
+    int maxd = (int)sqrt((double)r2);
+    if (maxd > L / 2) maxd = L / 2;
+    const cx* P = (const cx*)grid;
+    cx acc = 0;
+    long n = 0;
+    for (int x = 0; x < L; ++x)
+        for (int y = 0; y < L; ++y)
+            for (int z = 0; z < L; ++z) {
+                cx pm = P[((long)x * L + y) * L + z];
+                for (int dx = -maxd; dx <= maxd; ++dx) {
+                    if (dx == L / 2 && L % 2 == 0) continue;
+                    for (int dy = -maxd; dy <= maxd; ++dy) {
+                        if (dy == L / 2 && L % 2 == 0) continue;
+                        for (int dz = -maxd; dz <= maxd; ++dz) {
+                            if (dz == L / 2 && L % 2 == 0) continue;
+                            if (dx * dx + dy * dy + dz * dz != r2) continue;
+                            int nx = (x + dx + L) % L, ny = (y + dy + L) % L,
+                                nz = (z + dz + L) % L;
+                            acc += pm * conj(P[((long)nx * L + ny) * L + nz]);
+                            ++n;
+                        }
+                    }
+                }
+            }
+    if (n > 0) acc /= (double)n;
+    out2[0] = creal(acc);
+    out2[1] = cimag(acc);
+}
+
+/* ------------------------------------------------------------------------ */
+/* smearing                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Smearing.cpp:126-129: traceless anti-Hermitian part */
+static void proj_ah(const cx* m, cx* out)
+{
+    cx a[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            a[i * 3 + j] = 0.5 * (m[i * 3 + j] - conj(m[j * 3 + i]));
+    cx tr3 = (1.0 / 3.0) * m_tr(a);
+    for (int i = 0; i < 9; ++i) out[i] = a[i];
+    out[0] -= tr3; out[4] -= tr3; out[8] -= tr3;
+}
+
+/* U' = exp(coef * proj(G U^dag)) U, with exp(A) = exp(i (-i A)). */
+static int smear_link(const cx* G, const cx* Uold, double coef, cx* out)
+{
+    cx om[9], A[9], q[9], e[9];
+    m_mul_adj(G, Uold, om);
+    proj_ah(om, A);
+    for (int i = 0; i < 9; ++i) q[i] = -I * (A[i] * coef);
+    int st = expiq_cx(q, e);
+    if (st != ORC_OK) return st;
+    m_mul(e, Uold, out);
+    return ORC_OK;
+}
+
+int orc_stout(const int dims[4], double rho, int n_levels, double* U)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    long V = t.V;
+    double* old = (double*)malloc(sizeof(double) * 72 * V);
+    int bad = 0;
+    for (int lev = 0; lev < n_levels && !bad; ++lev) {
+        memcpy(old, U, sizeof(double) * 72 * V);
+#pragma omp parallel for schedule(static) reduction(| : bad)
+        for (long l = 0; l < 4 * V; ++l) {
+            long s = l / 4;
+            int mu = (int)(l % 4);
+            cx C[9], m1[9], m2[9];
+            for (int i = 0; i < 9; ++i) C[i] = 0;
+            for (int nu = 0; nu < 4; ++nu) {
+                if (nu == mu) continue;
+                long xn = t.up[s * 4 + nu], xm = t.up[s * 4 + mu];
+                long xd = t.dn[s * 4 + nu], xdm = t.up[xd * 4 + mu];
+                m_mul(link_at(old, s, nu), link_at(old, xn, mu), m1);
+                m_mul_adj(m1, link_at(old, xm, nu), m1);
+                for (int i = 0; i < 9; ++i) C[i] += m1[i];
+                m_adj(link_at(old, xd, nu), m2);
+                m_mul(m2, link_at(old, xd, mu), m2);
+                m_mul(m2, link_at(old, xdm, nu), m2);
+                for (int i = 0; i < 9; ++i) C[i] += m2[i];
+            }
+            if (smear_link(C, link_at(old, s, mu), rho, (cx*)(U + l * 18)) !=
+                ORC_OK)
+                bad = 1;
+        }
+    }
+    free(old);
+    tab_free(&t);
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
+/* HEX, Smearing.cpp:76-311.  Decorated fields are stored as
+ * [combo][site][9] with combo = (4 mu + nu) 4 + rho (level 1),
+ * 4 mu + nu (level 2), mu (level 3), as in the reference's flat indices
+ * (Smearing.cpp:14-73). */
+int orc_hex(const int dims[4], const double alphas[3], double* U)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    long V = t.V;
+    const cx* Uc = (const cx*)U;
+    cx* G1 = (cx*)malloc(sizeof(cx) * 9 * 64 * V);
+    cx* V1 = (cx*)malloc(sizeof(cx) * 9 * 64 * V);
+    cx* G2 = (cx*)malloc(sizeof(cx) * 9 * 16 * V);
+    cx* V2 = (cx*)malloc(sizeof(cx) * 9 * 16 * V);
+    cx* Unew = (cx*)malloc(sizeof(cx) * 9 * 4 * V);
+    int bad = 0;
+#define LNK(s, mu) (Uc + ((long)(s) * 4 + (mu)) * 9)
+#define F3(arr, a, b, c, s) ((arr) + ((((long)(a) * 4 + (b)) * 4 + (c)) * V + (s)) * 9)
+#define F2(arr, a, b, s) ((arr) + (((long)(a) * 4 + (b)) * V + (s)) * 9)
+    /* step 1 (Smearing.cpp:76-123) */
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = 0; nu < 4; ++nu)
+                for (int rh = 0; rh < 4; ++rh) {
+                    cx* g = F3(G1, mu, nu, rh, s);
+                    for (int i = 0; i < 9; ++i) g[i] = 0;
+                    for (int sg = 0; sg < 4; ++sg) {
+                        if (sg == mu || sg == nu || sg == rh) continue;
+                        long xs = t.up[s * 4 + sg], xm = t.up[s * 4 + mu];
+                        long xd = t.dn[s * 4 + sg], xdm = t.up[xd * 4 + mu];
+                        cx a[9], b[9];
+                        m_mul(LNK(s, sg), LNK(xs, mu), a);
+                        m_mul_adj(a, LNK(xm, sg), a);
+                        m_adj(LNK(xd, sg), b);
+                        m_mul(b, LNK(xd, mu), b);
+                        m_mul(b, LNK(xdm, sg), b);
+                        for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+                    }
+                }
+    /* step 2 (Smearing.cpp:132-155) */
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long s = 0; s < V; ++s)
+        for (int c = 0; c < 64; ++c) {
+            int mu = c / 16;
+            if (smear_link(G1 + ((long)c * V + s) * 9, LNK(s, mu),
+                           alphas[2] * 0.5, V1 + ((long)c * V + s) * 9) != ORC_OK)
+                bad = 1;
+        }
+    /* step 3 (Smearing.cpp:157-209) */
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = 0; nu < 4; ++nu) {
+                cx* g = F2(G2, mu, nu, s);
+                for (int i = 0; i < 9; ++i) g[i] = 0;
+                for (int sg = 0; sg < 4; ++sg) {
+                    if (sg == mu || sg == nu) continue;
+                    long xs = t.up[s * 4 + sg], xm = t.up[s * 4 + mu];
+                    long xd = t.dn[s * 4 + sg], xdm = t.up[xd * 4 + mu];
+                    cx a[9], b[9];
+                    m_mul(F3(V1, sg, mu, nu, s), F3(V1, mu, nu, sg, xs), a);
+                    m_mul_adj(a, F3(V1, sg, mu, nu, xm), a);
+                    m_adj(F3(V1, sg, mu, nu, xd), b);
+                    m_mul(b, F3(V1, mu, nu, sg, xd), b);
+                    m_mul(b, F3(V1, sg, mu, nu, xdm), b);
+                    for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+                }
+            }
+    /* step 4 (Smearing.cpp:213-234) */
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long s = 0; s < V; ++s)
+        for (int c = 0; c < 16; ++c) {
+            int mu = c / 4;
+            if (smear_link(G2 + ((long)c * V + s) * 9, LNK(s, mu),
+                           alphas[1] * 0.5, V2 + ((long)c * V + s) * 9) != ORC_OK)
+                bad = 1;
+        }
+    /* steps 5 and 6 (Smearing.cpp:236-301); Gamma_3 starts at zero */
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu) {
+            cx g[9];
+            for (int i = 0; i < 9; ++i) g[i] = 0;
+            for (int nu = 0; nu < 4; ++nu) {
+                if (nu == mu) continue;
+                long xn = t.up[s * 4 + nu], xm = t.up[s * 4 + mu];
+                long xd = t.dn[s * 4 + nu], xdm = t.up[xd * 4 + mu];
+                cx a[9], b[9];
+                m_mul(F2(V2, nu, mu, s), F2(V2, mu, nu, xn), a);
+                m_mul_adj(a, F2(V2, nu, mu, xm), a);
+                m_adj(F2(V2, nu, mu, xd), b);
+                m_mul(b, F2(V2, mu, nu, xd), b);
+                m_mul(b, F2(V2, nu, mu, xdm), b);
+                for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+            }
+            if (smear_link(g, LNK(s, mu), alphas[0] * 0.5,
+                           Unew + ((long)s * 4 + mu) * 9) != ORC_OK)
+                bad = 1;
+        }
+#undef LNK
+#undef F3
+#undef F2
+    if (!bad) memcpy(U, Unew, sizeof(cx) * 9 * 4 * V);
+    free(G1); free(V1); free(G2); free(V2); free(Unew);
+    tab_free(&t);
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}

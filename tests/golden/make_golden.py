@@ -1,0 +1,79 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own, unmodified functions (built by oracle/build_ref.py
+from the reference sources) on seeded inputs and stores inputs and outputs as
+compressed .npz files.  Needs the reference sources, so it runs only where
+they are present; the committed fixtures are what the tests read.
+
+usage: python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from oracle import build_ref  # noqa: E402
+
+# (L, T, mass, tol, gauge eps, seed, beta, md eps, md steps)
+FIXTURES = [
+    (4, 4, 0.1, 1e-12, 0.3, 1, 4.2, 0.1, 10),
+    (4, 6, 0.5, 1e-12, 1.0, 2, 4.2, 0.05, 4),
+]
+
+
+def exp_test_matrices(rng):
+    """Hermitian traceless inputs for exp(iQ): generic, tiny (small-c1 branch),
+    negative-determinant-sign and diagonal cases."""
+    H = oracle.random_hermitian(rng, 16)
+    scales = np.array([1.0, 0.3, 2.0, 1e-7, 0.05, 1.5, 3.0, 1e-4,
+                       0.7, 0.01, 5.0, 0.2, 1.0, 1.0, 0.9, 0.4])
+    H = H * scales[:, None]
+    H[12] = -H[0]                    # flips the sign of c0
+    d = np.zeros(18)
+    d[0], d[8], d[16] = 0.5, -0.2, -0.3  # diagonal
+    H[13] = d
+    return np.ascontiguousarray(H)
+
+
+def make(L, T, mass, tol, geps, seed, beta, eps, nsteps):
+    dims = (L, L, L, T)
+    exe = build_ref.build(L, T, mass, tol)
+    rng = np.random.default_rng(1000 + seed)
+    U = oracle.random_gauge(dims, geps, seed)
+    phi = rng.standard_normal(6 * oracle.volume(dims))
+    P = oracle.random_momenta(dims, 2000 + seed)
+    H = exp_test_matrices(rng)
+    with tempfile.TemporaryDirectory() as td:
+        ind, outd = os.path.join(td, "in"), os.path.join(td, "out")
+        os.makedirs(ind)
+        os.makedirs(outd)
+        for name, arr in (("U", U), ("phi", phi), ("P", P), ("H", H)):
+            arr.astype("<f8").tofile(os.path.join(ind, name + ".bin"))
+        subprocess.run([exe, "run", ind, outd, repr(beta), repr(eps), str(nsteps)],
+                       check=True)
+        res = {}
+        for f in sorted(os.listdir(outd)):
+            key = f.rsplit(".", 1)[0]
+            dt = "<i4" if f.endswith(".i32") else "<f8"
+            res[key] = np.fromfile(os.path.join(outd, f), dtype=dt)
+    meta = np.array([L, T, mass, tol, geps, seed, beta, eps, nsteps], dtype=np.float64)
+    path = os.path.join(HERE, f"ref_L{L}T{T}.npz")
+    np.savez_compressed(path, meta=meta, U=U, phi=phi, P=P, H=H, **res)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def main():
+    for fx in FIXTURES:
+        make(*fx)
+
+
+if __name__ == "__main__":
+    main()
