@@ -1,0 +1,428 @@
+#!/usr/bin/env python3
+"""Benchmark: mixed-precision batched CG solves/s on one B200 at 1e-10.
+
+Workload (the uneven batch): 64 independent D D^dag solves drawn with seed 7
+from lattices {8^4, 12^4, 16^4, 16^3x32}, masses {0.05, 0.1, 0.2}, gauge
+roughness eps {0.3, 1.0} and 1-8 Gaussian right-hand sides each, all solved by
+one persistent launch to an FP64 true relative residual of 1e-10.  A "solve"
+is one full-lattice solve of D D^dag X = phi (both parity blocks), the unit of
+the reference's solve_CG_DDdagger.  Inputs are synthetic: gauge links
+U = exp(i eps H) and N(0,1) sources from the library's seeded generators.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision f32|f16]
+    python bench.py --impl reference ...     (reference CPU arm)
+
+Prints one JSON line on rank 0.  Multi-GPU runs are replicas (weak scaling,
+no collective on the data path): every rank solves its own copy of the batch.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LATTICES = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 16), (16, 16, 16, 32)]
+MASSES = [0.05, 0.1, 0.2]
+EPSES = [0.3, 1.0]
+TOL = 1e-10
+MAXIT = 20000
+METRIC = "mixed-prec batched CG solves/s vs FP64 CG on 1 B200 @1e-10 resid; Dslash HBM GB/s"
+
+
+def batch_spec(seed=7, nsys=64):
+    rng = np.random.default_rng(seed)
+    spec = []
+    for k in range(nsys):
+        dims = LATTICES[int(rng.integers(len(LATTICES)))]
+        mass = MASSES[int(rng.integers(len(MASSES)))]
+        eps = EPSES[int(rng.integers(len(EPSES)))]
+        nrhs = int(rng.integers(1, 9))
+        spec.append({"dims": dims, "mass": mass, "eps": eps, "nrhs": nrhs,
+                     "gauge_seed": 1000 + k, "rhs_seed": 100000 + 100 * k})
+    return spec
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes of one batched solve (roofline section)
+# ---------------------------------------------------------------------------
+SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16}
+LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24}
+
+
+def solve_bytes(spec, infos, precision):
+    s = SPINOR_BYTES[precision]
+    sx = 48 if precision == "f64" else 24
+    lb = LINK_BYTES[precision]
+    total = 0.0
+    for k, sys_ in enumerate(spec):
+        Vh = int(np.prod(sys_["dims"])) // 2
+        group_iters = [0, 0]
+        for j in range(sys_["nrhs"]):
+            inf = infos[k][j]
+            for par in (0, 1):
+                it = inf["iters_parity"][par]
+                nru = inf["reliable_updates"] / 2.0
+                # per lane-iteration: P1 3s, P2 5s, P3 4s + 2 sx (x in the solver precision)
+                total += it * Vh * (12 * s + 2 * sx)
+                if precision != "f64":
+                    total += nru * Vh * (2 * 8 * 144 + 288 + 3 * 24 + s)
+                group_iters[par] = max(group_iters[par], it + nru)
+        # links: two hop phases per iteration, 8 links per output site
+        for par in (0, 1):
+            total += group_iters[par] * 2 * 8 * lb * Vh
+    return total
+
+
+def build_batch(sfh, spec, precision, device):
+    B = sfh.Batch([(s["dims"], s["mass"], s["nrhs"]) for s in spec], precision=precision, device=device)
+    for k, s in enumerate(spec):
+        B.random_gauge(k, s["eps"], s["gauge_seed"])
+        for j in range(s["nrhs"]):
+            B.random_rhs(k, j, s["rhs_seed"] + j)
+    return B
+
+
+def time_steps(torch, stream_ptr, fn, steps, warmup):
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ev = []
+    with torch.cuda.stream(stream):
+        for _ in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            ev.append((a, b))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines
+# ---------------------------------------------------------------------------
+def cpu_sample(spec, fields, budget_s=12.0, use_ref=True):
+    """Time CPU solves of the batch's own systems (same inputs) in batch order
+    until the budget is spent.  Returns (solves, seconds, kind, description)."""
+    import oracle
+    ref_ok = False
+    if use_ref:
+        from oracle import build_ref
+        ref_ok = True
+    solved, secs, used = 0, 0.0, []
+    kind = "port"
+    for k, s in enumerate(spec):
+        if secs >= budget_s:
+            break
+        U, rhs = fields(k)
+        exe = None
+        if ref_ok:
+            exe = build_ref.exe_path(s["dims"][0], s["dims"][3], s["mass"], TOL)
+            if not (s["dims"][0] == s["dims"][1] == s["dims"][2] and os.path.exists(exe)):
+                exe = None
+        for j, b in enumerate(rhs):
+            if secs >= budget_s:
+                break
+            if exe:
+                t = ref_time_solve(exe, U, b)
+                kind = "reference"
+            else:
+                t0 = time.perf_counter()
+                oracle.cg(s["dims"], s["mass"], U, b, TOL, MAXIT)
+                t = time.perf_counter() - t0
+            secs += t
+            solved += 1
+            used.append(f"{'x'.join(map(str, s['dims']))}/m{s['mass']}")
+    desc = f"first {solved} solves of the batch in order ({', '.join(sorted(set(used)))})"
+    return solved, secs, kind, desc
+
+
+def ref_time_solve(exe, U, b):
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        U.astype("<f8").tofile(os.path.join(td, "U.bin"))
+        b.astype("<f8").tofile(os.path.join(td, "phi.bin"))
+        out = subprocess.run([exe, "time", td, "1"], check=True, capture_output=True, text=True,
+                             env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count())))
+    return float(json.loads(out.stdout.strip().splitlines()[-1])["solve_s"])
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference_arm(args, spec):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    import oracle
+    oracle.lib()
+    total_rhs = sum(s["nrhs"] for s in spec)
+
+    # identical inputs, generated by the library's seeded generators on the GPU
+    # when available; the reference arm itself only times CPU work.
+    fields = make_host_fields(spec, local)
+    vals = []
+    desc = kind = None
+    for step in range(args.warmup + args.steps):
+        n, secs, kind, desc = cpu_sample(spec, fields, budget_s=args.ref_budget)
+        if step >= args.warmup:
+            vals.append(n / secs)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * total_rhs / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "uneven batch: 64 systems, seed 7", "total_solves": total_rhs},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": kind,
+                             "sample": desc},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def make_host_fields(spec, device):
+    cache = {}
+
+    def fields(k):
+        if k not in cache:
+            import staggered_fermions_hmc_b200 as sfh
+            s = spec[k]
+            B = build_batch(sfh, [s], "f64", device)
+            U = B.gauge(0)
+            rhs = [B.rhs(0, j) for j in range(s["nrhs"])]
+            B.close()
+            cache.clear()
+            cache[k] = (U, rhs)
+        return cache[k]
+    return fields
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="sfh", choices=["sfh", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--nsys", type=int, default=64)
+    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    spec = batch_spec(nsys=args.nsys)
+
+    if args.impl == "reference":
+        run_reference_arm(args, spec)
+        return
+
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import staggered_fermions_hmc_b200 as sfh
+    sfh.load_library()
+    total_rhs = sum(s["nrhs"] for s in spec)
+
+    B = build_batch(sfh, spec, args.precision, local)
+
+    def solve():
+        B.solve(tol=TOL, max_iter=MAXIT)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also establishes the iteration counts)
+    for _ in range(args.warmup):
+        solve()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    times = time_steps(torch, B.stream, solve, args.steps, 0)
+    barrier()
+    clk = clocks.stop()
+    infos = [[B.info(k, j) for j in range(s["nrhs"])] for k, s in enumerate(spec)]
+    worst = max(B.true_residual(k, j) for k, s in enumerate(spec) for j in range(s["nrhs"]))
+    ms = statistics.mean(times)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * total_rhs / (ms / 1000.0)
+
+    hbm, peak_kind = peaks()
+    alg_bytes = solve_bytes(spec, infos, args.precision)
+    achieved = alg_bytes / (ms / 1000.0) / 1e9
+
+    # FP64 batched CG on the same batch, same kernel family (the comparison)
+    B64 = build_batch(sfh, spec, "f64", local)
+    B64.solve(tol=TOL, max_iter=MAXIT)
+    t64 = time_steps(torch, B64.stream, lambda: B64.solve(tol=TOL, max_iter=MAXIT), max(2, args.steps // 2), 1)
+    ms64 = statistics.mean(t64)
+    fp64_value = total_rhs / (ms64 / 1000.0)
+    B64.close()
+
+    # end to end through the public API: host (pinned) buffers in and out
+    e2e = None
+    if not args.no_e2e:
+        host_U = []
+        host_b = []
+        for k, s in enumerate(spec):
+            V = int(np.prod(s["dims"]))
+            u = torch.empty(72 * V, dtype=torch.float64, pin_memory=True).numpy()
+            u[:] = B.gauge(k)
+            host_U.append(u)
+            bs = []
+            for j in range(s["nrhs"]):
+                x = torch.empty(6 * V, dtype=torch.float64, pin_memory=True).numpy()
+                x[:] = B.rhs(k, j)
+                bs.append(x)
+            host_b.append(bs)
+        host_x = [[torch.empty(6 * int(np.prod(s["dims"])), dtype=torch.float64, pin_memory=True).numpy()
+                   for _ in range(s["nrhs"])] for s in spec]
+        h2d = sum(u.nbytes for u in host_U) + sum(x.nbytes for bs in host_b for x in bs)
+        d2h = sum(x.nbytes for xs in host_x for x in xs)
+
+        def e2e_step():
+            for k, s in enumerate(spec):
+                B.set_gauge(k, host_U[k])
+                for j in range(s["nrhs"]):
+                    B.set_rhs(k, j, host_b[k][j])
+            B.solve(tol=TOL, max_iter=MAXIT)
+            for k, s in enumerate(spec):
+                for j in range(s["nrhs"]):
+                    host_x[k][j][:] = B.solution(k, j)
+
+        te = time_steps(torch, B.stream, e2e_step, max(2, args.steps // 2), 1)
+        mse = statistics.mean(te)
+        if world > 1:
+            t = torch.tensor([mse], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            mse = float(t.item())
+        e2e = {"value": world * total_rhs / (mse / 1000.0), "unit": "solves/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+        oracle.lib()
+
+        def fields(k):
+            s = spec[k]
+            return B.gauge(k), [B.rhs(k, j) for j in range(s["nrhs"])]
+
+        n, secs, kind, desc = cpu_sample(spec, fields, budget_s=args.ref_budget)
+        cpu = {"value": n / secs, "unit": "solves/s", "cores": os.cpu_count(), "kind": kind,
+               "sample": desc}
+
+    iters = [inf["iters"] for row in infos for inf in row]
+    nru = [inf["reliable_updates"] for row in infos for inf in row]
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "f32" else "f16",
+        "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
+        "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
+                               " x eps{0.3,1.0}, 1-8 RHS, seed 7",
+                   "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "cg_persistent", "alg_bytes_per_launch": alg_bytes},
+        "fp64_batched": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms64,
+                         "mixed_over_fp64": value / world / fp64_value},
+        "solver": {"iters_mean": float(np.mean(iters)), "iters_max": int(max(iters)),
+                   "reliable_updates_mean": float(np.mean(nru)), "worst_true_resid": worst},
+        "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "gpu_launches": args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    B.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,148 @@
+/*
+ * sfh.h — C ABI of the B200 staggered-fermion HMC hot path.
+ *
+ * Plain C: opaque handles, host pointers in the reference's layouts, int
+ * status codes, no exceptions cross this boundary.  Every entry point names
+ * the reference function (alexanderchasteen/Staggered_Fermions_HMC,
+ * file:line) it replaces.
+ *
+ * Host layouts (identical to the reference):
+ *   gauge links, momenta, forces: double[V][4][3][3][2]   (Lattice.cpp:135-168)
+ *   spinors (pseudofermion, X, Y): double[V][3][2]         (Fermions.cpp:99-116)
+ *   site index s = ((x*Ly + y)*Lz + z)*Lt + t              (Fermions.cpp:42)
+ * All four dimensions must be even (even-odd decomposition).
+ *
+ * Threading: one CUDA stream per context (or batch); calls on one handle are
+ * not re-entrant.  Separate handles may be used from separate threads.
+ */
+#ifndef SFH_H
+#define SFH_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the reference throws std::runtime_error / invalid_argument) */
+#define SFH_OK 0
+#define SFH_ERR_NOCONV 1        /* CG not converged (Fermions.cpp:609-614)          */
+#define SFH_ERR_BREAKDOWN 2     /* CG p.Ap or alpha/beta non-finite (:574-600)       */
+#define SFH_ERR_DOMAIN 3        /* exp(iQ) input outside its domain (:848-857)       */
+#define SFH_ERR_NOT_HERMITIAN 4 /* momentum not Hermitian/traceless (:714-716)       */
+#define SFH_ERR_TIMEOUT 5       /* a bounded device wait gave up                     */
+#define SFH_ERR_CUDA 6          /* CUDA runtime error (message in sfh_last_error)    */
+#define SFH_ERR_INVALID 7       /* invalid argument                                  */
+#define SFH_ERR_NOMEM 8         /* device allocation failed                          */
+
+/* solver precisions */
+#define SFH_PREC_F64 0   /* plain FP64 CG, FP64 links and vectors                     */
+#define SFH_PREC_F32 1   /* FP32 12-real links, FP32 vectors, FP64 reliable updates   */
+#define SFH_PREC_F16 2   /* FP16 12-real links, FP16+per-site-scale vectors, FP32 math,
+                            FP64 reliable updates                                      */
+
+typedef struct sfh_ctx sfh_ctx;
+typedef struct sfh_batch sfh_batch;
+
+typedef struct {
+    int dims[4];   /* Lx, Ly, Lz, Lt (Parameters.h:9-10 Spatial_Size, temporal_size) */
+    double mass;   /* staggered mass (Parameters.h:18 fermion_mass)                   */
+    double beta;   /* gauge coupling                                                 */
+    double c11;    /* Symanzik plaquette coefficient (Parameters.h:51), 0 => 5/3      */
+    double c12;    /* Symanzik rectangle coefficient (Parameters.h:52), 0 => -1/12    */
+    int device;    /* CUDA device ordinal                                            */
+} sfh_params;
+
+typedef struct {
+    int status;            /* SFH_OK or an error code                                 */
+    int iters;             /* Krylov iterations (operator applications)               */
+    int iters_parity[2];   /* per parity system in the even-odd solve                  */
+    int reliable_updates;  /* FP64 residual recomputations                             */
+    double rsq_rel;        /* final |r|^2 / |b|^2 of the solver's own residual          */
+    double true_resid;     /* |b - D D^dag x| / |b| recomputed in FP64                  */
+} sfh_cg_info;
+
+/* ---- library / context --------------------------------------------------- */
+int sfh_version(void);
+const char* sfh_status_string(int status);
+
+/* Replaces the compile-time lattice of Parameters.h:9-31 and the static
+ * LatticeTables (Fermions.cpp:20-96) with a runtime context. */
+int sfh_create(const sfh_params* params, sfh_ctx** ctx);
+int sfh_destroy(sfh_ctx* ctx);
+const char* sfh_last_error(const sfh_ctx* ctx);
+int sfh_set_stream(sfh_ctx* ctx, void* cuda_stream);
+void* sfh_get_stream(sfh_ctx* ctx);
+int sfh_set_mass(sfh_ctx* ctx, double mass);
+int sfh_synchronize(sfh_ctx* ctx);
+
+/* gauge field in, out (Lattice.cpp:135-168 get_SU3_at_link / set_link_SU3) */
+int sfh_upload_gauge(sfh_ctx* ctx, const double* links);
+int sfh_download_gauge(sfh_ctx* ctx, double* links);
+
+/* Seeded generators (the reference seeds from std::random_device, rng.cpp:7-15,
+ * and is not reproducible).  Gauge: U = exp(i eps H) per link, H traceless
+ * Hermitian with N(0,1) entries (the distribution of Lattice.cpp:1001-1033;
+ * replaces hot_start_array, Lattice.cpp:198).  Spinor: N(0, sigma^2) per real
+ * component (generateGaussianComplex, Fermions.cpp:207-212, has sigma = 1/sqrt2).
+ * Momenta: P = sum_a 1/2 p_a lambda_a (generate_conjugate_field_configuration,
+ * Fermions.cpp:342-360). */
+int sfh_random_gauge(sfh_ctx* ctx, double eps, unsigned long long seed);
+int sfh_gaussian_spinor(sfh_ctx* ctx, unsigned long long seed, double sigma, double* out);
+int sfh_random_momenta(sfh_ctx* ctx, unsigned long long seed);
+int sfh_upload_momenta(sfh_ctx* ctx, const double* P);
+int sfh_download_momenta(sfh_ctx* ctx, double* P);
+
+/* ---- operators ------------------------------------------------------------ */
+/* out = D in (dagger=0) or D^dag in (dagger=1) on the full lattice:
+ * apply_dirac_operator_at_site_s / apply_dirac_dagger_at_site_s
+ * (Fermions.cpp:218-283); dagger=1 is also solve_Y_field (Fermions.cpp:623-633). */
+int sfh_dirac(sfh_ctx* ctx, int dagger, const double* in, double* out);
+
+/* out = D D^dag in: apply_DDdagger (Fermions.cpp:530-547) */
+int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
+
+/* ---- solver --------------------------------------------------------------- */
+/* X = (D D^dag)^{-1} phi to |r| < tol |phi|: solve_CG_DDdagger / solve_X_field
+ * (Fermions.cpp:553-621).  SFH_PREC_F64 runs the reference's full-lattice CG
+ * (one set of CG scalars over both parities); the mixed precisions solve the
+ * two parity blocks as independent systems and stop on the FP64 true
+ * residual.  info may be NULL. */
+int sfh_cg_solve(sfh_ctx* ctx, const double* phi, double* X, double tol, int maxit,
+                 int precision, sfh_cg_info* info);
+
+/* ---- batched solver (many lattices, masses and right-hand sides) --------- */
+typedef struct {
+    int dims[4];
+    double mass;
+    int nrhs;
+} sfh_system_desc;
+
+#define SFH_BATCH_FULL_LATTICE 1  /* one CG per RHS over both parities, as the
+                                     reference's solve_CG_DDdagger               */
+
+/* No reference counterpart: the reference solves one system at a time
+ * (Fermions.cpp:553).  All systems are solved by one persistent launch. */
+int sfh_batch_create(int device, int nsys, const sfh_system_desc* systems, int precision,
+                     int flags, sfh_batch** batch);
+int sfh_batch_destroy(sfh_batch* batch);
+const char* sfh_batch_last_error(const sfh_batch* batch);
+int sfh_batch_set_stream(sfh_batch* batch, void* cuda_stream);
+void* sfh_batch_get_stream(sfh_batch* batch);
+/* RHS-block width for the fused hop (0 = automatic); the autotuner sets it */
+int sfh_batch_set_rhs_block(sfh_batch* batch, int width);
+int sfh_batch_set_gauge(sfh_batch* batch, int sys, const double* links);
+int sfh_batch_set_rhs(sfh_batch* batch, int sys, int rhs, const double* phi);
+int sfh_batch_solve(sfh_batch* batch, double tol, int maxit);
+int sfh_batch_get_solution(sfh_batch* batch, int sys, int rhs, double* X);
+int sfh_batch_get_info(sfh_batch* batch, int sys, int rhs, sfh_cg_info* info);
+/* seeded device generators and read-back for the batch's inputs */
+int sfh_batch_random_gauge(sfh_batch* batch, int sys, double eps, unsigned long long seed);
+int sfh_batch_random_rhs(sfh_batch* batch, int sys, int rhs, unsigned long long seed, double sigma);
+int sfh_batch_get_gauge(sfh_batch* batch, int sys, double* links);
+int sfh_batch_get_rhs(sfh_batch* batch, int sys, int rhs, double* phi);
+/* FP64 |b - D D^dag x| / |b| for one solution (diagnostic) */
+int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -26,13 +26,13 @@ OUT = os.path.join(HERE, "_ref")
 SOURCES = ["Lattice.cpp", "Fermions.cpp", "SU3_Sampling.cpp", "rng.cpp"]
 HEADERS = ["Lattice.h", "Fermions.h", "SU3_Sampling.h", "rng.h"]
 
-# (L, T, mass, tol): the golden-fixture lattices and the timing lattices
+# (L, T, mass, tol): the golden-fixture lattices, then the uneven-batch
+# benchmark lattices {8^4, 12^4, 16^4, 16^3x32} x masses {0.05, 0.1, 0.2}
 DEFAULT_CONFIGS = [
     (4, 4, 0.1, 1e-12),
     (4, 6, 0.5, 1e-12),
-    (8, 8, 0.1, 1e-10),
-    (16, 16, 0.1, 1e-10),
-]
+] + [(L, T, m, 1e-10) for (L, T) in ((8, 8), (12, 12), (16, 16), (16, 32))
+     for m in (0.05, 0.1, 0.2)]
 
 
 def tag(L, T, mass, tol):
@@ -98,6 +98,10 @@ def build(L, T, mass, tol, verbose=True):
     if verbose:
         print("build", tag(L, T, mass, tol), flush=True)
     subprocess.run(cmd, check=True)
+    # keep only the binary and the generated header: the links point into the
+    # reference tree, which does not travel with the repository
+    for f in SOURCES + HEADERS + ["ref_harness.cpp"]:
+        os.remove(os.path.join(d, f))
     return exe
 
 
@@ -114,8 +118,10 @@ def main(argv):
         configs = []
         for i in range(0, len(argv) - 3, 4):
             configs.append((int(argv[i]), int(argv[i + 1]), float(argv[i + 2]), float(argv[i + 3])))
-    for c in configs:
-        build(*c)
+    import concurrent.futures as cf
+    todo = [c for c in configs if not os.path.exists(exe_path(*c))]
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        list(ex.map(lambda c: build(*c), todo))
     return 0
 
 

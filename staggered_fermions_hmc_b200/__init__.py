@@ -1,0 +1,349 @@
+"""B200-native staggered-fermion HMC hot path (Python binding of libsfh.so).
+
+The product is the C ABI in include/sfh.h, implemented by the CUDA library
+libsfh.so built in-tree by ``staggered_fermions_hmc_b200.build``.  This module
+binds it with ctypes and mirrors the reference's function names
+(alexanderchasteen/Staggered_Fermions_HMC, Fermions.h / Lattice.h) so code
+written against the reference reads the same:
+
+    lat = Lattice(dims=(4, 4, 4, 4), mass=0.1, beta=4.2)
+    lat.upload_gauge(U)                    # double[V*72], reference layout
+    out = lat.apply_DDdagger(psi)          # Fermions.cpp:530
+    X = lat.solve_CG_DDdagger(phi, tol)    # Fermions.cpp:553
+    Y = lat.solve_Y_field(X)               # Fermions.cpp:623
+
+There is no CPU fallback: importing raises if libsfh.so is missing, and every
+call runs on the GPU.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libsfh.so")
+
+SFH_OK = 0
+SFH_ERR_NOCONV = 1
+SFH_ERR_BREAKDOWN = 2
+SFH_ERR_DOMAIN = 3
+SFH_ERR_NOT_HERMITIAN = 4
+SFH_ERR_TIMEOUT = 5
+SFH_ERR_CUDA = 6
+SFH_ERR_INVALID = 7
+SFH_ERR_NOMEM = 8
+
+PREC_F64, PREC_F32, PREC_F16 = 0, 1, 2
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16}
+BATCH_FULL_LATTICE = 1
+
+
+class SfhError(RuntimeError):
+    """Raised for a non-zero status; the reference throws std::runtime_error
+    (CG breakdown / non-convergence, Fermions.cpp:574-614) or
+    std::invalid_argument (exp domain, Fermions.cpp:848-857)."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+class CgParams(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 4), ("mass", ctypes.c_double), ("beta", ctypes.c_double),
+                ("c11", ctypes.c_double), ("c12", ctypes.c_double), ("device", ctypes.c_int)]
+
+
+class CgInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iters", ctypes.c_int), ("iters_parity", ctypes.c_int * 2),
+                ("reliable_updates", ctypes.c_int), ("rsq_rel", ctypes.c_double),
+                ("true_resid", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"status": self.status, "iters": self.iters,
+                "iters_parity": [self.iters_parity[0], self.iters_parity[1]],
+                "reliable_updates": self.reliable_updates, "rsq_rel": self.rsq_rel,
+                "true_resid": self.true_resid}
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int * 4), ("mass", ctypes.c_double), ("nrhs", ctypes.c_int)]
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+
+# name -> (restype, argtypes); the list is also the ABI symbol inventory
+SIGNATURES = {
+    "sfh_version": (ctypes.c_int, []),
+    "sfh_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "sfh_create": (ctypes.c_int, [ctypes.POINTER(CgParams), ctypes.POINTER(_VP)]),
+    "sfh_destroy": (ctypes.c_int, [_VP]),
+    "sfh_last_error": (ctypes.c_char_p, [_VP]),
+    "sfh_set_stream": (ctypes.c_int, [_VP, _VP]),
+    "sfh_get_stream": (_VP, [_VP]),
+    "sfh_set_mass": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "sfh_synchronize": (ctypes.c_int, [_VP]),
+    "sfh_upload_gauge": (ctypes.c_int, [_VP, _D]),
+    "sfh_download_gauge": (ctypes.c_int, [_VP, _D]),
+    "sfh_random_gauge": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_ulonglong]),
+    "sfh_gaussian_spinor": (ctypes.c_int, [_VP, ctypes.c_ulonglong, ctypes.c_double, _D]),
+    "sfh_random_momenta": (ctypes.c_int, [_VP, ctypes.c_ulonglong]),
+    "sfh_upload_momenta": (ctypes.c_int, [_VP, _D]),
+    "sfh_download_momenta": (ctypes.c_int, [_VP, _D]),
+    "sfh_dirac": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
+    "sfh_ddag": (ctypes.c_int, [_VP, _D, _D]),
+    "sfh_cg_solve": (ctypes.c_int, [_VP, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(CgInfo)]),
+    "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
+                                        ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
+    "sfh_batch_destroy": (ctypes.c_int, [_VP]),
+    "sfh_batch_last_error": (ctypes.c_char_p, [_VP]),
+    "sfh_batch_set_stream": (ctypes.c_int, [_VP, _VP]),
+    "sfh_batch_get_stream": (_VP, [_VP]),
+    "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sfh_batch_set_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "sfh_batch_set_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_batch_solve": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_batch_get_solution": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_batch_get_info": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CgInfo)]),
+    "sfh_batch_random_gauge": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong]),
+    "sfh_batch_random_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                            ctypes.c_double]),
+    "sfh_batch_get_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "sfh_batch_get_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_batch_true_residual": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+}
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load libsfh.so; raises (no fallback) if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with "
+                              "`python -m staggered_fermions_hmc_b200.build`")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _dptr(a):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_D)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def volume(dims):
+    return int(np.prod(dims))
+
+
+class Lattice:
+    """One lattice on one GPU: the runtime replacement of the reference's
+    compile-time lattice (Parameters.h) and its static tables
+    (Fermions.cpp:20-96).  Methods keep the reference's names."""
+
+    def __init__(self, dims, mass, beta=4.2, c11=5.0 / 3.0, c12=-1.0 / 12.0, device=0):
+        self.lib = load_library()
+        self.dims = tuple(int(d) for d in dims)
+        self.V = volume(self.dims)
+        p = CgParams((ctypes.c_int * 4)(*self.dims), mass, beta, c11, c12, device)
+        h = _VP()
+        st = self.lib.sfh_create(ctypes.byref(p), ctypes.byref(h))
+        if st != SFH_OK:
+            raise SfhError(st, f"sfh_create: {self.lib.sfh_status_string(st).decode()}")
+        self.h = h
+        self.mass = mass
+        self.beta = beta
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != SFH_OK:
+            msg = self.lib.sfh_last_error(self.h)
+            raise SfhError(st, f"{what}: {self.lib.sfh_status_string(st).decode()}: "
+                               f"{msg.decode() if msg else ''}")
+
+    @property
+    def stream(self):
+        return self.lib.sfh_get_stream(self.h)
+
+    def set_mass(self, m):
+        self._check(self.lib.sfh_set_mass(self.h, m), "set_mass")
+        self.mass = m
+
+    def upload_gauge(self, U):
+        U = _f64(U).reshape(-1)
+        assert U.size == 72 * self.V
+        self._check(self.lib.sfh_upload_gauge(self.h, _dptr(U)), "upload_gauge")
+
+    def download_gauge(self):
+        out = np.empty(72 * self.V)
+        self._check(self.lib.sfh_download_gauge(self.h, _dptr(out)), "download_gauge")
+        return out
+
+    # --- seeded generators ---------------------------------------------------
+    def random_gauge(self, eps, seed):
+        """U = exp(i eps H) on every link (seeded hot start)."""
+        self._check(self.lib.sfh_random_gauge(self.h, eps, seed), "random_gauge")
+
+    def gaussian_spinor(self, seed, sigma=1.0):
+        out = np.empty(6 * self.V)
+        self._check(self.lib.sfh_gaussian_spinor(self.h, seed, sigma, _dptr(out)), "gaussian_spinor")
+        return out
+
+    def generate_conjugate_field_configuration(self, seed):
+        """Fermions.cpp:342-360, seeded; stays on the device."""
+        self._check(self.lib.sfh_random_momenta(self.h, seed), "random_momenta")
+
+    def upload_momenta(self, P):
+        P = _f64(P).reshape(-1)
+        self._check(self.lib.sfh_upload_momenta(self.h, _dptr(P)), "upload_momenta")
+
+    def download_momenta(self):
+        out = np.empty(72 * self.V)
+        self._check(self.lib.sfh_download_momenta(self.h, _dptr(out)), "download_momenta")
+        return out
+
+    # --- Fermions.cpp:218-283 --------------------------------------------
+    def apply_dirac_operator(self, psi):
+        psi = _f64(psi).reshape(-1)
+        out = np.empty_like(psi)
+        self._check(self.lib.sfh_dirac(self.h, 0, _dptr(psi), _dptr(out)), "dirac")
+        return out
+
+    def apply_dirac_dagger(self, psi):
+        psi = _f64(psi).reshape(-1)
+        out = np.empty_like(psi)
+        self._check(self.lib.sfh_dirac(self.h, 1, _dptr(psi), _dptr(out)), "dirac_dagger")
+        return out
+
+    # --- Fermions.cpp:530-547 ----------------------------------------------
+    def apply_DDdagger(self, psi):
+        psi = _f64(psi).reshape(-1)
+        out = np.empty_like(psi)
+        self._check(self.lib.sfh_ddag(self.h, _dptr(psi), _dptr(out)), "apply_DDdagger")
+        return out
+
+    # --- Fermions.cpp:553-633 ----------------------------------------------
+    def solve_CG_DDdagger(self, phi, tol=1e-12, max_iter=50000, precision="f64", info=False):
+        phi = _f64(phi).reshape(-1)
+        X = np.empty_like(phi)
+        inf = CgInfo()
+        st = self.lib.sfh_cg_solve(self.h, _dptr(phi), _dptr(X), tol, max_iter,
+                                   PRECISIONS[precision], ctypes.byref(inf))
+        self._check(st, "solve_CG_DDdagger")
+        return (X, inf.as_dict()) if info else X
+
+    def solve_X_field(self, phi, tol=1e-12, max_iter=50000, precision="f64"):
+        return self.solve_CG_DDdagger(phi, tol, max_iter, precision)
+
+    def solve_Y_field(self, X):
+        return self.apply_dirac_dagger(X)
+
+
+class Batch:
+    """Many independent D D^dag solves (lattices, masses, right-hand sides)
+    solved by one persistent launch.  No reference counterpart."""
+
+    def __init__(self, systems, precision="f32", full_lattice=False, device=0):
+        self.lib = load_library()
+        n = len(systems)
+        arr = (SystemDesc * n)()
+        self.systems = []
+        for k, (dims, mass, nrhs) in enumerate(systems):
+            arr[k] = SystemDesc((ctypes.c_int * 4)(*dims), mass, nrhs)
+            self.systems.append((tuple(dims), float(mass), int(nrhs)))
+        h = _VP()
+        st = self.lib.sfh_batch_create(device, n, arr, PRECISIONS[precision],
+                                       BATCH_FULL_LATTICE if full_lattice else 0, ctypes.byref(h))
+        if st != SFH_OK:
+            raise SfhError(st, f"sfh_batch_create: {self.lib.sfh_status_string(st).decode()}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st != SFH_OK:
+            msg = self.lib.sfh_batch_last_error(self.h)
+            raise SfhError(st, f"{what}: {self.lib.sfh_status_string(st).decode()}: "
+                               f"{msg.decode() if msg else ''}")
+
+    @property
+    def stream(self):
+        return self.lib.sfh_batch_get_stream(self.h)
+
+    def set_rhs_block(self, width):
+        self._check(self.lib.sfh_batch_set_rhs_block(self.h, width), "set_rhs_block")
+
+    def set_gauge(self, k, U):
+        U = _f64(U).reshape(-1)
+        self._check(self.lib.sfh_batch_set_gauge(self.h, k, _dptr(U)), "set_gauge")
+
+    def set_rhs(self, k, j, phi):
+        phi = _f64(phi).reshape(-1)
+        self._check(self.lib.sfh_batch_set_rhs(self.h, k, j, _dptr(phi)), "set_rhs")
+
+    def random_gauge(self, k, eps, seed):
+        self._check(self.lib.sfh_batch_random_gauge(self.h, k, eps, seed), "random_gauge")
+
+    def random_rhs(self, k, j, seed, sigma=1.0):
+        self._check(self.lib.sfh_batch_random_rhs(self.h, k, j, seed, sigma), "random_rhs")
+
+    def gauge(self, k):
+        out = np.empty(72 * volume(self.systems[k][0]))
+        self._check(self.lib.sfh_batch_get_gauge(self.h, k, _dptr(out)), "get_gauge")
+        return out
+
+    def rhs(self, k, j):
+        out = np.empty(6 * volume(self.systems[k][0]))
+        self._check(self.lib.sfh_batch_get_rhs(self.h, k, j, _dptr(out)), "get_rhs")
+        return out
+
+    def solve(self, tol=1e-10, max_iter=50000, check=True):
+        st = self.lib.sfh_batch_solve(self.h, tol, max_iter)
+        if check:
+            self._check(st, "batch solve")
+        return st
+
+    def solution(self, k, j):
+        X = np.empty(6 * volume(self.systems[k][0]))
+        self._check(self.lib.sfh_batch_get_solution(self.h, k, j, _dptr(X)), "get_solution")
+        return X
+
+    def info(self, k, j):
+        inf = CgInfo()
+        self._check(self.lib.sfh_batch_get_info(self.h, k, j, ctypes.byref(inf)), "get_info")
+        return inf.as_dict()
+
+    def true_residual(self, k, j):
+        r = ctypes.c_double(0)
+        self._check(self.lib.sfh_batch_true_residual(self.h, k, j, ctypes.byref(r)), "true_residual")
+        return r.value

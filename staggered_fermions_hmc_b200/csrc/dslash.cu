@@ -1,0 +1,126 @@
+// dslash.cu — even-odd staggered hopping term (the Dslash).
+//
+// For output parity q the kernel computes, per checkerboard site x,
+//   out(x) = a*self(x) + b * 1/2 sum_mu eta_mu(x) [ bc+ U_mu(x) in(x+mu)
+//                                               - bc- U_mu(x-mu)^dag in(x-mu) ]
+// which is the hopping part K of the reference operators
+// D = m + K (Fermions.cpp:218-247) and D^dag = m - K (Fermions.cpp:254-283),
+// restricted to one parity (K only couples even and odd sites).  bc+ / bc-
+// are -1 on hops that wrap in time (anti-periodic), +1 otherwise.
+//
+// One thread per output site; the eight links and eight neighbour spinors
+// are read with coalesced SoA loads (neighbour spinors are re-read by up to
+// eight threads and are served from L1/L2).  The staggered phases and the
+// boundary signs are computed from the coordinates, so links stay pure SU(3)
+// and can be stored with 12 reals.
+#include "sfh_internal.h"
+
+namespace sfh {
+
+namespace {
+
+template <typename To, typename From>
+__device__ __forceinline__ Vec3<To> cvt(const Vec3<From>& v)
+{
+    Vec3<To> o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o.c[k] = {(To)v.c[k].re, (To)v.c[k].im};
+    return o;
+}
+
+template <typename R>
+__device__ __forceinline__ void acc_add(Vec3<R>& acc, const Vec3<R>& w, bool neg)
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (neg) { acc.c[k].re -= w.c[k].re; acc.c[k].im -= w.c[k].im; }
+        else     { acc.c[k].re += w.c[k].re; acc.c[k].im += w.c[k].im; }
+    }
+}
+
+}  // namespace
+
+// Hopping sum for one output site, shared with the solver kernels.
+template <int GP, int SPI>
+__device__ __forceinline__ Vec3<typename GaugeFmt<GP>::R> hop_site(const Geom& g, const Coord& c,
+                                                                   int q, int i, const void* gauge,
+                                                                   const void* in)
+{
+    typedef typename GaugeFmt<GP>::R R;
+    typedef typename SpinorFmt<SPI>::R RI;
+    Vec3<R> acc;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc.c[k] = {R(0), R(0)};
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        bool eta_neg = eta_sign(c, mu) < 0;
+        int lu = lex_up(g, c, mu) >> 1;
+        int ld = lex_dn(g, c, mu) >> 1;
+        bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
+        bool wrap_dn = (mu == 3) && (c.x[3] == 0);
+        Mat3<R> U = GaugeFmt<GP>::load(gauge, q, mu, i, g.Vh);
+        Vec3<R> v = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, lu, g.Vh));
+        acc_add(acc, mul_mv(U, v), eta_neg != wrap_up);
+        Mat3<R> Ud = GaugeFmt<GP>::load(gauge, 1 - q, mu, ld, g.Vh);
+        Vec3<R> w = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, ld, g.Vh));
+        acc_add(acc, mul_adj_mv(Ud, w), !(eta_neg != wrap_dn));
+    }
+    return acc;
+}
+
+namespace {
+
+template <int GP, int SPI, int SPO, bool SELF>
+__global__ void __launch_bounds__(256) hop_kernel(Geom g, const void* __restrict__ gauge,
+                                                  const void* __restrict__ in, const void* self,
+                                                  void* out, double a, double b, int q0)
+{
+    typedef typename GaugeFmt<GP>::R R;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int q = q0 + blockIdx.y;
+    if (i >= g.Vh) return;
+    Coord c = eo_coords(g, q, i);
+    Vec3<R> acc = hop_site<GP, SPI>(g, c, q, i, gauge, in);
+    R hb = (R)(0.5 * b);
+    Vec3<R> res;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) res.c[k] = {hb * acc.c[k].re, hb * acc.c[k].im};
+    if (SELF) {
+        Vec3<R> sv = cvt<R, typename SpinorFmt<SPO>::R>(SpinorFmt<SPO>::load(self, q, i, g.Vh));
+        R ra = (R)a;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            res.c[k].re = ra * sv.c[k].re + res.c[k].re;
+            res.c[k].im = ra * sv.c[k].im + res.c[k].im;
+        }
+    }
+    SpinorFmt<SPO>::store(out, q, i, g.Vh, cvt<typename SpinorFmt<SPO>::R, R>(res));
+}
+
+template <int GP, int SP>
+void launch_typed(const Geom& g, const void* gauge, const void* in, void* out, const void* self,
+                  double a, double b, int q0, int nq, cudaStream_t s)
+{
+    dim3 grid((g.Vh + 255) / 256, nq);
+    if (self)
+        hop_kernel<GP, SP, SP, true><<<grid, 256, 0, s>>>(g, gauge, in, self, out, a, b, q0);
+    else
+        hop_kernel<GP, SP, SP, false><<<grid, 256, 0, s>>>(g, gauge, in, self, out, a, b, q0);
+}
+
+}  // namespace
+
+void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,
+                int out_prec, void* out, const void* self, double a, double b, int q0, int nq,
+                cudaStream_t s)
+{
+    (void)out_prec;
+    if (gauge_prec == GP_F64_18 && in_prec == SP_F64)
+        launch_typed<GP_F64_18, SP_F64>(g, gauge, in, out, self, a, b, q0, nq, s);
+    else if (gauge_prec == GP_F32_12 && in_prec == SP_F32)
+        launch_typed<GP_F32_12, SP_F32>(g, gauge, in, out, self, a, b, q0, nq, s);
+    else if (gauge_prec == GP_F16_12 && in_prec == SP_F16)
+        launch_typed<GP_F16_12, SP_F16>(g, gauge, in, out, self, a, b, q0, nq, s);
+}
+
+}  // namespace sfh

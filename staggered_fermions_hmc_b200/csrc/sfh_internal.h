@@ -1,0 +1,67 @@
+// sfh_internal.h — host-side context shared by the library's translation
+// units.  Not part of the public C ABI (include/sfh.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sfh.h"
+#include "sfh_core.cuh"
+
+struct sfh_ctx {
+    sfh::Geom g;
+    double mass = 0.0, beta = 0.0, c11 = 5.0 / 3.0, c12 = -1.0 / 12.0;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // device fields (even-odd SoA, see sfh_core.cuh)
+    void* U64 = nullptr;       // gauge FP64 18-real
+    void* U32 = nullptr;       // gauge FP32 12-real (derived)
+    void* U16 = nullptr;       // gauge FP16 12-real (derived)
+    bool lowp_valid = false;   // derived copies match U64
+    void* Pmom = nullptr;      // momenta FP64 18-real
+    void* Fbuf = nullptr;      // force scratch FP64 18-real
+    void* stage = nullptr;     // device staging for host AoS transfers (72V doubles)
+    void* spin[6] = {};        // FP64 spinor work fields (6V doubles each)
+    double* red = nullptr;     // reduction partials / scalars
+    int* derr = nullptr;       // device error flags (DeviceErr bits)
+    void* pinned = nullptr;    // pinned host staging (72V doubles)
+    size_t pinned_bytes = 0;
+
+    std::string last_error;
+};
+
+namespace sfh {
+
+// error helpers
+int set_error(sfh_ctx* c, int code, const std::string& msg);
+int cuda_check(sfh_ctx* c, cudaError_t e, const char* what);
+
+// launch helpers implemented in layout.cu / dslash.cu
+void launch_spinor_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
+void launch_spinor_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
+void launch_links_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
+void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
+void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s);
+
+// out_q = a*self_q + b*K_{q,1-q} in  for q in [q0, q0+nq); precisions by enum
+void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,
+                int out_prec, void* out, const void* self, double a, double b, int q0, int nq,
+                cudaStream_t s);
+
+cudaError_t launch_random_gauge(const Geom& g, double eps, unsigned long long seed, void* U, int* d_err,
+                                cudaStream_t s);
+cudaError_t launch_random_spinor(const Geom& g, double sigma, unsigned long long seed, void* out,
+                                 cudaStream_t s);
+cudaError_t launch_random_momenta(const Geom& g, unsigned long long seed, void* P, cudaStream_t s);
+
+Geom make_geom(const int dims[4]);
+bool dims_ok(const int dims[4]);
+int ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
+                 sfh_cg_info* info);
+
+}  // namespace sfh

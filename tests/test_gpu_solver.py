@@ -1,0 +1,176 @@
+"""GPU parity: Dslash / D / D^dag / D D^dag and the CG solvers against the
+reference's own outputs (tests/golden) and the CPU oracle.
+
+Tolerances (FP64 path): operators 1e-12 relative (max-norm); the FP64
+full-lattice CG, which runs the reference's algorithm, matches the reference
+solution to 1e-11 and its iteration count to +-1.  Mixed-precision solvers
+stop on an FP64 true residual: |b - D D^dag x| / |b| < tol is checked in
+FP64 on the host, and the solution agrees with a tight FP64 oracle solve to
+100 * tol * cond-bound (see each test).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def load(path):
+    g = np.load(path)
+    L, T, mass, tol, geps, seed, beta, eps, nsteps = g["meta"]
+    return g, (int(L), int(L), int(L), int(T)), float(mass), float(tol), float(beta)
+
+
+@pytest.fixture(scope="module")
+def sfh():
+    import staggered_fermions_hmc_b200 as m
+    m.load_library()
+    return m
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_operators_vs_reference(sfh, path):
+    g, dims, mass, tol, beta = load(path)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(g["U"])
+    assert rel(lat.download_gauge(), g["U"]) == 0.0
+    assert rel(lat.apply_dirac_operator(g["phi"]), g["Dphi"]) < 1e-12
+    assert rel(lat.apply_dirac_dagger(g["phi"]), g["Ddagphi"]) < 1e-12
+    assert rel(lat.apply_DDdagger(g["phi"]), g["DDdagphi"]) < 1e-12
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_fp64_cg_vs_reference(sfh, orc, path):
+    g, dims, mass, tol, beta = load(path)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(g["U"])
+    X, info = lat.solve_CG_DDdagger(g["phi"], tol=tol, precision="f64", info=True)
+    assert rel(X, g["X"]) < 1e-11
+    _, it_ref, _, _ = orc.cg(dims, mass, g["U"], g["phi"], tol)
+    assert abs(info["iters"] - it_ref) <= 1
+    Y = lat.solve_Y_field(X)
+    assert rel(Y, g["Y"]) < 1e-11
+
+
+@pytest.mark.parametrize("dims,mass,geps", [((8, 8, 8, 8), 0.1, 0.3), ((4, 6, 8, 10), 0.25, 1.0)])
+def test_operators_vs_oracle(sfh, orc, dims, mass, geps):
+    U = orc.random_gauge(dims, geps, 31)
+    psi = orc.random_spinor(dims, 32)
+    lat = sfh.Lattice(dims, mass)
+    lat.upload_gauge(U)
+    assert rel(lat.apply_dirac_operator(psi), orc.dirac(dims, mass, U, psi)) < 1e-12
+    assert rel(lat.apply_dirac_dagger(psi), orc.dirac(dims, mass, U, psi, dagger=True)) < 1e-12
+    assert rel(lat.apply_DDdagger(psi), orc.ddag(dims, mass, U, psi)) < 1e-12
+
+
+def true_resid(orc, dims, mass, U, b, x):
+    r = b - orc.ddag(dims, mass, U, x)
+    return float(np.linalg.norm(r) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16"])
+def test_cg_precisions_true_residual(sfh, orc, precision):
+    dims, mass = (8, 8, 8, 8), 0.1
+    U = orc.random_gauge(dims, 0.3, 41)
+    b = orc.random_spinor(dims, 42)
+    lat = sfh.Lattice(dims, mass)
+    lat.upload_gauge(U)
+    tol = 1e-10
+    X, info = lat.solve_CG_DDdagger(b, tol=tol, precision=precision, info=True)
+    assert info["status"] == 0
+    assert true_resid(orc, dims, mass, U, b, X) < (1.01 if precision == "f64" else 1.0) * tol * 1.5
+    Xref, _, _, _ = orc.cg(dims, mass, U, b, 1e-13)
+    # |x - x*| / |x*| <= cond(M) * resid; cond <= (m^2 + 4) / m^2 = 401 here
+    assert np.linalg.norm(X - Xref) / np.linalg.norm(Xref) < 401 * tol * 2
+    if precision != "f64":
+        assert info["reliable_updates"] >= 1
+
+
+def test_cg_zero_rhs_returns_zero(sfh, orc):
+    """Fermions.cpp:562-564: |phi|^2 < 1e-28 returns X = 0."""
+    dims = (4, 4, 4, 4)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(orc.random_gauge(dims, 0.3, 1))
+    X = lat.solve_CG_DDdagger(np.zeros(6 * 256), precision="f64")
+    assert np.all(X == 0)
+
+
+def test_cg_noconv_raises(sfh, orc):
+    """Fermions.cpp:609-614: non-convergence is an error, not a silent result."""
+    dims = (4, 4, 4, 4)
+    lat = sfh.Lattice(dims, 0.05)
+    lat.upload_gauge(orc.random_gauge(dims, 1.0, 2))
+    b = orc.random_spinor(dims, 3)
+    for prec in ("f64", "f32"):
+        with pytest.raises(sfh.SfhError) as e:
+            lat.solve_CG_DDdagger(b, tol=1e-12, max_iter=5, precision=prec)
+        assert e.value.status == sfh.SFH_ERR_NOCONV
+
+
+def test_invalid_dims_rejected(sfh):
+    with pytest.raises(sfh.SfhError) as e:
+        sfh.Lattice((4, 4, 4, 5), 0.1)
+    assert e.value.status == sfh.SFH_ERR_INVALID
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16"])
+def test_batch_uneven_systems(sfh, orc, precision):
+    systems = [((4, 4, 4, 4), 0.2, 2), ((6, 6, 6, 8), 0.05, 3), ((8, 8, 8, 4), 0.1, 1),
+               ((4, 4, 8, 8), 0.1, 5)]
+    tol = 1e-10
+    B = sfh.Batch(systems, precision=precision)
+    data = []
+    for k, (dims, mass, nrhs) in enumerate(systems):
+        U = orc.random_gauge(dims, 0.3 if k % 2 == 0 else 1.0, 100 + k)
+        B.set_gauge(k, U)
+        bs = [orc.random_spinor(dims, 200 + 10 * k + j) for j in range(nrhs)]
+        for j, b in enumerate(bs):
+            B.set_rhs(k, j, b)
+        data.append((U, bs))
+    B.solve(tol=tol, max_iter=20000)
+    for k, (dims, mass, nrhs) in enumerate(systems):
+        U, bs = data[k]
+        for j in range(nrhs):
+            X = B.solution(k, j)
+            info = B.info(k, j)
+            assert info["status"] == 0
+            r = true_resid(orc, dims, mass, U, bs[j], X)
+            assert r < 1.5 * tol, (k, j, r, info)
+            assert abs(B.true_residual(k, j) - r) < 1e-3 * tol + 1e-3 * r
+
+
+def test_batch_full_lattice_matches_single(sfh, orc):
+    """Full-lattice batch lanes run the same algorithm as sfh_cg_solve(F64)."""
+    g, dims, mass, tol, beta = load(GOLDEN[0])
+    B = sfh.Batch([(dims, mass, 2)], precision="f64", full_lattice=True)
+    B.set_gauge(0, g["U"])
+    B.set_rhs(0, 0, g["phi"])
+    B.set_rhs(0, 1, 2.0 * g["phi"])
+    B.solve(tol=tol)
+    assert rel(B.solution(0, 0), g["X"]) < 1e-11
+    assert rel(B.solution(0, 1), 2.0 * g["X"]) < 1e-11
+
+
+def test_batch_rhs_block_widths_agree(sfh, orc):
+    """The RHS-block width changes scheduling only, not results."""
+    systems = [((4, 4, 4, 8), 0.1, 6)]
+    U = orc.random_gauge(systems[0][0], 0.5, 7)
+    out = []
+    for w in (1, 2, 4, 8):
+        B = sfh.Batch(systems, precision="f32")
+        B.set_rhs_block(w)
+        B.set_gauge(0, U)
+        for j in range(6):
+            B.set_rhs(0, j, orc.random_spinor(systems[0][0], 300 + j))
+        B.solve(tol=1e-10)
+        out.append(np.concatenate([B.solution(0, j) for j in range(6)]))
+    for o in out[1:]:
+        assert np.array_equal(o, out[0])
