@@ -271,6 +271,18 @@ def make_host_fields(spec, device):
     return fields
 
 
+def run_profile_case(args, spec):
+    import staggered_fermions_hmc_b200 as sfh
+    sfh.load_library()
+    B = build_batch(sfh, spec, args.precision, 0)
+    for _ in range(args.warmup):
+        B.solve(tol=TOL, max_iter=MAXIT)
+    st = B.solve(tol=TOL, max_iter=args.maxit, check=False)
+    print(json.dumps({"profile_case": True, "nsys": len(spec), "precision": args.precision,
+                      "maxit": args.maxit, "status": st}), flush=True)
+    B.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -282,8 +294,15 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="build the batch, run --warmup solves, then one solve capped at --maxit "
+                         "iterations (a short launch for kernel profiling); prints one line")
+    ap.add_argument("--maxit", type=int, default=MAXIT)
     args = ap.parse_args()
     spec = batch_spec(nsys=args.nsys)
+    if args.profile_case:
+        run_profile_case(args, spec)
+        return
 
     if args.impl == "reference":
         run_reference_arm(args, spec)
