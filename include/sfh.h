@@ -142,6 +142,32 @@ int sfh_batch_get_rhs(sfh_batch* batch, int sys, int rhs, double* phi);
 /* FP64 |b - D D^dag x| / |b| for one solution (diagnostic) */
 int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
 
+/* ---- allocation-free solve ------------------------------------------------ */
+/* No counterpart in the reference.  An FP64 CG solve of D D^dag X = phi (the
+ * reference's full-lattice algorithm, as sfh_cg_solve with SFH_PREC_F64) that
+ * allocates no device or host memory, for callers that cannot call cudaMalloc:
+ * code running while a stream is captured into a CUDA graph, runtimes that own
+ * all device memory through their own pool, and loops that must not allocate
+ * after start-up.  The solver's work vectors live in a fixed array inside the
+ * library (about 12.6 MB, reserved on every GPU that loads the library until
+ * the process exits), so the lattice may have at most SFH_NOALLOC_MAX_SITES
+ * sites; larger lattices return SFH_ERR_INVALID.
+ *
+ * All pointers are device pointers in the library's even-odd layout (site
+ * index i = s >> 1 within parity p = (x+y+z+t) & 1, s as above):
+ *   links_eo: double2 [p][mu][row*3+col][i]   (4*V*9 double2 = 72*V doubles)
+ *   phi_eo, x_eo: double2 [p][color][i]       (6*V doubles)
+ * The call runs on cuda_stream (0 = legacy default stream) of the current
+ * device and waits for it before returning; info may be NULL.  The first call
+ * on a device looks up the array's device address, which can load the
+ * library's device code on that device: make that first call before any
+ * stream capture.  Every call uses the same array, so calls whose work
+ * overlaps on the GPU (other threads, other streams) race and must be
+ * serialised by the caller. */
+#define SFH_NOALLOC_MAX_SITES 65536
+int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* links_eo, const void* phi_eo,
+                         void* x_eo, double tol, int maxit, void* cuda_stream, sfh_cg_info* info);
+
 #ifdef __cplusplus
 }
 #endif

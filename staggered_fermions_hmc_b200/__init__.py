@@ -112,7 +112,11 @@ SIGNATURES = {
     "sfh_batch_get_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_get_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_true_residual": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_cg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_double, _VP, _VP, _VP,
+                                            ctypes.c_double, ctypes.c_int, _VP, ctypes.POINTER(CgInfo)]),
 }
+
+NOALLOC_MAX_SITES = 65536
 
 _lib = None
 

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1327,3 +1328,171 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
     if (st) return st;
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
 }
+
+// ===========================================================================
+// Allocation-free CG entry point.
+//
+// For callers that cannot call cudaMalloc: code that runs while a stream is
+// being captured into a CUDA graph, host runtimes that own all device memory
+// through their own pool and forbid outside allocations, and trajectory loops
+// that must not allocate after start-up.  The solver's work vectors and
+// control data live in the file-scope array below instead of device
+// allocations; the caller passes device inputs and outputs.
+// ===========================================================================
+namespace sfh {
+namespace {
+
+constexpr int kNoAllocMaxSites = SFH_NOALLOC_MAX_SITES;
+constexpr int kNoAllocMaxTiles = kNoAllocMaxSites / kTile;  // 2 * tiles per parity
+constexpr size_t kAlign = 256;
+constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kOffSys = 0;
+constexpr size_t kOffRhs = align_up(kOffSys + sizeof(CgSys));
+constexpr size_t kOffLane = align_up(kOffRhs + sizeof(CgRhs));
+constexpr size_t kOffActive = align_up(kOffLane + sizeof(CgLane));
+constexpr size_t kOffTiles = align_up(kOffActive + sizeof(int));
+constexpr size_t kOffPartial = align_up(kOffTiles + sizeof(int) * kNoAllocMaxTiles);
+constexpr size_t kOffVec = align_up(kOffPartial + sizeof(double) * kNoAllocMaxTiles);
+constexpr size_t kVecBytes = (size_t)kNoAllocMaxSites * 6 * sizeof(double);
+constexpr size_t kNoAllocBytes = kOffVec + 4 * kVecBytes;  // r, p, v, t
+
+// 12.6 MB per device; held by every GPU that loads the library, until exit.
+static __device__ __align__(256) unsigned char sfh_noalloc_scratch[kNoAllocBytes];
+
+// Writes the solver's control data into the scratch array (zeroes the
+// tickets and partials left by the previous call).
+__global__ void noalloc_setup(CgSys S, CgRhs R, unsigned char* base)
+{
+    CgSys* sys = reinterpret_cast<CgSys*>(base + kOffSys);
+    CgRhs* rhs = reinterpret_cast<CgRhs*>(base + kOffRhs);
+    CgLane* lane = reinterpret_cast<CgLane*>(base + kOffLane);
+    int* active = reinterpret_cast<int*>(base + kOffActive);
+    int* tiles = reinterpret_cast<int*>(base + kOffTiles);
+    double* partial = reinterpret_cast<double*>(base + kOffPartial);
+    for (int k = threadIdx.x; k < 2 * S.ntq; k += blockDim.x) {
+        tiles[k] = 0;
+        partial[k] = 0.0;
+    }
+    if (threadIdx.x == 0) {
+        *sys = S;
+        *rhs = R;
+        CgLane L;
+        memset(&L, 0, sizeof(L));
+        L.sys = 0;
+        L.rhs = 0;
+        L.parity = 2;
+        L.poff = 0;
+        L.mode[0] = L.mode[1] = LM_ACTIVE;
+        *lane = L;
+        *active = 1;
+    }
+}
+
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned char* addr = nullptr;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[64];
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks it up with cudaGetSymbolAddress (this can load the
+// library's device code on that device).
+int noalloc_scratch(unsigned char** out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SFH_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, sfh_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) return SFH_ERR_CUDA;
+        d.addr = static_cast<unsigned char*>(p);
+        d.ready = true;
+    }
+    *out = d.addr;
+    return SFH_OK;
+}
+
+}  // namespace
+
+extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* links_eo,
+                                    const void* phi_eo, void* x_eo, double tol, int maxit,
+                                    void* cuda_stream, sfh_cg_info* info)
+{
+    if (!dims || !links_eo || !phi_eo || !x_eo || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    if (!sfh::dims_ok(dims)) return SFH_ERR_INVALID;
+    const long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
+    if (V > kNoAllocMaxSites) return SFH_ERR_INVALID;  // lattice larger than the scratch array
+    unsigned char* base = nullptr;
+    int st = noalloc_scratch(&base);
+    if (st) return st;
+    cudaStream_t stream = (cudaStream_t)cuda_stream;
+    int dev = 0, num_sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SFH_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return SFH_ERR_CUDA;
+
+    CgSys S;
+    S.g = make_geom(dims);
+    S.m2 = mass * mass;
+    S.U64 = links_eo;
+    S.Ulo = links_eo;
+    S.lane0 = 0;
+    S.nrhs = 1;
+    S.both = 1;
+    S.tile0 = 0;
+    S.ntq = (S.g.Vh + kTile - 1) / kTile;
+    CgRhs R;
+    R.b = const_cast<void*>(phi_eo);
+    R.xhi = x_eo;
+    R.thi = nullptr;
+    R.r = base + kOffVec;
+    R.p = base + kOffVec + kVecBytes;
+    R.v = base + kOffVec + 2 * kVecBytes;
+    R.t = base + kOffVec + 3 * kVecBytes;
+    R.xlo = x_eo;
+    noalloc_setup<<<1, 256, 0, stream>>>(S, R, base);
+    if (cudaGetLastError() != cudaSuccess) return SFH_ERR_CUDA;
+
+    CgArgs a;
+    a.nsys = 1;
+    a.nlanes = 1;
+    a.ntiles = 2 * S.ntq;
+    a.sys = reinterpret_cast<const CgSys*>(base + kOffSys);
+    a.rhs = reinterpret_cast<const CgRhs*>(base + kOffRhs);
+    a.lanes = reinterpret_cast<CgLane*>(base + kOffLane);
+    a.tile_sys = reinterpret_cast<const int*>(base + kOffTiles);
+    a.partial = reinterpret_cast<double*>(base + kOffPartial);
+    a.n_active = reinterpret_cast<int*>(base + kOffActive);
+    a.tol2 = tol * tol;
+    a.delta = 0.1;
+    a.maxit = maxit;
+    a.mixed = 0;
+    a.maxloop = maxit + 1;
+    CgKernel k = cg_persistent<GP_F64_18, SP_F64, 1>;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 0) != cudaSuccess || per_sm < 1)
+        return SFH_ERR_CUDA;
+    int grid = std::min(per_sm * num_sms, a.ntiles);
+    void* args[] = {&a};
+    if (cudaLaunchCooperativeKernel((const void*)k, dim3(grid), dim3(kTile), args, 0, stream) != cudaSuccess)
+        return SFH_ERR_CUDA;
+    CgLane L;
+    if (cudaMemcpyAsync(&L, a.lanes, sizeof(CgLane), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+        return SFH_ERR_CUDA;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return SFH_ERR_CUDA;
+    int status = L.status;
+    if (L.mode[0] == LM_ACTIVE || L.mode[0] == LM_RU) status = SFH_ERR_NOCONV;
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->status = status;
+        info->iters = L.iters;
+        info->iters_parity[0] = info->iters_parity[1] = L.iters;
+        info->rsq_rel = L.bb > 0 ? L.rr / L.bb : 0.0;
+        info->true_resid = -1.0;
+    }
+    return status;
+}
+
+}  // namespace sfh

@@ -1,0 +1,99 @@
+"""The allocation-free solve, sfh_cg_solve_noalloc, against the regular solve.
+
+Some callers of this library cannot call cudaMalloc: code that runs while a
+stream is captured into a CUDA graph, host runtimes that hand out all device
+memory from their own pool, and trajectory loops that must not allocate after
+start-up.  sfh_cg_solve_noalloc serves them by keeping the solver's work
+vectors in a fixed array inside the library; the caller brings its own device
+buffers for the links, the source and the solution.
+
+Here the test allocates those buffers itself (with torch), in the library's
+even-odd layout, calls the entry point twice in a row with different sources,
+and compares each solution with sfh_cg_solve (FP64) on the same inputs, to the
+1e-11 relative tolerance the FP64 solver tests use.  This file is named so
+that pytest collects it last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def eo_index(dims):
+    V = int(np.prod(dims))
+    c = np.indices(dims).reshape(4, V)
+    parity = c.sum(0) % 2
+    return parity, np.arange(V) // 2
+
+
+def spinor_to_eo(dims, aos):
+    V = int(np.prod(dims))
+    p, i = eo_index(dims)
+    eo = np.zeros((2, 3, V // 2, 2))
+    eo[p, :, i, :] = aos.reshape(V, 3, 2)
+    return np.ascontiguousarray(eo.reshape(-1))
+
+
+def spinor_from_eo(dims, eo):
+    V = int(np.prod(dims))
+    p, i = eo_index(dims)
+    return np.ascontiguousarray(eo.reshape(2, 3, V // 2, 2)[p, :, i, :].reshape(-1))
+
+
+def links_to_eo(dims, aos):
+    V = int(np.prod(dims))
+    p, i = eo_index(dims)
+    eo = np.zeros((2, 4, 9, V // 2, 2))
+    eo[p, :, :, i, :] = aos.reshape(V, 4, 9, 2)
+    return np.ascontiguousarray(eo.reshape(-1))
+
+
+def test_noalloc_solve_matches_regular_solve_twice(orc):
+    import torch
+
+    import staggered_fermions_hmc_b200 as sfh
+    lib = sfh.load_library()
+    dims, mass, tol = (8, 8, 8, 8), 0.1, 1e-10
+    U = orc.random_gauge(dims, 0.5, 77)
+    lat = sfh.Lattice(dims, mass)
+    lat.upload_gauge(U)
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    U_eo = torch.from_numpy(links_to_eo(dims, U)).to(dev)
+    cdims = (ctypes.c_int * 4)(*dims)
+    for seed in (78, 79):
+        phi = orc.random_spinor(dims, seed)
+        X_ref, info_ref = lat.solve_CG_DDdagger(phi, tol=tol, precision="f64", info=True)
+        phi_eo = torch.from_numpy(spinor_to_eo(dims, phi)).to(dev)
+        x_eo = torch.full_like(phi_eo, float("nan"))
+        torch.cuda.synchronize()
+        info = sfh.CgInfo()
+        st = lib.sfh_cg_solve_noalloc(cdims, mass, U_eo.data_ptr(), phi_eo.data_ptr(), x_eo.data_ptr(),
+                                      tol, 50000, stream, ctypes.byref(info))
+        assert st == sfh.SFH_OK
+        X = spinor_from_eo(dims, x_eo.cpu().numpy())
+        assert np.all(np.isfinite(X))
+        assert rel(X, X_ref) < 1e-11
+        assert info.iters == info_ref["iters"]
+        assert info.status == sfh.SFH_OK
+    lat.close()
+
+
+def test_noalloc_rejects_lattices_beyond_its_array():
+    import torch
+
+    import staggered_fermions_hmc_b200 as sfh
+    lib = sfh.load_library()
+    dims = (16, 16, 16, 32)
+    assert int(np.prod(dims)) > sfh.NOALLOC_MAX_SITES
+    buf = torch.zeros(16, dtype=torch.float64, device="cuda:0")
+    info = sfh.CgInfo()
+    st = lib.sfh_cg_solve_noalloc((ctypes.c_int * 4)(*dims), 0.1, buf.data_ptr(), buf.data_ptr(),
+                                  buf.data_ptr(), 1e-10, 100, None, ctypes.byref(info))
+    assert st == sfh.SFH_ERR_INVALID
