@@ -1,250 +1,149 @@
-// cg.cu — persistent, batched conjugate-gradient solver for D D^dag x = b.
+// cg.cu — batched conjugate-gradient solver for D D^dag x = b (two kernels
+// per iteration, replayed as CUDA-graph chunks).
 //
 // Restates solve_CG_DDdagger (Fermions.cpp:553-617) for the GPU.  D D^dag =
 // m^2 - K^2 and K couples only even and odd sites, so D D^dag is block
 // diagonal in parity: M_pp = m^2 - K_{p,1-p} K_{1-p,p}.
 //
-// One cooperative launch solves every "lane" of a batch: a lane is one
-// (system, right-hand side, parity block) CG, or one (system, RHS) CG over
-// both parities with shared scalars (the reference's full-lattice CG, used
-// for FP64 parity).  Systems may differ in lattice size and mass.  Each CG
-// iteration is three grid-wide phases separated by grid.sync():
+// A batch holds "lanes": one lane is the CG of one (system, right-hand side,
+// parity block), or of one (system, RHS) over both parities with shared
+// scalars (the reference's full-lattice CG).  Systems may differ in lattice
+// size and mass.  Iteration k of every lane is two grid-wide kernels:
 //
-//   P1  t = K p_new,     p_new = r + beta p computed at the neighbours
-//   P2  p = p_new, v = m^2 p - K t, partial <p, v>      -> alpha
-//   P3  x += alpha p, r -= alpha v, partial <r, r>       -> beta / convergence
+//   hop1   t = K p_k  with  r_k = r_{k-1} - alpha v,  p_k = r_k + beta p_{k-1}
+//          evaluated at the neighbours from the stored r, v, p
+//   hop2   the same update at the lane's own sites (r, p and x += alpha p
+//          stored), v = m^2 p_k - K t, and the four sums <p,v>, <r,v>, |v|^2,
+//          |r_k|^2
 //
-// Work is split into tiles of 256 sites of one system and one output parity;
-// every tile processes all lanes of its system that are active in the phase,
-// so a link loaded once serves every right-hand side (RHS blocking).
+// The tile that completes a lane's count of partial sums (atomic ticket) adds
+// them in a fixed order and advances the lane in FP64: alpha = |r_k|^2/<p,Ap>,
+// |r_{k+1}|^2 = |r_k|^2 - 2 alpha <r,v> + alpha^2 |v|^2 (anchored every
+// iteration on the exact |r_k|^2, so the recurrence does not drift),
+// beta = |r_{k+1}|^2/|r_k|^2, and the convergence test of the reference
+// (Fermions.cpp:569).  A lane that converges spends one more hop2 writing
+// x_{k+1} and stops.
 //
-// Reductions are deterministic: each tile writes one FP64 partial per lane;
-// the tile that completes a lane's count (atomic ticket) sums the partials in
-// a fixed order and updates that lane's FP64 scalars.
+// Work is split into tiles of 256 sites of one system and one output parity.
+// A tile processes all lanes of its system that are active in the phase, so a
+// link loaded once serves every right-hand side (RHS blocking).
 //
-// Mixed precision (FP32 or FP16+scale vectors with FP32/FP16 12-real links):
+// Mixed precision (FP32 or FP16+scale vectors with FP32 / FP16 12-real links):
 // x is accumulated in FP32 between reliable updates.  When |r| has dropped by
-// delta since the last update, or the iterated residual meets the target, the
-// lane spends one iteration on an FP64 reliable update: x_hi += x_lo and
-// r = b - M x_hi recomputed with FP64 links and vectors.  A mixed lane
-// converges only on that FP64 true residual.
-#include <cooperative_groups.h>
-
+// delta since the last update, or the recurrence meets the target, the lane
+// spends one iteration on an FP64 reliable update: x_hi += x_lo + alpha p and
+// r = b - M x_hi with FP64 links and vectors; p is kept and the next
+// direction is r + (|r|^2/|r_old|^2) p.  Mixed lanes converge only on that
+// FP64 true residual.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
-#include "sfh_internal.h"
-
-namespace cgrp = cooperative_groups;
+#include "cg_common.cuh"
 
 namespace sfh {
 
-enum { LM_ACTIVE = 0, LM_RU = 1, LM_DONE = 2, LM_FAILED = 3 };
-constexpr int kTile = 256;
-
-struct CgSys {
-    Geom g;
-    double m2;
-    const void* U64;
-    const void* Ulo;
-    int lane0, nrhs, both, tile0, ntq;
-};
-
-struct CgRhs {
-    void* b;    // FP64 right-hand side
-    void* xhi;  // FP64 solution
-    void* thi;  // FP64 temporary (reliable updates)
-    void* r;    // residual (solver precision)
-    void* p;    // search direction
-    void* v;    // M p
-    void* t;    // K p on the other parity
-    void* xlo;  // low-precision solution increment (FP32; == xhi for FP64)
-};
-
-struct CgLane {
-    int sys, rhs, parity, poff;
-    double bb, target, rr, rr_old, pAp, alpha, beta, rmax;
-    int mode[2];
-    int iters, nru, status, pad;
-    unsigned int ticket, pad2;
-};
-
-struct CgArgs {
-    int nsys, nlanes, ntiles;
-    const CgSys* sys;
-    const CgRhs* rhs;
-    CgLane* lanes;
-    const int* tile_sys;
-    double* partial;
-    int* n_active;
-    double tol2, delta;
-    int maxit, maxloop, mixed;
-};
-
 namespace {
 
-template <int SP> struct XFmt { static constexpr int v = SP_F32; };
-template <> struct XFmt<SP_F64> { static constexpr int v = SP_F64; };
+constexpr int kSums = 4;  // <p,v>, <r,v>, |v|^2, |r|^2
 
-__device__ __forceinline__ int ld_int(const int* p) { return __ldcg(p); }
-__device__ __forceinline__ double ld_dbl(const double* p) { return __ldcg(p); }
-
-__device__ __forceinline__ int lane_of(const CgSys& S, int rhs, int q, bool hop1)
-{
-    if (S.both) return S.lane0 + rhs;
-    int lp = hop1 ? 1 - q : q;
-    return S.lane0 + rhs * 2 + lp;
-}
-
-template <typename R>
-__device__ __forceinline__ void vzero(Vec3<R>& a)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) a.c[k] = {R(0), R(0)};
-}
-
-template <typename R>
-__device__ __forceinline__ void vacc(Vec3<R>& acc, const Vec3<R>& w, bool neg)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        if (neg) { acc.c[k].re -= w.c[k].re; acc.c[k].im -= w.c[k].im; }
-        else     { acc.c[k].re += w.c[k].re; acc.c[k].im += w.c[k].im; }
-    }
-}
-
-template <typename To, typename From>
-__device__ __forceinline__ Vec3<To> vcvt(const Vec3<From>& v)
-{
-    Vec3<To> o;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[k] = {(To)v.c[k].re, (To)v.c[k].im};
-    return o;
-}
-
-// a + s*b with explicit fused multiply-add (identical rounding in every phase)
-__device__ __forceinline__ Vec3<float> vaxpy(const Vec3<float>& a, float s, const Vec3<float>& b)
-{
-    Vec3<float> o;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[k] = {fmaf(s, b.c[k].re, a.c[k].re), fmaf(s, b.c[k].im, a.c[k].im)};
-    return o;
-}
-__device__ __forceinline__ Vec3<double> vaxpy(const Vec3<double>& a, double s, const Vec3<double>& b)
-{
-    Vec3<double> o;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[k] = {fma(s, b.c[k].re, a.c[k].re), fma(s, b.c[k].im, a.c[k].im)};
-    return o;
-}
-
-template <typename R>
-__device__ __forceinline__ double vdot_re(const Vec3<R>& a, const Vec3<R>& b)
-{
-    double s = 0.0;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) s += (double)a.c[k].re * (double)b.c[k].re + (double)a.c[k].im * (double)b.c[k].im;
-    return s;
-}
-
-// Block sum of N doubles; result valid in thread 0.  Fixed reduction tree.
-template <int N>
-__device__ __forceinline__ void block_sum(double (&v)[N], double* smem)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-    for (int k = 0; k < N; ++k)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < N; ++k) smem[warp * N + k] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            double x = lane < nw ? smem[lane * N + k] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-            v[k] = x;
-        }
-    }
-    __syncthreads();
-}
-
-// Sum of n partial slots by one warp in a fixed order (all lanes get it).
-__device__ __forceinline__ double warp_sum_slots(const double* slots, int n)
-{
-    const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int k = lane; k < n; k += 32) s += __ldcg(slots + k);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-__device__ __forceinline__ void set_mode_final(CgLane* L, int mode, int status, int* n_active)
-{
-    L->mode[0] = mode;
-    L->mode[1] = mode;
-    L->status = status;
-    atomicSub(n_active, 1);
-}
-
-struct TileInfo {
-    int q, slot, i;
-    bool valid;
+// one RHS pass of a tile: the lanes and their scalars
+template <int NB>
+struct LanePass {
+    int lane[NB], mode[NB], rid[NB];
+    double alpha[NB], beta[NB];
+    bool anyA, anyR, anyF;
 };
 
-__device__ __forceinline__ TileInfo decode_tile(const CgSys& S, int t)
-{
-    TileInfo ti;
-    int local = t - S.tile0;
-    ti.q = local >= S.ntq ? 1 : 0;
-    int j = local - ti.q * S.ntq;
-    ti.slot = local;
-    ti.i = j * kTile + (int)threadIdx.x;
-    ti.valid = ti.i < S.g.Vh;
-    return ti;
-}
-
-__device__ __forceinline__ int lane_slot0(const CgSys& S, int parity)
-{
-    return S.both ? 0 : parity * S.ntq;
-}
-
-__device__ __forceinline__ int lane_nslots(const CgSys& S) { return S.both ? 2 * S.ntq : S.ntq; }
-
-// pointer fields of the per-RHS vector table (read-only during the kernel)
-enum RhsField { F_B = 0, F_XHI, F_THI, F_R, F_P, F_V, F_T, F_XLO };
-__device__ __forceinline__ void* rhs_ptr(const CgArgs& a, int rid, int f)
-{
-    const unsigned long long* base = reinterpret_cast<const unsigned long long*>(a.rhs + rid);
-    return reinterpret_cast<void*>(__ldg(base + f));
-}
-
-// Publish this tile's partials and take the lanes' tickets; returns the mask
-// of lanes (within the pass) whose count this block completed.
 template <int NB>
-__device__ __forceinline__ unsigned arrive(const CgArgs& a, const CgSys& S, const int (&lanes)[NB],
-                                           const bool (&part)[NB], const double (&sums)[NB], int slot,
-                                           unsigned* s_mask)
+__device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int base, int q, bool hop1,
+                                            int cur, LanePass<NB>& P)
+{
+    const int cnt = min(NB, S.nrhs - base);
+    P.anyA = P.anyR = P.anyF = false;
+#pragma unroll
+    for (int l = 0; l < NB; ++l) {
+        P.lane[l] = 0;
+        P.mode[l] = LM_DONE;
+        P.rid[l] = 0;
+        P.alpha[l] = 0.0;
+        P.beta[l] = 0.0;
+        if (l < cnt) {
+            P.lane[l] = lane_of(S, base + l, q, hop1);
+            const CgLane* L = a.lanes + P.lane[l];
+            P.mode[l] = ld_int(&L->mode[cur]);
+            P.rid[l] = __ldg(&L->rhs);
+            if (P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU || P.mode[l] == LM_FINAL) {
+                P.alpha[l] = ld_dbl(&L->alpha);
+                P.beta[l] = ld_dbl(&L->beta);
+            }
+            P.anyA |= P.mode[l] == LM_ACTIVE;
+            P.anyR |= P.mode[l] == LM_RU;
+            P.anyF |= P.mode[l] == LM_FINAL;
+        }
+    }
+}
+
+// r' = r - alpha v, p' = r' + beta p, both rounded to the storage format;
+// identical arithmetic wherever it is evaluated (own site or neighbour).
+template <int SP>
+__device__ __forceinline__ void advance(const Vec3<typename SpinorFmt<SP>::R>& r,
+                                        const Vec3<typename SpinorFmt<SP>::R>& v,
+                                        const Vec3<typename SpinorFmt<SP>::R>& p,
+                                        typename SpinorFmt<SP>::R alpha, typename SpinorFmt<SP>::R beta,
+                                        Vec3<typename SpinorFmt<SP>::R>& rn, Vec3<typename SpinorFmt<SP>::R>& pn)
+{
+    rn = SpinorFmt<SP>::quantize(vaxpy(r, -alpha, v));
+    pn = SpinorFmt<SP>::quantize(vaxpy(rn, beta, p));
+}
+
+template <int SP>
+__device__ __forceinline__ Vec3<typename SpinorFmt<SP>::R> neighbour_p(const CgArgs& a, int rid, int par, int j,
+                                                                       int Vh, typename SpinorFmt<SP>::R alpha,
+                                                                       typename SpinorFmt<SP>::R beta)
+{
+    typedef typename SpinorFmt<SP>::R RS;
+    Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_R), par, j, Vh);
+    Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), par, j, Vh);
+    Vec3<RS> p = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_P), par, j, Vh);
+    Vec3<RS> rn, pn;
+    advance<SP>(r, v, p, alpha, beta, rn, pn);
+    return pn;
+}
+
+// stage the tile's system descriptor in shared memory (one tile per block)
+__device__ __forceinline__ void stage_sys(const CgArgs& a, CgSys* s_sys)
+{
+    if (threadIdx.x == 0) *s_sys = a.sys[__ldg(a.tile_sys + blockIdx.x)];
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// publish the tile's partial sums and take the lanes' tickets
+// ---------------------------------------------------------------------------
+template <int NB>
+__device__ __forceinline__ unsigned arrive_sums(const CgArgs& a, const CgSys& S, const LanePass<NB>& P,
+                                                const bool (&part)[NB], const double (&sums)[NB * kSums],
+                                                int slot, unsigned* s_mask)
 {
     if (threadIdx.x == 0) {
         unsigned mask = 0;
+        const int nslot = 2 * S.ntq;
 #pragma unroll
         for (int l = 0; l < NB; ++l)
-            if (part[l]) __stcg(a.partial + a.lanes[lanes[l]].poff + slot, sums[l]);
+            if (part[l]) {
+                double* dst = a.partial + a.lanes[P.lane[l]].poff + slot;
+#pragma unroll
+                for (int f = 0; f < kSums; ++f) __stcg(dst + f * nslot, sums[l * kSums + f]);
+            }
         __threadfence();
         const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
             if (!part[l]) continue;
-            CgLane* L = a.lanes + lanes[l];
+            CgLane* L = a.lanes + P.lane[l];
             unsigned old = atomicAdd(&L->ticket, 1u);
             if (old == expected - 1) {
                 L->ticket = 0;
@@ -258,165 +157,298 @@ __device__ __forceinline__ unsigned arrive(const CgArgs& a, const CgSys& S, cons
     return *s_mask;
 }
 
-// ---------------------------------------------------------------------------
-// lane scalar updates, run by warp 0 of the block that completed a ticket
-// ---------------------------------------------------------------------------
-__device__ __noinline__ void finish_init(const CgArgs& a, const CgSys& S, int lane)
+__device__ __forceinline__ void lane_stop(const CgArgs& a, CgLane* L, int cur, int mode_now, int mode_next,
+                                          int status)
 {
-    CgLane* L = a.lanes + lane;
-    double bb = warp_sum_slots(a.partial + L->poff + lane_slot0(S, L->parity), lane_nslots(S));
-    if (threadIdx.x == 0) {
-        L->bb = bb;
-        L->target = a.tol2 * bb;
-        L->rr = bb;
-        L->rr_old = bb;
-        L->rmax = sqrt(bb);
-        L->beta = 0.0;
-        L->alpha = 0.0;
-        L->iters = 0;
-        L->nru = 0;
-        if (bb < 1e-28) {  // Fermions.cpp:562-564: X = 0
-            set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
-        } else {
-            L->mode[0] = LM_ACTIVE;
-            L->mode[1] = LM_ACTIVE;
-        }
-    }
+    L->mode[cur] = mode_now;
+    L->mode[cur ^ 1] = mode_next;
+    L->status = status;
+    atomicSub(a.n_active, 1);
 }
 
-__device__ __noinline__ void finish_hop2(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
+// advance one lane's FP64 scalars from the summed partials (warp 0)
+__device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
 {
     CgLane* L = a.lanes + lane;
-    double s = warp_sum_slots(a.partial + L->poff + lane_slot0(S, L->parity), lane_nslots(S));
-    if (threadIdx.x != 0) return;
-    const int nxt = cur ^ 1;
-    if (mode == LM_ACTIVE) {  // s = <p, M p>; Fermions.cpp:573-586
-        L->pAp = s;
-        double alpha = L->rr / s;
-        if (!isfinite(s) || fabs(s) < 1e-30 || !isfinite(alpha)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else {
-            L->alpha = alpha;
-            L->mode[nxt] = LM_ACTIVE;
-        }
-    } else {  // reliable update finished: s = |b - M x|^2 in FP64
-        L->nru += 1;
-        if (s < L->target) {
-            L->rr = s;
-            set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
-        } else if (!isfinite(s)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else if (L->iters >= a.maxit) {
-            L->rr = s;
-            set_mode_final(L, LM_FAILED, SFH_ERR_NOCONV, a.n_active);
-        } else {
-            L->beta = s / L->rr_old;
-            L->rr = s;
-            L->rmax = sqrt(s);
-            L->mode[nxt] = LM_ACTIVE;
-        }
+    if (mode == LM_FINAL) {  // every tile has written x_{k+1}: retire the lane
+        if (threadIdx.x == 0) L->mode[cur] = LM_DONE;
+        return;
     }
-}
-
-__device__ __noinline__ void finish_update(const CgArgs& a, const CgSys& S, int lane, int cur)
-{
-    CgLane* L = a.lanes + lane;
-    double rn = warp_sum_slots(a.partial + L->poff + lane_slot0(S, L->parity), lane_nslots(S));
+    const int nslot = 2 * S.ntq;
+    const double* base = a.partial + L->poff + (S.both ? 0 : L->parity * S.ntq);
+    const int n = S.both ? 2 * S.ntq : S.ntq;
+    double s[kSums];
+#pragma unroll
+    for (int f = 0; f < kSums; ++f) s[f] = warp_sum_slots(base + f * nslot, n);
     if (threadIdx.x != 0) return;
     const int nxt = cur ^ 1;
-    L->iters += 1;
-    if (!isfinite(rn)) {
-        set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-    } else if (!a.mixed) {
-        double beta = rn / L->rr;  // Fermions.cpp:594-601
+    if (mode == LM_ACTIVE) {
+        const double rr = s[3], pAp = s[0];
+        const double alpha = rr / pAp;  // Fermions.cpp:573-586
+        if (!isfinite(pAp) || fabs(pAp) < 1e-30 || !isfinite(alpha)) {
+            lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);
+            return;
+        }
+        const double rr_next = rr - 2.0 * alpha * s[1] + alpha * alpha * s[2];
+        const double beta = rr_next / rr;  // Fermions.cpp:594-601
         if (!isfinite(beta)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else {
-            L->beta = beta;
-            L->rr = rn;
-            if (rn < L->target)  // Fermions.cpp:569
-                set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
+            lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);
+            return;
+        }
+        L->rr = rr;
+        L->pAp = pAp;
+        L->alpha = alpha;
+        L->beta = beta;
+        L->rr_next = rr_next;
+        L->iters += 1;
+        if (!a.mixed) {
+            if (rr_next < L->target)  // Fermions.cpp:569: write x_{k+1} and stop
+                lane_stop(a, L, cur, LM_DONE, LM_FINAL, SFH_OK);
             else if (L->iters >= a.maxit)  // Fermions.cpp:609-614
-                set_mode_final(L, LM_FAILED, SFH_ERR_NOCONV, a.n_active);
+                lane_stop(a, L, cur, LM_DONE, LM_FINAL, SFH_ERR_NOCONV);
             else
                 L->mode[nxt] = LM_ACTIVE;
-        }
-    } else {
-        double r = sqrt(rn);
-        if (rn < L->target || r < a.delta * L->rmax || L->iters >= a.maxit) {
-            L->rr_old = L->rr;
-            L->rr = rn;
-            L->mode[nxt] = LM_RU;
         } else {
-            L->beta = rn / L->rr;
-            L->rr = rn;
-            L->rmax = fmax(L->rmax, r);
+            const double r = sqrt(fmax(rr_next, 0.0));
+            if (rr_next < L->target || r < a.delta * L->rmax || L->iters >= a.maxit) {
+                L->mode[nxt] = LM_RU;
+            } else {
+                L->rmax = fmax(L->rmax, r);
+                L->mode[nxt] = LM_ACTIVE;
+            }
+        }
+    } else {  // reliable update: s[3] = |b - M x|^2 in FP64
+        const double rt = s[3];
+        L->nru += 1;
+        if (rt < L->target) {
+            L->rr_next = rt;
+            lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_OK);
+        } else if (!isfinite(rt)) {
+            lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);
+        } else if (L->iters >= a.maxit) {
+            L->rr_next = rt;
+            lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_ERR_NOCONV);
+        } else {
+            L->beta = rt / L->rr;  // keep the direction: p <- r_true + beta p
+            L->alpha = 0.0;
+            L->rr_next = rt;
+            L->rmax = sqrt(rt);
             L->mode[nxt] = LM_ACTIVE;
         }
     }
 }
 
+__device__ __noinline__ void finish_init_lane(const CgArgs& a, const CgSys& S, int lane)
+{
+    CgLane* L = a.lanes + lane;
+    const int nslot = 2 * S.ntq;
+    const double* base = a.partial + L->poff + 3 * nslot + (S.both ? 0 : L->parity * S.ntq);
+    double bb = warp_sum_slots(base, S.both ? 2 * S.ntq : S.ntq);
+    if (threadIdx.x != 0) return;
+    L->bb = bb;
+    L->target = a.tol2 * bb;
+    L->rr = bb;
+    L->rr_next = bb;
+    L->rmax = sqrt(bb);
+    L->alpha = 0.0;
+    L->beta = 0.0;
+    L->iters = 0;
+    L->nru = 0;
+    L->status = SFH_OK;
+    if (bb < 1e-28) {  // Fermions.cpp:562-564: X = 0
+        L->mode[0] = L->mode[1] = LM_DONE;
+        atomicSub(a.n_active, 1);
+    } else {
+        L->mode[0] = L->mode[1] = LM_ACTIVE;
+    }
+}
+
 // ---------------------------------------------------------------------------
-// reliable-update site kernels (FP64 links and vectors), rare
+// kernels
 // ---------------------------------------------------------------------------
-template <int XP>
-__device__ __noinline__ void ru_hop1_site(const CgArgs& a, const CgSys& S, const Coord& c, int q,
-                                          int i, int rid)
+
+// x = 0, r = b, p = v = 0, |b|^2
+template <int SP, int NB>
+__global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
+{
+    typedef typename SpinorFmt<SP>::R RS;
+    constexpr int XP = XFmt<SP>::v;
+    __shared__ CgSys s_sys;
+    __shared__ double smem[32 * NB * kSums];
+    __shared__ unsigned s_mask;
+    stage_sys(a, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, blockIdx.x);
+    const int Vh = S.g.Vh;
+    for (int base = 0; base < S.nrhs; base += NB) {
+        LanePass<NB> P;
+        const int cnt = min(NB, S.nrhs - base);
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            P.lane[l] = l < cnt ? lane_of(S, base + l, ti.q, false) : 0;
+            P.rid[l] = l < cnt ? __ldg(&a.lanes[P.lane[l]].rhs) : 0;
+        }
+        bool part[NB];
+        double sums[NB * kSums];
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            part[l] = l < cnt;
+#pragma unroll
+            for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
+            if (l >= cnt || !ti.valid) continue;
+            Vec3<double> b = SpinorFmt<SP_F64>::load(rhs_ptr(a, P.rid[l], F_B), ti.q, ti.i, Vh);
+            Vec3<double> z;
+            vzero(z);
+            SpinorFmt<SP_F64>::store(rhs_ptr(a, P.rid[l], F_XHI), ti.q, ti.i, Vh, z);
+            if (a.mixed)
+                SpinorFmt<XP>::store(rhs_ptr(a, P.rid[l], F_XLO), ti.q, ti.i, Vh, vcvt<typename SpinorFmt<XP>::R>(z));
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_R), ti.q, ti.i, Vh, vcvt<RS>(b));
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), ti.q, ti.i, Vh, vcvt<RS>(z));
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), ti.q, ti.i, Vh, vcvt<RS>(z));
+            sums[l * kSums + 3] = vdot_re(b, b);
+        }
+        block_sum<NB * kSums>(sums, smem);
+        unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
+        if (mask && threadIdx.x < 32) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (mask & (1u << l)) finish_init_lane(a, S, P.lane[l]);
+        }
+        __syncthreads();
+    }
+}
+
+// FP64 hop of (x_hi + x_lo + alpha p) for a lane in a reliable update
+template <int SP, int XP>
+__device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid,
+                                     double alpha)
 {
     const int nq = 1 - q, Vh = S.g.Vh;
     const void* xhi = rhs_ptr(a, rid, F_XHI);
     const void* xlo = rhs_ptr(a, rid, F_XLO);
+    const void* pp = rhs_ptr(a, rid, F_P);
     Vec3<double> acc;
     vzero(acc);
-#pragma unroll
+#pragma unroll 1
     for (int mu = 0; mu < 4; ++mu) {
         const bool eta_neg = eta_sign(c, mu) < 0;
         const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
         const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
         const bool wd = (mu == 3) && (c.x[3] == 0);
-        Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-        Vec3<double> xu = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, nq, lu, Vh), 1.0,
-                                vcvt<double>(SpinorFmt<XP>::load_cg(xlo, nq, lu, Vh)));
-        vacc(acc, mul_mv(U, xu), eta_neg != wu);
-        Mat3<double> Ud = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-        Vec3<double> xd = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, nq, ld, Vh), 1.0,
-                                vcvt<double>(SpinorFmt<XP>::load_cg(xlo, nq, ld, Vh)));
-        vacc(acc, mul_adj_mv(Ud, xd), !(eta_neg != wd));
+        {
+            Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
+            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, lu, Vh), 1.0,
+                                   vcvt<double>(SpinorFmt<XP>::load(xlo, nq, lu, Vh)));
+            x = vaxpy(x, alpha, vcvt<double>(SpinorFmt<SP>::load(pp, nq, lu, Vh)));
+            vacc(acc, mul_mv(U, x), eta_neg != wu);
+        }
+        {
+            Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
+            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, ld, Vh), 1.0,
+                                   vcvt<double>(SpinorFmt<XP>::load(xlo, nq, ld, Vh)));
+            x = vaxpy(x, alpha, vcvt<double>(SpinorFmt<SP>::load(pp, nq, ld, Vh)));
+            vacc(acc, mul_adj_mv(U, x), !(eta_neg != wd));
+        }
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc.c[k] = {0.5 * acc.c[k].re, 0.5 * acc.c[k].im};
     SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
 }
 
+// t = K p_k for active lanes (output parity q); thi for reliable updates
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
+{
+    typedef typename GaugeFmt<GP>::R R;
+    typedef typename SpinorFmt<SP>::R RS;
+    constexpr int XP = XFmt<SP>::v;
+    __shared__ CgSys s_sys;
+    stage_sys(a, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, blockIdx.x);
+    if (!ti.valid) return;
+    const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
+    const Coord c = eo_coords(S.g, q, ti.i);
+    for (int base = 0; base < S.nrhs; base += NB) {
+        LanePass<NB> P;
+        gather_pass<NB>(a, S, base, q, true, cur, P);
+        if (P.anyA) {
+            Vec3<R> acc[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) vzero(acc[l]);
+#pragma unroll 1
+            for (int mu = 0; mu < 4; ++mu) {
+                const bool eta_neg = eta_sign(c, mu) < 0;
+                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
+                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
+                const bool wd = (mu == 3) && (c.x[3] == 0);
+                {
+                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
+#pragma unroll
+                    for (int l = 0; l < NB; ++l) {
+                        if (P.mode[l] != LM_ACTIVE) continue;
+                        Vec3<R> pn = vcvt<R>(neighbour_p<SP>(a, P.rid[l], nq, lu, Vh, (RS)P.alpha[l], (RS)P.beta[l]));
+                        vacc(acc[l], mul_mv(U, pn), eta_neg != wu);
+                    }
+                }
+                {
+                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
+#pragma unroll
+                    for (int l = 0; l < NB; ++l) {
+                        if (P.mode[l] != LM_ACTIVE) continue;
+                        Vec3<R> pn = vcvt<R>(neighbour_p<SP>(a, P.rid[l], nq, ld, Vh, (RS)P.alpha[l], (RS)P.beta[l]));
+                        vacc(acc[l], mul_adj_mv(U, pn), !(eta_neg != wd));
+                    }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < NB; ++l) {
+                if (P.mode[l] != LM_ACTIVE) continue;
+                Vec3<R> o;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
+            }
+        }
+        if (P.anyR) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (P.mode[l] == LM_RU) ru_hop1<SP, XP>(a, S, c, q, ti.i, P.rid[l], P.alpha[l]);
+        }
+    }
+}
+
+// reliable update at the lane's own site: returns |b - M x|^2 contribution
 template <int SP, int XP>
-__device__ __noinline__ double ru_hop2_site(const CgArgs& a, const CgSys& S, const Coord& c, int q,
-                                            int i, int rid)
+__device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid,
+                                       double alpha)
 {
     typedef typename SpinorFmt<SP>::R RS;
     const int nq = 1 - q, Vh = S.g.Vh;
     const void* thi = rhs_ptr(a, rid, F_THI);
     Vec3<double> acc;
     vzero(acc);
-#pragma unroll
+#pragma unroll 1
     for (int mu = 0; mu < 4; ++mu) {
         const bool eta_neg = eta_sign(c, mu) < 0;
         const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
         const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
         const bool wd = (mu == 3) && (c.x[3] == 0);
         Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-        vacc(acc, mul_mv(U, SpinorFmt<SP_F64>::load_cg(thi, nq, lu, Vh)), eta_neg != wu);
+        vacc(acc, mul_mv(U, SpinorFmt<SP_F64>::load(thi, nq, lu, Vh)), eta_neg != wu);
         Mat3<double> Ud = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-        vacc(acc, mul_adj_mv(Ud, SpinorFmt<SP_F64>::load_cg(thi, nq, ld, Vh)), !(eta_neg != wd));
+        vacc(acc, mul_adj_mv(Ud, SpinorFmt<SP_F64>::load(thi, nq, ld, Vh)), !(eta_neg != wd));
     }
     void* xhi = rhs_ptr(a, rid, F_XHI);
     void* xlo = rhs_ptr(a, rid, F_XLO);
     Vec3<double> xn = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, q, i, Vh), 1.0,
                             vcvt<double>(SpinorFmt<XP>::load_cg(xlo, q, i, Vh)));
+    xn = vaxpy(xn, alpha, vcvt<double>(SpinorFmt<SP>::load_cg(rhs_ptr(a, rid, F_P), q, i, Vh)));
     SpinorFmt<SP_F64>::store(xhi, q, i, Vh, xn);
     Vec3<typename SpinorFmt<XP>::R> z;
     vzero(z);
     SpinorFmt<XP>::store(xlo, q, i, Vh, z);
-    Vec3<double> b = SpinorFmt<SP_F64>::load_cg(rhs_ptr(a, rid, F_B), q, i, Vh);
+    Vec3<double> b = SpinorFmt<SP_F64>::load(rhs_ptr(a, rid, F_B), q, i, Vh);
     Vec3<double> res;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -427,330 +459,112 @@ __device__ __noinline__ double ru_hop2_site(const CgArgs& a, const CgSys& S, con
     return vdot_re(res, res);
 }
 
-// gather the lanes of one RHS pass
-template <int NB>
-__device__ __forceinline__ void gather(const CgArgs& a, const CgSys& S, int base, int cnt, int q,
-                                       bool hop1, int cur, int (&lanes)[NB], int (&mode)[NB],
-                                       int (&rid)[NB])
-{
-#pragma unroll
-    for (int l = 0; l < NB; ++l) {
-        lanes[l] = 0;
-        mode[l] = LM_DONE;
-        rid[l] = 0;
-        if (l < cnt) {
-            lanes[l] = lane_of(S, base + l, q, hop1);
-            const CgLane* L = a.lanes + lanes[l];
-            mode[l] = ld_int(&L->mode[cur]);
-            rid[l] = __ldg(&L->rhs);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// P0: x = 0, r = b, p = 0; |b|^2
-// ---------------------------------------------------------------------------
+// own sites: r, p, x advanced and stored; v = m^2 p - K t; the four sums
 template <int GP, int SP, int NB>
-__device__ void phase_init(const CgArgs& a, const CgSys& S, int t, double* smem, unsigned* s_mask)
-{
-    typedef typename SpinorFmt<SP>::R R;
-    constexpr int XP = XFmt<SP>::v;
-    const TileInfo ti = decode_tile(S, t);
-    const int Vh = S.g.Vh;
-    for (int base = 0; base < S.nrhs; base += NB) {
-        const int cnt = min(NB, S.nrhs - base);
-        int lanes[NB], rid[NB], mode[NB];
-        bool part[NB];
-        double sums[NB];
-        gather<NB>(a, S, base, cnt, ti.q, false, 0, lanes, mode, rid);
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            sums[l] = 0.0;
-            part[l] = l < cnt;
-            if (l >= cnt || !ti.valid) continue;
-            Vec3<double> b = SpinorFmt<SP_F64>::load_cg(rhs_ptr(a, rid[l], F_B), ti.q, ti.i, Vh);
-            Vec3<double> z;
-            vzero(z);
-            SpinorFmt<SP_F64>::store(rhs_ptr(a, rid[l], F_XHI), ti.q, ti.i, Vh, z);
-            if (a.mixed)
-                SpinorFmt<XP>::store(rhs_ptr(a, rid[l], F_XLO), ti.q, ti.i, Vh,
-                                     vcvt<typename SpinorFmt<XP>::R>(z));
-            SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_R), ti.q, ti.i, Vh, vcvt<R>(b));
-            SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_P), ti.q, ti.i, Vh, vcvt<R>(z));
-            sums[l] = vdot_re(b, b);
-        }
-        block_sum<NB>(sums, smem);
-        unsigned mask = arrive<NB>(a, S, lanes, part, sums, ti.slot, s_mask);
-        if (mask && threadIdx.x < 32) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mask & (1u << l)) finish_init(a, S, lanes[l]);
-        }
-        __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// P1: t = K (r + beta p) for normal lanes; thi = K (x_hi + x_lo) for lanes in
-// a reliable update.  Output parity q, inputs on parity 1-q.
-// ---------------------------------------------------------------------------
-template <int GP, int SP, int NB>
-__device__ void phase_hop1(const CgArgs& a, const CgSys& S, int t, int cur)
+__global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
-    const TileInfo ti = decode_tile(S, t);
-    if (!ti.valid) return;
-    const Coord c = eo_coords(S.g, ti.q, ti.i);
-    const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
-    for (int base = 0; base < S.nrhs; base += NB) {
-        const int cnt = min(NB, S.nrhs - base);
-        int lanes[NB], rid[NB], mode[NB];
-        RS beta[NB];
-        gather<NB>(a, S, base, cnt, q, true, cur, lanes, mode, rid);
-        bool anyA = false, anyR = false;
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            anyA |= mode[l] == LM_ACTIVE;
-            anyR |= mode[l] == LM_RU;
-            beta[l] = mode[l] == LM_ACTIVE ? (RS)ld_dbl(&a.lanes[lanes[l]].beta) : RS(0);
-        }
-        if (anyA) {
-            Vec3<R> acc[NB];
-#pragma unroll
-            for (int l = 0; l < NB; ++l) vzero(acc[l]);
-#pragma unroll
-            for (int mu = 0; mu < 4; ++mu) {
-                const bool eta_neg = eta_sign(c, mu) < 0;
-                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-                const bool wd = (mu == 3) && (c.x[3] == 0);
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (mode[l] != LM_ACTIVE) continue;
-                        Vec3<RS> rr = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_R), nq, lu, Vh);
-                        Vec3<RS> pp = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_P), nq, lu, Vh);
-                        Vec3<R> pn = vcvt<R>(SpinorFmt<SP>::quantize(vaxpy(rr, beta[l], pp)));
-                        vacc(acc[l], mul_mv(U, pn), eta_neg != wu);
-                    }
-                }
-                {
-                    Mat3<R> Ud = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (mode[l] != LM_ACTIVE) continue;
-                        Vec3<RS> rr = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_R), nq, ld, Vh);
-                        Vec3<RS> pp = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_P), nq, ld, Vh);
-                        Vec3<R> pn = vcvt<R>(SpinorFmt<SP>::quantize(vaxpy(rr, beta[l], pp)));
-                        vacc(acc[l], mul_adj_mv(Ud, pn), !(eta_neg != wd));
-                    }
-                }
-            }
-#pragma unroll
-            for (int l = 0; l < NB; ++l) {
-                if (mode[l] != LM_ACTIVE) continue;
-                Vec3<R> o;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
-                SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
-            }
-        }
-        if (anyR) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mode[l] == LM_RU) ru_hop1_site<XP>(a, S, c, q, ti.i, rid[l]);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// P2: p = r + beta p, v = m^2 p - K t, <p,v> (normal lanes);
-//     x_hi += x_lo, x_lo = 0, r = b - (m^2 x_hi - K thi), |r|^2 (reliable update)
-// ---------------------------------------------------------------------------
-template <int GP, int SP, int NB>
-__device__ void phase_hop2(const CgArgs& a, const CgSys& S, int t, int cur, double* smem,
-                           unsigned* s_mask)
-{
-    typedef typename GaugeFmt<GP>::R R;
-    typedef typename SpinorFmt<SP>::R RS;
-    constexpr int XP = XFmt<SP>::v;
-    const TileInfo ti = decode_tile(S, t);
+    typedef typename SpinorFmt<XP>::R RX;
+    __shared__ CgSys s_sys;
+    __shared__ double smem[32 * NB * kSums];
+    __shared__ unsigned s_mask;
+    stage_sys(a, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, blockIdx.x);
     const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
     Coord c;
     if (ti.valid) c = eo_coords(S.g, q, ti.i);
     for (int base = 0; base < S.nrhs; base += NB) {
-        const int cnt = min(NB, S.nrhs - base);
-        int lanes[NB], rid[NB], mode[NB];
-        RS beta[NB];
+        LanePass<NB> P;
+        gather_pass<NB>(a, S, base, q, false, cur, P);
+        if (!(P.anyA || P.anyR || P.anyF)) continue;  // uniform across the block
         bool part[NB];
-        double sums[NB];
-        gather<NB>(a, S, base, cnt, q, false, cur, lanes, mode, rid);
-        bool anyA = false, anyR = false;
+        double sums[NB * kSums];
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
-            anyA |= mode[l] == LM_ACTIVE;
-            anyR |= mode[l] == LM_RU;
-            part[l] = mode[l] == LM_ACTIVE || mode[l] == LM_RU;
-            sums[l] = 0.0;
-            beta[l] = mode[l] == LM_ACTIVE ? (RS)ld_dbl(&a.lanes[lanes[l]].beta) : RS(0);
+            // FINAL lanes take the ticket too: the last tile retires them
+            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU || P.mode[l] == LM_FINAL;
+#pragma unroll
+            for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
         }
-        if (!anyA && !anyR) continue;  // uniform across the block
-        if (anyA && ti.valid) {
+        if (ti.valid && (P.anyA || P.anyF)) {
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
+            if (P.anyA) {
+#pragma unroll 1
+                for (int mu = 0; mu < 4; ++mu) {
+                    const bool eta_neg = eta_sign(c, mu) < 0;
+                    const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
+                    const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
+                    const bool wd = (mu == 3) && (c.x[3] == 0);
+                    {
+                        Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
 #pragma unroll
-            for (int mu = 0; mu < 4; ++mu) {
-                const bool eta_neg = eta_sign(c, mu) < 0;
-                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-                const bool wd = (mu == 3) && (c.x[3] == 0);
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (mode[l] != LM_ACTIVE) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_T), nq, lu, Vh));
-                        vacc(acc[l], mul_mv(U, w), eta_neg != wu);
+                        for (int l = 0; l < NB; ++l) {
+                            if (P.mode[l] != LM_ACTIVE) continue;
+                            Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_T), nq, lu, Vh));
+                            vacc(acc[l], mul_mv(U, w), eta_neg != wu);
+                        }
                     }
-                }
-                {
-                    Mat3<R> Ud = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
+                    {
+                        Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
 #pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (mode[l] != LM_ACTIVE) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_T), nq, ld, Vh));
-                        vacc(acc[l], mul_adj_mv(Ud, w), !(eta_neg != wd));
+                        for (int l = 0; l < NB; ++l) {
+                            if (P.mode[l] != LM_ACTIVE) continue;
+                            Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_T), nq, ld, Vh));
+                            vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
+                        }
                     }
                 }
             }
             const R m2 = (R)S.m2;
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
-                if (mode[l] != LM_ACTIVE) continue;
-                void* pptr = rhs_ptr(a, rid[l], F_P);
-                Vec3<RS> rr = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_R), q, ti.i, Vh);
-                Vec3<RS> pp = SpinorFmt<SP>::load_cg(pptr, q, ti.i, Vh);
-                Vec3<RS> pn = SpinorFmt<SP>::quantize(vaxpy(rr, beta[l], pp));
-                SpinorFmt<SP>::store(pptr, q, ti.i, Vh, pn);
-                Vec3<R> pr = vcvt<R>(pn), v;
+                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_FINAL) continue;
+                void* rp = rhs_ptr(a, P.rid[l], F_R);
+                void* vp = rhs_ptr(a, P.rid[l], F_V);
+                void* pp = rhs_ptr(a, P.rid[l], F_P);
+                void* xp = rhs_ptr(a, P.rid[l], F_XLO);
+                Vec3<RS> p = SpinorFmt<SP>::load_cg(pp, q, ti.i, Vh);
+                Vec3<RX> x = SpinorFmt<XP>::load_cg(xp, q, ti.i, Vh);
+                SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)P.alpha[l], vcvt<RX>(p)));
+                if (P.mode[l] == LM_FINAL) continue;
+                Vec3<RS> r = SpinorFmt<SP>::load_cg(rp, q, ti.i, Vh);
+                Vec3<RS> v = SpinorFmt<SP>::load_cg(vp, q, ti.i, Vh);
+                Vec3<RS> rn, pn;
+                advance<SP>(r, v, p, (RS)P.alpha[l], (RS)P.beta[l], rn, pn);
+                SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
+                SpinorFmt<SP>::store(pp, q, ti.i, Vh, pn);
+                Vec3<R> pr = vcvt<R>(pn), w;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    v.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
-                    v.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
+                    w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
+                    w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
                 }
-                Vec3<RS> vq = SpinorFmt<SP>::quantize(vcvt<RS>(v));
-                SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_V), q, ti.i, Vh, vq);
-                sums[l] = vdot_re(pn, vq);
+                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
+                SpinorFmt<SP>::store(vp, q, ti.i, Vh, vn);
+                sums[l * kSums + 0] = vdot_re(pn, vn);
+                sums[l * kSums + 1] = vdot_re(rn, vn);
+                sums[l * kSums + 2] = vdot_re(vn, vn);
+                sums[l * kSums + 3] = vdot_re(rn, rn);
             }
         }
-        if (anyR && ti.valid) {
+        if (ti.valid && P.anyR) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (mode[l] == LM_RU) sums[l] = ru_hop2_site<SP, XP>(a, S, c, q, ti.i, rid[l]);
+                if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l], P.alpha[l]);
         }
-        block_sum<NB>(sums, smem);
-        unsigned mask = arrive<NB>(a, S, lanes, part, sums, ti.slot, s_mask);
+        block_sum<NB * kSums>(sums, smem);
+        unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
         if (mask && threadIdx.x < 32) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (mask & (1u << l)) finish_hop2(a, S, lanes[l], mode[l], cur);
+                if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
         }
         __syncthreads();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// P3: x += alpha p, r -= alpha v, |r|^2 -> beta, convergence, reliable update
-// ---------------------------------------------------------------------------
-template <int GP, int SP, int NB>
-__device__ void phase_update(const CgArgs& a, const CgSys& S, int t, int cur, double* smem,
-                             unsigned* s_mask)
-{
-    typedef typename SpinorFmt<SP>::R RS;
-    constexpr int XP = XFmt<SP>::v;
-    typedef typename SpinorFmt<XP>::R RX;
-    const TileInfo ti = decode_tile(S, t);
-    const int q = ti.q, Vh = S.g.Vh;
-    for (int base = 0; base < S.nrhs; base += NB) {
-        const int cnt = min(NB, S.nrhs - base);
-        int lanes[NB], rid[NB], mode[NB];
-        bool part[NB];
-        double sums[NB];
-        gather<NB>(a, S, base, cnt, q, false, cur, lanes, mode, rid);
-        bool any = false;
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            part[l] = mode[l] == LM_ACTIVE;
-            any |= part[l];
-            sums[l] = 0.0;
-            if (part[l] && ti.valid) {
-                const double alpha = ld_dbl(&a.lanes[lanes[l]].alpha);
-                void* xptr = rhs_ptr(a, rid[l], F_XLO);
-                void* rptr = rhs_ptr(a, rid[l], F_R);
-                Vec3<RS> pp = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_P), q, ti.i, Vh);
-                Vec3<RS> vv = SpinorFmt<SP>::load_cg(rhs_ptr(a, rid[l], F_V), q, ti.i, Vh);
-                Vec3<RS> rr = SpinorFmt<SP>::load_cg(rptr, q, ti.i, Vh);
-                Vec3<RX> xx = SpinorFmt<XP>::load_cg(xptr, q, ti.i, Vh);
-                SpinorFmt<XP>::store(xptr, q, ti.i, Vh, vaxpy(xx, (RX)alpha, vcvt<RX>(pp)));
-                Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(rr, (RS)(-alpha), vv));
-                SpinorFmt<SP>::store(rptr, q, ti.i, Vh, rn);
-                sums[l] = vdot_re(rn, rn);
-            }
-        }
-        if (!any) continue;
-        block_sum<NB>(sums, smem);
-        unsigned mask = arrive<NB>(a, S, lanes, part, sums, ti.slot, s_mask);
-        if (mask && threadIdx.x < 32) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mask & (1u << l)) finish_update(a, S, lanes[l], cur);
-        }
-        __syncthreads();
-    }
-}
-
-// stage the tile's system descriptor in shared memory
-__device__ __forceinline__ void load_sys(const CgArgs& a, int t, CgSys* s_sys)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) *s_sys = a.sys[__ldg(a.tile_sys + t)];
-    __syncthreads();
-}
-
-template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (SP == SP_F64 ? 1 : 2)) cg_persistent(CgArgs a)
-{
-    cgrp::grid_group grid = cgrp::this_grid();
-    __shared__ double smem[32 * NB];
-    __shared__ unsigned s_mask;
-    __shared__ CgSys s_sys;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        load_sys(a, t, &s_sys);
-        phase_init<GP, SP, NB>(a, s_sys, t, smem, &s_mask);
-    }
-    grid.sync();
-    for (int it = 0; it < a.maxloop; ++it) {
-        if (__ldcg(a.n_active) == 0) break;
-        const int cur = it & 1;
-        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-            load_sys(a, t, &s_sys);
-            phase_hop1<GP, SP, NB>(a, s_sys, t, cur);
-        }
-        grid.sync();
-        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-            load_sys(a, t, &s_sys);
-            phase_hop2<GP, SP, NB>(a, s_sys, t, cur, smem, &s_mask);
-        }
-        grid.sync();
-        for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-            load_sys(a, t, &s_sys);
-            phase_update<GP, SP, NB>(a, s_sys, t, cur, smem, &s_mask);
-        }
-        grid.sync();
     }
 }
 
@@ -760,24 +574,50 @@ __global__ void __launch_bounds__(kTile, (SP == SP_F64 ? 1 : 2)) cg_persistent(C
 // host side
 // ---------------------------------------------------------------------------
 
-typedef void (*CgKernel)(CgArgs);
+typedef void (*InitKernel)(CgArgs);
+typedef void (*HopKernel)(CgArgs, int);
 
-static CgKernel pick_kernel(int prec, int nb)
+struct CgKernels {
+    InitKernel init;
+    HopKernel hop1, hop2;
+};
+
+template <int GP, int SP>
+static HopKernel pick_hop1(int nb)
 {
+    if constexpr (SP != SP_F64) {
+        if (nb >= 8) return cg_hop1<GP, SP, 8>;
+        if (nb >= 4) return cg_hop1<GP, SP, 4>;
+    }
+    if (nb >= 2) return cg_hop1<GP, SP, 2>;
+    return cg_hop1<GP, SP, 1>;
+}
+
+template <int GP, int SP>
+static void pick_hop2(int nb, HopKernel* hop2, InitKernel* init)
+{
+    if constexpr (SP != SP_F64) {
+        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4>; *init = cg_init<SP, 4>; return; }
+    }
+    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2>; *init = cg_init<SP, 2>; return; }
+    *hop2 = cg_hop2<GP, SP, 1>;
+    *init = cg_init<SP, 1>;
+}
+
+static CgKernels pick_kernels(int prec, int nb1, int nb2)
+{
+    CgKernels k;
     if (prec == SFH_PREC_F64) {
-        if (nb >= 2) return cg_persistent<GP_F64_18, SP_F64, 2>;
-        return cg_persistent<GP_F64_18, SP_F64, 1>;
+        k.hop1 = pick_hop1<GP_F64_18, SP_F64>(nb1);
+        pick_hop2<GP_F64_18, SP_F64>(nb2, &k.hop2, &k.init);
+    } else if (prec == SFH_PREC_F32) {
+        k.hop1 = pick_hop1<GP_F32_12, SP_F32>(nb1);
+        pick_hop2<GP_F32_12, SP_F32>(nb2, &k.hop2, &k.init);
+    } else {
+        k.hop1 = pick_hop1<GP_F16_12, SP_F16>(nb1);
+        pick_hop2<GP_F16_12, SP_F16>(nb2, &k.hop2, &k.init);
     }
-    if (prec == SFH_PREC_F32) {
-        if (nb >= 8) return cg_persistent<GP_F32_12, SP_F32, 8>;
-        if (nb >= 4) return cg_persistent<GP_F32_12, SP_F32, 4>;
-        if (nb >= 2) return cg_persistent<GP_F32_12, SP_F32, 2>;
-        return cg_persistent<GP_F32_12, SP_F32, 1>;
-    }
-    if (nb >= 8) return cg_persistent<GP_F16_12, SP_F16, 8>;
-    if (nb >= 4) return cg_persistent<GP_F16_12, SP_F16, 4>;
-    if (nb >= 2) return cg_persistent<GP_F16_12, SP_F16, 2>;
-    return cg_persistent<GP_F16_12, SP_F16, 1>;
+    return k;
 }
 
 static size_t spinor_bytes(int sp, int Vh)
@@ -810,10 +650,32 @@ struct CgWorkspace {
     int* d_active = nullptr;
     std::vector<void*> allocs;
     size_t bytes = 0;
+    // iteration chunks replayed as one graph launch each
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CgKernels gk = {};
+    double g_tol = -1.0, g_delta = -1.0;
+    int g_maxit = -1;
+    int* h_active = nullptr;  // pinned, two slots
+    cudaEvent_t ev[2] = {nullptr, nullptr};
 
     ~CgWorkspace() { release(); }
+    void release_graph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        g_tol = -1.0;
+    }
     void release()
     {
+        release_graph();
+        if (h_active) cudaFreeHost(h_active);
+        h_active = nullptr;
+        for (int k = 0; k < 2; ++k)
+            if (ev[k]) cudaEventDestroy(ev[k]);
+        ev[0] = ev[1] = nullptr;
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
         d_sys = nullptr; d_rhs = nullptr; d_lanes = nullptr;
@@ -884,7 +746,7 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
                 L.rhs = rid;
                 L.parity = both ? 2 : lp;
                 L.poff = poff;  // slots indexed by the tile's local index (both parities)
-                poff += 2 * S.ntq;
+                poff += kSums * 2 * S.ntq;
                 L.mode[0] = L.mode[1] = LM_ACTIVE;
                 w.lanes_h.push_back(L);
                 ++lane;
@@ -905,39 +767,23 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
     if (!w.rhs.empty())
         if ((e = cudaMemcpy(w.d_rhs, w.rhs.data(), sizeof(CgRhs) * w.rhs.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if ((e = cudaMemcpy(w.d_tile_sys, tile_sys.data(), sizeof(int) * tile_sys.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+    if ((e = cudaHostAlloc((void**)&w.h_active, 2 * sizeof(int), cudaHostAllocDefault)) != cudaSuccess) return e;
+    for (int k = 0; k < 2; ++k)
+        if ((e = cudaEventCreateWithFlags(&w.ev[k], cudaEventDisableTiming)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
-static int default_nb(int prec, int max_nrhs)
+static int default_nb(int max_nrhs, int cap)
 {
-    int cap = prec == SFH_PREC_F64 ? 2 : 8;
     int nb = 1;
     while (nb < max_nrhs && nb < cap) nb *= 2;
     return nb;
 }
 
-// Launch the persistent solver on a built workspace.  Returns a cudaError.
-static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb,
-                                   cudaStream_t stream, int num_sms)
+constexpr int kChunk = 16;  // CG iterations per graph launch (even)
+
+static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delta)
 {
-    int max_nrhs = 1;
-    for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
-    if (nb <= 0) nb = default_nb(w.prec, max_nrhs);
-    w.nb = nb;
-    for (CgLane& L : w.lanes_h) {
-        L.mode[0] = L.mode[1] = LM_ACTIVE;
-        L.ticket = 0;
-        L.iters = 0;
-        L.nru = 0;
-        L.status = SFH_OK;
-    }
-    cudaError_t e;
-    if ((e = cudaMemcpyAsync(w.d_lanes, w.lanes_h.data(), sizeof(CgLane) * w.nlanes,
-                             cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-        return e;
-    int nact = w.nlanes;
-    if ((e = cudaMemcpyAsync(w.d_active, &nact, sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-        return e;
     CgArgs a;
     a.nsys = w.nsys;
     a.nlanes = w.nlanes;
@@ -952,24 +798,103 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     a.delta = delta;
     a.maxit = maxit;
     a.mixed = w.prec != SFH_PREC_F64;
-    a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
-    CgKernel k = pick_kernel(w.prec, nb);
-    int per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 0)) != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-    int grid = std::min(per_sm * num_sms, w.ntiles);
-    void* args[] = {&a};
-    e = cudaLaunchCooperativeKernel((const void*)k, dim3(grid), dim3(kTile), args, 0, stream);
+    a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 2;
+    return a;
+}
+
+// (Re)build the graph of kChunk iterations: hop1, hop2, hop1, hop2, ...
+static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, double tol, int maxit,
+                                double delta)
+{
+    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.g_tol == tol && w.g_maxit == maxit &&
+        w.g_delta == delta)
+        return cudaSuccess;
+    w.release_graph();
+    cudaError_t e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
+    cudaGraphNode_t prev = nullptr;
+    for (int it = 0; it < kChunk; ++it) {
+        int cur = it & 1;
+        for (int ph = 0; ph < 2; ++ph) {
+            cudaKernelNodeParams p;
+            std::memset(&p, 0, sizeof(p));
+            p.func = (void*)(ph == 0 ? k.hop1 : k.hop2);
+            p.gridDim = dim3(w.ntiles);
+            p.blockDim = dim3(kTile);
+            void* args[] = {&a, &cur};
+            p.kernelParams = args;
+            cudaGraphNode_t node;
+            e = cudaGraphAddKernelNode(&node, w.graph, prev ? &prev : nullptr, prev ? 1 : 0, &p);
+            if (e != cudaSuccess) return e;
+            prev = node;
+        }
+    }
+    e = cudaGraphInstantiate(&w.exec, w.graph, 0);
+    if (e != cudaSuccess) return e;
+    w.gk = k;
+    w.g_tol = tol;
+    w.g_maxit = maxit;
+    w.g_delta = delta;
+    return cudaSuccess;
+}
+
+// Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
+// two hop kernels (0 = from the largest RHS count).  Returns a cudaError.
+static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
+                                   cudaStream_t stream)
+{
+    int max_nrhs = 1;
+    for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
+    const bool f64 = w.prec == SFH_PREC_F64;
+    if (nb1 <= 0) nb1 = default_nb(max_nrhs, f64 ? 2 : 8);
+    if (nb2 <= 0) nb2 = default_nb(max_nrhs, f64 ? 2 : 4);
+    w.nb = nb1;
+    for (CgLane& L : w.lanes_h) {
+        L.mode[0] = L.mode[1] = LM_ACTIVE;
+        L.ticket = 0;
+        L.iters = 0;
+        L.nru = 0;
+        L.status = SFH_OK;
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(w.d_lanes, w.lanes_h.data(), sizeof(CgLane) * w.nlanes,
+                             cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
+    w.h_active[0] = w.h_active[1] = w.nlanes;
+    if ((e = cudaMemcpyAsync(w.d_active, &w.h_active[0], sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
+    CgArgs a = make_args(w, tol, maxit, delta);
+    CgKernels k = pick_kernels(w.prec, nb1, nb2);
+    k.init<<<w.ntiles, kTile, 0, stream>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
+    const int max_chunks = a.maxloop / kChunk + 2;
+    // keep one chunk queued ahead of the convergence check
+    for (int c = 0; c < max_chunks; ++c) {
+        if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(w.ev[c & 1], stream)) != cudaSuccess) return e;
+        if (c >= 1) {
+            if ((e = cudaEventSynchronize(w.ev[(c - 1) & 1])) != cudaSuccess) return e;
+            if (w.h_active[(c - 1) & 1] == 0) break;
+        }
+    }
     e = cudaMemcpyAsync(w.lanes_h.data(), w.d_lanes, sizeof(CgLane) * w.nlanes, cudaMemcpyDeviceToHost, stream);
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
-    for (CgLane& L : w.lanes_h)
-        if (L.mode[0] == LM_ACTIVE || L.mode[0] == LM_RU) {
+    // a lane that stopped holds DONE or FAILED in one of its two mode slots
+    // (the other may still hold FINAL after its last x update)
+    for (CgLane& L : w.lanes_h) {
+        bool stopped = false;
+        for (int k = 0; k < 2; ++k) stopped |= L.mode[k] == LM_DONE || L.mode[k] == LM_FAILED;
+        if (!stopped) {
             L.status = SFH_ERR_NOCONV;
             L.mode[0] = L.mode[1] = LM_FAILED;
         }
+    }
     return cudaSuccess;
 }
 
@@ -982,7 +907,7 @@ struct sfh_batch {
     int device = 0, num_sms = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    int prec = 0, flags = 0, nb = 0;
+    int prec = 0, flags = 0, nb = 0, nb2 = 0;
     std::vector<sfh_system_desc> desc;
     std::vector<sfh::Geom> geoms;
     std::vector<void*> U64, U32, U16;
@@ -1114,6 +1039,7 @@ extern "C" int sfh_batch_set_rhs_block(sfh_batch* b, int width)
 {
     if (!b || width < 0 || width > 8) return SFH_ERR_INVALID;
     b->nb = width;
+    b->nb2 = width;
     return SFH_OK;
 }
 
@@ -1148,7 +1074,7 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
 {
     if (!b || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->stream, b->num_sms),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->stream),
                         "batched CG");
     if (st) return st;
     for (const sfh::CgLane& L : b->ws.lanes_h)
@@ -1183,7 +1109,7 @@ extern "C" int sfh_batch_get_info(sfh_batch* b, int k, int j, sfh_cg_info* info)
         if (L.parity < 2) info->iters_parity[L.parity] = L.iters;
         else info->iters_parity[0] = info->iters_parity[1] = L.iters;
         info->reliable_updates += L.nru;
-        rr += L.rr;
+        rr += L.rr_next;
         bb += L.bb;
     }
     info->rsq_rel = bb > 0 ? rr / bb : 0.0;
@@ -1249,7 +1175,7 @@ int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int 
     e = cudaMemcpyAsync(c->stage, phi, fs, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg upload");
     launch_spinor_aos_to_eo(c->g, (const double*)c->stage, w.rhs[0].b, c->stream);
-    e = workspace_solve(w, tol, maxit, 0.1, 0, c->stream, c->num_sms);
+    e = workspace_solve(w, tol, maxit, 0.1, 0, 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
     launch_spinor_eo_to_aos(c->g, w.rhs[0].xhi, (double*)c->stage, c->stream);
     e = cudaMemcpyAsync(X, c->stage, fs, cudaMemcpyDeviceToHost, c->stream);
@@ -1265,7 +1191,7 @@ int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int 
         if (L.parity < 2) inf.iters_parity[L.parity] = L.iters;
         else inf.iters_parity[0] = inf.iters_parity[1] = L.iters;
         inf.reliable_updates += L.nru;
-        rr += L.rr;
+        rr += L.rr_next;
         bb += L.bb;
     }
     inf.status = status;
@@ -1328,171 +1254,3 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
     if (st) return st;
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
 }
-
-// ===========================================================================
-// Allocation-free CG entry point.
-//
-// For callers that cannot call cudaMalloc: code that runs while a stream is
-// being captured into a CUDA graph, host runtimes that own all device memory
-// through their own pool and forbid outside allocations, and trajectory loops
-// that must not allocate after start-up.  The solver's work vectors and
-// control data live in the file-scope array below instead of device
-// allocations; the caller passes device inputs and outputs.
-// ===========================================================================
-namespace sfh {
-namespace {
-
-constexpr int kNoAllocMaxSites = SFH_NOALLOC_MAX_SITES;
-constexpr int kNoAllocMaxTiles = kNoAllocMaxSites / kTile;  // 2 * tiles per parity
-constexpr size_t kAlign = 256;
-constexpr size_t align_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
-constexpr size_t kOffSys = 0;
-constexpr size_t kOffRhs = align_up(kOffSys + sizeof(CgSys));
-constexpr size_t kOffLane = align_up(kOffRhs + sizeof(CgRhs));
-constexpr size_t kOffActive = align_up(kOffLane + sizeof(CgLane));
-constexpr size_t kOffTiles = align_up(kOffActive + sizeof(int));
-constexpr size_t kOffPartial = align_up(kOffTiles + sizeof(int) * kNoAllocMaxTiles);
-constexpr size_t kOffVec = align_up(kOffPartial + sizeof(double) * kNoAllocMaxTiles);
-constexpr size_t kVecBytes = (size_t)kNoAllocMaxSites * 6 * sizeof(double);
-constexpr size_t kNoAllocBytes = kOffVec + 4 * kVecBytes;  // r, p, v, t
-
-// 12.6 MB per device; held by every GPU that loads the library, until exit.
-static __device__ __align__(256) unsigned char sfh_noalloc_scratch[kNoAllocBytes];
-
-// Writes the solver's control data into the scratch array (zeroes the
-// tickets and partials left by the previous call).
-__global__ void noalloc_setup(CgSys S, CgRhs R, unsigned char* base)
-{
-    CgSys* sys = reinterpret_cast<CgSys*>(base + kOffSys);
-    CgRhs* rhs = reinterpret_cast<CgRhs*>(base + kOffRhs);
-    CgLane* lane = reinterpret_cast<CgLane*>(base + kOffLane);
-    int* active = reinterpret_cast<int*>(base + kOffActive);
-    int* tiles = reinterpret_cast<int*>(base + kOffTiles);
-    double* partial = reinterpret_cast<double*>(base + kOffPartial);
-    for (int k = threadIdx.x; k < 2 * S.ntq; k += blockDim.x) {
-        tiles[k] = 0;
-        partial[k] = 0.0;
-    }
-    if (threadIdx.x == 0) {
-        *sys = S;
-        *rhs = R;
-        CgLane L;
-        memset(&L, 0, sizeof(L));
-        L.sys = 0;
-        L.rhs = 0;
-        L.parity = 2;
-        L.poff = 0;
-        L.mode[0] = L.mode[1] = LM_ACTIVE;
-        *lane = L;
-        *active = 1;
-    }
-}
-
-struct NoAllocDevice {
-    bool ready = false;
-    unsigned char* addr = nullptr;
-};
-std::mutex g_noalloc_mu;
-NoAllocDevice g_noalloc_dev[64];
-
-// Device address of the scratch array on the current device.  The first call
-// on a device looks it up with cudaGetSymbolAddress (this can load the
-// library's device code on that device).
-int noalloc_scratch(unsigned char** out)
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return SFH_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    NoAllocDevice& d = g_noalloc_dev[dev];
-    if (!d.ready) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, sfh_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) return SFH_ERR_CUDA;
-        d.addr = static_cast<unsigned char*>(p);
-        d.ready = true;
-    }
-    *out = d.addr;
-    return SFH_OK;
-}
-
-}  // namespace
-
-extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* links_eo,
-                                    const void* phi_eo, void* x_eo, double tol, int maxit,
-                                    void* cuda_stream, sfh_cg_info* info)
-{
-    if (!dims || !links_eo || !phi_eo || !x_eo || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (!sfh::dims_ok(dims)) return SFH_ERR_INVALID;
-    const long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
-    if (V > kNoAllocMaxSites) return SFH_ERR_INVALID;  // lattice larger than the scratch array
-    unsigned char* base = nullptr;
-    int st = noalloc_scratch(&base);
-    if (st) return st;
-    cudaStream_t stream = (cudaStream_t)cuda_stream;
-    int dev = 0, num_sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return SFH_ERR_CUDA;
-    if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return SFH_ERR_CUDA;
-
-    CgSys S;
-    S.g = make_geom(dims);
-    S.m2 = mass * mass;
-    S.U64 = links_eo;
-    S.Ulo = links_eo;
-    S.lane0 = 0;
-    S.nrhs = 1;
-    S.both = 1;
-    S.tile0 = 0;
-    S.ntq = (S.g.Vh + kTile - 1) / kTile;
-    CgRhs R;
-    R.b = const_cast<void*>(phi_eo);
-    R.xhi = x_eo;
-    R.thi = nullptr;
-    R.r = base + kOffVec;
-    R.p = base + kOffVec + kVecBytes;
-    R.v = base + kOffVec + 2 * kVecBytes;
-    R.t = base + kOffVec + 3 * kVecBytes;
-    R.xlo = x_eo;
-    noalloc_setup<<<1, 256, 0, stream>>>(S, R, base);
-    if (cudaGetLastError() != cudaSuccess) return SFH_ERR_CUDA;
-
-    CgArgs a;
-    a.nsys = 1;
-    a.nlanes = 1;
-    a.ntiles = 2 * S.ntq;
-    a.sys = reinterpret_cast<const CgSys*>(base + kOffSys);
-    a.rhs = reinterpret_cast<const CgRhs*>(base + kOffRhs);
-    a.lanes = reinterpret_cast<CgLane*>(base + kOffLane);
-    a.tile_sys = reinterpret_cast<const int*>(base + kOffTiles);
-    a.partial = reinterpret_cast<double*>(base + kOffPartial);
-    a.n_active = reinterpret_cast<int*>(base + kOffActive);
-    a.tol2 = tol * tol;
-    a.delta = 0.1;
-    a.maxit = maxit;
-    a.mixed = 0;
-    a.maxloop = maxit + 1;
-    CgKernel k = cg_persistent<GP_F64_18, SP_F64, 1>;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 0) != cudaSuccess || per_sm < 1)
-        return SFH_ERR_CUDA;
-    int grid = std::min(per_sm * num_sms, a.ntiles);
-    void* args[] = {&a};
-    if (cudaLaunchCooperativeKernel((const void*)k, dim3(grid), dim3(kTile), args, 0, stream) != cudaSuccess)
-        return SFH_ERR_CUDA;
-    CgLane L;
-    if (cudaMemcpyAsync(&L, a.lanes, sizeof(CgLane), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-        return SFH_ERR_CUDA;
-    if (cudaStreamSynchronize(stream) != cudaSuccess) return SFH_ERR_CUDA;
-    int status = L.status;
-    if (L.mode[0] == LM_ACTIVE || L.mode[0] == LM_RU) status = SFH_ERR_NOCONV;
-    if (info) {
-        std::memset(info, 0, sizeof(*info));
-        info->status = status;
-        info->iters = L.iters;
-        info->iters_parity[0] = info->iters_parity[1] = L.iters;
-        info->rsq_rel = L.bb > 0 ? L.rr / L.bb : 0.0;
-        info->true_resid = -1.0;
-    }
-    return status;
-}
-
-}  // namespace sfh
