@@ -1,4 +1,4 @@
-// cg.cu — batched conjugate-gradient solver for D D^dag x = b (two kernels
+// cg.cu — batched conjugate-gradient solver for D D^dag x = b (three kernels
 // per iteration, replayed as CUDA-graph chunks).
 //
 // Restates solve_CG_DDdagger (Fermions.cpp:553-617) for the GPU.  D D^dag =
@@ -8,21 +8,18 @@
 // A batch holds "lanes": one lane is the CG of one (system, right-hand side,
 // parity block), or of one (system, RHS) over both parities with shared
 // scalars (the reference's full-lattice CG).  Systems may differ in lattice
-// size and mass.  Iteration k of every lane is two grid-wide kernels:
+// size and mass.  Iteration k of every lane is three grid-wide kernels:
 //
-//   hop1   t = K p_k  with  r_k = r_{k-1} - alpha v,  p_k = r_k + beta p_{k-1}
-//          evaluated at the neighbours from the stored r, v, p
-//   hop2   the same update at the lane's own sites (r, p and x += alpha p
-//          stored), v = m^2 p_k - K t, and the four sums <p,v>, <r,v>, |v|^2,
-//          |r_k|^2
+//   hop1    t = K p                                    (other parity)
+//   hop2    v = m^2 p - K t, sums <p,v>, <r,v>, |v|^2, |r|^2
+//   update  x += alpha p, r -= alpha v, p = r + beta p
 //
-// The tile that completes a lane's count of partial sums (atomic ticket) adds
-// them in a fixed order and advances the lane in FP64: alpha = |r_k|^2/<p,Ap>,
-// |r_{k+1}|^2 = |r_k|^2 - 2 alpha <r,v> + alpha^2 |v|^2 (anchored every
-// iteration on the exact |r_k|^2, so the recurrence does not drift),
-// beta = |r_{k+1}|^2/|r_k|^2, and the convergence test of the reference
-// (Fermions.cpp:569).  A lane that converges spends one more hop2 writing
-// x_{k+1} and stops.
+// The tile that completes a lane's count of hop2 partial sums (atomic ticket)
+// adds them in a fixed order and advances the lane in FP64:
+// alpha = |r|^2 / <p, M p>, |r - alpha v|^2 = |r|^2 - 2 alpha <r,v> +
+// alpha^2 |v|^2 (anchored each iteration on the exact |r|^2, so the
+// recurrence does not drift), beta = |r_new|^2 / |r|^2, and the reference's
+// convergence test (Fermions.cpp:569).  One reduction point per iteration.
 //
 // Work is split into tiles of 256 sites of one system and one output parity.
 // A tile processes all lanes of its system that are active in the phase, so a
@@ -31,10 +28,9 @@
 // Mixed precision (FP32 or FP16+scale vectors with FP32 / FP16 12-real links):
 // x is accumulated in FP32 between reliable updates.  When |r| has dropped by
 // delta since the last update, or the recurrence meets the target, the lane
-// spends one iteration on an FP64 reliable update: x_hi += x_lo + alpha p and
-// r = b - M x_hi with FP64 links and vectors; p is kept and the next
-// direction is r + (|r|^2/|r_old|^2) p.  Mixed lanes converge only on that
-// FP64 true residual.
+// spends its next iteration on an FP64 reliable update: x_hi += x_lo and
+// r = b - M x_hi with FP64 links and vectors, keeping p.  Mixed lanes
+// converge only on that FP64 true residual.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -54,15 +50,15 @@ template <int NB>
 struct LanePass {
     int lane[NB], mode[NB], rid[NB];
     double alpha[NB], beta[NB];
-    bool anyA, anyR, anyF;
+    bool anyA, anyR;
 };
 
 template <int NB>
 __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int base, int q, bool hop1,
-                                            int cur, LanePass<NB>& P)
+                                            int cur, bool scalars, LanePass<NB>& P)
 {
     const int cnt = min(NB, S.nrhs - base);
-    P.anyA = P.anyR = P.anyF = false;
+    P.anyA = P.anyR = false;
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
         P.lane[l] = 0;
@@ -75,42 +71,14 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
             const CgLane* L = a.lanes + P.lane[l];
             P.mode[l] = ld_int(&L->mode[cur]);
             P.rid[l] = __ldg(&L->rhs);
-            if (P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU || P.mode[l] == LM_FINAL) {
+            if (scalars && P.mode[l] == LM_ACTIVE) {
                 P.alpha[l] = ld_dbl(&L->alpha);
                 P.beta[l] = ld_dbl(&L->beta);
             }
             P.anyA |= P.mode[l] == LM_ACTIVE;
             P.anyR |= P.mode[l] == LM_RU;
-            P.anyF |= P.mode[l] == LM_FINAL;
         }
     }
-}
-
-// r' = r - alpha v, p' = r' + beta p, both rounded to the storage format;
-// identical arithmetic wherever it is evaluated (own site or neighbour).
-template <int SP>
-__device__ __forceinline__ void advance(const Vec3<typename SpinorFmt<SP>::R>& r,
-                                        const Vec3<typename SpinorFmt<SP>::R>& v,
-                                        const Vec3<typename SpinorFmt<SP>::R>& p,
-                                        typename SpinorFmt<SP>::R alpha, typename SpinorFmt<SP>::R beta,
-                                        Vec3<typename SpinorFmt<SP>::R>& rn, Vec3<typename SpinorFmt<SP>::R>& pn)
-{
-    rn = SpinorFmt<SP>::quantize(vaxpy(r, -alpha, v));
-    pn = SpinorFmt<SP>::quantize(vaxpy(rn, beta, p));
-}
-
-template <int SP>
-__device__ __forceinline__ Vec3<typename SpinorFmt<SP>::R> neighbour_p(const CgArgs& a, int rid, int par, int j,
-                                                                       int Vh, typename SpinorFmt<SP>::R alpha,
-                                                                       typename SpinorFmt<SP>::R beta)
-{
-    typedef typename SpinorFmt<SP>::R RS;
-    Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_R), par, j, Vh);
-    Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), par, j, Vh);
-    Vec3<RS> p = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_P), par, j, Vh);
-    Vec3<RS> rn, pn;
-    advance<SP>(r, v, p, alpha, beta, rn, pn);
-    return pn;
 }
 
 // stage the tile's system descriptor in shared memory (one tile per block)
@@ -157,6 +125,8 @@ __device__ __forceinline__ unsigned arrive_sums(const CgArgs& a, const CgSys& S,
     return *s_mask;
 }
 
+// Stop a lane.  mode_now is what the rest of this iteration sees (LM_LAST if
+// the update kernel must still run), mode_next what later iterations see.
 __device__ __forceinline__ void lane_stop(const CgArgs& a, CgLane* L, int cur, int mode_now, int mode_next,
                                           int status)
 {
@@ -166,14 +136,12 @@ __device__ __forceinline__ void lane_stop(const CgArgs& a, CgLane* L, int cur, i
     atomicSub(a.n_active, 1);
 }
 
-// advance one lane's FP64 scalars from the summed partials (warp 0)
+// Advance one lane's FP64 scalars from the summed partials of hop2 (warp 0).
+// The update of this iteration (x += alpha p, r -= alpha v, p = r + beta p)
+// still runs for an ACTIVE lane; the decision applies from the next one.
 __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
 {
     CgLane* L = a.lanes + lane;
-    if (mode == LM_FINAL) {  // every tile has written x_{k+1}: retire the lane
-        if (threadIdx.x == 0) L->mode[cur] = LM_DONE;
-        return;
-    }
     const int nslot = 2 * S.ntq;
     const double* base = a.partial + L->poff + (S.both ? 0 : L->parity * S.ntq);
     const int n = S.both ? 2 * S.ntq : S.ntq;
@@ -186,7 +154,7 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
         const double rr = s[3], pAp = s[0];
         const double alpha = rr / pAp;  // Fermions.cpp:573-586
         if (!isfinite(pAp) || fabs(pAp) < 1e-30 || !isfinite(alpha)) {
-            lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);
+            lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);  // no update
             return;
         }
         const double rr_next = rr - 2.0 * alpha * s[1] + alpha * alpha * s[2];
@@ -202,10 +170,10 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
         L->rr_next = rr_next;
         L->iters += 1;
         if (!a.mixed) {
-            if (rr_next < L->target)  // Fermions.cpp:569: write x_{k+1} and stop
-                lane_stop(a, L, cur, LM_DONE, LM_FINAL, SFH_OK);
+            if (rr_next < L->target)  // Fermions.cpp:569: this iteration's update, then stop
+                lane_stop(a, L, cur, LM_LAST, LM_DONE, SFH_OK);
             else if (L->iters >= a.maxit)  // Fermions.cpp:609-614
-                lane_stop(a, L, cur, LM_DONE, LM_FINAL, SFH_ERR_NOCONV);
+                lane_stop(a, L, cur, LM_LAST, LM_DONE, SFH_ERR_NOCONV);
             else
                 L->mode[nxt] = LM_ACTIVE;
         } else {
@@ -220,18 +188,14 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
     } else {  // reliable update: s[3] = |b - M x|^2 in FP64
         const double rt = s[3];
         L->nru += 1;
+        L->rr_next = rt;
         if (rt < L->target) {
-            L->rr_next = rt;
             lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_OK);
         } else if (!isfinite(rt)) {
             lane_stop(a, L, cur, LM_FAILED, LM_FAILED, SFH_ERR_BREAKDOWN);
         } else if (L->iters >= a.maxit) {
-            L->rr_next = rt;
             lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_ERR_NOCONV);
         } else {
-            L->beta = rt / L->rr;  // keep the direction: p <- r_true + beta p
-            L->alpha = 0.0;
-            L->rr_next = rt;
             L->rmax = sqrt(rt);
             L->mode[nxt] = LM_ACTIVE;
         }
@@ -267,7 +231,7 @@ __device__ __noinline__ void finish_init_lane(const CgArgs& a, const CgSys& S, i
 // kernels
 // ---------------------------------------------------------------------------
 
-// x = 0, r = b, p = v = 0, |b|^2
+// x = 0, r = p = b (solver precision), |b|^2
 template <int SP, int NB>
 __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
 {
@@ -302,9 +266,9 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
             SpinorFmt<SP_F64>::store(rhs_ptr(a, P.rid[l], F_XHI), ti.q, ti.i, Vh, z);
             if (a.mixed)
                 SpinorFmt<XP>::store(rhs_ptr(a, P.rid[l], F_XLO), ti.q, ti.i, Vh, vcvt<typename SpinorFmt<XP>::R>(z));
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_R), ti.q, ti.i, Vh, vcvt<RS>(b));
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), ti.q, ti.i, Vh, vcvt<RS>(z));
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), ti.q, ti.i, Vh, vcvt<RS>(z));
+            Vec3<RS> bq = SpinorFmt<SP>::quantize(vcvt<RS>(b));
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_R), ti.q, ti.i, Vh, bq);
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), ti.q, ti.i, Vh, bq);
             sums[l * kSums + 3] = vdot_re(b, b);
         }
         block_sum<NB * kSums>(sums, smem);
@@ -318,15 +282,13 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
     }
 }
 
-// FP64 hop of (x_hi + x_lo + alpha p) for a lane in a reliable update
-template <int SP, int XP>
-__device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid,
-                                     double alpha)
+// FP64 hop of x_hi + x_lo for a lane in a reliable update: thi = K x
+template <int XP>
+__device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     const int nq = 1 - q, Vh = S.g.Vh;
     const void* xhi = rhs_ptr(a, rid, F_XHI);
     const void* xlo = rhs_ptr(a, rid, F_XLO);
-    const void* pp = rhs_ptr(a, rid, F_P);
     Vec3<double> acc;
     vzero(acc);
 #pragma unroll 1
@@ -339,14 +301,12 @@ __device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coor
             Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
             Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, lu, Vh), 1.0,
                                    vcvt<double>(SpinorFmt<XP>::load(xlo, nq, lu, Vh)));
-            x = vaxpy(x, alpha, vcvt<double>(SpinorFmt<SP>::load(pp, nq, lu, Vh)));
             vacc(acc, mul_mv(U, x), eta_neg != wu);
         }
         {
             Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
             Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, ld, Vh), 1.0,
                                    vcvt<double>(SpinorFmt<XP>::load(xlo, nq, ld, Vh)));
-            x = vaxpy(x, alpha, vcvt<double>(SpinorFmt<SP>::load(pp, nq, ld, Vh)));
             vacc(acc, mul_adj_mv(U, x), !(eta_neg != wd));
         }
     }
@@ -355,7 +315,7 @@ __device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coor
     SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
 }
 
-// t = K p_k for active lanes (output parity q); thi for reliable updates
+// t = K p for active lanes (output parity q); thi for reliable updates
 template <int GP, int SP, int NB>
 __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
 {
@@ -371,8 +331,11 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
     const Coord c = eo_coords(S.g, q, ti.i);
     for (int base = 0; base < S.nrhs; base += NB) {
         LanePass<NB> P;
-        gather_pass<NB>(a, S, base, q, true, cur, P);
+        gather_pass<NB>(a, S, base, q, true, cur, false, P);
         if (P.anyA) {
+            const void* pin[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) pin[l] = rhs_ptr(a, P.rid[l], F_P);
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
@@ -387,8 +350,8 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
                         if (P.mode[l] != LM_ACTIVE) continue;
-                        Vec3<R> pn = vcvt<R>(neighbour_p<SP>(a, P.rid[l], nq, lu, Vh, (RS)P.alpha[l], (RS)P.beta[l]));
-                        vacc(acc[l], mul_mv(U, pn), eta_neg != wu);
+                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, lu, Vh));
+                        vacc(acc[l], mul_mv(U, w), eta_neg != wu);
                     }
                 }
                 {
@@ -396,8 +359,8 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
                         if (P.mode[l] != LM_ACTIVE) continue;
-                        Vec3<R> pn = vcvt<R>(neighbour_p<SP>(a, P.rid[l], nq, ld, Vh, (RS)P.alpha[l], (RS)P.beta[l]));
-                        vacc(acc[l], mul_adj_mv(U, pn), !(eta_neg != wd));
+                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, ld, Vh));
+                        vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
                     }
                 }
             }
@@ -413,15 +376,15 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
         if (P.anyR) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) ru_hop1<SP, XP>(a, S, c, q, ti.i, P.rid[l], P.alpha[l]);
+                if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
         }
     }
 }
 
-// reliable update at the lane's own site: returns |b - M x|^2 contribution
+// reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
+// r = b - M x_hi; returns the |r|^2 contribution (FP64)
 template <int SP, int XP>
-__device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid,
-                                       double alpha)
+__device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     typedef typename SpinorFmt<SP>::R RS;
     const int nq = 1 - q, Vh = S.g.Vh;
@@ -443,7 +406,6 @@ __device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Co
     void* xlo = rhs_ptr(a, rid, F_XLO);
     Vec3<double> xn = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, q, i, Vh), 1.0,
                             vcvt<double>(SpinorFmt<XP>::load_cg(xlo, q, i, Vh)));
-    xn = vaxpy(xn, alpha, vcvt<double>(SpinorFmt<SP>::load_cg(rhs_ptr(a, rid, F_P), q, i, Vh)));
     SpinorFmt<SP_F64>::store(xhi, q, i, Vh, xn);
     Vec3<typename SpinorFmt<XP>::R> z;
     vzero(z);
@@ -459,14 +421,13 @@ __device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Co
     return vdot_re(res, res);
 }
 
-// own sites: r, p, x advanced and stored; v = m^2 p - K t; the four sums
+// own sites: v = m^2 p - K t and the four sums; reliable-update residuals
 template <int GP, int SP, int NB>
 __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
-    typedef typename SpinorFmt<XP>::R RX;
     __shared__ CgSys s_sys;
     __shared__ double smem[32 * NB * kSums];
     __shared__ unsigned s_mask;
@@ -478,84 +439,72 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
     if (ti.valid) c = eo_coords(S.g, q, ti.i);
     for (int base = 0; base < S.nrhs; base += NB) {
         LanePass<NB> P;
-        gather_pass<NB>(a, S, base, q, false, cur, P);
-        if (!(P.anyA || P.anyR || P.anyF)) continue;  // uniform across the block
+        gather_pass<NB>(a, S, base, q, false, cur, false, P);
+        if (!(P.anyA || P.anyR)) continue;  // uniform across the block
         bool part[NB];
         double sums[NB * kSums];
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
-            // FINAL lanes take the ticket too: the last tile retires them
-            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU || P.mode[l] == LM_FINAL;
+            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU;
 #pragma unroll
             for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
         }
-        if (ti.valid && (P.anyA || P.anyF)) {
+        if (ti.valid && P.anyA) {
+            const void* tin[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) tin[l] = rhs_ptr(a, P.rid[l], F_T);
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
-            if (P.anyA) {
 #pragma unroll 1
-                for (int mu = 0; mu < 4; ++mu) {
-                    const bool eta_neg = eta_sign(c, mu) < 0;
-                    const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-                    const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-                    const bool wd = (mu == 3) && (c.x[3] == 0);
-                    {
-                        Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
+            for (int mu = 0; mu < 4; ++mu) {
+                const bool eta_neg = eta_sign(c, mu) < 0;
+                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
+                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
+                const bool wd = (mu == 3) && (c.x[3] == 0);
+                {
+                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
 #pragma unroll
-                        for (int l = 0; l < NB; ++l) {
-                            if (P.mode[l] != LM_ACTIVE) continue;
-                            Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_T), nq, lu, Vh));
-                            vacc(acc[l], mul_mv(U, w), eta_neg != wu);
-                        }
+                    for (int l = 0; l < NB; ++l) {
+                        if (P.mode[l] != LM_ACTIVE) continue;
+                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, lu, Vh));
+                        vacc(acc[l], mul_mv(U, w), eta_neg != wu);
                     }
-                    {
-                        Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
+                }
+                {
+                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
 #pragma unroll
-                        for (int l = 0; l < NB; ++l) {
-                            if (P.mode[l] != LM_ACTIVE) continue;
-                            Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_T), nq, ld, Vh));
-                            vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
-                        }
+                    for (int l = 0; l < NB; ++l) {
+                        if (P.mode[l] != LM_ACTIVE) continue;
+                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, ld, Vh));
+                        vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
                     }
                 }
             }
             const R m2 = (R)S.m2;
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
-                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_FINAL) continue;
-                void* rp = rhs_ptr(a, P.rid[l], F_R);
-                void* vp = rhs_ptr(a, P.rid[l], F_V);
-                void* pp = rhs_ptr(a, P.rid[l], F_P);
-                void* xp = rhs_ptr(a, P.rid[l], F_XLO);
-                Vec3<RS> p = SpinorFmt<SP>::load_cg(pp, q, ti.i, Vh);
-                Vec3<RX> x = SpinorFmt<XP>::load_cg(xp, q, ti.i, Vh);
-                SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)P.alpha[l], vcvt<RX>(p)));
-                if (P.mode[l] == LM_FINAL) continue;
-                Vec3<RS> r = SpinorFmt<SP>::load_cg(rp, q, ti.i, Vh);
-                Vec3<RS> v = SpinorFmt<SP>::load_cg(vp, q, ti.i, Vh);
-                Vec3<RS> rn, pn;
-                advance<SP>(r, v, p, (RS)P.alpha[l], (RS)P.beta[l], rn, pn);
-                SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
-                SpinorFmt<SP>::store(pp, q, ti.i, Vh, pn);
-                Vec3<R> pr = vcvt<R>(pn), w;
+                if (P.mode[l] != LM_ACTIVE) continue;
+                Vec3<RS> p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+                Vec3<R> pr = vcvt<R>(p), w;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
                     w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
                 }
                 Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
-                SpinorFmt<SP>::store(vp, q, ti.i, Vh, vn);
-                sums[l * kSums + 0] = vdot_re(pn, vn);
-                sums[l * kSums + 1] = vdot_re(rn, vn);
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+                sums[l * kSums + 0] = vdot_re(p, vn);
+                sums[l * kSums + 1] = vdot_re(r, vn);
                 sums[l * kSums + 2] = vdot_re(vn, vn);
-                sums[l * kSums + 3] = vdot_re(rn, rn);
+                sums[l * kSums + 3] = vdot_re(r, r);
             }
         }
         if (ti.valid && P.anyR) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l], P.alpha[l]);
+                if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
         }
         block_sum<NB * kSums>(sums, smem);
         unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
@@ -565,6 +514,46 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
                 if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
         }
         __syncthreads();
+    }
+}
+
+// own sites of ACTIVE lanes: x += alpha p, r -= alpha v, p = r + beta p
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_update(CgArgs a, int cur)
+{
+    typedef typename SpinorFmt<SP>::R RS;
+    constexpr int XP = XFmt<SP>::v;
+    typedef typename SpinorFmt<XP>::R RX;
+    __shared__ CgSys s_sys;
+    stage_sys(a, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, blockIdx.x);
+    if (!ti.valid) return;
+    const int q = ti.q, Vh = S.g.Vh;
+    for (int rhs = 0; rhs < S.nrhs; ++rhs) {
+        CgLane* L = a.lanes + lane_of(S, rhs, q, false);
+        const int mode = ld_int(&L->mode[cur]);
+        if (mode != LM_ACTIVE && mode != LM_LAST) continue;
+        if (mode == LM_LAST && threadIdx.x == 0) {  // the last tile retires the lane
+            const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
+            if (atomicAdd(&L->ticket, 1u) == expected - 1) {
+                L->ticket = 0;
+                L->mode[cur] = LM_DONE;
+            }
+        }
+        const double alpha = ld_dbl(&L->alpha), beta = ld_dbl(&L->beta);
+        const int rid = __ldg(&L->rhs);
+        void* pp = rhs_ptr(a, rid, F_P);
+        void* rp = rhs_ptr(a, rid, F_R);
+        void* xp = rhs_ptr(a, rid, F_XLO);
+        Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
+        Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
+        Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), q, ti.i, Vh);
+        Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
+        SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
+        Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
+        SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
+        SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
     }
 }
 
@@ -579,7 +568,7 @@ typedef void (*HopKernel)(CgArgs, int);
 
 struct CgKernels {
     InitKernel init;
-    HopKernel hop1, hop2;
+    HopKernel hop1, hop2, update;
 };
 
 template <int GP, int SP>
@@ -610,12 +599,15 @@ static CgKernels pick_kernels(int prec, int nb1, int nb2)
     if (prec == SFH_PREC_F64) {
         k.hop1 = pick_hop1<GP_F64_18, SP_F64>(nb1);
         pick_hop2<GP_F64_18, SP_F64>(nb2, &k.hop2, &k.init);
+        k.update = cg_update<SP_F64>;
     } else if (prec == SFH_PREC_F32) {
         k.hop1 = pick_hop1<GP_F32_12, SP_F32>(nb1);
         pick_hop2<GP_F32_12, SP_F32>(nb2, &k.hop2, &k.init);
+        k.update = cg_update<SP_F32>;
     } else {
         k.hop1 = pick_hop1<GP_F16_12, SP_F16>(nb1);
         pick_hop2<GP_F16_12, SP_F16>(nb2, &k.hop2, &k.init);
+        k.update = cg_update<SP_F16>;
     }
     return k;
 }
@@ -798,15 +790,16 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.delta = delta;
     a.maxit = maxit;
     a.mixed = w.prec != SFH_PREC_F64;
-    a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 2;
+    a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
     return a;
 }
 
-// (Re)build the graph of kChunk iterations: hop1, hop2, hop1, hop2, ...
+// (Re)build the graph of kChunk iterations: hop1, hop2, update, hop1, ...
 static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, double tol, int maxit,
                                 double delta)
 {
-    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.g_tol == tol && w.g_maxit == maxit &&
+    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.g_tol == tol &&
+        w.g_maxit == maxit &&
         w.g_delta == delta)
         return cudaSuccess;
     w.release_graph();
@@ -815,10 +808,10 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     cudaGraphNode_t prev = nullptr;
     for (int it = 0; it < kChunk; ++it) {
         int cur = it & 1;
-        for (int ph = 0; ph < 2; ++ph) {
+        for (int ph = 0; ph < 3; ++ph) {
             cudaKernelNodeParams p;
             std::memset(&p, 0, sizeof(p));
-            p.func = (void*)(ph == 0 ? k.hop1 : k.hop2);
+            p.func = (void*)(ph == 0 ? k.hop1 : (ph == 1 ? k.hop2 : k.update));
             p.gridDim = dim3(w.ntiles);
             p.blockDim = dim3(kTile);
             void* args[] = {&a, &cur};
@@ -878,7 +871,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         if ((e = cudaEventRecord(w.ev[c & 1], stream)) != cudaSuccess) return e;
         if (c >= 1) {
             if ((e = cudaEventSynchronize(w.ev[(c - 1) & 1])) != cudaSuccess) return e;
-            if (w.h_active[(c - 1) & 1] == 0) break;
+            if (w.h_active[(c - 1) & 1] <= 0) break;
         }
     }
     e = cudaMemcpyAsync(w.lanes_h.data(), w.d_lanes, sizeof(CgLane) * w.nlanes, cudaMemcpyDeviceToHost, stream);
@@ -886,7 +879,6 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
     // a lane that stopped holds DONE or FAILED in one of its two mode slots
-    // (the other may still hold FINAL after its last x update)
     for (CgLane& L : w.lanes_h) {
         bool stopped = false;
         for (int k = 0; k < 2; ++k) stopped |= L.mode[k] == LM_DONE || L.mode[k] == LM_FAILED;

@@ -9,7 +9,9 @@
 
 namespace sfh {
 
-enum { LM_ACTIVE = 0, LM_RU = 1, LM_DONE = 2, LM_FAILED = 3, LM_FINAL = 4 };
+// lane modes; LM_LAST: the update kernel of this iteration still runs for the
+// lane, then retires it (DONE)
+enum { LM_ACTIVE = 0, LM_RU = 1, LM_DONE = 2, LM_FAILED = 3, LM_LAST = 4 };
 constexpr int kTile = 256;
 
 struct CgSys {
