@@ -109,6 +109,67 @@ int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
 int sfh_cg_solve(sfh_ctx* ctx, const double* phi, double* X, double tol, int maxit,
                  int precision, sfh_cg_info* info);
 
+/* ---- forces, link update, observables (context's device fields) --------- */
+/* Per-link staple sums A1 (plaquette) and A2 (rectangle):
+ * compute_staple_sum_at_link / compute_rectangle_staple_sum_at_link
+ * (Lattice.cpp:249-499).  A1, A2: link-field layout. */
+int sfh_staples(sfh_ctx* ctx, double* A1, double* A2);
+/* Symanzik gauge force on every link: compute_gauge_force_at_link
+ * (Fermions.cpp:372-384), as compute_gauge_only_force_field (Fermions.cpp:1278). */
+int sfh_gauge_force(sfh_ctx* ctx, double* F);
+/* Fermion force: compute_fermion_force_at_link (Fermions.cpp:443-515) on every
+ * link, as compute_fermion_only_force_field (Fermions.cpp:1114-1134). */
+int sfh_fermion_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
+/* Gauge + fermion force: compute_full_force_field (Fermions.cpp:640-659). */
+int sfh_full_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
+/* U <- exp(i eps P) U with the context's momenta (Fermions.cpp:699-723 with
+ * check = 1, which rejects a non-Hermitian P as the reference does;
+ * Fermions.cpp:984-994 with check = 0). */
+int sfh_link_update(sfh_ctx* ctx, double eps, int check);
+/* sum over links of Re Tr P^2: compute_Tr_P2 (Fermions.cpp:662-678) */
+int sfh_trp2(sfh_ctx* ctx, double* out);
+/* Symanzik gauge action: compute_action (Lattice.cpp:759-781) */
+int sfh_gauge_action(sfh_ctx* ctx, double* out);
+/* average plaquette in the reference's normalisation (6.0 on a cold field):
+ * compute_avg_plaq (Lattice.cpp:784-804) */
+int sfh_plaquette(sfh_ctx* ctx, double* out);
+int sfh_set_beta(sfh_ctx* ctx, double beta);
+
+/* ---- molecular dynamics ---------------------------------------------------- */
+typedef struct {
+    int status;
+    int accepted;          /* Metropolis outcome                                   */
+    int solves;            /* CG solves in the trajectory                          */
+    int pad;
+    long cg_iters;         /* summed CG iterations                                 */
+    double dH;             /* H_final - H_initial                                  */
+    double H_initial[3];   /* Tr P^2, S_gauge, phi.X                               */
+    double H_final[3];
+    double uniform;        /* the Metropolis uniform                               */
+    double plaquette;      /* after the accept / reject                            */
+    double seconds;
+} sfh_traj_info;
+
+/* One leapfrog trajectory on the context's gauge field and momenta with
+ * explicit step size and count: local_initial_half_step, local_leapfrog_steps,
+ * local_final_step (Fermions.cpp:967-1028).  X_out (may be NULL) receives the
+ * last solve; cg_iters (may be NULL) the summed CG iterations. */
+int sfh_leapfrog(sfh_ctx* ctx, const double* phi, double eps, int nsteps, double tol, int maxit,
+                 int precision, double* X_out, long* cg_iters);
+/* A full HMC update: single_sweep_monte_carlo_update_WITH_FERMIONS
+ * (Fermions.cpp:812-828) with seeded phi = D chi, momenta and Metropolis
+ * uniform (Monte_carlo_step, Fermions.cpp:778-810). */
+int sfh_hmc_trajectory(sfh_ctx* ctx, double eps, int nsteps, unsigned long long seed, double tol, int maxit,
+                       int precision, sfh_traj_info* info);
+
+/* ---- smearing ------------------------------------------------------------- */
+/* nlevels stout levels U <- exp(rho proj(C U^dag)) U with plaquette staples
+ * (the single-level analogue of the HEX steps of Smearing.cpp:132-155). */
+int sfh_smear_stout(sfh_ctx* ctx, double rho, int nlevels);
+/* npasses HEX passes: Apply_HEX_smearing (Smearing.cpp:304-311); npasses = 4
+ * is Apply_4HEX_smearing (Smearing.cpp:313-318).  Alphas as Smearing.h:7-9. */
+int sfh_smear_hex(sfh_ctx* ctx, double alpha1, double alpha2, double alpha3, int npasses);
+
 /* ---- batched solver (many lattices, masses and right-hand sides) --------- */
 typedef struct {
     int dims[4];

@@ -65,6 +65,19 @@ class CgInfo(ctypes.Structure):
                 "true_resid": self.true_resid}
 
 
+class TrajInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("accepted", ctypes.c_int), ("solves", ctypes.c_int),
+                ("pad", ctypes.c_int), ("cg_iters", ctypes.c_long), ("dH", ctypes.c_double),
+                ("H_initial", ctypes.c_double * 3), ("H_final", ctypes.c_double * 3),
+                ("uniform", ctypes.c_double), ("plaquette", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"status": self.status, "accepted": bool(self.accepted), "solves": self.solves,
+                "cg_iters": self.cg_iters, "dH": self.dH, "H_initial": list(self.H_initial),
+                "H_final": list(self.H_final), "uniform": self.uniform, "plaquette": self.plaquette,
+                "seconds": self.seconds}
+
+
 class SystemDesc(ctypes.Structure):
     _fields_ = [("dims", ctypes.c_int * 4), ("mass", ctypes.c_double), ("nrhs", ctypes.c_int)]
 
@@ -94,6 +107,22 @@ SIGNATURES = {
     "sfh_ddag": (ctypes.c_int, [_VP, _D, _D]),
     "sfh_cg_solve": (ctypes.c_int, [_VP, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(CgInfo)]),
+    "sfh_staples": (ctypes.c_int, [_VP, _D, _D]),
+    "sfh_gauge_force": (ctypes.c_int, [_VP, _D]),
+    "sfh_fermion_force": (ctypes.c_int, [_VP, _D, _D, _D]),
+    "sfh_full_force": (ctypes.c_int, [_VP, _D, _D, _D]),
+    "sfh_link_update": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_trp2": (ctypes.c_int, [_VP, _D]),
+    "sfh_gauge_action": (ctypes.c_int, [_VP, _D]),
+    "sfh_plaquette": (ctypes.c_int, [_VP, _D]),
+    "sfh_set_beta": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "sfh_leapfrog": (ctypes.c_int, [_VP, _D, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_int, _D, ctypes.POINTER(ctypes.c_long)]),
+    "sfh_hmc_trajectory": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(TrajInfo)]),
+    "sfh_smear_stout": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_smear_hex": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -262,6 +291,80 @@ class Lattice:
 
     def solve_Y_field(self, X):
         return self.apply_dirac_dagger(X)
+
+    # --- forces, link update, observables (Fermions.cpp:372-828, Lattice.cpp:249-804)
+    def _link_field(self):
+        return np.empty(72 * self.V)
+
+    def staples(self):
+        A1, A2 = self._link_field(), self._link_field()
+        self._check(self.lib.sfh_staples(self.h, _dptr(A1), _dptr(A2)), "staples")
+        return A1, A2
+
+    def compute_gauge_only_force_field(self):
+        F = self._link_field()
+        self._check(self.lib.sfh_gauge_force(self.h, _dptr(F)), "gauge force")
+        return F
+
+    def compute_fermion_only_force_field(self, X, Y):
+        X, Y, F = _f64(X).reshape(-1), _f64(Y).reshape(-1), self._link_field()
+        self._check(self.lib.sfh_fermion_force(self.h, _dptr(X), _dptr(Y), _dptr(F)), "fermion force")
+        return F
+
+    def compute_full_force_field(self, X, Y):
+        X, Y, F = _f64(X).reshape(-1), _f64(Y).reshape(-1), self._link_field()
+        self._check(self.lib.sfh_full_force(self.h, _dptr(X), _dptr(Y), _dptr(F)), "full force")
+        return F
+
+    def link_update(self, eps, check=False):
+        self._check(self.lib.sfh_link_update(self.h, eps, 1 if check else 0), "link update")
+
+    def _scalar(self, fn, what):
+        out = ctypes.c_double(0.0)
+        self._check(fn(self.h, ctypes.byref(out)), what)
+        return out.value
+
+    def compute_Tr_P2(self):
+        return self._scalar(self.lib.sfh_trp2, "Tr P^2")
+
+    def compute_action(self):
+        return self._scalar(self.lib.sfh_gauge_action, "gauge action")
+
+    def compute_avg_plaq(self):
+        return self._scalar(self.lib.sfh_plaquette, "plaquette")
+
+    def set_beta(self, beta):
+        self._check(self.lib.sfh_set_beta(self.h, beta), "set_beta")
+        self.beta = beta
+
+    def leapfrog(self, phi, eps, n_steps, tol=1e-12, max_iter=50000, precision="f64"):
+        """local_initial_half_step + local_leapfrog_steps + local_final_step
+        (Fermions.cpp:967-1028) on the device gauge field and momenta."""
+        phi = _f64(phi).reshape(-1)
+        X = np.empty_like(phi)
+        its = ctypes.c_long(0)
+        st = self.lib.sfh_leapfrog(self.h, _dptr(phi), eps, n_steps, tol, max_iter, PRECISIONS[precision],
+                                   _dptr(X), ctypes.byref(its))
+        self._check(st, "leapfrog")
+        return X, its.value
+
+    def hmc_trajectory(self, eps, n_steps, seed, tol=1e-10, max_iter=50000, precision="f64"):
+        """single_sweep_monte_carlo_update_WITH_FERMIONS (Fermions.cpp:812-828)."""
+        inf = TrajInfo()
+        st = self.lib.sfh_hmc_trajectory(self.h, eps, n_steps, seed, tol, max_iter, PRECISIONS[precision],
+                                         ctypes.byref(inf))
+        self._check(st, "hmc trajectory")
+        return inf.as_dict()
+
+    # --- smearing (Smearing.cpp) ---------------------------------------------
+    def smear_stout(self, rho, n_levels=1):
+        self._check(self.lib.sfh_smear_stout(self.h, rho, n_levels), "stout smearing")
+
+    def Apply_HEX_smearing(self, alphas=(0.95, 0.76, 0.38), passes=1):
+        self._check(self.lib.sfh_smear_hex(self.h, alphas[0], alphas[1], alphas[2], passes), "HEX smearing")
+
+    def Apply_4HEX_smearing(self, alphas=(0.95, 0.76, 0.38)):
+        self.Apply_HEX_smearing(alphas, passes=4)
 
 
 class Batch:

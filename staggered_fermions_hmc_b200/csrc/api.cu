@@ -113,7 +113,9 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     if (!c) return SFH_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* ptrs[] = {c->U64, c->U32, c->U16, c->Pmom, c->Fbuf, c->stage, c->red, c->derr};
+    for (int k = 0; k < 3; ++k)
+        if (c->ws[k]) workspace_free(c->ws[k]);
+    void* ptrs[] = {c->U64, c->U32, c->U16, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial, c->smear};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : c->spin)

@@ -1139,21 +1139,18 @@ extern "C" int sfh_batch_true_residual(sfh_batch* b, int k, int j, double* rel)
 }
 
 // ===========================================================================
-// single-context solve: a batch of one over the context's own gauge field
+// device-resident single-context solve with a cached workspace (used by the
+// trajectory), and the host-pointer solve built on it
 // ===========================================================================
 namespace sfh {
-int ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
-                 sfh_cg_info* info);
-}
 
-int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
-                      sfh_cg_info* info)
+void workspace_free(CgWorkspace* w) { delete w; }
+
+static CgWorkspace* ctx_workspace(sfh_ctx* c, int prec, cudaError_t* err)
 {
-    if (prec != SFH_PREC_F64 && !c->lowp_valid) {
-        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream);
-        c->lowp_valid = true;
-    }
-    CgWorkspace w;
+    *err = cudaSuccess;
+    if (c->ws[prec]) return c->ws[prec];
+    CgWorkspace* w = new CgWorkspace();
     SolverSystemHost h;
     h.g = c->g;
     h.mass = c->mass;
@@ -1161,23 +1158,42 @@ int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int 
     h.U64 = c->U64;
     h.Ulo = prec == SFH_PREC_F32 ? c->U32 : (prec == SFH_PREC_F16 ? c->U16 : c->U64);
     std::vector<SolverSystemHost> hs(1, h);
-    cudaError_t e = workspace_build(w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
-    if (e != cudaSuccess) return cuda_check(c, e, "cg workspace");
+    *err = workspace_build(*w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
+    if (*err != cudaSuccess) {
+        delete w;
+        return nullptr;
+    }
+    c->ws[prec] = w;
+    c->ws_mass[prec] = c->mass;
+    return w;
+}
+
+int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int maxit, int prec,
+                     sfh_cg_info* info)
+{
+    if (prec != SFH_PREC_F64 && !c->lowp_valid) {
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream);
+        c->lowp_valid = true;
+    }
+    if (c->ws[prec] && c->ws_mass[prec] != c->mass) {  // mass is baked into the system table
+        workspace_free(c->ws[prec]);
+        c->ws[prec] = nullptr;
+    }
+    cudaError_t e;
+    CgWorkspace* w = ctx_workspace(c, prec, &e);
+    if (!w) return cuda_check(c, e, "cg workspace");
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
-    e = cudaMemcpyAsync(c->stage, phi, fs, cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return cuda_check(c, e, "cg upload");
-    launch_spinor_aos_to_eo(c->g, (const double*)c->stage, w.rhs[0].b, c->stream);
-    e = workspace_solve(w, tol, maxit, 0.1, 0, 0, c->stream);
+    e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");
+    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
-    launch_spinor_eo_to_aos(c->g, w.rhs[0].xhi, (double*)c->stage, c->stream);
-    e = cudaMemcpyAsync(X, c->stage, fs, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return cuda_check(c, e, "cg download");
+    e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cg solution");
     int status = SFH_OK;
     sfh_cg_info inf;
     std::memset(&inf, 0, sizeof(inf));
     double rr = 0, bb = 0;
-    for (const CgLane& L : w.lanes_h) {
+    for (const CgLane& L : w->lanes_h) {
         if (L.status != SFH_OK && status == SFH_OK) status = L.status;
         inf.iters = std::max(inf.iters, L.iters);
         if (L.parity < 2) inf.iters_parity[L.parity] = L.iters;
@@ -1191,9 +1207,34 @@ int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int 
     inf.true_resid = -1.0;
     if (info) *info = inf;
     if (status != SFH_OK)
-        return set_error(c, status, status == SFH_ERR_NOCONV ? "CG Solver failed to converge"
-                                                             : "CG breakdown");
+        return set_error(c, status, status == SFH_ERR_NOCONV ? "CG Solver failed to converge" : "CG breakdown");
     return SFH_OK;
+}
+
+}  // namespace sfh
+
+// ===========================================================================
+// single-context solve: a batch of one over the context's own gauge field
+// ===========================================================================
+namespace sfh {
+int ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
+                 sfh_cg_info* info);
+}
+
+int sfh::ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
+                      sfh_cg_info* info)
+{
+    size_t fs = (size_t)c->g.V * 6 * sizeof(double);
+    cudaError_t e = cudaMemcpyAsync(c->stage, phi, fs, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cg upload");
+    launch_spinor_aos_to_eo(c->g, (const double*)c->stage, c->spin[3], c->stream);
+    int st = ctx_solve_device(c, c->spin[3], c->spin[4], tol, maxit, prec, info);
+    if (st != SFH_OK && st != SFH_ERR_NOCONV && st != SFH_ERR_BREAKDOWN) return st;
+    launch_spinor_eo_to_aos(c->g, c->spin[4], (double*)c->stage, c->stream);
+    e = cudaMemcpyAsync(X, c->stage, fs, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cg download");
+    return st;
 }
 
 extern "C" int sfh_batch_random_gauge(sfh_batch* b, int k, double eps, unsigned long long seed)

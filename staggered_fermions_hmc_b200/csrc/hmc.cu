@@ -1,0 +1,336 @@
+// hmc.cu — C ABI for forces, the link update, observables and the leapfrog /
+// HMC trajectory, all on the context's device-resident fields.
+//
+// The trajectory follows single_sweep_monte_carlo_update_WITH_FERMIONS
+// (Fermions.cpp:812-828): S_g, phi = D chi, P, Tr P^2, X0 = (D D^dag)^-1 phi,
+// phi.X0, leapfrog (half kick, N-1 x (link update, kick), link update, half
+// kick; Fermions.cpp:684-776 / 967-1028), then H_final and the Metropolis
+// test of Monte_carlo_step (Fermions.cpp:778-810).  Every force evaluation is
+// one CG solve, Y = D^dag X and one fused kernel P -= k (F_gauge + F_fermion).
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "sfh_internal.h"
+
+namespace sfh {
+int set_error(sfh_ctx* c, int code, const std::string& msg);
+int cuda_check(sfh_ctx* c, cudaError_t e, const char* what);
+}  // namespace sfh
+
+using namespace sfh;
+
+namespace {
+
+size_t spinor_bytes(const sfh_ctx* c) { return (size_t)c->g.V * 6 * sizeof(double); }
+size_t link_bytes(const sfh_ctx* c) { return (size_t)c->g.V * 72 * sizeof(double); }
+
+int take_device_error(sfh_ctx* c, const char* what)
+{
+    int h = 0;
+    int st = cuda_check(c, cudaMemcpyAsync(&h, c->derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream), what);
+    if (!st) st = cuda_check(c, cudaMemsetAsync(c->derr, 0, sizeof(int), c->stream), what);
+    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), what);
+    if (st) return st;
+    if (h & DEV_ERR_NOT_HERMITIAN)  // Fermions.cpp:714-716
+        return set_error(c, SFH_ERR_NOT_HERMITIAN, std::string(what) + ": P_pre is not Hermitian or not traceless");
+    if (h & DEV_ERR_DOMAIN)  // Fermions.cpp:848-857
+        return set_error(c, SFH_ERR_DOMAIN, std::string(what) + ": exp(iQ) argument outside its domain");
+    return SFH_OK;
+}
+
+int spinor_in(sfh_ctx* c, const double* host, void* eo)
+{
+    int st = cuda_check(c, cudaMemcpyAsync(c->stage, host, spinor_bytes(c), cudaMemcpyHostToDevice, c->stream),
+                        "spinor upload");
+    if (st) return st;
+    launch_spinor_aos_to_eo(c->g, (const double*)c->stage, eo, c->stream);
+    return SFH_OK;
+}
+
+int spinor_out(sfh_ctx* c, const void* eo, double* host)
+{
+    launch_spinor_eo_to_aos(c->g, eo, (double*)c->stage, c->stream);
+    int st = cuda_check(c, cudaMemcpyAsync(host, c->stage, spinor_bytes(c), cudaMemcpyDeviceToHost, c->stream),
+                        "spinor download");
+    if (st) return st;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "spinor download");
+}
+
+int links_out(sfh_ctx* c, const void* eo, double* host)
+{
+    launch_links_eo_to_aos(c->g, eo, (double*)c->stage, c->stream);
+    int st = cuda_check(c, cudaMemcpyAsync(host, c->stage, link_bytes(c), cudaMemcpyDeviceToHost, c->stream),
+                        "link field download");
+    if (st) return st;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "link field download");
+}
+
+int reduce(sfh_ctx* c, int kind, const void* A, const void* B, double* out)
+{
+    int st = cuda_check(c, launch_reduce(c->g, kind, A, B, c->beta, c->c11, c->c12, c->red, c->red + 2048,
+                                         c->stream), "reduction");
+    if (st) return st;
+    st = cuda_check(c, cudaMemcpyAsync(out, c->red + 2048, sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                    "reduction");
+    if (st) return st;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "reduction");
+}
+
+// one force evaluation and momentum kick: X = (D D^dag)^-1 phi, Y = D^dag X,
+// P -= kick (F_g + F_f)  (local_* of Fermions.cpp:967-1028)
+int force_and_kick(sfh_ctx* c, const void* phi, void* X, void* Y, double kick, double tol, int maxit, int prec,
+                   long* iters, int* solves)
+{
+    sfh_cg_info inf;
+    int st = ctx_solve_device(c, phi, X, tol, maxit, prec, &inf);
+    if (iters) *iters += inf.iters;
+    if (solves) *solves += 1;
+    if (st) return st;
+    launch_hop(c->g, GP_F64_18, c->U64, SP_F64, X, SP_F64, Y, X, c->mass, -1.0, 0, 2, c->stream);
+    return cuda_check(c, launch_force(c->g, c->U64, X, Y, c->beta, c->c11, c->c12, 3, nullptr, c->Pmom, kick,
+                                      c->stream), "force");
+}
+
+int link_update(sfh_ctx* c, double eps, int check)
+{
+    int st = cuda_check(c, launch_link_update(c->g, c->U64, c->Pmom, eps, check, c->derr, c->stream), "link update");
+    c->lowp_valid = false;
+    return st;
+}
+
+int leapfrog(sfh_ctx* c, const void* phi, void* X, void* Y, double eps, int nsteps, double tol, int maxit,
+             int prec, int check, long* iters, int* solves)
+{
+    int st = force_and_kick(c, phi, X, Y, 0.5 * eps, tol, maxit, prec, iters, solves);
+    for (int n = 1; st == SFH_OK && n < nsteps; ++n) {
+        st = link_update(c, eps, check);
+        if (!st) st = take_device_error(c, "leapfrog");
+        if (!st) st = force_and_kick(c, phi, X, Y, eps, tol, maxit, prec, iters, solves);
+    }
+    if (!st) st = link_update(c, eps, check);
+    if (!st) st = take_device_error(c, "leapfrog");
+    if (!st) st = force_and_kick(c, phi, X, Y, 0.5 * eps, tol, maxit, prec, iters, solves);
+    return st;
+}
+
+}  // namespace
+
+namespace sfh {
+// scratch of n FP64 link fields (smearing, staples), grown on demand
+int ensure_scratch(sfh_ctx* c, int nfields)
+{
+    size_t need = (size_t)nfields * c->g.V * 4 * 9 * 16;
+    if (c->smear && c->smear_bytes >= need) return SFH_OK;
+    if (c->smear) cudaFree(c->smear);
+    c->smear = nullptr;
+    c->smear_bytes = 0;
+    int st = cuda_check(c, cudaMalloc(&c->smear, need), "scratch fields");
+    if (!st) c->smear_bytes = need;
+    return st;
+}
+}  // namespace sfh
+
+namespace {
+
+// uniform in [0,1) from a 64-bit seed (SplitMix64 finaliser, Steele et al. 2014)
+double uniform_from_seed(unsigned long long s)
+{
+    unsigned long long z = s + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace
+
+extern "C" int sfh_staples(sfh_ctx* c, double* A1, double* A2)
+{
+    if (!c || !A1 || !A2) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = ensure_scratch(c, 1);
+    if (!st) st = cuda_check(c, launch_staples(c->g, c->U64, c->Fbuf, c->smear, c->stream), "staples");
+    if (!st) st = links_out(c, c->Fbuf, A1);
+    if (!st) st = links_out(c, c->smear, A2);
+    return st;
+}
+
+extern "C" int sfh_gauge_force(sfh_ctx* c, double* F)
+{
+    if (!c || !F) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = cuda_check(c, launch_force(c->g, c->U64, nullptr, nullptr, c->beta, c->c11, c->c12, 1, c->Fbuf,
+                                        nullptr, 0.0, c->stream), "gauge force");
+    if (st) return st;
+    return links_out(c, c->Fbuf, F);
+}
+
+extern "C" int sfh_fermion_force(sfh_ctx* c, const double* X, const double* Y, double* F)
+{
+    if (!c || !X || !Y || !F) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = spinor_in(c, X, c->spin[1]);
+    if (!st) st = spinor_in(c, Y, c->spin[2]);
+    if (!st) st = cuda_check(c, launch_force(c->g, c->U64, c->spin[1], c->spin[2], c->beta, c->c11, c->c12, 2,
+                                             c->Fbuf, nullptr, 0.0, c->stream), "fermion force");
+    if (st) return st;
+    return links_out(c, c->Fbuf, F);
+}
+
+extern "C" int sfh_full_force(sfh_ctx* c, const double* X, const double* Y, double* F)
+{
+    if (!c || !X || !Y || !F) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = spinor_in(c, X, c->spin[1]);
+    if (!st) st = spinor_in(c, Y, c->spin[2]);
+    if (!st) st = cuda_check(c, launch_force(c->g, c->U64, c->spin[1], c->spin[2], c->beta, c->c11, c->c12, 3,
+                                             c->Fbuf, nullptr, 0.0, c->stream), "full force");
+    if (st) return st;
+    return links_out(c, c->Fbuf, F);
+}
+
+extern "C" int sfh_link_update(sfh_ctx* c, double eps, int check)
+{
+    if (!c) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = link_update(c, eps, check);
+    if (st) return st;
+    return take_device_error(c, "link update");
+}
+
+extern "C" int sfh_trp2(sfh_ctx* c, double* out)
+{
+    if (!c || !out) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    return reduce(c, RED_TRP2, c->Pmom, nullptr, out);
+}
+
+extern "C" int sfh_gauge_action(sfh_ctx* c, double* out)
+{
+    if (!c || !out) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    return reduce(c, RED_ACTION, c->U64, nullptr, out);
+}
+
+extern "C" int sfh_plaquette(sfh_ctx* c, double* out)
+{
+    if (!c || !out) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    double s = 0.0;
+    int st = reduce(c, RED_PLAQ, c->U64, nullptr, &s);
+    if (st) return st;
+    *out = s / (4.0 * (double)c->g.V);  // Lattice.cpp:803
+    return SFH_OK;
+}
+
+extern "C" int sfh_set_beta(sfh_ctx* c, double beta)
+{
+    if (!c) return SFH_ERR_INVALID;
+    c->beta = beta;
+    return SFH_OK;
+}
+
+extern "C" int sfh_leapfrog(sfh_ctx* c, const double* phi, double eps, int nsteps, double tol, int maxit,
+                            int precision, double* X_out, long* cg_iters)
+{
+    if (!c || !phi || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = spinor_in(c, phi, c->spin[5]);
+    if (st) return st;
+    long its = 0;
+    st = leapfrog(c, c->spin[5], c->spin[4], c->spin[2], eps, nsteps, tol, maxit, precision, 0, &its, nullptr);
+    if (cg_iters) *cg_iters = its;
+    if (st) return st;
+    if (X_out) return spinor_out(c, c->spin[4], X_out);
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "leapfrog");
+}
+
+extern "C" int sfh_hmc_trajectory(sfh_ctx* c, double eps, int nsteps, unsigned long long seed, double tol,
+                                  int maxit, int precision, sfh_traj_info* info)
+{
+    if (!c || !info || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    std::memset(info, 0, sizeof(*info));
+    auto t0 = std::chrono::steady_clock::now();
+    int st = SFH_OK;
+    if (!c->Utrial) st = cuda_check(c, cudaMalloc(&c->Utrial, (size_t)c->g.V * 4 * 9 * 16), "trajectory buffer");
+    if (st) return st;
+    void *chi = c->spin[0], *phi = c->spin[5], *X = c->spin[4], *Y = c->spin[2];
+    double Sg0 = 0, T0 = 0, F0 = 0;
+    st = reduce(c, RED_ACTION, c->U64, nullptr, &Sg0);  // Fermions.cpp:813
+    // phi = D chi, chi complex Gaussian with variance 1/2 per real part
+    // (Fermions.cpp:207-212, 302-314)
+    if (!st) st = cuda_check(c, launch_random_spinor(c->g, 1.0 / std::sqrt(2.0), seed, chi, c->stream), "chi");
+    if (!st) launch_hop(c->g, GP_F64_18, c->U64, SP_F64, chi, SP_F64, phi, chi, c->mass, 1.0, 0, 2, c->stream);
+    if (!st) st = cuda_check(c, launch_random_momenta(c->g, seed + 1, c->Pmom, c->stream), "momenta");
+    if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T0);
+    sfh_cg_info inf;
+    if (!st) st = ctx_solve_device(c, phi, X, tol, maxit, precision, &inf);  // Fermions.cpp:819
+    info->cg_iters += inf.iters;
+    info->solves += 1;
+    if (!st) st = reduce(c, RED_DOT, phi, X, &F0);
+    if (!st) st = cuda_check(c, cudaMemcpyAsync(c->Utrial, c->U64, (size_t)c->g.V * 4 * 9 * 16,
+                                                cudaMemcpyDeviceToDevice, c->stream), "gauge backup");
+    if (!st) st = leapfrog(c, phi, X, Y, eps, nsteps, tol, maxit, precision, 1, &info->cg_iters, &info->solves);
+    double T1 = 0, Sg1 = 0, F1 = 0;
+    if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T1);
+    if (!st) st = reduce(c, RED_ACTION, c->U64, nullptr, &Sg1);
+    if (!st) st = reduce(c, RED_DOT, phi, X, &F1);
+    if (st) {  // leave the field as it was before the trajectory
+        cudaMemcpyAsync(c->U64, c->Utrial, (size_t)c->g.V * 4 * 9 * 16, cudaMemcpyDeviceToDevice, c->stream);
+        cudaStreamSynchronize(c->stream);
+        c->lowp_valid = false;
+        info->status = st;
+        return st;
+    }
+    info->H_initial[0] = T0;
+    info->H_initial[1] = Sg0;
+    info->H_initial[2] = F0;
+    info->H_final[0] = T1;
+    info->H_final[1] = Sg1;
+    info->H_final[2] = F1;
+    // Fermions.cpp:794-809: accept if u < exp(H_initial - H_final)
+    double d = (T0 - T1) + (Sg0 - Sg1) + (F0 - F1);
+    info->dH = -d;
+    info->uniform = uniform_from_seed(seed + 2);
+    info->accepted = info->uniform < std::exp(d) ? 1 : 0;
+    if (!info->accepted) {
+        st = cuda_check(c, cudaMemcpyAsync(c->U64, c->Utrial, (size_t)c->g.V * 4 * 9 * 16, cudaMemcpyDeviceToDevice,
+                                           c->stream), "gauge restore");
+        c->lowp_valid = false;
+    }
+    double s = 0.0;
+    if (!st) st = reduce(c, RED_PLAQ, c->U64, nullptr, &s);
+    info->plaquette = s / (4.0 * (double)c->g.V);
+    info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    info->status = st;
+    return st;
+}
+
+extern "C" int sfh_smear_stout(sfh_ctx* c, double rho, int nlevels)
+{
+    if (!c || nlevels < 0) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = ensure_scratch(c, 1);
+    if (!st) st = cuda_check(c, launch_stout(c->g, c->U64, c->smear, rho, nlevels, c->derr, c->stream), "stout");
+    c->lowp_valid = false;
+    if (st) return st;
+    return take_device_error(c, "stout smearing");
+}
+
+extern "C" int sfh_smear_hex(sfh_ctx* c, double alpha1, double alpha2, double alpha3, int npasses)
+{
+    if (!c || npasses < 0) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = ensure_scratch(c, 6);
+    if (!st)
+        st = cuda_check(c, launch_hex(c->g, c->U64, c->smear, alpha1, alpha2, alpha3, npasses, c->derr, c->stream),
+                        "hex");
+    c->lowp_valid = false;
+    if (st) return st;
+    return take_device_error(c, "HEX smearing");
+}

@@ -10,6 +10,10 @@
 #include "../../include/sfh.h"
 #include "sfh_core.cuh"
 
+namespace sfh {
+struct CgWorkspace;
+}
+
 struct sfh_ctx {
     sfh::Geom g;
     double mass = 0.0, beta = 0.0, c11 = 5.0 / 3.0, c12 = -1.0 / 12.0;
@@ -31,6 +35,12 @@ struct sfh_ctx {
     int* derr = nullptr;       // device error flags (DeviceErr bits)
     void* pinned = nullptr;    // pinned host staging (72V doubles)
     size_t pinned_bytes = 0;
+
+    sfh::CgWorkspace* ws[3] = {};  // cached solver workspaces per precision
+    double ws_mass[3] = {};
+    void* Utrial = nullptr;        // gauge backup for the Metropolis step
+    void* smear = nullptr;         // scratch link fields (smearing, staples)
+    size_t smear_bytes = 0;
 
     std::string last_error;
 };
@@ -63,5 +73,23 @@ Geom make_geom(const int dims[4]);
 bool dims_ok(const int dims[4]);
 int ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit, int prec,
                  sfh_cg_info* info);
+int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int maxit, int prec,
+                     sfh_cg_info* info);
+void workspace_free(CgWorkspace* w);
+int ensure_scratch(sfh_ctx* c, int nfields);
+
+// gauge.cu
+cudaError_t launch_force(const Geom& g, const void* U, const void* X, const void* Y, double beta, double c11,
+                         double c12, int what, void* out, void* mom, double kick, cudaStream_t s);
+cudaError_t launch_staples(const Geom& g, const void* U, void* A1, void* A2, cudaStream_t s);
+cudaError_t launch_link_update(const Geom& g, void* U, const void* P, double eps, int check, int* err,
+                               cudaStream_t s);
+enum { RED_TRP2 = 0, RED_ACTION = 1, RED_PLAQ = 2, RED_DOT = 3 };
+// smear.cu
+cudaError_t launch_stout(const Geom& g, void* U, void* tmp, double rho, int n, int* err, cudaStream_t s);
+cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double a2, double a3, int n, int* err,
+                       cudaStream_t s);
+cudaError_t launch_reduce(const Geom& g, int kind, const void* A, const void* B, double beta, double c11,
+                          double c12, double* partial, double* out, cudaStream_t s);
 
 }  // namespace sfh

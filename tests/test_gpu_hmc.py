@@ -1,0 +1,234 @@
+"""GPU parity for the HMC path: staples, gauge and fermion forces, the link
+update, Tr P^2 / action / plaquette, the leapfrog trajectory, the full HMC
+update and link smearing.
+
+Tolerances: per-link quantities (staples, forces, exp) 1e-12 relative
+(max-norm over the field); reductions 1e-12 relative; a trajectory 1e-10
+relative against the reference's own trajectory (it contains 11 CG solves at
+the reference's 1e-12 tolerance); reversibility 1e-10 absolute on the links
+(Fermions.cpp:947); dH(eps)/dH(eps/2) in [3.5, 4.5] (Fermions.cpp:1098).
+Smearing compares with the oracle restatement (parity with the reference
+itself is not possible: its HEX code cannot run, see the oracle's header).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_*.npz")))
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def load(path):
+    g = np.load(path)
+    L, T, mass, tol, geps, seed, beta, eps, nsteps = g["meta"]
+    return g, (int(L), int(L), int(L), int(T)), float(mass), float(tol), float(beta), float(eps), int(nsteps)
+
+
+@pytest.fixture(scope="module")
+def sfh():
+    import staggered_fermions_hmc_b200 as m
+    m.load_library()
+    return m
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_staples_forces_scalars_vs_reference(sfh, path):
+    g, dims, mass, tol, beta, eps, nsteps = load(path)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(g["U"])
+    A1, A2 = lat.staples()
+    assert rel(A1, g["A1"]) < 1e-12
+    assert rel(A2, g["A2"]) < 1e-12
+    assert rel(lat.compute_gauge_only_force_field(), g["Fgauge"]) < 1e-12
+    assert rel(lat.compute_fermion_only_force_field(g["X"], g["Y"]), g["Ffermion"]) < 1e-12
+    assert rel(lat.compute_full_force_field(g["X"], g["Y"]), g["Ffull"]) < 1e-12
+    act, plaq, trp2, phix = g["scalars"]
+    assert abs(lat.compute_action() - act) <= 1e-12 * abs(act)
+    assert abs(lat.compute_avg_plaq() - plaq) <= 1e-12 * max(abs(plaq), 1.0)
+    lat.upload_momenta(g["P"])
+    assert rel(lat.download_momenta(), g["P"]) == 0.0
+    assert abs(lat.compute_Tr_P2() - trp2) <= 1e-12 * abs(trp2)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_leapfrog_vs_reference(sfh, path):
+    """local_initial_half_step / local_leapfrog_steps / local_final_step
+    (Fermions.cpp:967-1028) from the same (U, P, phi)."""
+    g, dims, mass, tol, beta, eps, nsteps = load(path)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(g["U"])
+    lat.upload_momenta(g["P"])
+    X, its = lat.leapfrog(g["phi"], eps, nsteps, tol=tol, precision="f64")
+    assert rel(lat.download_gauge(), g["traj_U"]) < 1e-10
+    assert rel(lat.download_momenta(), g["traj_P"]) < 1e-10
+    assert rel(X, g["traj_X"]) < 1e-9
+    h = g["traj_H"]
+    h1 = np.array([lat.compute_Tr_P2(), lat.compute_action(), float(np.dot(g["phi"], X))])
+    assert np.allclose(h1, h[3:], rtol=1e-10, atol=1e-9)
+
+
+@pytest.mark.parametrize("dims,geps", [((6, 6, 6, 6), 0.5), ((4, 6, 8, 10), 0.3)])
+def test_forces_vs_oracle(sfh, orc, dims, geps):
+    mass, beta = 0.2, 4.2
+    U = orc.random_gauge(dims, geps, 61)
+    X = orc.random_spinor(dims, 62)
+    Y = orc.random_spinor(dims, 63)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(U)
+    assert rel(lat.compute_gauge_only_force_field(), orc.gauge_force(dims, beta, U)) < 1e-12
+    assert rel(lat.compute_fermion_only_force_field(X, Y), orc.fermion_force(dims, U, X, Y)) < 1e-12
+    assert abs(lat.compute_action() - orc.action(dims, beta, U)) < 1e-12 * abs(orc.action(dims, beta, U))
+
+
+def test_link_update_vs_oracle(sfh, orc):
+    dims = (4, 4, 4, 8)
+    U = orc.random_gauge(dims, 0.7, 71)
+    P = orc.random_momenta(dims, 72)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    lat.link_update(0.05, check=True)
+    assert rel(lat.download_gauge(), orc.link_update(dims, 0.05, P, U)) < 1e-13
+
+
+def test_link_update_rejects_non_hermitian_momentum(sfh, orc):
+    """Fermions.cpp:712-716: a non-Hermitian P_pre is an error."""
+    dims = (4, 4, 4, 4)
+    U = orc.random_gauge(dims, 0.3, 73)
+    P = orc.random_momenta(dims, 74)
+    P[1] += 0.5  # imaginary part of P_00 on one link: no longer Hermitian
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    with pytest.raises(sfh.SfhError) as e:
+        lat.link_update(0.1, check=True)
+    assert e.value.status == sfh.SFH_ERR_NOT_HERMITIAN
+
+
+def test_cold_start_kats_on_gpu(sfh, orc):
+    """ai_check.cpp:172-333, Lattice.cpp:784-804 on the GPU path."""
+    dims = (4, 4, 4, 6)
+    V = int(np.prod(dims))
+    lat = sfh.Lattice(dims, 0.1, 4.2)
+    lat.upload_gauge(orc.cold_gauge(dims))
+    A1, A2 = lat.staples()
+    eye = np.zeros((3, 3, 2))
+    for i in range(3):
+        eye[i, i, 0] = 1
+    assert np.abs(A1.reshape(-1, 3, 3, 2) - 6 * eye).max() < 1e-12
+    assert np.abs(A2.reshape(-1, 3, 3, 2) - 18 * eye).max() < 1e-12
+    c11, c12 = 5.0 / 3.0, -1.0 / 12.0
+    assert abs(lat.compute_action() + 4.2 * (c11 * 6 * V + c12 * 12 * V)) < 1e-10
+    assert abs(lat.compute_avg_plaq() - 6.0) < 1e-12
+    assert np.abs(lat.compute_gauge_only_force_field()).max() < 1e-12
+
+
+def test_reversibility(sfh, orc):
+    """Fermions.cpp:908-955: forward, flip P, backward returns to U within 1e-10."""
+    dims = (4, 4, 4, 4)
+    U = orc.random_gauge(dims, 0.2, 81)
+    P = orc.random_momenta(dims, 82)
+    phi = orc.random_spinor(dims, 83)
+    lat = sfh.Lattice(dims, 0.5, 4.2)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    lat.leapfrog(phi, 0.02, 10, tol=1e-14)
+    lat.upload_momenta(-lat.download_momenta())
+    lat.leapfrog(phi, 0.02, 10, tol=1e-14)
+    assert np.abs(lat.download_gauge() - U).max() < 1e-10
+    assert np.abs(lat.download_momenta() + P).max() < 1e-9
+
+
+def test_delta_h_step_scaling(sfh, orc):
+    """Fermions.cpp:1061-1108 (with a consistent H): dH(eps)/dH(eps/2) ~ 4."""
+    dims = (4, 4, 4, 4)
+    U = orc.random_gauge(dims, 0.15, 91)
+    P = orc.random_momenta(dims, 92)
+    phi = orc.random_spinor(dims, 93)
+    lat = sfh.Lattice(dims, 0.5, 4.2)
+
+    def dH(eps, n):
+        lat.upload_gauge(U)
+        lat.upload_momenta(P)
+        X0 = lat.solve_CG_DDdagger(phi, tol=1e-14)
+        h0 = lat.compute_Tr_P2() + lat.compute_action() + float(np.dot(phi, X0))
+        X, _ = lat.leapfrog(phi, eps, n, tol=1e-14)
+        h1 = lat.compute_Tr_P2() + lat.compute_action() + float(np.dot(phi, X))
+        return h1 - h0
+
+    d1 = dH(0.02, 10)
+    d2 = dH(0.01, 20)
+    ratio = abs(d1) / abs(d2)
+    assert 3.5 < ratio < 4.5, (d1, d2, ratio)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_hmc_trajectory(sfh, orc, precision):
+    """single_sweep_monte_carlo_update_WITH_FERMIONS: H bookkeeping and the
+    Metropolis decision are self-consistent, and a rejected trajectory leaves
+    the field unchanged."""
+    dims = (4, 4, 4, 4)
+    U = orc.random_gauge(dims, 0.3, 101)
+    lat = sfh.Lattice(dims, 0.1, 4.2)
+    lat.upload_gauge(U)
+    info = lat.hmc_trajectory(0.1, 10, seed=5, tol=1e-10, precision=precision)
+    assert info["status"] == 0
+    dH = sum(info["H_final"]) - sum(info["H_initial"])
+    assert abs(dH - info["dH"]) < 1e-8 * max(1.0, abs(dH))
+    assert info["accepted"] == (info["uniform"] < np.exp(-info["dH"]))
+    assert info["solves"] == 12  # initial solve + N + 1 force solves
+    U1 = lat.download_gauge()
+    if not info["accepted"]:
+        assert np.array_equal(U1, U)
+    assert abs(lat.compute_avg_plaq() - info["plaquette"]) < 1e-14
+
+
+def test_hmc_trajectory_accepts_small_steps(sfh, orc):
+    dims = (4, 4, 4, 4)
+    lat = sfh.Lattice(dims, 0.5, 4.2)
+    lat.upload_gauge(orc.random_gauge(dims, 0.05, 111))
+    info = lat.hmc_trajectory(0.005, 10, seed=9, tol=1e-12)
+    assert info["status"] == 0
+    assert abs(info["dH"]) < 0.1
+
+
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 4, 6, 8)])
+def test_stout_vs_oracle(sfh, orc, dims):
+    U = orc.random_gauge(dims, 0.3, 121)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(U)
+    lat.smear_stout(0.125, 4)
+    assert rel(lat.download_gauge(), orc.stout(dims, 0.125, 4, U)) < 1e-12
+
+
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 4, 6, 8)])
+def test_hex_vs_oracle(sfh, orc, dims):
+    U = orc.random_gauge(dims, 0.3, 131)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(U)
+    lat.Apply_HEX_smearing()
+    assert rel(lat.download_gauge(), orc.hex_smear(dims, U)) < 1e-12
+    lat.upload_gauge(U)
+    lat.Apply_4HEX_smearing()
+    ref = U
+    for _ in range(4):
+        ref = orc.hex_smear(dims, ref)
+    assert rel(lat.download_gauge(), ref) < 1e-11
+
+
+def test_smeared_links_stay_special_unitary(sfh, orc):
+    dims = (4, 4, 4, 4)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(orc.random_gauge(dims, 1.0, 141))
+    lat.Apply_4HEX_smearing()
+    lat.smear_stout(0.125, 4)
+    M = lat.download_gauge().view(np.complex128).reshape(-1, 3, 3)
+    assert np.abs(np.einsum("nji,njk->nik", M.conj(), M) - np.eye(3)).max() < 1e-12
+    assert np.abs(np.linalg.det(M) - 1).max() < 1e-12
