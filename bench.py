@@ -113,8 +113,8 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # algorithmic bytes of one batched solve (roofline section)
 # ---------------------------------------------------------------------------
-SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16}
-LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24}
+SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24}
+LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72}
 
 
 def solve_bytes(spec, infos, precision):
@@ -271,6 +271,101 @@ def make_host_fields(spec, device):
     return fields
 
 
+DSLASH_BYTES = {0: 1248, 1: 432, 2: 224, 3: 624}   # per output site, see DESIGN.md
+DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18"}
+
+
+def run_extras(sfh, hbm, quick=False):
+    """Secondary measurements on the other configurations of the workload
+    family: Dslash GB/s at 32^3x64, the ill-conditioned 32^3x64 solve, the
+    16^4 precision grid, the 4^4 trajectory and a 24^4 trajectory."""
+    import oracle
+    ex = {}
+    # Dslash at 32^3x64 (eps = 1.0 links), one parity per hop, inputs >> L2
+    dims = (32, 32, 32, 64)
+    lat = sfh.Lattice(dims, 0.01, 4.2)
+    lat.random_gauge(1.0, 3)
+    Vh = int(np.prod(dims)) // 2
+    ds = {}
+    for st in (0, 3, 1, 2):
+        ms = lat.dslash_timing(st, nrep=20)
+        gbs = DSLASH_BYTES[st] * Vh / (ms * 1e-3) / 1e9
+        ds[DSLASH_NAMES[st]] = {"ms_per_hop": ms, "GB/s": gbs, "frac": gbs / hbm,
+                                "bytes_per_site": DSLASH_BYTES[st]}
+    ex["dslash_32x32x32x64"] = ds
+    # ill-conditioned single solve: 32^3x64, eps = 1.0, m = 0.01
+    phi = lat.gaussian_spinor(11)
+    sol = {}
+    t0 = time.perf_counter()
+    X64, i64 = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision="f64", info=True)
+    t64 = time.perf_counter() - t0
+    sol["f64"] = {"iters": i64["iters"], "seconds": t64}
+    for prec in ("f16", "f32"):
+        t0 = time.perf_counter()
+        Xm, im = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+        tm = time.perf_counter() - t0
+        sol[prec] = {"iters": im["iters"], "reliable_updates": im["reliable_updates"], "seconds": tm,
+                     "err_vs_f64": float(np.linalg.norm(Xm - X64) / np.linalg.norm(X64)),
+                     "speedup_vs_f64": t64 / tm}
+    ex["c3_32x32x32x64_m0.01"] = sol
+    lat.close()
+    if quick:
+        return ex
+    # 16^4 grid: eps {0.3, 1.0} x m {0.1, 0.02} x storage
+    grid = {}
+    lat = sfh.Lattice((16, 16, 16, 16), 0.1, 4.2)
+    for geps in (0.3, 1.0):
+        lat.random_gauge(geps, 21)
+        phi = lat.gaussian_spinor(22)
+        for m in (0.1, 0.02):
+            lat.set_mass(m)
+            row = {}
+            for prec in ("f64", "f32_18", "f32", "f16"):
+                t0 = time.perf_counter()
+                _, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+                row[prec] = {"iters": inf["iters"], "ms": 1e3 * (time.perf_counter() - t0)}
+            grid[f"eps{geps}_m{m}"] = row
+    ex["c2_16^4"] = grid
+    lat.close()
+    # 4^4 trajectory (beta 4.2, m 0.1, eps_md 0.1, N 10) and its CPU time
+    dims = (4, 4, 4, 4)
+    U = oracle.random_gauge(dims, 0.3, 1)
+    P = oracle.random_momenta(dims, 2)
+    phi = oracle.random_spinor(dims, 3) / np.sqrt(2.0)
+    lat = sfh.Lattice(dims, 0.1, 4.2)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    t0 = time.perf_counter()
+    X, its = lat.leapfrog(phi, 0.1, 10, tol=TOL)
+    tg = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    P2, U2, X2, its2 = oracle.leapfrog(dims, 0.1, 4.2, 0.1, 10, phi, P, U, tol=TOL)
+    tc = time.perf_counter() - t0
+    ex["c1_4^4_trajectory"] = {"gpu_seconds": tg, "cpu_seconds_port": tc, "cg_iters": its,
+                               "max_abs_diff_U_vs_cpu": float(np.abs(lat.download_gauge() - U2).max()),
+                               "plaquette": lat.compute_avg_plaq()}
+    info = lat.hmc_trajectory(0.1, 10, seed=1, tol=TOL)
+    ex["c1_4^4_trajectory"]["hmc"] = {"dH": info["dH"], "accepted": info["accepted"],
+                                      "plaquette": info["plaquette"], "seconds": info["seconds"]}
+    lat.close()
+    # 24^4 trajectories (beta 4.2, one pseudofermion m 0.02, no smearing in the
+    # fermion action: the mass split and smeared-link force are not built)
+    lat = sfh.Lattice((24, 24, 24, 24), 0.02, 4.2)
+    lat.random_gauge(0.3, 5)
+    trajs = []
+    for k in range(2):
+        info = lat.hmc_trajectory(1.0 / 20, 20, seed=100 + 10 * k, tol=TOL, precision="f32")
+        trajs.append({"dH": info["dH"], "accepted": info["accepted"], "plaquette": info["plaquette"],
+                      "seconds": info["seconds"], "cg_iters": info["cg_iters"], "solves": info["solves"]})
+    poly = lat.precompute_polyakov_grid()
+    ex["c5_24^4_trajectory"] = {"trajectories": trajs, "polyakov_mean": [float(poly.mean().real),
+                                                                          float(poly.mean().imag)],
+                                "trajectories_per_hour": 3600.0 / np.mean([t["seconds"] for t in trajs]),
+                                "note": "single pseudofermion, unsmeared fermion links"}
+    lat.close()
+    return ex
+
+
 def run_profile_case(args, spec):
     import staggered_fermions_hmc_b200 as sfh
     sfh.load_library()
@@ -289,11 +384,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sfh", choices=["sfh", "reference"])
-    ap.add_argument("--precision", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f16", "f32_18"])
     ap.add_argument("--nsys", type=int, default=64)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
@@ -340,6 +436,7 @@ def main():
     barrier()
     clk = clocks.stop()
     infos = [[B.info(k, j) for j in range(s["nrhs"])] for k, s in enumerate(spec)]
+    launches_per_solve = B.kernel_launches()
     worst = max(B.true_residual(k, j) for k, s in enumerate(spec) for j in range(s["nrhs"]))
     ms = statistics.mean(times)
     if world > 1:
@@ -413,13 +510,18 @@ def main():
         cpu = {"value": n / secs, "unit": "solves/s", "cores": os.cpu_count(), "kind": kind,
                "sample": desc}
 
+    extras = None
+    if rank == 0 and not args.no_extras:
+        B.close()
+        extras = run_extras(sfh, hbm)
+
     iters = [inf["iters"] for row in infos for inf in row]
     nru = [inf["reliable_updates"] for row in infos for inf in row]
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if args.precision == "f32" else "f16",
+        "dtype": {"f32": "f32", "f16": "f16", "f32_18": "f32"}[args.precision],
         "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
         "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
                                " x eps{0.3,1.0}, 1-8 RHS, seed 7",
@@ -428,13 +530,15 @@ def main():
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "cg_persistent", "alg_bytes_per_launch": alg_bytes},
+                     "kernel": "batched CG solve (cg_hop1 + cg_hop2 + cg_update, graph chunks)",
+                     "alg_bytes_per_launch": alg_bytes},
         "fp64_batched": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms64,
                          "mixed_over_fp64": value / world / fp64_value},
         "solver": {"iters_mean": float(np.mean(iters)), "iters_max": int(max(iters)),
                    "reliable_updates_mean": float(np.mean(nru)), "worst_true_resid": worst},
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * launches_per_solve,
+        "extras": extras,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

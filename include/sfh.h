@@ -32,12 +32,15 @@ extern "C" {
 #define SFH_ERR_CUDA 6          /* CUDA runtime error (message in sfh_last_error)    */
 #define SFH_ERR_INVALID 7       /* invalid argument                                  */
 #define SFH_ERR_NOMEM 8         /* device allocation failed                          */
+#define SFH_ERR_IO 9            /* checkpoint file could not be read or written      */
 
 /* solver precisions */
 #define SFH_PREC_F64 0   /* plain FP64 CG, FP64 links and vectors                     */
 #define SFH_PREC_F32 1   /* FP32 12-real links, FP32 vectors, FP64 reliable updates   */
 #define SFH_PREC_F16 2   /* FP16 12-real links, FP16+per-site-scale vectors, FP32 math,
                             FP64 reliable updates                                      */
+#define SFH_PREC_F32_18 3 /* FP32 18-real links (no reconstruction), FP32 vectors,
+                             FP64 reliable updates                                     */
 
 typedef struct sfh_ctx sfh_ctx;
 typedef struct sfh_batch sfh_batch;
@@ -99,6 +102,12 @@ int sfh_dirac(sfh_ctx* ctx, int dagger, const double* in, double* out);
 
 /* out = D D^dag in: apply_DDdagger (Fermions.cpp:530-547) */
 int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
+
+/* Device time of one even-odd hop (V/2 output sites, the hopping part of
+ * Fermions.cpp:218-283) in a storage format: 0 FP64 18-real, 1 FP32 12-real,
+ * 2 FP16 12-real with per-site spinor scale, 3 FP32 18-real.  Benchmark aid;
+ * the input is all zeros, so the value of the output is meaningless. */
+int sfh_dslash_timing(sfh_ctx* ctx, int storage, int nrep, double* ms_per_hop);
 
 /* ---- solver --------------------------------------------------------------- */
 /* X = (D D^dag)^{-1} phi to |r| < tol |phi|: solve_CG_DDdagger / solve_X_field
@@ -162,6 +171,18 @@ int sfh_leapfrog(sfh_ctx* ctx, const double* phi, double eps, int nsteps, double
 int sfh_hmc_trajectory(sfh_ctx* ctx, double eps, int nsteps, unsigned long long seed, double tol, int maxit,
                        int precision, sfh_traj_info* info);
 
+/* ---- observables and checkpoints ------------------------------------------ */
+/* Polyakov loops Tr prod_t U_t(x,y,z,t) on the spatial grid, (re, im) pairs in
+ * (x*Ly + y)*Lz + z order: precompute_polyakov_grid (Lattice.cpp:869-882). */
+int sfh_polyakov_grid(sfh_ctx* ctx, double* out);
+/* <P(m) conj(P(m+d))> over |d|^2 = r2: correlator_over_fixed_distance_fast
+ * (Lattice.cpp:886-948).  out2 = (re, im). */
+int sfh_polyakov_correlator(sfh_ctx* ctx, int r2, double* out2);
+/* Raw gauge checkpoint in the reference layout (save_all_lattice_configs /
+ * load_all_lattice_configs for one coupling, Lattice.cpp:810-847). */
+int sfh_save_gauge(sfh_ctx* ctx, const char* path);
+int sfh_load_gauge(sfh_ctx* ctx, const char* path);
+
 /* ---- smearing ------------------------------------------------------------- */
 /* nlevels stout levels U <- exp(rho proj(C U^dag)) U with plaquette staples
  * (the single-level analogue of the HEX steps of Smearing.cpp:132-155). */
@@ -200,6 +221,8 @@ int sfh_batch_random_gauge(sfh_batch* batch, int sys, double eps, unsigned long 
 int sfh_batch_random_rhs(sfh_batch* batch, int sys, int rhs, unsigned long long seed, double sigma);
 int sfh_batch_get_gauge(sfh_batch* batch, int sys, double* links);
 int sfh_batch_get_rhs(sfh_batch* batch, int sys, int rhs, double* phi);
+/* number of kernels the last sfh_batch_solve launched (init + graph chunks) */
+int sfh_batch_kernel_launches(sfh_batch* batch, long* n);
 /* FP64 |b - D D^dag x| / |b| for one solution (diagnostic) */
 int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
 

@@ -32,9 +32,10 @@ SFH_ERR_TIMEOUT = 5
 SFH_ERR_CUDA = 6
 SFH_ERR_INVALID = 7
 SFH_ERR_NOMEM = 8
+SFH_ERR_IO = 9
 
-PREC_F64, PREC_F32, PREC_F16 = 0, 1, 2
-PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16}
+PREC_F64, PREC_F32, PREC_F16, PREC_F32_18 = 0, 1, 2, 3
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "f32_18": PREC_F32_18}
 BATCH_FULL_LATTICE = 1
 
 
@@ -105,6 +106,7 @@ SIGNATURES = {
     "sfh_download_momenta": (ctypes.c_int, [_VP, _D]),
     "sfh_dirac": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_ddag": (ctypes.c_int, [_VP, _D, _D]),
+    "sfh_dslash_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_cg_solve": (ctypes.c_int, [_VP, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(CgInfo)]),
     "sfh_staples": (ctypes.c_int, [_VP, _D, _D]),
@@ -121,6 +123,10 @@ SIGNATURES = {
     "sfh_hmc_trajectory": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(TrajInfo)]),
+    "sfh_polyakov_grid": (ctypes.c_int, [_VP, _D]),
+    "sfh_polyakov_correlator": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "sfh_save_gauge": (ctypes.c_int, [_VP, ctypes.c_char_p]),
+    "sfh_load_gauge": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "sfh_smear_stout": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_smear_hex": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
@@ -141,6 +147,7 @@ SIGNATURES = {
     "sfh_batch_get_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_get_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_true_residual": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_batch_kernel_launches": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_long)]),
     "sfh_cg_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_double, _VP, _VP, _VP,
                                             ctypes.c_double, ctypes.c_int, _VP, ctypes.POINTER(CgInfo)]),
 }
@@ -269,6 +276,13 @@ class Lattice:
         self._check(self.lib.sfh_dirac(self.h, 1, _dptr(psi), _dptr(out)), "dirac_dagger")
         return out
 
+    def dslash_timing(self, storage, nrep=20):
+        """ms per even-odd hop (V/2 output sites); storage 0 FP64-18, 1 FP32-12,
+        2 FP16-12, 3 FP32-18."""
+        ms = ctypes.c_double(0.0)
+        self._check(self.lib.sfh_dslash_timing(self.h, storage, nrep, ctypes.byref(ms)), "dslash timing")
+        return ms.value
+
     # --- Fermions.cpp:530-547 ----------------------------------------------
     def apply_DDdagger(self, psi):
         psi = _f64(psi).reshape(-1)
@@ -355,6 +369,23 @@ class Lattice:
                                          ctypes.byref(inf))
         self._check(st, "hmc trajectory")
         return inf.as_dict()
+
+    # --- observables, checkpoints (Lattice.cpp:810-948) ------------------------
+    def precompute_polyakov_grid(self):
+        out = np.empty(2 * self.dims[0] * self.dims[1] * self.dims[2])
+        self._check(self.lib.sfh_polyakov_grid(self.h, _dptr(out)), "polyakov grid")
+        return out.view(np.complex128)
+
+    def correlator_over_fixed_distance(self, r_squared):
+        out = np.empty(2)
+        self._check(self.lib.sfh_polyakov_correlator(self.h, int(r_squared), _dptr(out)), "polyakov correlator")
+        return complex(out[0], out[1])
+
+    def save_lattice_config(self, path):
+        self._check(self.lib.sfh_save_gauge(self.h, os.fsencode(path)), "save_lattice_config")
+
+    def load_lattice_config(self, path):
+        self._check(self.lib.sfh_load_gauge(self.h, os.fsencode(path)), "load_lattice_config")
 
     # --- smearing (Smearing.cpp) ---------------------------------------------
     def smear_stout(self, rho, n_levels=1):
@@ -449,6 +480,11 @@ class Batch:
         inf = CgInfo()
         self._check(self.lib.sfh_batch_get_info(self.h, k, j, ctypes.byref(inf)), "get_info")
         return inf.as_dict()
+
+    def kernel_launches(self):
+        n = ctypes.c_long(0)
+        self._check(self.lib.sfh_batch_kernel_launches(self.h, ctypes.byref(n)), "kernel_launches")
+        return n.value
 
     def true_residual(self, k, j):
         r = ctypes.c_double(0)

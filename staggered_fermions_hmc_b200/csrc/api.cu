@@ -62,6 +62,7 @@ extern "C" const char* sfh_status_string(int s)
         case SFH_ERR_CUDA: return "CUDA error";
         case SFH_ERR_INVALID: return "invalid argument";
         case SFH_ERR_NOMEM: return "device allocation failed";
+        case SFH_ERR_IO: return "checkpoint file could not be read or written";
         default: return "unknown status";
     }
 }
@@ -91,6 +92,7 @@ extern "C" int sfh_create(const sfh_params* p, sfh_ctx** out)
     e = cudaMalloc(&c->U64, links64);
     if (e == cudaSuccess) e = cudaMalloc(&c->U32, V * 4 * 3 * 16);
     if (e == cudaSuccess) e = cudaMalloc(&c->U16, V * 4 * 3 * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&c->U32_18, V * 4 * 9 * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->Pmom, links64);
     if (e == cudaSuccess) e = cudaMalloc(&c->Fbuf, links64);
     if (e == cudaSuccess) e = cudaMalloc(&c->stage, V * 72 * sizeof(double));
@@ -113,9 +115,10 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     if (!c) return SFH_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 4; ++k)
         if (c->ws[k]) workspace_free(c->ws[k]);
-    void* ptrs[] = {c->U64, c->U32, c->U16, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial, c->smear};
+    void* ptrs[] = {c->U64, c->U32, c->U16, c->U32_18, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
+                    c->smear};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : c->spin)
@@ -230,7 +233,7 @@ extern "C" int sfh_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol
                             int precision, sfh_cg_info* info)
 {
     if (!c || !phi || !X || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     return ctx_cg_solve(c, phi, X, tol, maxit, precision, info);
 }
@@ -298,4 +301,43 @@ extern "C" int sfh_download_momenta(sfh_ctx* c, double* P)
     int st = cuda_check(c, cudaMemcpyAsync(P, c->stage, n, cudaMemcpyDeviceToHost, c->stream), "momenta download");
     if (st) return st;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "momenta download");
+}
+
+// Device time of one even-odd hop (V/2 output sites) in a storage format:
+// 0 FP64 18-real, 1 FP32 12-real, 2 FP16 12-real + scale, 3 FP32 18-real.
+// Uses the context's gauge field and a zero input (the memory traffic and
+// arithmetic do not depend on the values); nrep timed hops after three
+// untimed ones, measured with CUDA events on the context's stream.
+extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_per_hop)
+{
+    if (!c || !ms_per_hop || storage < 0 || storage > 3 || nrep < 1) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (!c->lowp_valid) {
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18);
+        c->lowp_valid = true;
+    }
+    static const int gp[4] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18};
+    static const int sp[4] = {SP_F64, SP_F32, SP_F16, SP_F32};
+    const void* U = storage == 0 ? c->U64 : (storage == 1 ? c->U32 : (storage == 2 ? c->U16 : c->U32_18));
+    int st = SFH_OK;
+    void* in = c->spin[0];
+    void* out = c->spin[1];
+    cudaMemsetAsync(in, 0, (size_t)c->g.V * 48, c->stream);
+    cudaMemsetAsync(out, 0, (size_t)c->g.V * 48, c->stream);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int k = 0; k < 3; ++k) launch_hop(c->g, gp[storage], U, sp[storage], in, sp[storage], out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    cudaEventRecord(e0, c->stream);
+    for (int k = 0; k < nrep; ++k)
+        launch_hop(c->g, gp[storage], U, sp[storage], in, sp[storage], out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    cudaEventRecord(e1, c->stream);
+    st = cuda_check(c, cudaEventSynchronize(e1), "dslash timing");
+    float ms = 0.f;
+    if (!st) st = cuda_check(c, cudaEventElapsedTime(&ms, e0, e1), "dslash timing");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    *ms_per_hop = (double)ms / nrep;
+    return SFH_OK;
 }

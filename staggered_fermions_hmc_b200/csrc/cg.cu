@@ -604,6 +604,10 @@ static CgKernels pick_kernels(int prec, int nb1, int nb2)
         k.hop1 = pick_hop1<GP_F32_12, SP_F32>(nb1);
         pick_hop2<GP_F32_12, SP_F32>(nb2, &k.hop2, &k.init);
         k.update = cg_update<SP_F32>;
+    } else if (prec == SFH_PREC_F32_18) {
+        k.hop1 = pick_hop1<GP_F32_18, SP_F32>(nb1);
+        pick_hop2<GP_F32_18, SP_F32>(nb2, &k.hop2, &k.init);
+        k.update = cg_update<SP_F32>;
     } else {
         k.hop1 = pick_hop1<GP_F16_12, SP_F16>(nb1);
         pick_hop2<GP_F16_12, SP_F16>(nb2, &k.hop2, &k.init);
@@ -650,6 +654,7 @@ struct CgWorkspace {
     int g_maxit = -1;
     int* h_active = nullptr;  // pinned, two slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    long launches = 0;        // kernels launched by the last solve
 
     ~CgWorkspace() { release(); }
     void release_graph()
@@ -689,7 +694,7 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
     w.both = both;
     w.nsys = (int)systems.size();
     w.sys.clear(); w.rhs.clear(); w.rhs0.clear(); w.lanes_h.clear();
-    const int sp = prec == SFH_PREC_F64 ? SP_F64 : (prec == SFH_PREC_F32 ? SP_F32 : SP_F16);
+    const int sp = prec == SFH_PREC_F64 ? SP_F64 : (prec == SFH_PREC_F16 ? SP_F16 : SP_F32);
     int tile = 0, lane = 0, poff = 0;
     std::vector<int> tile_sys;
     for (int k = 0; k < w.nsys; ++k) {
@@ -859,12 +864,14 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     CgArgs a = make_args(w, tol, maxit, delta);
     CgKernels k = pick_kernels(w.prec, nb1, nb2);
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
+    w.launches = 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
     const int max_chunks = a.maxloop / kChunk + 2;
     // keep one chunk queued ahead of the convergence check
     for (int c = 0; c < max_chunks; ++c) {
         if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) return e;
+        w.launches += 3 * kChunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
@@ -918,6 +925,17 @@ Geom make_geom(const int dims[4]);
 bool dims_ok(const int dims[4]);
 }
 
+// derived reduced-precision links of system k (U32 holds the 18-real FP32
+// field for SFH_PREC_F32_18)
+static void batch_make_lowp(sfh_batch* b, int k)
+{
+    if (b->prec == SFH_PREC_F64) return;
+    if (b->prec == SFH_PREC_F32_18)
+        sfh::launch_make_lowp_gauge(b->geoms[k], b->U64[k], nullptr, nullptr, b->stream, b->U32[k]);
+    else
+        sfh::launch_make_lowp_gauge(b->geoms[k], b->U64[k], b->U32[k], b->U16[k], b->stream);
+}
+
 static int batch_err(sfh_batch* b, int code, const std::string& m)
 {
     if (b) b->last_error = m;
@@ -935,7 +953,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
                                 int flags, sfh_batch** out)
 {
     if (!out || nsys <= 0 || !systems) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
     if ((flags & SFH_BATCH_FULL_LATTICE) && precision != SFH_PREC_F64) return SFH_ERR_INVALID;
     for (int k = 0; k < nsys; ++k)
         if (!sfh::dims_ok(systems[k].dims) || systems[k].nrhs <= 0 || systems[k].nrhs > 64)
@@ -961,6 +979,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
         e = cudaMalloc(&u64, n64);
         if (e == cudaSuccess && precision == SFH_PREC_F32) e = cudaMalloc(&u32, (size_t)g.V * 4 * 3 * 16);
         if (e == cudaSuccess && precision == SFH_PREC_F16) e = cudaMalloc(&u16, (size_t)g.V * 4 * 3 * 8);
+        if (e == cudaSuccess && precision == SFH_PREC_F32_18) e = cudaMalloc(&u32, (size_t)g.V * 4 * 9 * 8);
         b->U64.push_back(u64);
         b->U32.push_back(u32);
         b->U16.push_back(u16);
@@ -980,7 +999,9 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
         h.mass = systems[k].mass;
         h.nrhs = systems[k].nrhs;
         h.U64 = b->U64[k];
-        h.Ulo = precision == SFH_PREC_F32 ? b->U32[k] : (precision == SFH_PREC_F16 ? b->U16[k] : b->U64[k]);
+        h.Ulo = (precision == SFH_PREC_F32 || precision == SFH_PREC_F32_18)
+                    ? b->U32[k]
+                    : (precision == SFH_PREC_F16 ? b->U16[k] : b->U64[k]);
         hs.push_back(h);
     }
     e = sfh::workspace_build(b->ws, hs, precision, (flags & SFH_BATCH_FULL_LATTICE) ? 1 : 0);
@@ -1045,7 +1066,7 @@ extern "C" int sfh_batch_set_gauge(sfh_batch* b, int k, const double* links)
     if (st) return st;
     sfh::launch_links_aos_to_eo(g, (const double*)b->stage, b->U64[k], b->stream);
     if (b->prec != SFH_PREC_F64)
-        sfh::launch_make_lowp_gauge(g, b->U64[k], b->U32[k], b->U16[k], b->stream);
+        batch_make_lowp(b, k);
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "gauge convert");
 }
 
@@ -1156,7 +1177,7 @@ static CgWorkspace* ctx_workspace(sfh_ctx* c, int prec, cudaError_t* err)
     h.mass = c->mass;
     h.nrhs = 1;
     h.U64 = c->U64;
-    h.Ulo = prec == SFH_PREC_F32 ? c->U32 : (prec == SFH_PREC_F16 ? c->U16 : c->U64);
+    h.Ulo = prec == SFH_PREC_F32 ? c->U32 : (prec == SFH_PREC_F16 ? c->U16 : (prec == SFH_PREC_F32_18 ? c->U32_18 : c->U64));
     std::vector<SolverSystemHost> hs(1, h);
     *err = workspace_build(*w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
     if (*err != cudaSuccess) {
@@ -1172,7 +1193,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
                      sfh_cg_info* info)
 {
     if (prec != SFH_PREC_F64 && !c->lowp_valid) {
-        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream);
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18);
         c->lowp_valid = true;
     }
     if (c->ws[prec] && c->ws_mass[prec] != c->mass) {  // mass is baked into the system table
@@ -1244,7 +1265,7 @@ extern "C" int sfh_batch_random_gauge(sfh_batch* b, int k, double eps, unsigned 
     const sfh::Geom& g = b->geoms[k];
     int st = batch_cuda(b, sfh::launch_random_gauge(g, eps, seed, b->U64[k], b->derr, b->stream), "random gauge");
     if (st) return st;
-    if (b->prec != SFH_PREC_F64) sfh::launch_make_lowp_gauge(g, b->U64[k], b->U32[k], b->U16[k], b->stream);
+    batch_make_lowp(b, k);
     int h = 0;
     st = batch_cuda(b, cudaMemcpyAsync(&h, b->derr, sizeof(int), cudaMemcpyDeviceToHost, b->stream), "random gauge");
     if (!st) st = batch_cuda(b, cudaStreamSynchronize(b->stream), "random gauge");
@@ -1286,4 +1307,11 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
                                            cudaMemcpyDeviceToHost, b->stream), "rhs download");
     if (st) return st;
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
+}
+
+extern "C" int sfh_batch_kernel_launches(sfh_batch* b, long* n)
+{
+    if (!b || !n) return SFH_ERR_INVALID;
+    *n = b->ws.launches;
+    return SFH_OK;
 }

@@ -236,7 +236,7 @@ extern "C" int sfh_leapfrog(sfh_ctx* c, const double* phi, double eps, int nstep
                             int precision, double* X_out, long* cg_iters)
 {
     if (!c || !phi || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     int st = spinor_in(c, phi, c->spin[5]);
     if (st) return st;
@@ -252,7 +252,7 @@ extern "C" int sfh_hmc_trajectory(sfh_ctx* c, double eps, int nsteps, unsigned l
                                   int maxit, int precision, sfh_traj_info* info)
 {
     if (!c || !info || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F16) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     std::memset(info, 0, sizeof(*info));
     auto t0 = std::chrono::steady_clock::now();

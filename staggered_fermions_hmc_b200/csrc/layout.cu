@@ -67,12 +67,18 @@ __global__ void links_eo_to_aos(Geom g, const double2* __restrict__ eo, double* 
 
 // FP64 18-real -> FP32 12-real (float4 x3) and FP16 12-real (uint2 x3)
 __global__ void make_lowp(Geom g, const double2* __restrict__ U64, float4* __restrict__ U32,
-                          uint2* __restrict__ U16)
+                          uint2* __restrict__ U16, float2* __restrict__ U32_18)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int pm = blockIdx.y;  // p*4+mu
     if (i >= g.Vh) return;
     const double2* src = U64 + (size_t)pm * 9 * g.Vh + i;
+    if (U32_18)
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            double2 a = src[(size_t)k * g.Vh];
+            U32_18[((size_t)pm * 9 + k) * g.Vh + i] = make_float2((float)a.x, (float)a.y);
+        }
     double2 e[6];
 #pragma unroll
     for (int k = 0; k < 6; ++k) e[k] = src[(size_t)k * g.Vh];
@@ -115,10 +121,10 @@ void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStre
     links_eo_to_aos<<<dim3(blocks_for(g.Vh), 8), kThreads, 0, s>>>(g, (const double2*)eo, aos);
 }
 
-void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s)
+void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s, void* U32_18)
 {
     make_lowp<<<dim3(blocks_for(g.Vh), 8), kThreads, 0, s>>>(g, (const double2*)U64, (float4*)U32,
-                                                              (uint2*)U16);
+                                                              (uint2*)U16, (float2*)U32_18);
 }
 
 }  // namespace sfh

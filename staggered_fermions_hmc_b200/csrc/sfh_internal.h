@@ -26,6 +26,7 @@ struct sfh_ctx {
     void* U64 = nullptr;       // gauge FP64 18-real
     void* U32 = nullptr;       // gauge FP32 12-real (derived)
     void* U16 = nullptr;       // gauge FP16 12-real (derived)
+    void* U32_18 = nullptr;    // gauge FP32 18-real (derived)
     bool lowp_valid = false;   // derived copies match U64
     void* Pmom = nullptr;      // momenta FP64 18-real
     void* Fbuf = nullptr;      // force scratch FP64 18-real
@@ -36,8 +37,8 @@ struct sfh_ctx {
     void* pinned = nullptr;    // pinned host staging (72V doubles)
     size_t pinned_bytes = 0;
 
-    sfh::CgWorkspace* ws[3] = {};  // cached solver workspaces per precision
-    double ws_mass[3] = {};
+    sfh::CgWorkspace* ws[4] = {};  // cached solver workspaces per precision
+    double ws_mass[4] = {};
     void* Utrial = nullptr;        // gauge backup for the Metropolis step
     void* smear = nullptr;         // scratch link fields (smearing, staples)
     size_t smear_bytes = 0;
@@ -56,7 +57,8 @@ void launch_spinor_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStr
 void launch_spinor_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
 void launch_links_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
 void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
-void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s);
+void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s,
+                            void* U32_18 = nullptr);
 
 // out_q = a*self_q + b*K_{q,1-q} in  for q in [q0, q0+nq); precisions by enum
 void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,

@@ -232,3 +232,36 @@ def test_smeared_links_stay_special_unitary(sfh, orc):
     M = lat.download_gauge().view(np.complex128).reshape(-1, 3, 3)
     assert np.abs(np.einsum("nji,njk->nik", M.conj(), M) - np.eye(3)).max() < 1e-12
     assert np.abs(np.linalg.det(M) - 1).max() < 1e-12
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_polyakov_vs_reference(sfh, path):
+    """precompute_polyakov_grid and correlator_over_fixed_distance_fast
+    (Lattice.cpp:869-948) against the reference's outputs."""
+    g, dims, mass, tol, beta, eps, nsteps = load(path)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(g["U"])
+    grid = lat.precompute_polyakov_grid()
+    assert rel(grid.view(np.float64), g["poly_grid"]) < 1e-12
+    corr = g["poly_corr"].reshape(-1, 2)
+    for r2 in (1, 2, 3):
+        c = lat.correlator_over_fixed_distance(r2)
+        assert abs(c - complex(*corr[r2 - 1])) <= 1e-12 * max(abs(c), 1.0)
+
+
+def test_checkpoint_round_trip_is_byte_exact(sfh, orc, tmp_path):
+    """save_all_lattice_configs / load_all_lattice_configs (Lattice.cpp:810-847):
+    the file is the reference's raw double array."""
+    dims = (4, 4, 4, 6)
+    U = orc.random_gauge(dims, 0.4, 151)
+    lat = sfh.Lattice(dims, 0.1)
+    lat.upload_gauge(U)
+    path = tmp_path / "final_lattice_configs.bin"
+    lat.save_lattice_config(str(path))
+    assert path.read_bytes() == U.astype("<f8").tobytes()
+    lat2 = sfh.Lattice(dims, 0.1)
+    lat2.load_lattice_config(str(path))
+    assert np.array_equal(lat2.download_gauge(), U)
+    with pytest.raises(sfh.SfhError) as e:
+        lat2.load_lattice_config(str(tmp_path / "missing.bin"))
+    assert e.value.status == sfh.SFH_ERR_IO

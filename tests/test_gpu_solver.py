@@ -76,7 +76,7 @@ def true_resid(orc, dims, mass, U, b, x):
     return float(np.linalg.norm(r) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("precision", ["f64", "f32", "f16"])
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18"])
 def test_cg_precisions_true_residual(sfh, orc, precision):
     dims, mass = (8, 8, 8, 8), 0.1
     U = orc.random_gauge(dims, 0.3, 41)
@@ -121,7 +121,7 @@ def test_invalid_dims_rejected(sfh):
     assert e.value.status == sfh.SFH_ERR_INVALID
 
 
-@pytest.mark.parametrize("precision", ["f64", "f32", "f16"])
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18"])
 def test_batch_uneven_systems(sfh, orc, precision):
     systems = [((4, 4, 4, 4), 0.2, 2), ((6, 6, 6, 8), 0.05, 3), ((8, 8, 8, 4), 0.1, 1),
                ((4, 4, 8, 8), 0.1, 5)]
