@@ -302,7 +302,11 @@ def run_extras(sfh, hbm, quick=False):
     sol["f64"] = {"iters": i64["iters"], "seconds": t64}
     for prec in ("f16", "f32"):
         t0 = time.perf_counter()
-        Xm, im = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+        try:
+            Xm, im = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+        except sfh.SfhError as e:
+            sol[prec] = {"error": str(e)}
+            continue
         tm = time.perf_counter() - t0
         sol[prec] = {"iters": im["iters"], "reliable_updates": im["reliable_updates"], "seconds": tm,
                      "err_vs_f64": float(np.linalg.norm(Xm - X64) / np.linalg.norm(X64)),
@@ -513,7 +517,10 @@ def main():
     extras = None
     if rank == 0 and not args.no_extras:
         B.close()
-        extras = run_extras(sfh, hbm)
+        try:
+            extras = run_extras(sfh, hbm)
+        except Exception as e:  # secondary measurements never hide the headline
+            extras = {"error": f"{type(e).__name__}: {e}"}
 
     iters = [inf["iters"] for row in infos for inf in row]
     nru = [inf["reliable_updates"] for row in infos for inf in row]

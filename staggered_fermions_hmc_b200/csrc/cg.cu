@@ -75,7 +75,7 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
                 P.alpha[l] = ld_dbl(&L->alpha);
                 P.beta[l] = ld_dbl(&L->beta);
             }
-            P.anyA |= P.mode[l] == LM_ACTIVE;
+            P.anyA |= P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
             P.anyR |= P.mode[l] == LM_RU;
         }
     }
@@ -150,7 +150,7 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
     for (int f = 0; f < kSums; ++f) s[f] = warp_sum_slots(base + f * nslot, n);
     if (threadIdx.x != 0) return;
     const int nxt = cur ^ 1;
-    if (mode == LM_ACTIVE) {
+    if (mode == LM_ACTIVE || mode == LM_RESTART) {
         const double rr = s[3], pAp = s[0];
         const double alpha = rr / pAp;  // Fermions.cpp:573-586
         if (!isfinite(pAp) || fabs(pAp) < 1e-30 || !isfinite(alpha)) {
@@ -178,7 +178,10 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
                 L->mode[nxt] = LM_ACTIVE;
         } else {
             const double r = sqrt(fmax(rr_next, 0.0));
-            if (rr_next < L->target || r < a.delta * L->rmax || L->iters >= a.maxit) {
+            // update on a drop by delta, at the target, at maxit, or when the
+            // iterated residual has grown well past the last true residual
+            if (rr_next < L->target || r < a.delta * L->rmax || L->iters >= a.maxit ||
+                rr_next > 4.0 * L->rr_old) {
                 L->mode[nxt] = LM_RU;
             } else {
                 L->rmax = fmax(L->rmax, r);
@@ -196,8 +199,12 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
         } else if (L->iters >= a.maxit) {
             lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_ERR_NOCONV);
         } else {
+            // keep the search direction, or restart it (p = r) when the lane
+            // restarts after every update or the last stretch made little progress
+            const bool restart = a.restart || rt > 0.5 * L->rr_old;
+            L->rr_old = rt;
             L->rmax = sqrt(rt);
-            L->mode[nxt] = LM_ACTIVE;
+            L->mode[nxt] = restart ? LM_RESTART : LM_ACTIVE;
         }
     }
 }
@@ -213,6 +220,7 @@ __device__ __noinline__ void finish_init_lane(const CgArgs& a, const CgSys& S, i
     L->target = a.tol2 * bb;
     L->rr = bb;
     L->rr_next = bb;
+    L->rr_old = bb;
     L->rmax = sqrt(bb);
     L->alpha = 0.0;
     L->beta = 0.0;
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
         if (P.anyA) {
             const void* pin[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) pin[l] = rhs_ptr(a, P.rid[l], F_P);
+            for (int l = 0; l < NB; ++l) pin[l] = rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P);
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
@@ -349,7 +357,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
                     Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE) continue;
+                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                         Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, lu, Vh));
                         vacc(acc[l], mul_mv(U, w), eta_neg != wu);
                     }
@@ -358,7 +366,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
                     Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE) continue;
+                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                         Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, ld, Vh));
                         vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
                     }
@@ -366,7 +374,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
             }
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
-                if (P.mode[l] != LM_ACTIVE) continue;
+                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                 Vec3<R> o;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
@@ -445,7 +453,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
         double sums[NB * kSums];
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
-            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RU;
+            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART || P.mode[l] == LM_RU;
 #pragma unroll
             for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
         }
@@ -466,7 +474,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
                     Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE) continue;
+                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                         Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, lu, Vh));
                         vacc(acc[l], mul_mv(U, w), eta_neg != wu);
                     }
@@ -475,7 +483,7 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
                     Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
 #pragma unroll
                     for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE) continue;
+                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                         Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, ld, Vh));
                         vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
                     }
@@ -484,9 +492,13 @@ __global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
             const R m2 = (R)S.m2;
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
-                if (P.mode[l] != LM_ACTIVE) continue;
-                Vec3<RS> p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
                 Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+                Vec3<RS> p = r;
+                if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
+                    SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
+                else
+                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
                 Vec3<R> pr = vcvt<R>(p), w;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -533,7 +545,7 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, int cur)
     for (int rhs = 0; rhs < S.nrhs; ++rhs) {
         CgLane* L = a.lanes + lane_of(S, rhs, q, false);
         const int mode = ld_int(&L->mode[cur]);
-        if (mode != LM_ACTIVE && mode != LM_LAST) continue;
+        if (mode != LM_ACTIVE && mode != LM_RESTART && mode != LM_LAST) continue;
         if (mode == LM_LAST && threadIdx.x == 0) {  // the last tile retires the lane
             const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
             if (atomicAdd(&L->ticket, 1u) == expected - 1) {
@@ -795,6 +807,7 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.delta = delta;
     a.maxit = maxit;
     a.mixed = w.prec != SFH_PREC_F64;
+    a.restart = w.prec == SFH_PREC_F16;  // FP16: defect correction (restart after each update)
     a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
     return a;
 }

@@ -11,7 +11,9 @@ namespace sfh {
 
 // lane modes; LM_LAST: the update kernel of this iteration still runs for the
 // lane, then retires it (DONE)
-enum { LM_ACTIVE = 0, LM_RU = 1, LM_DONE = 2, LM_FAILED = 3, LM_LAST = 4 };
+// LM_RESTART: an active iteration that first restarts the search direction
+// (p = r), used after the FP64 residual update of restarting lanes
+enum { LM_ACTIVE = 0, LM_RU = 1, LM_DONE = 2, LM_FAILED = 3, LM_LAST = 4, LM_RESTART = 5 };
 constexpr int kTile = 256;
 
 struct CgSys {
@@ -51,6 +53,7 @@ struct CgArgs {
     int* n_active;
     double tol2, delta;
     int maxit, maxloop, mixed;
+    int restart;  // restart the Krylov space after every residual update
 };
 
 namespace {

@@ -691,6 +691,7 @@ extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* 
     a.delta = 0.1;
     a.maxit = maxit;
     a.mixed = 0;
+    a.restart = 0;
     a.maxloop = maxit + 1;
     PersistentKernel k = cg_persistent<GP_F64_18, SP_F64, 1>;
     int per_sm = 0;
