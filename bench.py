@@ -394,6 +394,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
@@ -420,6 +421,7 @@ def main():
     total_rhs = sum(s["nrhs"] for s in spec)
 
     B = build_batch(sfh, spec, args.precision, local)
+    rhs_block = B.autotune() if not args.no_autotune else 0
 
     def solve():
         B.solve(tol=TOL, max_iter=MAXIT)
@@ -455,6 +457,8 @@ def main():
 
     # FP64 batched CG on the same batch, same kernel family (the comparison)
     B64 = build_batch(sfh, spec, "f64", local)
+    if not args.no_autotune:
+        B64.autotune()
     B64.solve(tol=TOL, max_iter=MAXIT)
     t64 = time_steps(torch, B64.stream, lambda: B64.solve(tol=TOL, max_iter=MAXIT), max(2, args.steps // 2), 1)
     ms64 = statistics.mean(t64)
@@ -533,7 +537,7 @@ def main():
         "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
                                " x eps{0.3,1.0}, 1-8 RHS, seed 7",
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
-                   "parallelism": f"replicas x{world}",
+                   "parallelism": f"replicas x{world}", "rhs_block": rhs_block,
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,

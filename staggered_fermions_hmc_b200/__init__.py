@@ -136,6 +136,7 @@ SIGNATURES = {
     "sfh_batch_set_stream": (ctypes.c_int, [_VP, _VP]),
     "sfh_batch_get_stream": (_VP, [_VP]),
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_set_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_solve": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
@@ -440,6 +441,12 @@ class Batch:
 
     def set_rhs_block(self, width):
         self._check(self.lib.sfh_batch_set_rhs_block(self.h, width), "set_rhs_block")
+
+    def autotune(self, probe_iters=48):
+        """Pick the fastest RHS-block width for this batch (schedule only)."""
+        w = ctypes.c_int(0)
+        self._check(self.lib.sfh_batch_autotune(self.h, probe_iters, ctypes.byref(w)), "autotune")
+        return w.value
 
     def set_gauge(self, k, U):
         U = _f64(U).reshape(-1)

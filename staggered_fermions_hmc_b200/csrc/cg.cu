@@ -32,6 +32,7 @@
 // r = b - M x_hi with FP64 links and vectors, keeping p.  Mixed lanes
 // converge only on that FP64 true residual.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -44,6 +45,12 @@ namespace sfh {
 namespace {
 
 constexpr int kSums = 4;  // <p,v>, <r,v>, |v|^2, |r|^2
+
+// resident 256-thread blocks per SM the hop kernels are compiled for: one
+// RHS per thread needs few registers, RHS blocks and FP64 / 18-real links more
+template <int GP, int SP, int NB, bool SUMS> struct HopOcc {
+    static constexpr int v = (SP == SP_F64 || NB > 1) ? 2 : ((SUMS || GP == GP_F32_18) ? 3 : 4);
+};
 
 // one RHS pass of a tile: the lanes and their scalars
 template <int NB>
@@ -325,7 +332,7 @@ __device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coor
 
 // t = K p for active lanes (output parity q); thi for reliable updates
 template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, 2) cg_hop1(CgArgs a, int cur)
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v)) cg_hop1(CgArgs a, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
@@ -431,7 +438,7 @@ __device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Co
 
 // own sites: v = m^2 p - K t and the four sums; reliable-update residuals
 template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, 2) cg_hop2(CgArgs a, int cur)
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v)) cg_hop2(CgArgs a, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
@@ -1326,5 +1333,36 @@ extern "C" int sfh_batch_kernel_launches(sfh_batch* b, long* n)
 {
     if (!b || !n) return SFH_ERR_INVALID;
     *n = b->ws.launches;
+    return SFH_OK;
+}
+
+// Autotuner: times a capped solve (probe_iters iterations, no lane converges)
+// for each RHS-block width and keeps the fastest.  Results do not depend on
+// the width; only the schedule does.
+extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width)
+{
+    if (!b || probe_iters < 1) return SFH_ERR_INVALID;
+    cudaSetDevice(b->device);
+    const int widths64[] = {1, 2};
+    const int widths[] = {1, 2, 4, 8};
+    const int* cand = b->prec == SFH_PREC_F64 ? widths64 : widths;
+    const int ncand = b->prec == SFH_PREC_F64 ? 2 : 4;
+    double best = 1e300;
+    int bw = 1;
+    for (int c = 0; c < ncand; ++c) {
+        double t = 0.0;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
+            auto t0 = std::chrono::steady_clock::now();
+            cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], b->stream);
+            if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
+            t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (t < best) {
+            best = t;
+            bw = cand[c];
+        }
+    }
+    b->nb = b->nb2 = bw;
+    if (best_width) *best_width = bw;
     return SFH_OK;
 }

@@ -174,3 +174,20 @@ def test_batch_rhs_block_widths_agree(sfh, orc):
         out.append(np.concatenate([B.solution(0, j) for j in range(6)]))
     for o in out[1:]:
         assert np.array_equal(o, out[0])
+
+
+def test_batch_autotune_keeps_results(sfh, orc):
+    """The autotuner only changes the schedule: solutions are bit-identical."""
+    systems = [((4, 4, 4, 8), 0.1, 3), ((6, 6, 6, 6), 0.2, 2)]
+    outs = []
+    for tune in (False, True):
+        B = sfh.Batch(systems, precision="f32")
+        for k, (dims, m, n) in enumerate(systems):
+            B.set_gauge(k, orc.random_gauge(dims, 0.5, 400 + k))
+            for j in range(n):
+                B.set_rhs(k, j, orc.random_spinor(dims, 500 + 10 * k + j))
+        if tune:
+            assert B.autotune(probe_iters=16) in (1, 2, 4, 8)
+        B.solve(tol=1e-10)
+        outs.append(np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)]))
+    assert np.array_equal(outs[0], outs[1])
