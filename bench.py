@@ -374,6 +374,7 @@ def run_profile_case(args, spec):
     import staggered_fermions_hmc_b200 as sfh
     sfh.load_library()
     B = build_batch(sfh, spec, args.precision, 0)
+    B.set_rhs_block(args.rhs_block or 1)
     for _ in range(args.warmup):
         B.solve(tol=TOL, max_iter=MAXIT)
     st = B.solve(tol=TOL, max_iter=args.maxit, check=False)
@@ -394,7 +395,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--rhs-block", type=int, default=0,
+                    help="RHS-block width of the hop kernels (0: time the widths and keep the fastest)")
     ap.add_argument("--profile-case", action="store_true",
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
@@ -421,7 +423,9 @@ def main():
     total_rhs = sum(s["nrhs"] for s in spec)
 
     B = build_batch(sfh, spec, args.precision, local)
-    rhs_block = B.autotune() if not args.no_autotune else 0
+    if args.rhs_block:
+        B.set_rhs_block(args.rhs_block)
+    rhs_block = args.rhs_block or B.autotune()
 
     def solve():
         B.solve(tol=TOL, max_iter=MAXIT)
@@ -457,7 +461,9 @@ def main():
 
     # FP64 batched CG on the same batch, same kernel family (the comparison)
     B64 = build_batch(sfh, spec, "f64", local)
-    if not args.no_autotune:
+    if args.rhs_block:
+        B64.set_rhs_block(min(args.rhs_block, 2))
+    else:
         B64.autotune()
     B64.solve(tol=TOL, max_iter=MAXIT)
     t64 = time_steps(torch, B64.stream, lambda: B64.solve(tol=TOL, max_iter=MAXIT), max(2, args.steps // 2), 1)

@@ -131,6 +131,18 @@ int sfh_gauge_force(sfh_ctx* ctx, double* F);
 int sfh_fermion_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
 /* Gauge + fermion force: compute_full_force_field (Fermions.cpp:640-659). */
 int sfh_full_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
+/* P <- P - dt F on the context's momenta, F the force selected by `forces`
+ * (SFH_FORCE_GAUGE: compute_gauge_only_force_field, Fermions.cpp:1278;
+ * SFH_FORCE_FERMION: X = (D D^dag)^{-1} phi, Y = D^dag X,
+ * compute_fermion_only_force_field, Fermions.cpp:1114-1134; both:
+ * compute_full_force_field, Fermions.cpp:640-659).  This is the momentum
+ * update of apply_initial_step_to_conjugate_field / the intermediate and
+ * final steps (Fermions.cpp:690-695, 730-735, 767-773).  X_out (may be NULL)
+ * receives the solve, cg_iters (may be NULL) its iterations. */
+#define SFH_FORCE_GAUGE 1
+#define SFH_FORCE_FERMION 2
+int sfh_momentum_kick(sfh_ctx* ctx, int forces, const double* phi, double dt, double tol, int maxit,
+                      int precision, double* X_out, long* cg_iters);
 /* U <- exp(i eps P) U with the context's momenta (Fermions.cpp:699-723 with
  * check = 1, which rejects a non-Hermitian P as the reference does;
  * Fermions.cpp:984-994 with check = 0). */
@@ -178,6 +190,11 @@ int sfh_polyakov_grid(sfh_ctx* ctx, double* out);
 /* <P(m) conj(P(m+d))> over |d|^2 = r2: correlator_over_fixed_distance_fast
  * (Lattice.cpp:886-948).  out2 = (re, im). */
 int sfh_polyakov_correlator(sfh_ctx* ctx, int r2, double* out2);
+/* The same correlator from a given Polyakov grid (as precompute_polyakov_grid
+ * returns it), so callers holding a grid need no gauge field:
+ * correlator_over_fixed_distance_fast(P_grid, r2) (Lattice.cpp:886-948).
+ * The spatial sizes are the context's. */
+int sfh_polyakov_correlator_grid(sfh_ctx* ctx, const double* grid, int r2, double* out2);
 /* Raw gauge checkpoint in the reference layout (save_all_lattice_configs /
  * load_all_lattice_configs for one coupling, Lattice.cpp:810-847). */
 int sfh_save_gauge(sfh_ctx* ctx, const char* path);

@@ -11,7 +11,9 @@ symbolic links to the unmodified reference files, next to:
   * the project's Eigen-API subset header (oracle/eigen_subset).
 
 Only Lattice.cpp, Fermions.cpp, SU3_Sampling.cpp and rng.cpp are compiled,
-together with oracle/ref_harness.cpp.  Outputs go to oracle/_ref/<tag>/ only.
+together with oracle/ref_harness.cpp, and once more with
+oracle/compat_check.cpp and libsfh.so (the side-by-side check of the
+reference-API layer).  Outputs go to oracle/_ref/ only.
 Nothing here runs the reference's own build (submit_roar.slurm).
 
 usage: python oracle/build_ref.py [L T mass tol] ...   (default: the fixture set)
@@ -105,6 +107,53 @@ def build(L, T, mass, tol, verbose=True):
     return exe
 
 
+# (L, T, mass, tol, eps, nsteps) of the reference-API layer check: a short
+# production trajectory (global step size and count) on a 4^3x6 lattice
+COMPAT_CONFIG = (4, 6, 0.2, 1e-12, 0.02, 4)
+COMPAT_SOURCES = [os.path.join(HERE, "compat_check.cpp"),
+                  os.path.join(os.path.dirname(HERE), "include", "sfh_compat.hpp")]
+
+
+def compat_path():
+    L, T, mass, tol, eps, nsteps = COMPAT_CONFIG
+    return os.path.join(OUT, "compat_" + tag(L, T, mass, tol), "compat_check")
+
+
+def build_compat(verbose=True):
+    """Reference sources + oracle/compat_check.cpp, linked with libsfh.so
+    (found at run time through an rpath relative to the binary)."""
+    L, T, mass, tol, eps, nsteps = COMPAT_CONFIG
+    exe = compat_path()
+    d = os.path.dirname(exe)
+    root = os.path.dirname(HERE)
+    pkg = os.path.join(root, "staggered_fermions_hmc_b200")
+    lib = os.path.join(pkg, "libsfh.so")
+    if not os.path.exists(lib):
+        raise RuntimeError("build libsfh.so first")
+    if os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(f) for f in COMPAT_SOURCES):
+        return exe
+    os.makedirs(d, exist_ok=True)
+    for f in SOURCES + HEADERS:
+        link = os.path.join(d, f)
+        if not os.path.lexists(link):
+            os.symlink(os.path.join(REF, f), link)
+    with open(os.path.join(d, "Parameters.h"), "w") as fh:
+        fh.write(parameters_h(L, T, mass, tol, eps=eps, nsteps=nsteps))
+    rpath = "$ORIGIN/" + os.path.relpath(pkg, d)
+    cmd = ["g++", "-std=c++17", "-O2", "-fopenmp", "-w",
+           "-I" + os.path.join(HERE, "eigen_subset"), "-I" + d, "-I" + os.path.join(root, "include"),
+           "-o", exe] + [os.path.join(d, f) for f in SOURCES] + [COMPAT_SOURCES[0]]
+    cmd += ["-L" + pkg, "-lsfh", "-Wl,-rpath," + rpath]
+    if verbose:
+        print("build compat_check", flush=True)
+    try:
+        subprocess.run(cmd, check=True)
+    finally:
+        for f in SOURCES + HEADERS:
+            os.remove(os.path.join(d, f))
+    return exe
+
+
 def exe_path(L, T, mass, tol):
     return os.path.join(OUT, tag(L, T, mass, tol), "ref_harness")
 
@@ -122,6 +171,8 @@ def main(argv):
     todo = [c for c in configs if not os.path.exists(exe_path(*c))]
     with cf.ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
         list(ex.map(lambda c: build(*c), todo))
+    if len(argv) < 4:
+        build_compat()
     return 0
 
 

@@ -33,6 +33,8 @@ SFH_ERR_CUDA = 6
 SFH_ERR_INVALID = 7
 SFH_ERR_NOMEM = 8
 SFH_ERR_IO = 9
+FORCE_GAUGE = 1
+FORCE_FERMION = 2
 
 PREC_F64, PREC_F32, PREC_F16, PREC_F32_18 = 0, 1, 2, 3
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "f32_18": PREC_F32_18}
@@ -114,6 +116,8 @@ SIGNATURES = {
     "sfh_fermion_force": (ctypes.c_int, [_VP, _D, _D, _D]),
     "sfh_full_force": (ctypes.c_int, [_VP, _D, _D, _D]),
     "sfh_link_update": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_momentum_kick": (ctypes.c_int, [_VP, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                         ctypes.c_int, _D, ctypes.POINTER(ctypes.c_long)]),
     "sfh_trp2": (ctypes.c_int, [_VP, _D]),
     "sfh_gauge_action": (ctypes.c_int, [_VP, _D]),
     "sfh_plaquette": (ctypes.c_int, [_VP, _D]),
@@ -125,6 +129,7 @@ SIGNATURES = {
                                           ctypes.POINTER(TrajInfo)]),
     "sfh_polyakov_grid": (ctypes.c_int, [_VP, _D]),
     "sfh_polyakov_correlator": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
+    "sfh_polyakov_correlator_grid": (ctypes.c_int, [_VP, _D, ctypes.c_int, _D]),
     "sfh_save_gauge": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "sfh_load_gauge": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "sfh_smear_stout": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
@@ -363,6 +368,24 @@ class Lattice:
         self._check(st, "leapfrog")
         return X, its.value
 
+    def momentum_kick(self, dt, phi=None, forces="full", tol=1e-12, max_iter=50000, precision="f64"):
+        """P -= dt F on the device momenta, F the gauge, fermion or full force
+        (Fermions.cpp:690-695, 730-735, 767-773).  Returns (X, cg_iters); X is
+        None for the gauge force alone."""
+        bits = {"gauge": FORCE_GAUGE, "fermion": FORCE_FERMION, "full": FORCE_GAUGE | FORCE_FERMION}[forces]
+        its = ctypes.c_long(0)
+        if bits & FORCE_FERMION:
+            phi = _f64(phi).reshape(-1)
+            X = np.empty_like(phi)
+            st = self.lib.sfh_momentum_kick(self.h, bits, _dptr(phi), dt, tol, max_iter, PRECISIONS[precision],
+                                            _dptr(X), ctypes.byref(its))
+        else:
+            X = None
+            st = self.lib.sfh_momentum_kick(self.h, bits, None, dt, tol, max_iter, PRECISIONS[precision],
+                                            None, ctypes.byref(its))
+        self._check(st, "momentum kick")
+        return X, its.value
+
     def hmc_trajectory(self, eps, n_steps, seed, tol=1e-10, max_iter=50000, precision="f64"):
         """single_sweep_monte_carlo_update_WITH_FERMIONS (Fermions.cpp:812-828)."""
         inf = TrajInfo()
@@ -380,6 +403,17 @@ class Lattice:
     def correlator_over_fixed_distance(self, r_squared):
         out = np.empty(2)
         self._check(self.lib.sfh_polyakov_correlator(self.h, int(r_squared), _dptr(out)), "polyakov correlator")
+        return complex(out[0], out[1])
+
+    def correlator_over_fixed_distance_fast(self, P_grid, r_squared):
+        """correlator_over_fixed_distance_fast(P_grid, r2) (Lattice.cpp:886-948)
+        from a grid as precompute_polyakov_grid returns it."""
+        g = np.ascontiguousarray(np.asarray(P_grid, dtype=np.complex128)).view(np.float64)
+        if g.size != 2 * self.dims[0] * self.dims[1] * self.dims[2]:
+            raise ValueError("P_grid must hold one complex value per spatial site")
+        out = np.empty(2)
+        self._check(self.lib.sfh_polyakov_correlator_grid(self.h, _dptr(g), int(r_squared), _dptr(out)),
+                    "polyakov correlator")
         return complex(out[0], out[1])
 
     def save_lattice_config(self, path):

@@ -2,7 +2,8 @@
 
     python -m staggered_fermions_hmc_b200.build [--verbose]
 
-Every csrc/*.cu is compiled by nvcc for sm_100a only and linked into
+Every csrc/*.cu is compiled by nvcc for sm_100a only and, with the host C++
+of csrc/*.cpp (the reference-API layer of include/sfh_compat.hpp), linked into
 staggered_fermions_hmc_b200/libsfh.so.  Objects go to _build/ (untracked).
 """
 import concurrent.futures as cf
@@ -24,12 +25,12 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 
 
 def _sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
 
 
 def _headers():
     return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-            + glob.glob(os.path.join(ROOT, "include", "*.h")))
+            + glob.glob(os.path.join(ROOT, "include", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.hpp")))
 
 
 def _stale(target, deps):
@@ -46,7 +47,7 @@ def build(verbose=False, force=False, extra_flags=()):
     objs = []
     jobs = []
     for s in srcs:
-        o = os.path.join(BUILD, os.path.basename(s)[:-3] + ".o")
+        o = os.path.join(BUILD, os.path.splitext(os.path.basename(s))[0] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             cmd = [NVCC] + ARCH + FLAGS + list(extra_flags) + ["-c", s, "-o", o]

@@ -191,6 +191,33 @@ extern "C" int sfh_full_force(sfh_ctx* c, const double* X, const double* Y, doub
     return links_out(c, c->Fbuf, F);
 }
 
+extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, double dt, double tol, int maxit,
+                                 int precision, double* X_out, long* cg_iters)
+{
+    if (!c || forces < SFH_FORCE_GAUGE || forces > (SFH_FORCE_GAUGE | SFH_FORCE_FERMION)) return SFH_ERR_INVALID;
+    const bool ferm = (forces & SFH_FORCE_FERMION) != 0;
+    if (ferm && (!phi || !(tol > 0.0) || maxit <= 0)) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (cg_iters) *cg_iters = 0;
+    void *X = c->spin[4], *Y = c->spin[2];
+    int st = SFH_OK;
+    if (ferm) {
+        sfh_cg_info inf;
+        std::memset(&inf, 0, sizeof(inf));
+        st = spinor_in(c, phi, c->spin[5]);
+        if (!st) st = ctx_solve_device(c, c->spin[5], X, tol, maxit, precision, &inf);
+        if (cg_iters) *cg_iters = inf.iters;
+        if (st) return st;
+        launch_hop(c->g, GP_F64_18, c->U64, SP_F64, X, SP_F64, Y, X, c->mass, -1.0, 0, 2, c->stream);  // Y = D^dag X
+    }
+    st = cuda_check(c, launch_force(c->g, c->U64, ferm ? X : nullptr, ferm ? Y : nullptr, c->beta, c->c11, c->c12,
+                                    forces, nullptr, c->Pmom, dt, c->stream), "momentum kick");
+    if (st) return st;
+    if (ferm && X_out) return spinor_out(c, X, X_out);
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "momentum kick");
+}
+
 extern "C" int sfh_link_update(sfh_ctx* c, double eps, int check)
 {
     if (!c) return SFH_ERR_INVALID;

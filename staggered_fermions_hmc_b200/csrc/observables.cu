@@ -12,6 +12,7 @@
 // Checkpoints are the reference's raw format: the link array in its own
 // layout as native doubles (save_all_lattice_configs / load_all_lattice_configs
 // for one coupling, Lattice.cpp:810-847).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -96,11 +97,12 @@ extern "C" int sfh_polyakov_grid(sfh_ctx* c, double* out)
     return st;
 }
 
-extern "C" int sfh_polyakov_correlator(sfh_ctx* c, int r2, double* out2)
+namespace {
+
+// displacements d with |d|^2 = r2, |d_i| <= min(floor(sqrt(r2)), L_i/2) and
+// d_i != L_i/2 for even L_i (Lattice.cpp:893-915)
+std::vector<int> correlator_displacements(const int* L, int r2)
 {
-    if (!c || !out2 || r2 < 0) return SFH_ERR_INVALID;
-    cudaSetDevice(c->device);
-    const int* L = c->g.L;
     std::vector<int> disp;
     int root = (int)std::sqrt((double)r2);
     int md[3];
@@ -119,6 +121,14 @@ extern "C" int sfh_polyakov_correlator(sfh_ctx* c, int r2, double* out2)
             }
         }
     }
+    return disp;
+}
+
+// correlator over the grid already in stage (or copied there from host_grid)
+int correlator_on_stage(sfh_ctx* c, const double* host_grid, int r2, double* out2)
+{
+    const int* L = c->g.L;
+    std::vector<int> disp = correlator_displacements(L, r2);
     out2[0] = out2[1] = 0.0;
     int nd = (int)disp.size() / 3;
     if (nd == 0) return SFH_OK;  // Lattice.cpp:910
@@ -127,9 +137,14 @@ extern "C" int sfh_polyakov_correlator(sfh_ctx* c, int r2, double* out2)
     double2* grid = (double2*)c->stage;
     double2* part = grid + ns;
     int* ddisp = (int*)(part + nb);
-    polyakov_grid_kernel<<<(ns + 127) / 128, 128, 0, c->stream>>>(c->g, c->U64, grid);
-    int st = cuda_check(c, cudaMemcpyAsync(ddisp, disp.data(), sizeof(int) * disp.size(), cudaMemcpyHostToDevice,
-                                           c->stream), "polyakov correlator");
+    int st = SFH_OK;
+    if (host_grid)
+        st = cuda_check(c, cudaMemcpyAsync(grid, host_grid, sizeof(double2) * ns, cudaMemcpyHostToDevice, c->stream),
+                        "polyakov correlator");
+    else
+        polyakov_grid_kernel<<<(ns + 127) / 128, 128, 0, c->stream>>>(c->g, c->U64, grid);
+    if (!st) st = cuda_check(c, cudaMemcpyAsync(ddisp, disp.data(), sizeof(int) * disp.size(), cudaMemcpyHostToDevice,
+                                               c->stream), "polyakov correlator");
     if (st) return st;
     polyakov_corr_kernel<<<nb, 256, 0, c->stream>>>(c->g, grid, ddisp, nd, part);
     std::vector<double2> hp(nb);
@@ -146,6 +161,22 @@ extern "C" int sfh_polyakov_correlator(sfh_ctx* c, int r2, double* out2)
     out2[0] = re / n;
     out2[1] = im / n;
     return SFH_OK;
+}
+
+}  // namespace
+
+extern "C" int sfh_polyakov_correlator(sfh_ctx* c, int r2, double* out2)
+{
+    if (!c || !out2 || r2 < 0) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    return correlator_on_stage(c, nullptr, r2, out2);
+}
+
+extern "C" int sfh_polyakov_correlator_grid(sfh_ctx* c, const double* grid, int r2, double* out2)
+{
+    if (!c || !grid || !out2 || r2 < 0) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    return correlator_on_stage(c, grid, r2, out2);
 }
 
 extern "C" int sfh_save_gauge(sfh_ctx* c, const char* path)

@@ -59,3 +59,39 @@ def test_fastdiv_host_emulation():
     for d in list(range(1, 130)) + [192, 256, 1000]:
         for n in [0, 1, d - 1, d, d + 1, 2 ** 31 - 1, 2 ** 28] + [rnd.randrange(2 ** 31) for _ in range(200)]:
             assert fastdiv(n, d) == n // d, (n, d)
+
+
+COMPAT_FUNCTIONS = [
+    "configure", "settings", "shutdown", "apply_DDdagger", "solve_CG_DDdagger", "solve_X_field", "solve_Y_field",
+    "compute_full_force_field", "compute_fermion_only_force_field", "compute_gauge_only_force_field",
+    "compute_Tr_P2", "generate_phi_field", "generate_conjugate_field_configuration",
+    "apply_initial_step_to_conjugate_field", "apply_intermediate_update_to_gauge_field_and_conjugate_field",
+    "apply_final_step", "Monte_carlo_step", "single_sweep_monte_carlo_update_WITH_FERMIONS",
+    "local_initial_half_step", "local_leapfrog_steps", "local_final_step", "local_initial_half_step_fermion",
+    "local_leapfrog_steps_fermion", "local_final_step_fermion", "local_initial_half_step_gauge",
+    "local_leapfrog_steps_gauge", "local_final_step_gauge", "compute_action", "compute_avg_plaq",
+    "precompute_polyakov_grid", "correlator_over_fixed_distance_fast", "save_lattice_configs",
+    "load_lattice_configs", "Apply_HEX_smearing", "Apply_4HEX_smearing",
+]
+
+
+def test_compat_header_declares_and_library_defines():
+    """include/sfh_compat.hpp compiles on its own and every function it
+    declares is defined in libsfh.so (no GPU needed)."""
+    import shutil
+    import subprocess
+    import staggered_fermions_hmc_b200 as sfh
+    hdr = os.path.join(ROOT, "include", "sfh_compat.hpp")
+    text = open(hdr).read()
+    for name in COMPAT_FUNCTIONS:
+        assert re.search(r"\b" + name + r"\(", text), name
+    gxx = shutil.which("g++")
+    if gxx:
+        r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-x", "c++", "-I" + os.path.join(ROOT, "include"),
+                            hdr], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    nm = shutil.which("nm")
+    if nm:
+        out = subprocess.run([nm, "-DC", "--defined-only", sfh.LIB_PATH], capture_output=True, text=True).stdout
+        missing = [n for n in COMPAT_FUNCTIONS if "sfh_compat::" + n + "(" not in out]
+        assert not missing, missing

@@ -87,6 +87,56 @@ def test_forces_vs_oracle(sfh, orc, dims, geps):
     assert abs(lat.compute_action() - orc.action(dims, beta, U)) < 1e-12 * abs(orc.action(dims, beta, U))
 
 
+@pytest.mark.parametrize("forces", ["gauge", "fermion", "full"])
+def test_momentum_kick_vs_oracle(sfh, orc, forces):
+    """P -= dt F (Fermions.cpp:690-695) with F from the oracle's forces on
+    X = (D D^dag)^-1 phi, Y = D^dag X."""
+    dims, mass, beta, dt = (4, 4, 6, 8), 0.2, 4.2, 0.05
+    U = orc.random_gauge(dims, 0.4, 65)
+    P = orc.random_momenta(dims, 66)
+    phi = orc.random_spinor(dims, 67)
+    lat = sfh.Lattice(dims, mass, beta)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    X, its = lat.momentum_kick(dt, phi, forces=forces, tol=1e-13)
+    F = np.zeros_like(P)
+    if forces != "fermion":
+        F += orc.gauge_force(dims, beta, U)
+    if forces != "gauge":
+        Xo, _, _, _ = orc.cg(dims, mass, U, phi, 1e-13)
+        Yo = orc.dirac(dims, mass, U, Xo, dagger=True)
+        assert rel(X, Xo) < 1e-10 and its > 0
+        F += orc.fermion_force(dims, U, Xo, Yo)
+    else:
+        assert X is None and its == 0
+    assert rel(lat.download_momenta(), P - dt * F) < 1e-11
+
+
+def test_staged_leapfrog_equals_fused(sfh, orc):
+    """kick(eps/2), [update(eps), kick(eps)] x (N-1), update(eps), kick(eps/2)
+    through the single-step entries reproduces sfh_leapfrog exactly."""
+    dims, mass, beta, eps, n = (4, 4, 4, 8), 0.2, 4.2, 0.05, 3
+    U = orc.random_gauge(dims, 0.3, 68)
+    P = orc.random_momenta(dims, 69)
+    phi = orc.random_spinor(dims, 70)
+    a = sfh.Lattice(dims, mass, beta)
+    a.upload_gauge(U)
+    a.upload_momenta(P)
+    Xa, _ = a.leapfrog(phi, eps, n, tol=1e-12)
+    b = sfh.Lattice(dims, mass, beta)
+    b.upload_gauge(U)
+    b.upload_momenta(P)
+    b.momentum_kick(0.5 * eps, phi, tol=1e-12)
+    for _ in range(n - 1):
+        b.link_update(eps, check=False)
+        b.momentum_kick(eps, phi, tol=1e-12)
+    b.link_update(eps, check=False)
+    Xb, _ = b.momentum_kick(0.5 * eps, phi, tol=1e-12)
+    assert np.array_equal(a.download_gauge(), b.download_gauge())
+    assert np.array_equal(a.download_momenta(), b.download_momenta())
+    assert np.array_equal(Xa, Xb)
+
+
 def test_link_update_vs_oracle(sfh, orc):
     dims = (4, 4, 4, 8)
     U = orc.random_gauge(dims, 0.7, 71)
@@ -247,6 +297,8 @@ def test_polyakov_vs_reference(sfh, path):
     for r2 in (1, 2, 3):
         c = lat.correlator_over_fixed_distance(r2)
         assert abs(c - complex(*corr[r2 - 1])) <= 1e-12 * max(abs(c), 1.0)
+        cg = lat.correlator_over_fixed_distance_fast(grid, r2)
+        assert cg == c
 
 
 def test_checkpoint_round_trip_is_byte_exact(sfh, orc, tmp_path):
