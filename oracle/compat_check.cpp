@@ -113,7 +113,7 @@ int main(int argc, char** argv)
     const double beta = 4.2;
     sfh_compat::configure(SFH_COMPAT_PARAMETERS());
 
-    std::vector<double> a, b;
+    std::vector<double> a(6 * V), b(6 * V);  // the reference writes into a sized field
     apply_DDdagger(phi, U, a);
     sfh_compat::apply_DDdagger(phi, U, b);
     put("apply_DDdagger", rel(b, a));

@@ -46,10 +46,11 @@ namespace {
 
 constexpr int kSums = 4;  // <p,v>, <r,v>, |v|^2, |r|^2
 
-// resident 256-thread blocks per SM the hop kernels are compiled for: one
-// RHS per thread needs few registers, RHS blocks and FP64 / 18-real links more
+// resident 256-thread blocks per SM the hop kernels are compiled for (at most
+// 85 registers a thread for three): up to two lanes a block fit three blocks,
+// wider RHS groups and FP64 take 128 registers and two
 template <int GP, int SP, int NB, bool SUMS> struct HopOcc {
-    static constexpr int v = (SP == SP_F64 || NB > 1) ? 2 : ((SUMS || GP == GP_F32_18) ? 3 : 4);
+    static constexpr int v = (SP == SP_F64 || NB > 2) ? 2 : 3;
 };
 
 // one RHS pass of a tile: the lanes and their scalars
@@ -89,10 +90,64 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
 }
 
 // stage the tile's system descriptor in shared memory (one tile per block)
-__device__ __forceinline__ void stage_sys(const CgArgs& a, CgSys* s_sys)
+__device__ __forceinline__ void stage_sys(const CgArgs& a, int tile, CgSys* s_sys)
 {
-    if (threadIdx.x == 0) *s_sys = a.sys[__ldg(a.tile_sys + blockIdx.x)];
+    if (threadIdx.x == 0) *s_sys = a.sys[__ldg(a.tile_sys + tile)];
     __syncthreads();
+}
+
+// neighbour checkerboard indices and hop signs of one output site, computed
+// once and shared by every lane of the block
+struct Nbr {
+    int up[4], dn[4];
+    unsigned neg;  // bit 2mu: the forward hop enters with -, bit 2mu+1: the backward hop
+};
+
+__device__ __forceinline__ Nbr neighbours(const Geom& g, const Coord& c)
+{
+    Nbr n;
+    n.neg = 0;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        n.up[mu] = lex_up(g, c, mu) >> 1;
+        n.dn[mu] = lex_dn(g, c, mu) >> 1;
+        const bool eta_neg = eta_sign(c, mu) < 0;
+        const bool wu = (mu == 3) && (c.x[3] == g.L[3] - 1);  // anti-periodic time wrap
+        const bool wd = (mu == 3) && (c.x[3] == 0);
+        if (eta_neg != wu) n.neg |= 1u << (2 * mu);
+        if (!(eta_neg != wd)) n.neg |= 1u << (2 * mu + 1);
+    }
+    return n;
+}
+
+// acc[l] += sum_mu eta bc [U_mu(x) in_l(x+mu) - U_mu(x-mu)^dag in_l(x-mu)] for
+// the lanes with on[l]; each link is loaded once for all lanes of the block
+template <int GP, int SP, int NB>
+__device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, int i, int Vh,
+                                          const void* const (&in)[NB], const bool (&on)[NB],
+                                          Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
+{
+    typedef typename GaugeFmt<GP>::R R;
+    const int nq = 1 - q;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        {
+            const Mat3<R> U = GaugeFmt<GP>::load(Ulo, q, mu, i, Vh);
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (on[l])
+                    vacc(acc[l], mul_mv(U, vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh))),
+                         (n.neg >> (2 * mu)) & 1u);
+        }
+        {
+            const Mat3<R> U = GaugeFmt<GP>::load(Ulo, nq, mu, n.dn[mu], Vh);
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (on[l])
+                    vacc(acc[l], mul_adj_mv(U, vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh))),
+                         (n.neg >> (2 * mu + 1)) & 1u);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -255,7 +310,7 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
     __shared__ CgSys s_sys;
     __shared__ double smem[32 * NB * kSums];
     __shared__ unsigned s_mask;
-    stage_sys(a, &s_sys);
+    stage_sys(a, blockIdx.x, &s_sys);
     const CgSys& S = s_sys;
     const TileInfo ti = decode_tile(S, blockIdx.x);
     const int Vh = S.g.Vh;
@@ -330,69 +385,51 @@ __device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coor
     SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
 }
 
-// t = K p for active lanes (output parity q); thi for reliable updates
+// t = K p for the active lanes of one (tile, RHS group) work item (output
+// parity q); thi for lanes in a reliable update
 template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v)) cg_hop1(CgArgs a, int cur)
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
+    cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
-    stage_sys(a, &s_sys);
+    stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, blockIdx.x);
+    const TileInfo ti = decode_tile(S, it.x);
     if (!ti.valid) return;
-    const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
+    const int q = ti.q, Vh = S.g.Vh;
+    LanePass<NB> P;
+    gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
+    if (!(P.anyA || P.anyR)) return;
     const Coord c = eo_coords(S.g, q, ti.i);
-    for (int base = 0; base < S.nrhs; base += NB) {
-        LanePass<NB> P;
-        gather_pass<NB>(a, S, base, q, true, cur, false, P);
-        if (P.anyA) {
-            const void* pin[NB];
+    if (P.anyA) {
+        const Nbr n = neighbours(S.g, c);
+        const void* pin[NB];
+        bool on[NB];
+        Vec3<R> acc[NB];
 #pragma unroll
-            for (int l = 0; l < NB; ++l) pin[l] = rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P);
-            Vec3<R> acc[NB];
-#pragma unroll
-            for (int l = 0; l < NB; ++l) vzero(acc[l]);
-#pragma unroll 1
-            for (int mu = 0; mu < 4; ++mu) {
-                const bool eta_neg = eta_sign(c, mu) < 0;
-                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-                const bool wd = (mu == 3) && (c.x[3] == 0);
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, lu, Vh));
-                        vacc(acc[l], mul_mv(U, w), eta_neg != wu);
-                    }
-                }
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(pin[l], nq, ld, Vh));
-                        vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
-                    }
-                }
-            }
-#pragma unroll
-            for (int l = 0; l < NB; ++l) {
-                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                Vec3<R> o;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
-                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
-            }
+        for (int l = 0; l < NB; ++l) {
+            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+            pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
+            vzero(acc[l]);
         }
-        if (P.anyR) {
+        hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, pin, on, acc);
 #pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
+        for (int l = 0; l < NB; ++l) {
+            if (!on[l]) continue;
+            Vec3<R> o;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
         }
+    }
+    if (P.anyR) {
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+            if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
     }
 }
 
@@ -436,144 +473,123 @@ __device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Co
     return vdot_re(res, res);
 }
 
-// own sites: v = m^2 p - K t and the four sums; reliable-update residuals
+// own sites of one (tile, RHS group) work item: v = m^2 p - K t and the four
+// sums; reliable-update residuals
 template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v)) cg_hop2(CgArgs a, int cur)
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
+    cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
     __shared__ double smem[32 * NB * kSums];
     __shared__ unsigned s_mask;
-    stage_sys(a, &s_sys);
+    stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, blockIdx.x);
-    const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
-    Coord c;
-    if (ti.valid) c = eo_coords(S.g, q, ti.i);
-    for (int base = 0; base < S.nrhs; base += NB) {
-        LanePass<NB> P;
-        gather_pass<NB>(a, S, base, q, false, cur, false, P);
-        if (!(P.anyA || P.anyR)) continue;  // uniform across the block
-        bool part[NB];
-        double sums[NB * kSums];
+    const TileInfo ti = decode_tile(S, it.x);
+    const int q = ti.q, Vh = S.g.Vh;
+    LanePass<NB> P;
+    gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
+    if (!(P.anyA || P.anyR)) return;  // uniform across the block
+    bool part[NB];
+    double sums[NB * kSums];
+#pragma unroll
+    for (int l = 0; l < NB; ++l) {
+        part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART || P.mode[l] == LM_RU;
+#pragma unroll
+        for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
+    }
+    if (ti.valid && P.anyA) {
+        const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+        const void* tin[NB];
+        bool on[NB];
+        Vec3<R> acc[NB];
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
-            part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART || P.mode[l] == LM_RU;
-#pragma unroll
-            for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
+            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+            tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
+            vzero(acc[l]);
         }
-        if (ti.valid && P.anyA) {
-            const void* tin[NB];
+        hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, tin, on, acc);
+        const R m2 = (R)S.m2;
 #pragma unroll
-            for (int l = 0; l < NB; ++l) tin[l] = rhs_ptr(a, P.rid[l], F_T);
-            Vec3<R> acc[NB];
+        for (int l = 0; l < NB; ++l) {
+            if (!on[l]) continue;
+            Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+            Vec3<RS> p = r;
+            if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
+            else
+                p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+            Vec3<R> pr = vcvt<R>(p), w;
 #pragma unroll
-            for (int l = 0; l < NB; ++l) vzero(acc[l]);
-#pragma unroll 1
-            for (int mu = 0; mu < 4; ++mu) {
-                const bool eta_neg = eta_sign(c, mu) < 0;
-                const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-                const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-                const bool wd = (mu == 3) && (c.x[3] == 0);
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, q, mu, ti.i, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, lu, Vh));
-                        vacc(acc[l], mul_mv(U, w), eta_neg != wu);
-                    }
-                }
-                {
-                    Mat3<R> U = GaugeFmt<GP>::load(S.Ulo, nq, mu, ld, Vh);
-#pragma unroll
-                    for (int l = 0; l < NB; ++l) {
-                        if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                        Vec3<R> w = vcvt<R>(SpinorFmt<SP>::load(tin[l], nq, ld, Vh));
-                        vacc(acc[l], mul_adj_mv(U, w), !(eta_neg != wd));
-                    }
-                }
+            for (int k = 0; k < 3; ++k) {
+                w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
+                w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
             }
-            const R m2 = (R)S.m2;
-#pragma unroll
-            for (int l = 0; l < NB; ++l) {
-                if (P.mode[l] != LM_ACTIVE && P.mode[l] != LM_RESTART) continue;
-                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
-                Vec3<RS> p = r;
-                if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
-                    SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
-                else
-                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
-                Vec3<R> pr = vcvt<R>(p), w;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
-                    w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
-                }
-                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
-                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
-                sums[l * kSums + 0] = vdot_re(p, vn);
-                sums[l * kSums + 1] = vdot_re(r, vn);
-                sums[l * kSums + 2] = vdot_re(vn, vn);
-                sums[l * kSums + 3] = vdot_re(r, r);
-            }
+            Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
+            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+            sums[l * kSums + 0] = vdot_re(p, vn);
+            sums[l * kSums + 1] = vdot_re(r, vn);
+            sums[l * kSums + 2] = vdot_re(vn, vn);
+            sums[l * kSums + 3] = vdot_re(r, r);
         }
-        if (ti.valid && P.anyR) {
+    }
+    if (ti.valid && P.anyR) {
+        const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
-        }
-        block_sum<NB * kSums>(sums, smem);
-        unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
-        if (mask && threadIdx.x < 32) {
+        for (int l = 0; l < NB; ++l)
+            if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+    }
+    block_sum<NB * kSums>(sums, smem);
+    unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
+    if (mask && threadIdx.x < 32) {
 #pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
-        }
-        __syncthreads();
+        for (int l = 0; l < NB; ++l)
+            if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
     }
 }
 
-// own sites of ACTIVE lanes: x += alpha p, r -= alpha v, p = r + beta p
+// own sites of one lane (work item: tile, RHS) if ACTIVE:
+// x += alpha p, r -= alpha v, p = r + beta p
 template <int SP>
-__global__ void __launch_bounds__(kTile) cg_update(CgArgs a, int cur)
+__global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restrict__ items, int cur)
 {
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
     typedef typename SpinorFmt<XP>::R RX;
+    const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
-    stage_sys(a, &s_sys);
+    stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, blockIdx.x);
-    if (!ti.valid) return;
+    const TileInfo ti = decode_tile(S, it.x);
     const int q = ti.q, Vh = S.g.Vh;
-    for (int rhs = 0; rhs < S.nrhs; ++rhs) {
-        CgLane* L = a.lanes + lane_of(S, rhs, q, false);
-        const int mode = ld_int(&L->mode[cur]);
-        if (mode != LM_ACTIVE && mode != LM_RESTART && mode != LM_LAST) continue;
-        if (mode == LM_LAST && threadIdx.x == 0) {  // the last tile retires the lane
-            const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
-            if (atomicAdd(&L->ticket, 1u) == expected - 1) {
-                L->ticket = 0;
-                L->mode[cur] = LM_DONE;
-            }
+    CgLane* L = a.lanes + lane_of(S, it.y, q, false);
+    const int mode = ld_int(&L->mode[cur]);
+    if (mode != LM_ACTIVE && mode != LM_RESTART && mode != LM_LAST) return;
+    if (mode == LM_LAST && threadIdx.x == 0) {  // the last tile retires the lane
+        const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
+        if (atomicAdd(&L->ticket, 1u) == expected - 1) {
+            L->ticket = 0;
+            L->mode[cur] = LM_DONE;
         }
-        const double alpha = ld_dbl(&L->alpha), beta = ld_dbl(&L->beta);
-        const int rid = __ldg(&L->rhs);
-        void* pp = rhs_ptr(a, rid, F_P);
-        void* rp = rhs_ptr(a, rid, F_R);
-        void* xp = rhs_ptr(a, rid, F_XLO);
-        Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
-        Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
-        Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), q, ti.i, Vh);
-        Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
-        SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
-        Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
-        SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
-        SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
     }
+    if (!ti.valid) return;
+    const double alpha = ld_dbl(&L->alpha), beta = ld_dbl(&L->beta);
+    const int rid = __ldg(&L->rhs);
+    void* pp = rhs_ptr(a, rid, F_P);
+    void* rp = rhs_ptr(a, rid, F_R);
+    void* xp = rhs_ptr(a, rid, F_XLO);
+    Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
+    Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
+    Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), q, ti.i, Vh);
+    Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
+    SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
+    Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
+    SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
+    SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
 }
 
 }  // namespace
@@ -583,56 +599,54 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, int cur)
 // ---------------------------------------------------------------------------
 
 typedef void (*InitKernel)(CgArgs);
-typedef void (*HopKernel)(CgArgs, int);
+typedef void (*HopKernel)(CgArgs, const int2*, int);
 
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
+    int nb1, nb2;  // RHS-group widths the hop kernels are compiled for
 };
 
 template <int GP, int SP>
-static HopKernel pick_hop1(int nb)
+static HopKernel pick_hop1(int nb, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 8) return cg_hop1<GP, SP, 8>;
-        if (nb >= 4) return cg_hop1<GP, SP, 4>;
+        if (nb >= 8) { *nb_eff = 8; return cg_hop1<GP, SP, 8>; }
+        if (nb >= 4) { *nb_eff = 4; return cg_hop1<GP, SP, 4>; }
     }
-    if (nb >= 2) return cg_hop1<GP, SP, 2>;
+    if (nb >= 2) { *nb_eff = 2; return cg_hop1<GP, SP, 2>; }
+    *nb_eff = 1;
     return cg_hop1<GP, SP, 1>;
 }
 
 template <int GP, int SP>
-static void pick_hop2(int nb, HopKernel* hop2, InitKernel* init)
+static void pick_hop2(int nb, HopKernel* hop2, InitKernel* init, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4>; *init = cg_init<SP, 4>; return; }
+        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4>; *init = cg_init<SP, 4>; *nb_eff = 4; return; }
     }
-    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2>; *init = cg_init<SP, 2>; return; }
+    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2>; *init = cg_init<SP, 2>; *nb_eff = 2; return; }
     *hop2 = cg_hop2<GP, SP, 1>;
     *init = cg_init<SP, 1>;
+    *nb_eff = 1;
+}
+
+template <int GP, int SP>
+static CgKernels pick_typed(int nb1, int nb2)
+{
+    CgKernels k;
+    k.hop1 = pick_hop1<GP, SP>(nb1, &k.nb1);
+    pick_hop2<GP, SP>(nb2, &k.hop2, &k.init, &k.nb2);
+    k.update = cg_update<SP>;
+    return k;
 }
 
 static CgKernels pick_kernels(int prec, int nb1, int nb2)
 {
-    CgKernels k;
-    if (prec == SFH_PREC_F64) {
-        k.hop1 = pick_hop1<GP_F64_18, SP_F64>(nb1);
-        pick_hop2<GP_F64_18, SP_F64>(nb2, &k.hop2, &k.init);
-        k.update = cg_update<SP_F64>;
-    } else if (prec == SFH_PREC_F32) {
-        k.hop1 = pick_hop1<GP_F32_12, SP_F32>(nb1);
-        pick_hop2<GP_F32_12, SP_F32>(nb2, &k.hop2, &k.init);
-        k.update = cg_update<SP_F32>;
-    } else if (prec == SFH_PREC_F32_18) {
-        k.hop1 = pick_hop1<GP_F32_18, SP_F32>(nb1);
-        pick_hop2<GP_F32_18, SP_F32>(nb2, &k.hop2, &k.init);
-        k.update = cg_update<SP_F32>;
-    } else {
-        k.hop1 = pick_hop1<GP_F16_12, SP_F16>(nb1);
-        pick_hop2<GP_F16_12, SP_F16>(nb2, &k.hop2, &k.init);
-        k.update = cg_update<SP_F16>;
-    }
-    return k;
+    if (prec == SFH_PREC_F64) return pick_typed<GP_F64_18, SP_F64>(nb1, nb2);
+    if (prec == SFH_PREC_F32) return pick_typed<GP_F32_12, SP_F32>(nb1, nb2);
+    if (prec == SFH_PREC_F32_18) return pick_typed<GP_F32_18, SP_F32>(nb1, nb2);
+    return pick_typed<GP_F16_12, SP_F16>(nb1, nb2);
 }
 
 static size_t spinor_bytes(int sp, int Vh)
@@ -674,6 +688,12 @@ struct CgWorkspace {
     int* h_active = nullptr;  // pinned, two slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
     long launches = 0;        // kernels launched by the last solve
+    struct Items {
+        int nb;
+        int2* ptr;
+        int n;
+    };
+    std::vector<Items> item_cache;  // work-item lists by RHS-group width
 
     ~CgWorkspace() { release(); }
     void release_graph()
@@ -694,6 +714,7 @@ struct CgWorkspace {
         ev[0] = ev[1] = nullptr;
         for (void* p : allocs) cudaFree(p);
         allocs.clear();
+        item_cache.clear();
         d_sys = nullptr; d_rhs = nullptr; d_lanes = nullptr;
         d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr;
     }
@@ -798,6 +819,32 @@ static int default_nb(int max_nrhs, int cap)
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
 
+// Work items (tile, first RHS) for RHS groups of width nb: one block each.
+// The groups of a tile are adjacent, so the blocks sharing its links run
+// side by side and the second and later reads of a link hit L2.
+static cudaError_t items_for(CgWorkspace& w, int nb, const int2** d, int* n)
+{
+    for (const CgWorkspace::Items& c : w.item_cache)
+        if (c.nb == nb) {
+            *d = c.ptr;
+            *n = c.n;
+            return cudaSuccess;
+        }
+    std::vector<int2> h;
+    for (const CgSys& S : w.sys)
+        for (int t = 0; t < 2 * S.ntq; ++t)
+            for (int b = 0; b < S.nrhs; b += nb) h.push_back(make_int2(S.tile0 + t, b));
+    int2* p = nullptr;
+    cudaError_t e = w.alloc((void**)&p, sizeof(int2) * std::max<size_t>(1, h.size()));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(p, h.data(), sizeof(int2) * h.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    w.item_cache.push_back({nb, p, (int)h.size()});
+    *d = p;
+    *n = (int)h.size();
+    return cudaSuccess;
+}
+
 static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delta)
 {
     CgArgs a;
@@ -828,7 +875,13 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
         w.g_delta == delta)
         return cudaSuccess;
     w.release_graph();
-    cudaError_t e = cudaGraphCreate(&w.graph, 0);
+    const int2* items[3];
+    int nitems[3];
+    const int widths[3] = {k.nb1, k.nb2, 1};
+    cudaError_t e;
+    for (int ph = 0; ph < 3; ++ph)
+        if ((e = items_for(w, widths[ph], &items[ph], &nitems[ph])) != cudaSuccess) return e;
+    e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
     cudaGraphNode_t prev = nullptr;
     for (int it = 0; it < kChunk; ++it) {
@@ -837,9 +890,9 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
             cudaKernelNodeParams p;
             std::memset(&p, 0, sizeof(p));
             p.func = (void*)(ph == 0 ? k.hop1 : (ph == 1 ? k.hop2 : k.update));
-            p.gridDim = dim3(w.ntiles);
+            p.gridDim = dim3(nitems[ph]);
             p.blockDim = dim3(kTile);
-            void* args[] = {&a, &cur};
+            void* args[] = {&a, (void*)&items[ph], &cur};
             p.kernelParams = args;
             cudaGraphNode_t node;
             e = cudaGraphAddKernelNode(&node, w.graph, prev ? &prev : nullptr, prev ? 1 : 0, &p);
