@@ -218,6 +218,23 @@ def ref_time_solve(exe, U, b):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks(x, world, device="cuda"):
+    """The step time of a replica run: the slowest rank's (all ranks call it
+    in the same order)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, solves_per_rank, ms):
+    """Whole-job solves/s: every rank solves its own copy of the batch."""
+    return world * solves_per_rank / (ms / 1000.0)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -374,7 +391,7 @@ def run_profile_case(args, spec):
     import staggered_fermions_hmc_b200 as sfh
     sfh.load_library()
     B = build_batch(sfh, spec, args.precision, 0)
-    B.set_rhs_block(args.rhs_block or 1)
+    B.set_schedule(args.rhs_block or 2, args.tiles)
     for _ in range(args.warmup):
         B.solve(tol=TOL, max_iter=MAXIT)
     st = B.solve(tol=TOL, max_iter=args.maxit, check=False)
@@ -396,7 +413,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--rhs-block", type=int, default=0,
-                    help="RHS-block width of the hop kernels (0: time the widths and keep the fastest)")
+                    help="RHS-block width of the hop kernels (0: time the schedules and keep the fastest)")
+    ap.add_argument("--tiles", type=int, default=2, help="tiles per block with --rhs-block")
     ap.add_argument("--profile-case", action="store_true",
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
@@ -424,8 +442,10 @@ def main():
 
     B = build_batch(sfh, spec, args.precision, local)
     if args.rhs_block:
-        B.set_rhs_block(args.rhs_block)
-    rhs_block = args.rhs_block or B.autotune()
+        B.set_schedule(args.rhs_block, args.tiles)
+    else:
+        B.autotune()
+    schedule = B.schedule()
 
     def solve():
         B.solve(tol=TOL, max_iter=MAXIT)
@@ -448,12 +468,8 @@ def main():
     infos = [[B.info(k, j) for j in range(s["nrhs"])] for k, s in enumerate(spec)]
     launches_per_solve = B.kernel_launches()
     worst = max(B.true_residual(k, j) for k, s in enumerate(spec) for j in range(s["nrhs"]))
-    ms = statistics.mean(times)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * total_rhs / (ms / 1000.0)
+    ms = max_over_ranks(statistics.mean(times), world)
+    value = replica_value(world, total_rhs, ms)
 
     hbm, peak_kind = peaks()
     alg_bytes = solve_bytes(spec, infos, args.precision)
@@ -462,7 +478,7 @@ def main():
     # FP64 batched CG on the same batch, same kernel family (the comparison)
     B64 = build_batch(sfh, spec, "f64", local)
     if args.rhs_block:
-        B64.set_rhs_block(min(args.rhs_block, 2))
+        B64.set_schedule(min(args.rhs_block, 2), args.tiles)
     else:
         B64.autotune()
     B64.solve(tol=TOL, max_iter=MAXIT)
@@ -503,12 +519,8 @@ def main():
                     host_x[k][j][:] = B.solution(k, j)
 
         te = time_steps(torch, B.stream, e2e_step, max(2, args.steps // 2), 1)
-        mse = statistics.mean(te)
-        if world > 1:
-            t = torch.tensor([mse], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            mse = float(t.item())
-        e2e = {"value": world * total_rhs / (mse / 1000.0), "unit": "solves/s",
+        mse = max_over_ranks(statistics.mean(te), world)
+        e2e = {"value": replica_value(world, total_rhs, mse), "unit": "solves/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
     cpu = None
@@ -543,7 +555,7 @@ def main():
         "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
                                " x eps{0.3,1.0}, 1-8 RHS, seed 7",
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
-                   "parallelism": f"replicas x{world}", "rhs_block": rhs_block,
+                   "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1]},
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,

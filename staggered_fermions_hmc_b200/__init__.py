@@ -142,6 +142,8 @@ SIGNATURES = {
     "sfh_batch_get_stream": (_VP, [_VP]),
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_set_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_solve": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
@@ -477,10 +479,20 @@ class Batch:
         self._check(self.lib.sfh_batch_set_rhs_block(self.h, width), "set_rhs_block")
 
     def autotune(self, probe_iters=48):
-        """Pick the fastest RHS-block width for this batch (schedule only)."""
+        """Pick the fastest RHS-block width and tiles per block for this batch
+        (schedule only); returns the width."""
         w = ctypes.c_int(0)
         self._check(self.lib.sfh_batch_autotune(self.h, probe_iters, ctypes.byref(w)), "autotune")
         return w.value
+
+    def set_schedule(self, width, tiles_per_block):
+        self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block), "set_schedule")
+
+    def schedule(self):
+        """(RHS-block width, tiles per block) the next solve uses."""
+        w, t = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.sfh_batch_get_schedule(self.h, ctypes.byref(w), ctypes.byref(t)), "schedule")
+        return w.value, t.value
 
     def set_gauge(self, k, U):
         U = _f64(U).reshape(-1)

@@ -96,6 +96,28 @@ __device__ __forceinline__ void stage_sys(const CgArgs& a, int tile, CgSys* s_sy
     __syncthreads();
 }
 
+// the tiles of one work item: tpi consecutive tiles of one parity of a system
+struct ItemRange {
+    int first, end;  // tile indices [first, end)
+    int q;           // output parity
+    int slot;        // the item's partial-sum slot of its lanes
+};
+
+// work items per parity of a system's lane (their partial-sum slots)
+__device__ __forceinline__ int item_groups(const CgArgs& a, const CgSys& S) { return (S.ntq + a.tpi - 1) / a.tpi; }
+
+__device__ __forceinline__ ItemRange item_range(const CgArgs& a, const CgSys& S, int first)
+{
+    ItemRange r;
+    const int local = first - S.tile0;
+    r.q = local >= S.ntq ? 1 : 0;
+    const int j = local - r.q * S.ntq;
+    r.first = first;
+    r.end = min(first + a.tpi, S.tile0 + (r.q + 1) * S.ntq);
+    r.slot = r.q * item_groups(a, S) + j / a.tpi;
+    return r;
+}
+
 // neighbour checkerboard indices and hop signs of one output site, computed
 // once and shared by every lane of the block
 struct Nbr {
@@ -156,7 +178,7 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, 
 template <int NB>
 __device__ __forceinline__ unsigned arrive_sums(const CgArgs& a, const CgSys& S, const LanePass<NB>& P,
                                                 const bool (&part)[NB], const double (&sums)[NB * kSums],
-                                                int slot, unsigned* s_mask)
+                                                int slot, unsigned expected, unsigned* s_mask)
 {
     if (threadIdx.x == 0) {
         unsigned mask = 0;
@@ -169,7 +191,6 @@ __device__ __forceinline__ unsigned arrive_sums(const CgArgs& a, const CgSys& S,
                 for (int f = 0; f < kSums; ++f) __stcg(dst + f * nslot, sums[l * kSums + f]);
             }
         __threadfence();
-        const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
             if (!part[l]) continue;
@@ -205,8 +226,9 @@ __device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int la
 {
     CgLane* L = a.lanes + lane;
     const int nslot = 2 * S.ntq;
-    const double* base = a.partial + L->poff + (S.both ? 0 : L->parity * S.ntq);
-    const int n = S.both ? 2 * S.ntq : S.ntq;
+    const int nsq = item_groups(a, S);
+    const double* base = a.partial + L->poff + (S.both ? 0 : L->parity * nsq);
+    const int n = S.both ? 2 * nsq : nsq;
     double s[kSums];
 #pragma unroll
     for (int f = 0; f < kSums; ++f) s[f] = warp_sum_slots(base + f * nslot, n);
@@ -342,7 +364,8 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
             sums[l * kSums + 3] = vdot_re(b, b);
         }
         block_sum<NB * kSums>(sums, smem);
-        unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
+        unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, S.both ? 2u * S.ntq : (unsigned)S.ntq,
+                                        &s_mask);
         if (mask && threadIdx.x < 32) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
@@ -385,8 +408,8 @@ __device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coor
     SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
 }
 
-// t = K p for the active lanes of one (tile, RHS group) work item (output
-// parity q); thi for lanes in a reliable update
+// t = K p for the active lanes of one work item (tpi tiles of output parity
+// q, one RHS group); thi for lanes in a reliable update
 template <int GP, int SP, int NB>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
@@ -398,38 +421,44 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     __shared__ CgSys s_sys;
     stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
-    if (!ti.valid) return;
-    const int q = ti.q, Vh = S.g.Vh;
+    const ItemRange ir = item_range(a, S, it.x);
+    const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
     gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
     if (!(P.anyA || P.anyR)) return;
-    const Coord c = eo_coords(S.g, q, ti.i);
-    if (P.anyA) {
-        const Nbr n = neighbours(S.g, c);
-        const void* pin[NB];
-        bool on[NB];
-        Vec3<R> acc[NB];
+    const void* pin[NB];
+    const void* tout[NB];
+    bool on[NB];
 #pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
-            pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
-            vzero(acc[l]);
-        }
-        hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, pin, on, acc);
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            if (!on[l]) continue;
-            Vec3<R> o;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
-        }
+    for (int l = 0; l < NB; ++l) {
+        on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+        pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
+        tout[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
     }
-    if (P.anyR) {
+    for (int t = ir.first; t < ir.end; ++t) {
+        const TileInfo ti = decode_tile(S, t);
+        if (!ti.valid) break;  // only the parity's last tile is partial
+        const Coord c = eo_coords(S.g, q, ti.i);
+        if (P.anyA) {
+            const Nbr n = neighbours(S.g, c);
+            Vec3<R> acc[NB];
 #pragma unroll
-        for (int l = 0; l < NB; ++l)
-            if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
+            for (int l = 0; l < NB; ++l) vzero(acc[l]);
+            hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, pin, on, acc);
+#pragma unroll
+            for (int l = 0; l < NB; ++l) {
+                if (!on[l]) continue;
+                Vec3<R> o;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
+                SpinorFmt<SP>::store(const_cast<void*>(tout[l]), q, ti.i, Vh, vcvt<RS>(o));
+            }
+        }
+        if (P.anyR) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
+        }
     }
 }
 
@@ -473,8 +502,8 @@ __device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Co
     return vdot_re(res, res);
 }
 
-// own sites of one (tile, RHS group) work item: v = m^2 p - K t and the four
-// sums; reliable-update residuals
+// own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
+// the four sums; reliable-update residuals
 template <int GP, int SP, int NB>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
@@ -488,63 +517,65 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     __shared__ unsigned s_mask;
     stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
-    const int q = ti.q, Vh = S.g.Vh;
+    const ItemRange ir = item_range(a, S, it.x);
+    const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
     gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
     if (!(P.anyA || P.anyR)) return;  // uniform across the block
-    bool part[NB];
+    bool part[NB], on[NB];
     double sums[NB * kSums];
+    const void* tin[NB];
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
         part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART || P.mode[l] == LM_RU;
+        on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+        tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
 #pragma unroll
         for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
     }
-    if (ti.valid && P.anyA) {
-        const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
-        const void* tin[NB];
-        bool on[NB];
-        Vec3<R> acc[NB];
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
-            tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
-            vzero(acc[l]);
-        }
-        hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, tin, on, acc);
-        const R m2 = (R)S.m2;
-#pragma unroll
-        for (int l = 0; l < NB; ++l) {
-            if (!on[l]) continue;
-            Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
-            Vec3<RS> p = r;
-            if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
-                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
-            else
-                p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
-            Vec3<R> pr = vcvt<R>(p), w;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
-                w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
-            }
-            Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
-            sums[l * kSums + 0] = vdot_re(p, vn);
-            sums[l * kSums + 1] = vdot_re(r, vn);
-            sums[l * kSums + 2] = vdot_re(vn, vn);
-            sums[l * kSums + 3] = vdot_re(r, r);
-        }
-    }
-    if (ti.valid && P.anyR) {
+    for (int t = ir.first; t < ir.end; ++t) {
+        const TileInfo ti = decode_tile(S, t);
+        if (!ti.valid) break;  // no barrier inside the loop
         const Coord c = eo_coords(S.g, q, ti.i);
+        if (P.anyA) {
+            const Nbr n = neighbours(S.g, c);
+            Vec3<R> acc[NB];
 #pragma unroll
-        for (int l = 0; l < NB; ++l)
-            if (P.mode[l] == LM_RU) sums[l * kSums + 3] = ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+            for (int l = 0; l < NB; ++l) vzero(acc[l]);
+            hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, tin, on, acc);
+            const R m2 = (R)S.m2;
+#pragma unroll
+            for (int l = 0; l < NB; ++l) {
+                if (!on[l]) continue;
+                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+                Vec3<RS> p = r;
+                if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
+                    SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
+                else
+                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+                Vec3<R> pr = vcvt<R>(p), w;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
+                    w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
+                }
+                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+                sums[l * kSums + 0] += vdot_re(p, vn);
+                sums[l * kSums + 1] += vdot_re(r, vn);
+                sums[l * kSums + 2] += vdot_re(vn, vn);
+                sums[l * kSums + 3] += vdot_re(r, r);
+            }
+        }
+        if (P.anyR) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+        }
     }
     block_sum<NB * kSums>(sums, smem);
-    unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ti.slot, &s_mask);
+    const unsigned nsq = (unsigned)item_groups(a, S);
+    unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ir.slot, S.both ? 2u * nsq : nsq, &s_mask);
     if (mask && threadIdx.x < 32) {
 #pragma unroll
         for (int l = 0; l < NB; ++l)
@@ -552,7 +583,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     }
 }
 
-// own sites of one lane (work item: tile, RHS) if ACTIVE:
+// own sites of one lane (work item: tpi tiles, one RHS) if ACTIVE:
 // x += alpha p, r -= alpha v, p = r + beta p
 template <int SP>
 __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restrict__ items, int cur)
@@ -564,32 +595,37 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restr
     __shared__ CgSys s_sys;
     stage_sys(a, it.x, &s_sys);
     const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
-    const int q = ti.q, Vh = S.g.Vh;
+    const ItemRange ir = item_range(a, S, it.x);
+    const int q = ir.q, Vh = S.g.Vh;
     CgLane* L = a.lanes + lane_of(S, it.y, q, false);
     const int mode = ld_int(&L->mode[cur]);
     if (mode != LM_ACTIVE && mode != LM_RESTART && mode != LM_LAST) return;
-    if (mode == LM_LAST && threadIdx.x == 0) {  // the last tile retires the lane
-        const unsigned expected = S.both ? 2u * S.ntq : (unsigned)S.ntq;
+    if (mode == LM_LAST && threadIdx.x == 0) {  // the last item retires the lane
+        const unsigned nsq = (unsigned)item_groups(a, S);
+        const unsigned expected = S.both ? 2u * nsq : nsq;
         if (atomicAdd(&L->ticket, 1u) == expected - 1) {
             L->ticket = 0;
             L->mode[cur] = LM_DONE;
         }
     }
-    if (!ti.valid) return;
     const double alpha = ld_dbl(&L->alpha), beta = ld_dbl(&L->beta);
     const int rid = __ldg(&L->rhs);
     void* pp = rhs_ptr(a, rid, F_P);
     void* rp = rhs_ptr(a, rid, F_R);
     void* xp = rhs_ptr(a, rid, F_XLO);
-    Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
-    Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
-    Vec3<RS> v = SpinorFmt<SP>::load(rhs_ptr(a, rid, F_V), q, ti.i, Vh);
-    Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
-    SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
-    Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
-    SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
-    SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
+    const void* vp = rhs_ptr(a, rid, F_V);
+    for (int t = ir.first; t < ir.end; ++t) {
+        const TileInfo ti = decode_tile(S, t);
+        if (!ti.valid) break;
+        Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
+        Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
+        Vec3<RS> v = SpinorFmt<SP>::load(vp, q, ti.i, Vh);
+        Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
+        SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
+        Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
+        SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
+        SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
+    }
 }
 
 }  // namespace
@@ -684,12 +720,12 @@ struct CgWorkspace {
     cudaGraphExec_t exec = nullptr;
     CgKernels gk = {};
     double g_tol = -1.0, g_delta = -1.0;
-    int g_maxit = -1;
+    int g_maxit = -1, g_tpi = -1;
     int* h_active = nullptr;  // pinned, two slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
     long launches = 0;        // kernels launched by the last solve
     struct Items {
-        int nb;
+        int nb, tpi;
         int2* ptr;
         int n;
     };
@@ -819,33 +855,35 @@ static int default_nb(int max_nrhs, int cap)
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
 
-// Work items (tile, first RHS) for RHS groups of width nb: one block each.
-// The groups of a tile are adjacent, so the blocks sharing its links run
-// side by side and the second and later reads of a link hit L2.
-static cudaError_t items_for(CgWorkspace& w, int nb, const int2** d, int* n)
+// Work items (first tile, first RHS): tpi tiles of one parity of a system and
+// one RHS group of width nb; one block each.  The groups of a tile range are
+// adjacent, so the blocks sharing its links run side by side and the second
+// and later reads of a link hit L2.
+static cudaError_t items_for(CgWorkspace& w, int nb, int tpi, const int2** d, int* n)
 {
     for (const CgWorkspace::Items& c : w.item_cache)
-        if (c.nb == nb) {
+        if (c.nb == nb && c.tpi == tpi) {
             *d = c.ptr;
             *n = c.n;
             return cudaSuccess;
         }
     std::vector<int2> h;
     for (const CgSys& S : w.sys)
-        for (int t = 0; t < 2 * S.ntq; ++t)
-            for (int b = 0; b < S.nrhs; b += nb) h.push_back(make_int2(S.tile0 + t, b));
+        for (int q = 0; q < 2; ++q)
+            for (int j = 0; j < S.ntq; j += tpi)
+                for (int b = 0; b < S.nrhs; b += nb) h.push_back(make_int2(S.tile0 + q * S.ntq + j, b));
     int2* p = nullptr;
     cudaError_t e = w.alloc((void**)&p, sizeof(int2) * std::max<size_t>(1, h.size()));
     if (e != cudaSuccess) return e;
     e = cudaMemcpy(p, h.data(), sizeof(int2) * h.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
-    w.item_cache.push_back({nb, p, (int)h.size()});
+    w.item_cache.push_back({nb, tpi, p, (int)h.size()});
     *d = p;
     *n = (int)h.size();
     return cudaSuccess;
 }
 
-static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delta)
+static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delta, int tpi)
 {
     CgArgs a;
     a.nsys = w.nsys;
@@ -863,6 +901,7 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.mixed = w.prec != SFH_PREC_F64;
     a.restart = w.prec == SFH_PREC_F16;  // FP16: defect correction (restart after each update)
     a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
+    a.tpi = tpi;
     return a;
 }
 
@@ -871,6 +910,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
                                 double delta)
 {
     if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.g_tol == tol &&
+        w.g_tpi == a.tpi &&
         w.g_maxit == maxit &&
         w.g_delta == delta)
         return cudaSuccess;
@@ -880,7 +920,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     const int widths[3] = {k.nb1, k.nb2, 1};
     cudaError_t e;
     for (int ph = 0; ph < 3; ++ph)
-        if ((e = items_for(w, widths[ph], &items[ph], &nitems[ph])) != cudaSuccess) return e;
+        if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
     e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
     cudaGraphNode_t prev = nullptr;
@@ -906,13 +946,15 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     w.g_tol = tol;
     w.g_maxit = maxit;
     w.g_delta = delta;
+    w.g_tpi = a.tpi;
     return cudaSuccess;
 }
 
 // Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
-// two hop kernels (0 = from the largest RHS count).  Returns a cudaError.
+// two hop kernels (0 = from the largest RHS count); tpi: tiles per block of
+// the iteration kernels (0 = 2).  Returns a cudaError.
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
-                                   cudaStream_t stream)
+                                   int tpi, cudaStream_t stream)
 {
     int max_nrhs = 1;
     for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
@@ -934,7 +976,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     w.h_active[0] = w.h_active[1] = w.nlanes;
     if ((e = cudaMemcpyAsync(w.d_active, &w.h_active[0], sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
-    CgArgs a = make_args(w, tol, maxit, delta);
+    CgArgs a = make_args(w, tol, maxit, delta, tpi > 0 ? tpi : 2);
     CgKernels k = pick_kernels(w.prec, nb1, nb2);
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
@@ -979,7 +1021,7 @@ struct sfh_batch {
     int device = 0, num_sms = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    int prec = 0, flags = 0, nb = 0, nb2 = 0;
+    int prec = 0, flags = 0, nb = 0, nb2 = 0, tpi = 0;
     std::vector<sfh_system_desc> desc;
     std::vector<sfh::Geom> geoms;
     std::vector<void*> U64, U32, U16;
@@ -1160,7 +1202,7 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
 {
     if (!b || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->stream),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stream),
                         "batched CG");
     if (st) return st;
     for (const sfh::CgLane& L : b->ws.lanes_h)
@@ -1279,7 +1321,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");
-    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, c->stream);
+    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
     e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solution");
@@ -1390,32 +1432,53 @@ extern "C" int sfh_batch_kernel_launches(sfh_batch* b, long* n)
 }
 
 // Autotuner: times a capped solve (probe_iters iterations, no lane converges)
-// for each RHS-block width and keeps the fastest.  Results do not depend on
-// the width; only the schedule does.
+// for every RHS-block width and tiles-per-block count and keeps the fastest.
+// Results do not depend on either; only the schedule does.
 extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width)
 {
     if (!b || probe_iters < 1) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
     const int widths64[] = {1, 2};
     const int widths[] = {1, 2, 4, 8};
+    const int tiles[] = {1, 2, 4};
     const int* cand = b->prec == SFH_PREC_F64 ? widths64 : widths;
     const int ncand = b->prec == SFH_PREC_F64 ? 2 : 4;
     double best = 1e300;
-    int bw = 1;
-    for (int c = 0; c < ncand; ++c) {
-        double t = 0.0;
-        for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
-            auto t0 = std::chrono::steady_clock::now();
-            cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], b->stream);
-            if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
-            t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    int bw = 1, bt = 2;
+    for (int c = 0; c < ncand; ++c)
+        for (int tp : tiles) {
+            double t = 0.0;
+            for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
+                auto t0 = std::chrono::steady_clock::now();
+                cudaError_t e =
+                    sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], tp, b->stream);
+                if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
+                t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            }
+            if (t < best) {
+                best = t;
+                bw = cand[c];
+                bt = tp;
+            }
         }
-        if (t < best) {
-            best = t;
-            bw = cand[c];
-        }
-    }
     b->nb = b->nb2 = bw;
+    b->tpi = bt;
     if (best_width) *best_width = bw;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_block)
+{
+    if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
+    b->nb = b->nb2 = width;
+    b->tpi = tiles_per_block;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_get_schedule(sfh_batch* b, int* width, int* tiles_per_block)
+{
+    if (!b) return SFH_ERR_INVALID;
+    if (width) *width = b->nb;
+    if (tiles_per_block) *tiles_per_block = b->tpi;
     return SFH_OK;
 }

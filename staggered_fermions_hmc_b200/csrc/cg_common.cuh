@@ -54,6 +54,7 @@ struct CgArgs {
     double tol2, delta;
     int maxit, maxloop, mixed;
     int restart;  // restart the Krylov space after every residual update
+    int tpi;      // tiles per work item of the iteration kernels
 };
 
 namespace {

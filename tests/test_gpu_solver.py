@@ -160,13 +160,15 @@ def test_batch_full_lattice_matches_single(sfh, orc):
 
 
 def test_batch_rhs_block_widths_agree(sfh, orc):
-    """The RHS-block width changes scheduling only, not results."""
+    """The RHS-block width and the tiles per block change scheduling only,
+    not results (bit-identical solutions)."""
     systems = [((4, 4, 4, 8), 0.1, 6)]
     U = orc.random_gauge(systems[0][0], 0.5, 7)
     out = []
-    for w in (1, 2, 4, 8):
+    for w, tiles in ((1, 1), (2, 2), (4, 3), (8, 4), (2, 1)):
         B = sfh.Batch(systems, precision="f32")
-        B.set_rhs_block(w)
+        B.set_schedule(w, tiles)
+        assert B.schedule() == (w, tiles)
         B.set_gauge(0, U)
         for j in range(6):
             B.set_rhs(0, j, orc.random_spinor(systems[0][0], 300 + j))
