@@ -111,17 +111,30 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# algorithmic bytes of one batched solve (roofline section)
+# algorithmic bytes of one batched solve, per iteration kernel
+#
+# Per lane (one parity system of one RHS) and CG iteration, per site of the
+# lane's parity (s = spinor bytes, sx = bytes of the solution increment):
+#   cg_hop1   reads p, writes t                       2 s
+#   cg_hop2   reads t, r, p, writes v                 4 s
+#   cg_update reads p, r, v, x, writes x, r, p        5 s + 2 sx
+# Links: each hop kernel reads the 8 links of every output site once per
+# (system, parity, iteration), shared by all RHS of the system.  A reliable
+# update (mixed precision) adds an FP64 hop in each hop kernel (8 FP64 links,
+# the FP64 solution or temporary) and the FP64 residual in cg_hop2.
 # ---------------------------------------------------------------------------
 SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24}
 LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72}
+KERNELS = ("cg_hop1", "cg_hop2", "cg_update")
 
 
-def solve_bytes(spec, infos, precision):
+def kernel_bytes(spec, infos, precision):
+    """{kernel: algorithmic bytes over one solve} from the lanes' iteration
+    and reliable-update counts."""
     s = SPINOR_BYTES[precision]
     sx = 48 if precision == "f64" else 24
     lb = LINK_BYTES[precision]
-    total = 0.0
+    out = dict.fromkeys(KERNELS, 0.0)
     for k, sys_ in enumerate(spec):
         Vh = int(np.prod(sys_["dims"])) // 2
         group_iters = [0, 0]
@@ -130,15 +143,32 @@ def solve_bytes(spec, infos, precision):
             for par in (0, 1):
                 it = inf["iters_parity"][par]
                 nru = inf["reliable_updates"] / 2.0
-                # per lane-iteration: P1 3s, P2 5s, P3 4s + 2 sx (x in the solver precision)
-                total += it * Vh * (12 * s + 2 * sx)
+                out["cg_hop1"] += it * Vh * 2 * s
+                out["cg_hop2"] += it * Vh * 4 * s
+                out["cg_update"] += it * Vh * (5 * s + 2 * sx)
                 if precision != "f64":
-                    total += nru * Vh * (2 * 8 * 144 + 288 + 3 * 24 + s)
-                group_iters[par] = max(group_iters[par], it + nru)
-        # links: two hop phases per iteration, 8 links per output site
+                    # FP64 hop of x (links, x_hi + x_lo in, t_hi out); FP64
+                    # hop of t_hi, x_hi, x_lo, b in, x_hi, x_lo, r out
+                    out["cg_hop1"] += nru * Vh * (8 * 144 + 48 + 24 + 48)
+                    out["cg_hop2"] += nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s)
+                group_iters[par] = max(group_iters[par], it)
         for par in (0, 1):
-            total += group_iters[par] * 2 * 8 * lb * Vh
-    return total
+            out["cg_hop1"] += group_iters[par] * 8 * lb * Vh
+            out["cg_hop2"] += group_iters[par] * 8 * lb * Vh
+    return out
+
+
+def solve_bytes(spec, infos, precision):
+    return sum(kernel_bytes(spec, infos, precision).values())
+
+
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
+# algorithmic byte of cg_hop2, f32, RHS groups of 2, 4 tiles per block: one
+# launch of the first 8 systems of the batch with every lane active (553.2 MB
+# of DRAM traffic for 491.0 MB of algorithmic bytes), the capture summarised
+# in profiles/cg_iteration_kernels_f32_batch8_ncu.md.  The bench scales it to
+# its own launches by their algorithmic bytes.
+HOP2_TRAFFIC_PER_ALG_BYTE = 553.2 / 491.0
 
 
 def build_batch(sfh, spec, precision, device):
@@ -474,6 +504,21 @@ def main():
     hbm, peak_kind = peaks()
     alg_bytes = solve_bytes(spec, infos, args.precision)
     achieved = alg_bytes / (ms / 1000.0) / 1e9
+    # per-kernel device time: one more solve with the kernels launched one by
+    # one between CUDA events on the batch's stream (same kernels and results)
+    per_kernel = B.solve_timed(tol=TOL, max_iter=MAXIT)
+    kbytes = kernel_bytes(spec, infos, args.precision)
+    ktot = sum(v[0] for v in per_kernel.values())
+    kernels = {}
+    for name, (kms, kn) in per_kernel.items():
+        kernels[name] = {"launches": kn, "ms_total": kms, "share": kms / ktot if ktot else None,
+                         "alg_bytes_total": kbytes[name],
+                         "GB/s": kbytes[name] / (kms / 1000.0) / 1e9 if kms else None}
+    top = max(kernels, key=lambda n: kernels[n]["ms_total"])
+    top_n = max(1, kernels[top]["launches"])
+    top_gbs = kernels[top]["GB/s"]
+    top_traffic = (HOP2_TRAFFIC_PER_ALG_BYTE * kbytes[top] / top_n
+                   if (HOP2_TRAFFIC_PER_ALG_BYTE and top == "cg_hop2") else None)
 
     # FP64 batched CG on the same batch, same kernel family (the comparison)
     B64 = build_batch(sfh, spec, "f64", local)
@@ -557,10 +602,14 @@ def main():
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
                    "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1]},
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "batched CG solve (cg_hop1 + cg_hop2 + cg_update, graph chunks)",
-                     "alg_bytes_per_launch": alg_bytes},
+        "roofline": {"bound": "hbm", "achieved": top_gbs, "peak": hbm, "unit": "GB/s",
+                     "frac": top_gbs / hbm, "traffic": top_traffic, "peak_kind": peak_kind,
+                     "kernel": top, "alg_bytes_per_launch": kbytes[top] / top_n,
+                     "ms_per_launch": kernels[top]["ms_total"] / top_n},
+        "kernels": kernels,
+        "solve_roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                           "alg_bytes_per_step": alg_bytes,
+                           "what": "all three iteration kernels, graph replay, per timed step"},
         "fp64_batched": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms64,
                          "mixed_over_fp64": value / world / fp64_value},
         "solver": {"iters_mean": float(np.mean(iters)), "iters_max": int(max(iters)),

@@ -249,6 +249,12 @@ int sfh_batch_get_gauge(sfh_batch* batch, int sys, double* links);
 int sfh_batch_get_rhs(sfh_batch* batch, int sys, int rhs, double* phi);
 /* number of kernels the last sfh_batch_solve launched (init + graph chunks) */
 int sfh_batch_kernel_launches(sfh_batch* batch, long* n);
+/* sfh_batch_solve with the iteration kernels launched one by one between CUDA
+ * events on the batch's stream (no graph replay): ms3 / n3 receive the summed
+ * device time and launch count of the three kernels (t = K p; v = m^2 p - K t
+ * with the CG sums; the x, r, p update).  Same kernels, same results; a
+ * measurement aid with no counterpart in the reference. */
+int sfh_batch_solve_timed(sfh_batch* batch, double tol, int maxit, double* ms3, long* n3);
 /* FP64 |b - D D^dag x| / |b| for one solution (diagnostic) */
 int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
 

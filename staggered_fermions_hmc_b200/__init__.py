@@ -143,6 +143,8 @@ SIGNATURES = {
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_solve_timed": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, _D,
+                                             ctypes.POINTER(ctypes.c_long)]),
     "sfh_batch_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_set_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
@@ -484,6 +486,13 @@ class Batch:
         w = ctypes.c_int(0)
         self._check(self.lib.sfh_batch_autotune(self.h, probe_iters, ctypes.byref(w)), "autotune")
         return w.value
+
+    def solve_timed(self, tol=1e-10, max_iter=20000):
+        """Solve with per-kernel CUDA-event timing; returns {kernel: (ms, launches)}."""
+        ms = np.zeros(3)
+        n = (ctypes.c_long * 3)()
+        self._check(self.lib.sfh_batch_solve_timed(self.h, tol, max_iter, _dptr(ms), n), "solve_timed")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(("cg_hop1", "cg_hop2", "cg_update"))}
 
     def set_schedule(self, width, tiles_per_block):
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block), "set_schedule")

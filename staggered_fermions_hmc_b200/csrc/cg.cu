@@ -953,8 +953,15 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
 // Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
 // two hop kernels (0 = from the largest RHS count); tpi: tiles per block of
 // the iteration kernels (0 = 2).  Returns a cudaError.
+// Device time of each iteration kernel over one solve (timed solves launch
+// the kernels one by one between CUDA events instead of replaying the graph).
+struct PhaseTimes {
+    double ms[3];  // hop1, hop2, update
+    long n[3];
+};
+
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
-                                   int tpi, cudaStream_t stream)
+                                   int tpi, cudaStream_t stream, PhaseTimes* timing = nullptr)
 {
     int max_nrhs = 1;
     for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
@@ -981,21 +988,72 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
+    if (!timing && (e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
+    // timed solves: the same kernels and work items, launched one by one
+    const int2* items[3];
+    int nitems[3];
+    const int widths[3] = {k.nb1, k.nb2, 1};
+    HopKernel fn[3] = {k.hop1, k.hop2, k.update};
+    std::vector<cudaEvent_t> tev;
+    if (timing) {
+        for (int ph = 0; ph < 3; ++ph) {
+            if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
+            timing->ms[ph] = 0.0;
+            timing->n[ph] = 0;
+        }
+        tev.resize(2 * (3 * kChunk + 1));
+        for (cudaEvent_t& ev : tev)
+            if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
+    }
+    auto destroy_events = [&]() {
+        for (cudaEvent_t ev : tev)
+            if (ev) cudaEventDestroy(ev);
+        tev.clear();
+    };
+    auto accumulate = [&](int pool) {  // a finished chunk's per-kernel times
+        cudaEvent_t* ev = tev.data() + pool * (3 * kChunk + 1);
+        for (int j = 0; j < 3 * kChunk; ++j) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
+            timing->ms[j % 3] += ms;
+            timing->n[j % 3] += 1;
+        }
+    };
     const int max_chunks = a.maxloop / kChunk + 2;
     // keep one chunk queued ahead of the convergence check
     for (int c = 0; c < max_chunks; ++c) {
-        if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) return e;
+        if (timing) {
+            cudaEvent_t* ev = tev.data() + (c & 1) * (3 * kChunk + 1);
+            if ((e = cudaEventRecord(ev[0], stream)) != cudaSuccess) { destroy_events(); return e; }
+            for (int it = 0; it < kChunk; ++it)
+                for (int ph = 0; ph < 3; ++ph) {
+                    fn[ph]<<<nitems[ph], kTile, 0, stream>>>(a, items[ph], it & 1);
+                    if ((e = cudaEventRecord(ev[3 * it + ph + 1], stream)) != cudaSuccess) {
+                        destroy_events();
+                        return e;
+                    }
+                }
+        } else if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) {
+            return e;
+        }
         w.launches += 3 * kChunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
         if ((e = cudaEventRecord(w.ev[c & 1], stream)) != cudaSuccess) return e;
         if (c >= 1) {
-            if ((e = cudaEventSynchronize(w.ev[(c - 1) & 1])) != cudaSuccess) return e;
-            if (w.h_active[(c - 1) & 1] <= 0) break;
+            if ((e = cudaEventSynchronize(w.ev[(c - 1) & 1])) != cudaSuccess) { destroy_events(); return e; }
+            if (timing) accumulate((c - 1) & 1);
+            if (w.h_active[(c - 1) & 1] <= 0) {
+                if (timing) {  // the chunk queued ahead ran as well
+                    if ((e = cudaEventSynchronize(w.ev[c & 1])) != cudaSuccess) { destroy_events(); return e; }
+                    accumulate(c & 1);
+                }
+                break;
+            }
         }
     }
+    destroy_events();
     e = cudaMemcpyAsync(w.lanes_h.data(), w.d_lanes, sizeof(CgLane) * w.nlanes, cudaMemcpyDeviceToHost, stream);
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(stream);
@@ -1422,6 +1480,23 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
                                            cudaMemcpyDeviceToHost, b->stream), "rhs download");
     if (st) return st;
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
+}
+
+extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double* ms3, long* n3)
+{
+    if (!b || !ms3 || !n3 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    cudaSetDevice(b->device);
+    sfh::PhaseTimes t;
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stream, &t),
+                        "timed batched CG");
+    if (st) return st;
+    for (int k = 0; k < 3; ++k) {
+        ms3[k] = t.ms[k];
+        n3[k] = t.n[k];
+    }
+    for (const sfh::CgLane& L : b->ws.lanes_h)
+        if (L.status != SFH_OK) return L.status;
+    return SFH_OK;
 }
 
 extern "C" int sfh_batch_kernel_launches(sfh_batch* b, long* n)

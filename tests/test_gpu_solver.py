@@ -193,3 +193,25 @@ def test_batch_autotune_keeps_results(sfh, orc):
         B.solve(tol=1e-10)
         outs.append(np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)]))
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_batch_timed_solve_matches_graph_solve(sfh, orc):
+    """The per-kernel timed solve runs the same kernels: identical solutions,
+    every iteration's three kernels timed."""
+    systems = [((4, 4, 4, 8), 0.1, 3), ((6, 6, 6, 6), 0.2, 2)]
+    outs, times = [], None
+    for timed in (False, True):
+        B = sfh.Batch(systems, precision="f32")
+        for k, (dims, m, n) in enumerate(systems):
+            B.set_gauge(k, orc.random_gauge(dims, 0.5, 600 + k))
+            for j in range(n):
+                B.set_rhs(k, j, orc.random_spinor(dims, 700 + 10 * k + j))
+        if timed:
+            times = B.solve_timed(tol=1e-10)
+        else:
+            B.solve(tol=1e-10)
+        outs.append(np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)]))
+    assert np.array_equal(outs[0], outs[1])
+    n = [times[k][1] for k in ("cg_hop1", "cg_hop2", "cg_update")]
+    assert n[0] == n[1] == n[2] > 0
+    assert all(times[k][0] > 0 for k in times)
