@@ -222,7 +222,7 @@ __device__ __forceinline__ void lane_stop(const CgArgs& a, CgLane* L, int cur, i
 // Advance one lane's FP64 scalars from the summed partials of hop2 (warp 0).
 // The update of this iteration (x += alpha p, r -= alpha v, p = r + beta p)
 // still runs for an ACTIVE lane; the decision applies from the next one.
-__device__ __noinline__ void finish_lane(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
+__device__ __forceinline__ void finish_lane(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
 {
     CgLane* L = a.lanes + lane;
     const int nslot = 2 * S.ntq;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
 
 // FP64 hop of x_hi + x_lo for a lane in a reliable update: thi = K x
 template <int XP>
-__device__ __noinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
+__device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     const int nq = 1 - q, Vh = S.g.Vh;
     const void* xhi = rhs_ptr(a, rid, F_XHI);
@@ -435,12 +435,11 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
         pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
         tout[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
     }
-    for (int t = ir.first; t < ir.end; ++t) {
-        const TileInfo ti = decode_tile(S, t);
-        if (!ti.valid) break;  // only the parity's last tile is partial
-        const Coord c = eo_coords(S.g, q, ti.i);
-        if (P.anyA) {
-            const Nbr n = neighbours(S.g, c);
+    if (P.anyA) {
+        for (int t = ir.first; t < ir.end; ++t) {
+            const TileInfo ti = decode_tile(S, t);
+            if (!ti.valid) break;  // only the parity's last tile is partial
+            const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
@@ -454,8 +453,15 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
                 SpinorFmt<SP>::store(const_cast<void*>(tout[l]), q, ti.i, Vh, vcvt<RS>(o));
             }
         }
-        if (P.anyR) {
-#pragma unroll
+    }
+    // reliable updates in a loop of their own: no call inside the hop loop
+    // (a call there makes the compiler keep the hop's registers on the stack)
+    if (P.anyR) {
+        for (int t = ir.first; t < ir.end; ++t) {
+            const TileInfo ti = decode_tile(S, t);
+            if (!ti.valid) break;
+            const Coord c = eo_coords(S.g, q, ti.i);
+#pragma unroll 1
             for (int l = 0; l < NB; ++l)
                 if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
         }
@@ -465,7 +471,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
 // reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
 // r = b - M x_hi; returns the |r|^2 contribution (FP64)
 template <int SP, int XP>
-__device__ __noinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
+__device__ __forceinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     typedef typename SpinorFmt<SP>::R RS;
     const int nq = 1 - q, Vh = S.g.Vh;
@@ -533,12 +539,11 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
 #pragma unroll
         for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
     }
-    for (int t = ir.first; t < ir.end; ++t) {
-        const TileInfo ti = decode_tile(S, t);
-        if (!ti.valid) break;  // no barrier inside the loop
-        const Coord c = eo_coords(S.g, q, ti.i);
-        if (P.anyA) {
-            const Nbr n = neighbours(S.g, c);
+    if (P.anyA) {
+        for (int t = ir.first; t < ir.end; ++t) {
+            const TileInfo ti = decode_tile(S, t);
+            if (!ti.valid) break;  // no barrier inside the loop
+            const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
@@ -567,7 +572,13 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
                 sums[l * kSums + 3] += vdot_re(r, r);
             }
         }
-        if (P.anyR) {
+    }
+    // reliable updates in a loop of their own (no call inside the hop loop)
+    if (P.anyR) {
+        for (int t = ir.first; t < ir.end; ++t) {
+            const TileInfo ti = decode_tile(S, t);
+            if (!ti.valid) break;
+            const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
