@@ -122,28 +122,88 @@ __device__ __forceinline__ ItemRange item_range(const CgArgs& a, const CgSys& S,
 // once and shared by every lane of the block
 struct Nbr {
     int up[4], dn[4];
-    unsigned neg;  // bit 2mu: the forward hop enters with -, bit 2mu+1: the backward hop
+    unsigned eta;  // bit mu: eta_mu(x) = -1
+    bool wu, wd;   // the forward / backward time hop wraps (anti-periodic sign)
 };
 
 __device__ __forceinline__ Nbr neighbours(const Geom& g, const Coord& c)
 {
     Nbr n;
-    n.neg = 0;
+    n.eta = 0;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
         n.up[mu] = lex_up(g, c, mu) >> 1;
         n.dn[mu] = lex_dn(g, c, mu) >> 1;
-        const bool eta_neg = eta_sign(c, mu) < 0;
-        const bool wu = (mu == 3) && (c.x[3] == g.L[3] - 1);  // anti-periodic time wrap
-        const bool wd = (mu == 3) && (c.x[3] == 0);
-        if (eta_neg != wu) n.neg |= 1u << (2 * mu);
-        if (!(eta_neg != wd)) n.neg |= 1u << (2 * mu + 1);
+        if (eta_sign(c, mu) < 0) n.eta |= 1u << mu;
     }
+    n.wu = c.x[3] == g.L[3] - 1;
+    n.wd = c.x[3] == 0;
     return n;
 }
 
-// acc[l] += sum_mu eta bc [U_mu(x) in_l(x+mu) - U_mu(x-mu)^dag in_l(x-mu)] for
-// the lanes with on[l]; each link is loaded once for all lanes of the block
+// w = U v (FIRST) or w += U v, as FMA chains
+template <bool FIRST, typename R>
+__device__ __forceinline__ void mv_add(Vec3<R>& w, const Mat3<R>& U, const Vec3<R>& v)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const Cx<R>* u = &U.e[3 * i];
+        R re = FIRST ? u[0].re * v.c[0].re : fma(u[0].re, v.c[0].re, w.c[i].re);
+        R im = FIRST ? u[0].re * v.c[0].im : fma(u[0].re, v.c[0].im, w.c[i].im);
+        re = fma(-u[0].im, v.c[0].im, re);
+        im = fma(u[0].im, v.c[0].re, im);
+#pragma unroll
+        for (int k = 1; k < 3; ++k) {
+            re = fma(u[k].re, v.c[k].re, re);
+            re = fma(-u[k].im, v.c[k].im, re);
+            im = fma(u[k].re, v.c[k].im, im);
+            im = fma(u[k].im, v.c[k].re, im);
+        }
+        w.c[i] = {re, im};
+    }
+}
+
+// w -= U^dag v, as FMA chains: (U^dag v)_i = sum_k conj(U_ki) v_k
+template <typename R>
+__device__ __forceinline__ void mdv_sub(Vec3<R>& w, const Mat3<R>& U, const Vec3<R>& v)
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R re = w.c[i].re, im = w.c[i].im;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const Cx<R> u = U.e[3 * k + i];
+            re = fma(-u.re, v.c[k].re, re);
+            re = fma(-u.im, v.c[k].im, re);
+            im = fma(-u.re, v.c[k].im, im);
+            im = fma(u.im, v.c[k].re, im);
+        }
+        w.c[i] = {re, im};
+    }
+}
+
+// acc += s w
+template <typename R>
+__device__ __forceinline__ void vfma(Vec3<R>& acc, R s, const Vec3<R>& w)
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc.c[k] = {fma(s, w.c[k].re, acc.c[k].re), fma(s, w.c[k].im, acc.c[k].im)};
+}
+
+template <typename R>
+__device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg)
+{
+    const R s = neg ? R(-1) : R(1);
+    Vec3<R> o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o.c[k] = {s * v.c[k].re, s * v.c[k].im};
+    return o;
+}
+
+// acc[l] += 1/2 sum_mu eta_mu(x) [bc U_mu(x) in_l(x+mu) - bc U_mu(x-mu)^dag in_l(x-mu)]
+// (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
+// link is loaded once for all lanes of the block.  The time-wrap signs apply
+// to the input vectors of mu = 3, eta / 2 to the sum of both hops.
 template <int GP, int SP, int NB>
 __device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, int i, int Vh,
                                           const void* const (&in)[NB], const bool (&on)[NB],
@@ -153,22 +213,31 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, 
     const int nq = 1 - q;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
+        Vec3<R> w[NB];
         {
             const Mat3<R> U = GaugeFmt<GP>::load(Ulo, q, mu, i, Vh);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l])
-                    vacc(acc[l], mul_mv(U, vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh))),
-                         (n.neg >> (2 * mu)) & 1u);
+                if (on[l]) {
+                    Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh));
+                    if (mu == 3) v = vneg_if(v, n.wu);
+                    mv_add<true>(w[l], U, v);
+                }
         }
         {
             const Mat3<R> U = GaugeFmt<GP>::load(Ulo, nq, mu, n.dn[mu], Vh);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l])
-                    vacc(acc[l], mul_adj_mv(U, vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh))),
-                         (n.neg >> (2 * mu + 1)) & 1u);
+                if (on[l]) {
+                    Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh));
+                    if (mu == 3) v = vneg_if(v, n.wd);
+                    mdv_sub(w[l], U, v);
+                }
         }
+        const R s = ((n.eta >> mu) & 1u) ? R(-0.5) : R(0.5);
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+            if (on[l]) vfma(acc[l], s, w[l]);
     }
 }
 
@@ -447,10 +516,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
                 if (!on[l]) continue;
-                Vec3<R> o;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) o.c[k] = {R(0.5) * acc[l].c[k].re, R(0.5) * acc[l].c[k].im};
-                SpinorFmt<SP>::store(const_cast<void*>(tout[l]), q, ti.i, Vh, vcvt<RS>(o));
+                SpinorFmt<SP>::store(const_cast<void*>(tout[l]), q, ti.i, Vh, vcvt<RS>(acc[l]));
             }
         }
     }
@@ -561,8 +627,8 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
                 Vec3<R> pr = vcvt<R>(p), w;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    w.c[k].re = m2 * pr.c[k].re - R(0.5) * acc[l].c[k].re;
-                    w.c[k].im = m2 * pr.c[k].im - R(0.5) * acc[l].c[k].im;
+                    w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
+                    w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
                 }
                 Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
                 SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);

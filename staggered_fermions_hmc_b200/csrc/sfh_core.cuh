@@ -182,15 +182,23 @@ __device__ __forceinline__ Vec3<R> mul_adj_mv(const Mat3<R>& U, const Vec3<R>& v
 template <typename R>
 __device__ __forceinline__ void reconstruct_row2(Mat3<R>& U)
 {
-    // row2 = conj(row0 x row1) for a special-unitary matrix
+    // row2 = conj(row0 x row1) for a special-unitary matrix, as FMA chains:
+    // e[6+m] = conj(a_j b_k - a_k b_j) with (j, k) = (1, 2), (2, 0), (0, 1)
     const Cx<R>* a = &U.e[0];
     const Cx<R>* b = &U.e[3];
-    Cx<R> c0 = cmul(a[1], b[2]), c0b = cmul(a[2], b[1]);
-    Cx<R> c1 = cmul(a[2], b[0]), c1b = cmul(a[0], b[2]);
-    Cx<R> c2 = cmul(a[0], b[1]), c2b = cmul(a[1], b[0]);
-    U.e[6] = {c0.re - c0b.re, -(c0.im - c0b.im)};
-    U.e[7] = {c1.re - c1b.re, -(c1.im - c1b.im)};
-    U.e[8] = {c2.re - c2b.re, -(c2.im - c2b.im)};
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const int j = (m + 1) % 3, k = (m + 2) % 3;
+        R re = a[j].re * b[k].re;
+        re = fma(-a[j].im, b[k].im, re);
+        re = fma(-a[k].re, b[j].re, re);
+        re = fma(a[k].im, b[j].im, re);
+        R im = -a[j].re * b[k].im;
+        im = fma(-a[j].im, b[k].re, im);
+        im = fma(a[k].re, b[j].im, im);
+        im = fma(a[k].im, b[j].re, im);
+        U.e[6 + m] = {re, im};
+    }
 }
 
 // ---------------------------------------------------------------------------
