@@ -421,7 +421,7 @@ def run_profile_case(args, spec):
     import staggered_fermions_hmc_b200 as sfh
     sfh.load_library()
     B = build_batch(sfh, spec, args.precision, 0)
-    B.set_schedule(args.rhs_block or 2, args.tiles)
+    B.set_schedule(args.rhs_block or 2, args.tiles, args.stage)
     for _ in range(args.warmup):
         B.solve(tol=TOL, max_iter=MAXIT)
     st = B.solve(tol=TOL, max_iter=args.maxit, check=False)
@@ -445,6 +445,7 @@ def main():
     ap.add_argument("--rhs-block", type=int, default=0,
                     help="RHS-block width of the hop kernels (0: time the schedules and keep the fastest)")
     ap.add_argument("--tiles", type=int, default=2, help="tiles per block with --rhs-block")
+    ap.add_argument("--stage", type=int, default=0, help="stage links in shared memory with --rhs-block (0/1)")
     ap.add_argument("--profile-case", action="store_true",
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
@@ -472,7 +473,7 @@ def main():
 
     B = build_batch(sfh, spec, args.precision, local)
     if args.rhs_block:
-        B.set_schedule(args.rhs_block, args.tiles)
+        B.set_schedule(args.rhs_block, args.tiles, args.stage)
     else:
         B.autotune()
     schedule = B.schedule()
@@ -523,7 +524,7 @@ def main():
     # FP64 batched CG on the same batch, same kernel family (the comparison)
     B64 = build_batch(sfh, spec, "f64", local)
     if args.rhs_block:
-        B64.set_schedule(min(args.rhs_block, 2), args.tiles)
+        B64.set_schedule(min(args.rhs_block, 2), args.tiles, False)
     else:
         B64.autotune()
     B64.solve(tol=TOL, max_iter=MAXIT)
@@ -600,7 +601,8 @@ def main():
         "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
                                " x eps{0.3,1.0}, 1-8 RHS, seed 7",
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
-                   "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1]},
+                   "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
+                                                                      "staged_links": schedule[2]},
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
         "roofline": {"bound": "hbm", "achieved": top_gbs, "peak": hbm, "unit": "GB/s",
                      "frac": top_gbs / hbm, "traffic": top_traffic, "peak_kind": peak_kind,

@@ -229,14 +229,17 @@ void* sfh_batch_get_stream(sfh_batch* batch);
 /* RHS-block width for the fused hop (0 = automatic); the autotuner sets it */
 int sfh_batch_set_rhs_block(sfh_batch* batch, int width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
- * (1, 2, 4, 8; FP64: 1, 2) and tiles-per-block count (1, 2, 4) on the batch's
- * current inputs and keep the fastest pair.  The schedule never changes the
- * results.  No counterpart in the reference (its solver has no schedule). */
+ * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
+ * (off / on; FP64: off) on the batch's current inputs and keep the fastest.
+ * The schedule never changes the results.  No counterpart in the reference
+ * (its solver has no schedule). */
 int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
-/* The schedule directly: RHS-block width (0 = automatic) and 256-site tiles
- * per block of the iteration kernels (0 = 2); and its current values. */
-int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block);
-int sfh_batch_get_schedule(sfh_batch* batch, int* width, int* tiles_per_block);
+/* The schedule directly: RHS-block width (0 = automatic), 256-site tiles per
+ * block of the iteration kernels (0 = 2), and whether the hop kernels stage
+ * their links in shared memory with asynchronous copies (reduced precisions
+ * only); and its current values. */
+int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
+int sfh_batch_get_schedule(sfh_batch* batch, int* width, int* tiles_per_block, int* stage_links);
 int sfh_batch_set_gauge(sfh_batch* batch, int sys, const double* links);
 int sfh_batch_set_rhs(sfh_batch* batch, int sys, int rhs, const double* phi);
 int sfh_batch_solve(sfh_batch* batch, double tol, int maxit);

@@ -142,10 +142,11 @@ SIGNATURES = {
     "sfh_batch_get_stream": (_VP, [_VP]),
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
-    "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sfh_batch_solve_timed": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, _D,
                                              ctypes.POINTER(ctypes.c_long)]),
-    "sfh_batch_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "sfh_batch_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_gauge": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "sfh_batch_set_rhs": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_solve": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
@@ -494,14 +495,16 @@ class Batch:
         self._check(self.lib.sfh_batch_solve_timed(self.h, tol, max_iter, _dptr(ms), n), "solve_timed")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(("cg_hop1", "cg_hop2", "cg_update"))}
 
-    def set_schedule(self, width, tiles_per_block):
-        self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block), "set_schedule")
+    def set_schedule(self, width, tiles_per_block, stage_links=False):
+        self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, 1 if stage_links else 0),
+                    "set_schedule")
 
     def schedule(self):
-        """(RHS-block width, tiles per block) the next solve uses."""
-        w, t = ctypes.c_int(0), ctypes.c_int(0)
-        self._check(self.lib.sfh_batch_get_schedule(self.h, ctypes.byref(w), ctypes.byref(t)), "schedule")
-        return w.value, t.value
+        """(RHS-block width, tiles per block, links staged) the next solve uses."""
+        w, t, g = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.sfh_batch_get_schedule(self.h, ctypes.byref(w), ctypes.byref(t), ctypes.byref(g)),
+                    "schedule")
+        return w.value, t.value, bool(g.value)
 
     def set_gauge(self, k, U):
         U = _f64(U).reshape(-1)

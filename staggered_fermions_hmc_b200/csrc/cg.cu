@@ -200,13 +200,68 @@ __device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg)
     return o;
 }
 
+// Link staging: every thread copies the 8 links of its site (4 forward at
+// the site, 4 backward at its neighbours) into its own columns of shared
+// memory with asynchronous copies, [direction][element][thread], so that all
+// of them are in flight at once without holding registers.  FP64 links
+// (36 KB per 256 sites and direction pair) are not staged.
+template <int GP> struct StageBytes {
+    static constexpr size_t v = (GP == GP_F64_18) ? 0 : 8 * GaugeFmt<GP>::K * kTile * sizeof(typename GaugeFmt<GP>::E);
+};
+
+template <int N>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem), "n"(N) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int GP>
+__device__ __forceinline__ void stage_links(typename GaugeFmt<GP>::E* s, const void* Ulo, const Nbr& n, int q, int i,
+                                            int Vh)
+{
+    typedef GaugeFmt<GP> F;
+    typedef typename F::E E;
+    const E* U = (const E*)Ulo;
+    const int nq = 1 - q, t = threadIdx.x;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+        for (int k = 0; k < F::K; ++k) {
+            cp_async<sizeof(E)>(s + ((2 * mu) * F::K + k) * kTile + t, U + ((size_t)(q * 4 + mu) * F::K + k) * Vh + i);
+            cp_async<sizeof(E)>(s + ((2 * mu + 1) * F::K + k) * kTile + t,
+                                U + ((size_t)(nq * 4 + mu) * F::K + k) * Vh + n.dn[mu]);
+        }
+}
+
+template <int GP, bool STG>
+__device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typename GaugeFmt<GP>::E* s, const void* Ulo,
+                                                                   int d, int p, int mu, int i, int Vh)
+{
+    typedef GaugeFmt<GP> F;
+    if constexpr (STG) {
+        typename F::E w[F::K];
+#pragma unroll
+        for (int k = 0; k < F::K; ++k) w[k] = s[(d * F::K + k) * kTile + threadIdx.x];
+        return F::unpack(w);
+    } else {
+        return F::load(Ulo, p, mu, i, Vh);
+    }
+}
+
 // acc[l] += 1/2 sum_mu eta_mu(x) [bc U_mu(x) in_l(x+mu) - bc U_mu(x-mu)^dag in_l(x-mu)]
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
-template <int GP, int SP, int NB>
-__device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, int i, int Vh,
-                                          const void* const (&in)[NB], const bool (&on)[NB],
+template <int GP, int SP, int NB, bool STG>
+__device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeFmt<GP>::E* sl, const Nbr& n, int q,
+                                          int i, int Vh, const void* const (&in)[NB], const bool (&on)[NB],
                                           Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
 {
     typedef typename GaugeFmt<GP>::R R;
@@ -215,7 +270,7 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, 
     for (int mu = 0; mu < 4; ++mu) {
         Vec3<R> w[NB];
         {
-            const Mat3<R> U = GaugeFmt<GP>::load(Ulo, q, mu, i, Vh);
+            const Mat3<R> U = hop_link<GP, STG>(sl, Ulo, 2 * mu, q, mu, i, Vh);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
@@ -225,7 +280,7 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const Nbr& n, int q, 
                 }
         }
         {
-            const Mat3<R> U = GaugeFmt<GP>::load(Ulo, nq, mu, n.dn[mu], Vh);
+            const Mat3<R> U = hop_link<GP, STG>(sl, Ulo, 2 * mu + 1, nq, mu, n.dn[mu], Vh);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
@@ -479,10 +534,12 @@ __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const C
 
 // t = K p for the active lanes of one work item (tpi tiles of output parity
 // q, one RHS group); thi for lanes in a reliable update
-template <int GP, int SP, int NB>
+template <int GP, int SP, int NB, bool STG>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
 {
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    typename GaugeFmt<GP>::E* sl = reinterpret_cast<typename GaugeFmt<GP>::E*>(s_dyn);
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
@@ -509,10 +566,14 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
             const TileInfo ti = decode_tile(S, t);
             if (!ti.valid) break;  // only the parity's last tile is partial
             const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+            if constexpr (STG) {
+                stage_links<GP>(sl, S.Ulo, n, q, ti.i, Vh);
+                cp_async_wait_all();
+            }
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
-            hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, pin, on, acc);
+            hop_lanes<GP, SP, NB, STG>(S.Ulo, sl, n, q, ti.i, Vh, pin, on, acc);
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
                 if (!on[l]) continue;
@@ -576,10 +637,12 @@ __device__ __forceinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const
 
 // own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
 // the four sums; reliable-update residuals
-template <int GP, int SP, int NB>
+template <int GP, int SP, int NB, bool STG>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
 {
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    typename GaugeFmt<GP>::E* sl = reinterpret_cast<typename GaugeFmt<GP>::E*>(s_dyn);
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
@@ -610,10 +673,14 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
             const TileInfo ti = decode_tile(S, t);
             if (!ti.valid) break;  // no barrier inside the loop
             const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+            if constexpr (STG) {
+                stage_links<GP>(sl, S.Ulo, n, q, ti.i, Vh);
+                cp_async_wait_all();
+            }
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
-            hop_lanes<GP, SP, NB>(S.Ulo, n, q, ti.i, Vh, tin, on, acc);
+            hop_lanes<GP, SP, NB, STG>(S.Ulo, sl, n, q, ti.i, Vh, tin, on, acc);
             const R m2 = (R)S.m2;
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
@@ -717,49 +784,67 @@ typedef void (*HopKernel)(CgArgs, const int2*, int);
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
-    int nb1, nb2;  // RHS-group widths the hop kernels are compiled for
+    int nb1, nb2;   // RHS-group widths the hop kernels are compiled for
+    size_t smem;    // dynamic shared memory of the hop kernels (staged links)
 };
 
-template <int GP, int SP>
+template <int GP, int SP, bool STG>
 static HopKernel pick_hop1(int nb, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 8) { *nb_eff = 8; return cg_hop1<GP, SP, 8>; }
-        if (nb >= 4) { *nb_eff = 4; return cg_hop1<GP, SP, 4>; }
+        if (nb >= 8) { *nb_eff = 8; return cg_hop1<GP, SP, 8, STG>; }
+        if (nb >= 4) { *nb_eff = 4; return cg_hop1<GP, SP, 4, STG>; }
     }
-    if (nb >= 2) { *nb_eff = 2; return cg_hop1<GP, SP, 2>; }
+    if (nb >= 2) { *nb_eff = 2; return cg_hop1<GP, SP, 2, STG>; }
     *nb_eff = 1;
-    return cg_hop1<GP, SP, 1>;
+    return cg_hop1<GP, SP, 1, STG>;
 }
 
-template <int GP, int SP>
+template <int GP, int SP, bool STG>
 static void pick_hop2(int nb, HopKernel* hop2, InitKernel* init, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4>; *init = cg_init<SP, 4>; *nb_eff = 4; return; }
+        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4, STG>; *init = cg_init<SP, 4>; *nb_eff = 4; return; }
     }
-    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2>; *init = cg_init<SP, 2>; *nb_eff = 2; return; }
-    *hop2 = cg_hop2<GP, SP, 1>;
+    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2, STG>; *init = cg_init<SP, 2>; *nb_eff = 2; return; }
+    *hop2 = cg_hop2<GP, SP, 1, STG>;
     *init = cg_init<SP, 1>;
     *nb_eff = 1;
 }
 
-template <int GP, int SP>
+template <int GP, int SP, bool STG>
 static CgKernels pick_typed(int nb1, int nb2)
 {
     CgKernels k;
-    k.hop1 = pick_hop1<GP, SP>(nb1, &k.nb1);
-    pick_hop2<GP, SP>(nb2, &k.hop2, &k.init, &k.nb2);
+    k.hop1 = pick_hop1<GP, SP, STG>(nb1, &k.nb1);
+    pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
+    k.smem = STG ? StageBytes<GP>::v : 0;
     return k;
 }
 
-static CgKernels pick_kernels(int prec, int nb1, int nb2)
+template <int GP, int SP>
+static CgKernels pick_staged(int nb1, int nb2, bool stage)
 {
-    if (prec == SFH_PREC_F64) return pick_typed<GP_F64_18, SP_F64>(nb1, nb2);
-    if (prec == SFH_PREC_F32) return pick_typed<GP_F32_12, SP_F32>(nb1, nb2);
-    if (prec == SFH_PREC_F32_18) return pick_typed<GP_F32_18, SP_F32>(nb1, nb2);
-    return pick_typed<GP_F16_12, SP_F16>(nb1, nb2);
+    if constexpr (GP == GP_F64_18) {
+        return pick_typed<GP, SP, false>(nb1, nb2);
+    } else {
+        return stage ? pick_typed<GP, SP, true>(nb1, nb2) : pick_typed<GP, SP, false>(nb1, nb2);
+    }
+}
+
+static CgKernels pick_kernels(int prec, int nb1, int nb2, bool stage)
+{
+    CgKernels k;
+    if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false);
+    else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage);
+    else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage);
+    else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stage);
+    if (k.smem) {  // opt in to the staged kernels' shared memory (idempotent)
+        cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+        cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+    }
+    return k;
 }
 
 static size_t spinor_bytes(int sp, int Vh)
@@ -1009,6 +1094,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
             p.func = (void*)(ph == 0 ? k.hop1 : (ph == 1 ? k.hop2 : k.update));
             p.gridDim = dim3(nitems[ph]);
             p.blockDim = dim3(kTile);
+            p.sharedMemBytes = ph < 2 ? (unsigned)k.smem : 0u;
             void* args[] = {&a, (void*)&items[ph], &cur};
             p.kernelParams = args;
             cudaGraphNode_t node;
@@ -1029,7 +1115,8 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
 
 // Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
 // two hop kernels (0 = from the largest RHS count); tpi: tiles per block of
-// the iteration kernels (0 = 2).  Returns a cudaError.
+// the iteration kernels (0 = 2); stage: hop kernels stage their links in
+// shared memory (reduced precisions only).  Returns a cudaError.
 // Device time of each iteration kernel over one solve (timed solves launch
 // the kernels one by one between CUDA events instead of replaying the graph).
 struct PhaseTimes {
@@ -1038,7 +1125,7 @@ struct PhaseTimes {
 };
 
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
-                                   int tpi, cudaStream_t stream, PhaseTimes* timing = nullptr)
+                                   int tpi, bool stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
 {
     int max_nrhs = 1;
     for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
@@ -1061,7 +1148,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     if ((e = cudaMemcpyAsync(w.d_active, &w.h_active[0], sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
     CgArgs a = make_args(w, tol, maxit, delta, tpi > 0 ? tpi : 2);
-    CgKernels k = pick_kernels(w.prec, nb1, nb2);
+    CgKernels k = pick_kernels(w.prec, nb1, nb2, stage);
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1104,7 +1191,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
             if ((e = cudaEventRecord(ev[0], stream)) != cudaSuccess) { destroy_events(); return e; }
             for (int it = 0; it < kChunk; ++it)
                 for (int ph = 0; ph < 3; ++ph) {
-                    fn[ph]<<<nitems[ph], kTile, 0, stream>>>(a, items[ph], it & 1);
+                    fn[ph]<<<nitems[ph], kTile, ph < 2 ? k.smem : 0, stream>>>(a, items[ph], it & 1);
                     if ((e = cudaEventRecord(ev[3 * it + ph + 1], stream)) != cudaSuccess) {
                         destroy_events();
                         return e;
@@ -1156,7 +1243,7 @@ struct sfh_batch {
     int device = 0, num_sms = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    int prec = 0, flags = 0, nb = 0, nb2 = 0, tpi = 0;
+    int prec = 0, flags = 0, nb = 0, nb2 = 0, tpi = 0, stage_links = 0;
     std::vector<sfh_system_desc> desc;
     std::vector<sfh::Geom> geoms;
     std::vector<void*> U64, U32, U16;
@@ -1337,7 +1424,7 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
 {
     if (!b || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stream),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stage_links != 0, b->stream),
                         "batched CG");
     if (st) return st;
     for (const sfh::CgLane& L : b->ws.lanes_h)
@@ -1456,7 +1543,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");
-    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, 0, c->stream);
+    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, 0, false, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
     e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solution");
@@ -1564,7 +1651,7 @@ extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double
     if (!b || !ms3 || !n3 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
     sfh::PhaseTimes t;
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stream, &t),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, 0.1, b->nb, b->nb2, b->tpi, b->stage_links != 0, b->stream, &t),
                         "timed batched CG");
     if (st) return st;
     for (int k = 0; k < 3; ++k) {
@@ -1593,44 +1680,50 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int widths64[] = {1, 2};
     const int widths[] = {1, 2, 4, 8};
     const int tiles[] = {1, 2, 4};
-    const int* cand = b->prec == SFH_PREC_F64 ? widths64 : widths;
-    const int ncand = b->prec == SFH_PREC_F64 ? 2 : 4;
+    const bool f64 = b->prec == SFH_PREC_F64;
+    const int* cand = f64 ? widths64 : widths;
+    const int ncand = f64 ? 2 : 4;
     double best = 1e300;
-    int bw = 1, bt = 2;
-    for (int c = 0; c < ncand; ++c)
-        for (int tp : tiles) {
-            double t = 0.0;
-            for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
-                auto t0 = std::chrono::steady_clock::now();
-                cudaError_t e =
-                    sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], tp, b->stream);
-                if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
-                t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    int bw = 1, bt = 2, bs = 0;
+    for (int stage = 0; stage < (f64 ? 1 : 2); ++stage)
+        for (int c = 0; c < ncand; ++c)
+            for (int tp : tiles) {
+                double t = 0.0;
+                for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
+                    auto t0 = std::chrono::steady_clock::now();
+                    cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], tp,
+                                                         stage != 0, b->stream);
+                    if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
+                    t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                }
+                if (t < best) {
+                    best = t;
+                    bw = cand[c];
+                    bt = tp;
+                    bs = stage;
+                }
             }
-            if (t < best) {
-                best = t;
-                bw = cand[c];
-                bt = tp;
-            }
-        }
     b->nb = b->nb2 = bw;
     b->tpi = bt;
+    b->stage_links = bs;
     if (best_width) *best_width = bw;
     return SFH_OK;
 }
 
-extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_block)
+extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_block, int stage_links)
 {
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
+    b->stage_links = stage_links ? 1 : 0;
     return SFH_OK;
 }
 
-extern "C" int sfh_batch_get_schedule(sfh_batch* b, int* width, int* tiles_per_block)
+extern "C" int sfh_batch_get_schedule(sfh_batch* b, int* width, int* tiles_per_block, int* stage_links)
 {
     if (!b) return SFH_ERR_INVALID;
     if (width) *width = b->nb;
     if (tiles_per_block) *tiles_per_block = b->tpi;
+    if (stage_links) *stage_links = b->stage_links;
     return SFH_OK;
 }

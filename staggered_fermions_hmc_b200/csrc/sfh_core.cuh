@@ -340,6 +340,8 @@ template <int GP> struct GaugeFmt;
 
 template <> struct GaugeFmt<GP_F64_18> {
     typedef double R;
+    typedef double2 E;
+    static constexpr int K = 9;
     static constexpr size_t link_bytes = 144;
     __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
     {
@@ -356,55 +358,78 @@ template <> struct GaugeFmt<GP_F64_18> {
 
 template <> struct GaugeFmt<GP_F32_18> {
     typedef float R;
+    typedef float2 E;  // storage element: K of them per link, [p][mu][k][i]
+    static constexpr int K = 9;
     static constexpr size_t link_bytes = 72;
-    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    __device__ static __forceinline__ Mat3<R> unpack(const E (&w)[K])
     {
-        const float2* b = (const float2*)base + ((size_t)(p * 4 + mu) * 9) * Vh + i;
         Mat3<R> U;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            float2 w = __ldg(b + (size_t)k * Vh);
-            U.e[k] = {w.x, w.y};
-        }
+        for (int k = 0; k < 9; ++k) U.e[k] = {w[k].x, w[k].y};
         return U;
+    }
+    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    {
+        const E* b = (const E*)base + ((size_t)(p * 4 + mu) * K) * Vh + i;
+        E w[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) w[k] = __ldg(b + (size_t)k * Vh);
+        return unpack(w);
     }
 };
 
 template <> struct GaugeFmt<GP_F32_12> {
     typedef float R;
+    typedef float4 E;
+    static constexpr int K = 3;
     static constexpr size_t link_bytes = 48;
-    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    __device__ static __forceinline__ Mat3<R> unpack(const E (&w)[K])
     {
-        const float4* b = (const float4*)base + ((size_t)(p * 4 + mu) * 3) * Vh + i;
         Mat3<R> U;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            float4 w = __ldg(b + (size_t)k * Vh);
-            U.e[2 * k] = {w.x, w.y};
-            U.e[2 * k + 1] = {w.z, w.w};
+            U.e[2 * k] = {w[k].x, w[k].y};
+            U.e[2 * k + 1] = {w[k].z, w[k].w};
         }
         reconstruct_row2(U);
         return U;
+    }
+    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    {
+        const E* b = (const E*)base + ((size_t)(p * 4 + mu) * K) * Vh + i;
+        E w[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) w[k] = __ldg(b + (size_t)k * Vh);
+        return unpack(w);
     }
 };
 
 template <> struct GaugeFmt<GP_F16_12> {
     typedef float R;
+    typedef uint2 E;
+    static constexpr int K = 3;
     static constexpr size_t link_bytes = 24;
-    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    __device__ static __forceinline__ Mat3<R> unpack(const E (&w)[K])
     {
-        const uint2* b = (const uint2*)base + ((size_t)(p * 4 + mu) * 3) * Vh + i;
         Mat3<R> U;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            uint2 w = __ldg(b + (size_t)k * Vh);
-            float2 f0 = __half22float2(*reinterpret_cast<__half2*>(&w.x));
-            float2 f1 = __half22float2(*reinterpret_cast<__half2*>(&w.y));
+            uint2 x = w[k];
+            float2 f0 = __half22float2(*reinterpret_cast<__half2*>(&x.x));
+            float2 f1 = __half22float2(*reinterpret_cast<__half2*>(&x.y));
             U.e[2 * k] = {f0.x, f0.y};
             U.e[2 * k + 1] = {f1.x, f1.y};
         }
         reconstruct_row2(U);
         return U;
+    }
+    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    {
+        const E* b = (const E*)base + ((size_t)(p * 4 + mu) * K) * Vh + i;
+        E w[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) w[k] = __ldg(b + (size_t)k * Vh);
+        return unpack(w);
     }
 };
 

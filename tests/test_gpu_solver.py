@@ -160,15 +160,15 @@ def test_batch_full_lattice_matches_single(sfh, orc):
 
 
 def test_batch_rhs_block_widths_agree(sfh, orc):
-    """The RHS-block width and the tiles per block change scheduling only,
-    not results (bit-identical solutions)."""
+    """The RHS-block width, the tiles per block and link staging change
+    scheduling only, not results (bit-identical solutions)."""
     systems = [((4, 4, 4, 8), 0.1, 6)]
     U = orc.random_gauge(systems[0][0], 0.5, 7)
     out = []
-    for w, tiles in ((1, 1), (2, 2), (4, 3), (8, 4), (2, 1)):
+    for w, tiles, stage in ((1, 1, False), (2, 2, True), (4, 3, False), (8, 4, True), (2, 1, True)):
         B = sfh.Batch(systems, precision="f32")
-        B.set_schedule(w, tiles)
-        assert B.schedule() == (w, tiles)
+        B.set_schedule(w, tiles, stage)
+        assert B.schedule() == (w, tiles, stage)
         B.set_gauge(0, U)
         for j in range(6):
             B.set_rhs(0, j, orc.random_spinor(systems[0][0], 300 + j))
@@ -190,6 +190,7 @@ def test_batch_autotune_keeps_results(sfh, orc):
                 B.set_rhs(k, j, orc.random_spinor(dims, 500 + 10 * k + j))
         if tune:
             assert B.autotune(probe_iters=16) in (1, 2, 4, 8)
+            assert B.schedule()[1] in (1, 2, 4)
         B.solve(tol=1e-10)
         outs.append(np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)]))
     assert np.array_equal(outs[0], outs[1])
