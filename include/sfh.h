@@ -143,6 +143,19 @@ int sfh_full_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
 #define SFH_FORCE_FERMION 2
 int sfh_momentum_kick(sfh_ctx* ctx, int forces, const double* phi, double dt, double tol, int maxit,
                       int precision, double* X_out, long* cg_iters);
+/* Stout-smeared fermion links (no counterpart in the reference, which has no
+ * smeared-link HMC): with nlevels > 0 the fermion operator of sfh_leapfrog,
+ * sfh_hmc_trajectory and sfh_momentum_kick uses V = stout^nlevels(U) with
+ * parameter rho (plaquette staples, as sfh_smear_stout); the gauge action
+ * stays on U, and the fermion force reaches U by the chain rule through the
+ * levels (Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501).
+ * nlevels = 0 (the default) restores thin links.  At most 16 levels. */
+int sfh_set_fermion_smearing(sfh_ctx* ctx, double rho, int nlevels);
+/* The fermion force on the thin links under that smearing: X = (D D^dag)^{-1}
+ * phi and Y = D^dag X with V, compute_fermion_force_at_link (Fermions.cpp:443-515)
+ * on V, then the chain rule.  F: link-field layout; X_out may be NULL. */
+int sfh_smeared_fermion_force(sfh_ctx* ctx, const double* phi, double tol, int maxit, int precision,
+                              double* F, double* X_out);
 /* U <- exp(i eps P) U with the context's momenta (Fermions.cpp:699-723 with
  * check = 1, which rejects a non-Hermitian P as the reference does;
  * Fermions.cpp:984-994 with check = 0). */

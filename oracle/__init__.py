@@ -73,6 +73,7 @@ def lib():
             "orc_polyakov_corr": (None, [dims, D, ctypes.c_int, D]),
             "orc_stout": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_int, D]),
             "orc_hex": (ctypes.c_int, [dims, D, D]),
+            "orc_stout_force": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_int, D, D, D]),
             "orc_exp_field": (ctypes.c_int, [ctypes.c_long, ctypes.c_double, D, D]),
         }
         for name, (res, args) in sig.items():
@@ -235,6 +236,16 @@ def stout(dims, rho, n_levels, U):
     if st != ORC_OK:
         raise OracleError(st, "stout")
     return U
+
+
+def stout_force(dims, rho, n_levels, U, F_top):
+    """Thin-link force of an action on n_levels stout levels of U, given the
+    force on the smeared links (chain rule; no reference counterpart)."""
+    F = np.empty_like(U)
+    st = lib().orc_stout_force(_dims(dims), rho, n_levels, _d(U), _d(F_top), _d(F))
+    if st != ORC_OK:
+        raise OracleError(st, "stout_force")
+    return F
 
 
 def hex_smear(dims, U, alphas=(0.95, 0.76, 0.38)):

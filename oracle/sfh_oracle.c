@@ -831,6 +831,276 @@ int orc_stout(const int dims[4], double rho, int n_levels, double* U)
     return bad ? ORC_ERR_DOMAIN : ORC_OK;
 }
 
+/* ------------------------------------------------------------------------ */
+/* smeared-link force: the chain rule through stout levels                   */
+/* ------------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference (it has no smeared-link HMC).  Method of
+ * Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501, restated:
+ *
+ *   level k:  C = sum of plaquette staples of U (orientation as orc_stout),
+ *             Q = -i rho TA(C U^dag),  V = exp(iQ) U.
+ *   With dS = sum_links Re Tr(G dV) (G = dS/dV), the generator form of the
+ *   reference's force (dS/deps = 2 Tr(F H) under U -> exp(i eps H) U) gives
+ *   G = -2i V^dag F at the top level and F = 1/2 TH(i U G) at the bottom.
+ *   One level down:
+ *     Re Tr(U G d exp(iQ)) = Re Tr(L dQ),  L = TH(b0 Q^2 + b1 Q + f1 B + f2 (Q B + B Q)),
+ *       B = U G, b0 = sum_j Tr(B Q^j) df_j/dc0, b1 = sum_j Tr(B Q^j) df_j/dc1
+ *       (exp(iQ) = f0 + f1 Q + f2 Q^2, c0 = det Q, c1 = Tr Q^2 / 2);
+ *     K = -i rho L, W = U^dag K;
+ *     dS/dU(link) = G exp(iQ) - C^dag K + the staple terms of W (stout_gather).
+ */
+
+/* xi1(w) = cos(w)/w^2 - sin(w)/w^3, series below 0.05 */
+static double xi1_stable(double w)
+{
+    if (fabs(w) < 0.05) {
+        double w2 = w * w;
+        return -1.0 / 3.0 + w2 / 30.0 - w2 * w2 / 840.0 + w2 * w2 * w2 / 45360.0;
+    }
+    return (cos(w) - sin(w) / w) / (w * w);
+}
+
+/* f_j of exp(iQ) and df_j/dc0, df_j/dc1.  h_j as in expiq_cx; with
+ * D = 9u^2 - w^2, f_j = h_j / D, dh_j/dw = w g_j (h_j are even in w),
+ * c0 = 2u(u^2 - w^2), c1 = 3u^2 + w^2. */
+static int expiq_coeffs(const cx* Q, cx f[3], cx d0[3], cx d1[3])
+{
+    cx Q2[9], Q3[9];
+    m_mul(Q, Q, Q2);
+    m_mul(Q2, Q, Q3);
+    double c0 = creal(m_tr(Q3)) / 3.0;
+    double c1 = 0.5 * creal(m_tr(Q2));
+    if (c1 < 0.0) return ORC_ERR_DOMAIN;
+    if (c1 < 1e-12) {  /* exp(iQ) = 1 + iQ - Q^2/2 to this order */
+        f[0] = 1; f[1] = I; f[2] = -0.5;
+        for (int j = 0; j < 3; ++j) d0[j] = d1[j] = 0;
+        return ORC_OK;
+    }
+    int neg = c0 < 0.0;
+    c0 = fabs(c0);
+    double c0max = 2.0 * sqrt(c1 * c1 * c1 / 27.0);
+    double ratio = c0max > 0.0 ? c0 / c0max : 1.0;
+    if (ratio > 1.0) ratio = 1.0;
+    double theta = acos(ratio);
+    double w = sqrt(c1) * sin(theta / 3.0);
+    double u = sqrt(c1 / 3.0) * cos(theta / 3.0);
+    double u2 = u * u, w2 = w * w;
+    double xi0 = sinc_stable(w), xi1 = xi1_stable(w), cw = cos(w);
+    cx E = cexp(2.0 * I * u), e = cexp(-I * u);
+    cx P0 = 8.0 * u2 * cw + 2.0 * I * u * (3.0 * u2 + w2) * xi0;
+    cx P1 = 2.0 * u * cw - I * (3.0 * u2 - w2) * xi0;
+    cx P2 = cw + 3.0 * I * u * xi0;
+    cx h[3], hu[3], g[3];
+    h[0] = (u2 - w2) * E + e * P0;
+    h[1] = 2.0 * u * E - e * P1;
+    h[2] = E - e * P2;
+    hu[0] = 2.0 * u * E + 2.0 * I * (u2 - w2) * E - I * e * P0 +
+            e * (16.0 * u * cw + 2.0 * I * (9.0 * u2 + w2) * xi0);
+    hu[1] = 2.0 * E + 4.0 * I * u * E + I * e * P1 - e * (2.0 * cw - 6.0 * I * u * xi0);
+    hu[2] = 2.0 * I * E + I * e * P2 - e * (3.0 * I * xi0);
+    g[0] = -2.0 * E + e * (-8.0 * u2 * xi0 + 2.0 * I * u * (2.0 * xi0 + (3.0 * u2 + w2) * xi1));
+    g[1] = e * (2.0 * u * xi0 - 2.0 * I * xi0 + I * (3.0 * u2 - w2) * xi1);
+    g[2] = e * (xi0 - 3.0 * I * u * xi1);
+    double D = 9.0 * u2 - w2;
+    for (int j = 0; j < 3; ++j) {
+        cx fu = (hu[j] * D - 18.0 * u * h[j]) / (D * D);
+        cx k = (g[j] * D + 2.0 * h[j]) / (D * D);
+        f[j] = h[j] / D;
+        d0[j] = (fu - 3.0 * u * k) / (2.0 * D);
+        d1[j] = (u * fu + 0.5 * (3.0 * u2 - w2) * k) / D;
+    }
+    if (neg) {  /* f_j(Q) = (-1)^j conj(f_j(-Q)); c0 changes sign */
+        f[0] = conj(f[0]); f[1] = -conj(f[1]); f[2] = conj(f[2]);
+        d1[0] = conj(d1[0]); d1[1] = -conj(d1[1]); d1[2] = conj(d1[2]);
+        d0[0] = -conj(d0[0]); d0[1] = conj(d0[1]); d0[2] = -conj(d0[2]);
+    }
+    return ORC_OK;
+}
+
+/* traceless Hermitian part */
+static void m_th(const cx* a, cx* out)
+{
+    cx t[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i * 3 + j] = 0.5 * (a[i * 3 + j] + conj(a[j * 3 + i]));
+    cx tr = m_tr(t) / 3.0;
+    for (int i = 0; i < 9; ++i) out[i] = t[i];
+    out[0] -= tr; out[4] -= tr; out[8] -= tr;
+}
+
+/* plaquette staple sum of link (s, mu), orientation as orc_stout */
+static void stout_staple(const tab_t* t, const double* U, long s, int mu, cx* C)
+{
+    cx m1[9], m2[9];
+    for (int i = 0; i < 9; ++i) C[i] = 0;
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        long xn = t->up[s * 4 + nu], xm = t->up[s * 4 + mu];
+        long xd = t->dn[s * 4 + nu], xdm = t->up[xd * 4 + mu];
+        m_mul(link_at(U, s, nu), link_at(U, xn, mu), m1);
+        m_mul_adj(m1, link_at(U, xm, nu), m1);
+        for (int i = 0; i < 9; ++i) C[i] += m1[i];
+        m_adj(link_at(U, xd, nu), m2);
+        m_mul(m2, link_at(U, xd, mu), m2);
+        m_mul(m2, link_at(U, xdm, nu), m2);
+        for (int i = 0; i < 9; ++i) C[i] += m2[i];
+    }
+}
+
+/* out += a b c with each factor optionally adjoint */
+static void acc3(cx* out, const cx* a, int ad, const cx* b, int bd, const cx* c, int cd)
+{
+    cx A[9], B[9], Cm[9], t1[9], t2[9];
+    if (ad) m_adj(a, A); else memcpy(A, a, sizeof(A));
+    if (bd) m_adj(b, B); else memcpy(B, b, sizeof(B));
+    if (cd) m_adj(c, Cm); else memcpy(Cm, c, sizeof(Cm));
+    m_mul(A, B, t1);
+    m_mul(t1, Cm, t2);
+    for (int i = 0; i < 9; ++i) out[i] += t2[i];
+}
+
+/* dS/dU of link m = (y, a) from the staple terms Re Tr(W_l dC_l) of every
+ * link l whose staple contains m (six positions, three directions each). */
+static void stout_gather(const tab_t* t, const double* U, const cx* W, long y, int a, cx* out)
+{
+#define LK(s, d) link_at(U, (s), (d))
+#define WK(s, d) (W + ((s) * 4 + (d)) * 9)
+#define UP(s, d) ((long)t->up[(s) * 4 + (d)])
+#define DN(s, d) ((long)t->dn[(s) * 4 + (d)])
+    for (int m = 0; m < 4; ++m) {
+        if (m == a) continue;
+        /* m is U_nu(x) of an upper staple of (x, mu): nu = a, x = y */
+        acc3(out, LK(UP(y, a), m), 0, LK(UP(y, m), a), 1, WK(y, m), 0);
+        /* m is U_mu(x+nu) of an upper staple: mu = a, x = y - nu */
+        {
+            long x = DN(y, m);
+            acc3(out, LK(UP(x, a), m), 1, WK(x, a), 0, LK(x, m), 0);
+        }
+        /* m is U_nu(x+mu) of an upper staple: nu = a, x = y - mu */
+        {
+            long x = DN(y, m);
+            cx t1[9];
+            for (int i = 0; i < 9; ++i) t1[i] = 0;
+            acc3(t1, WK(x, m), 0, LK(x, a), 0, LK(UP(x, a), m), 0);  /* (B^dag A^dag W^dag)^dag = W A B */
+            cx t2[9];
+            m_adj(t1, t2);
+            for (int i = 0; i < 9; ++i) out[i] += t2[i];
+        }
+        /* m is U_nu(x-nu) of a lower staple: nu = a, x = y + a */
+        {
+            long x = UP(y, a);
+            cx t1[9];
+            for (int i = 0; i < 9; ++i) t1[i] = 0;
+            acc3(t1, LK(y, m), 0, LK(UP(y, m), a), 0, WK(x, m), 0);  /* (W^dag G^dag F^dag)^dag = F G W */
+            cx t2[9];
+            m_adj(t1, t2);
+            for (int i = 0; i < 9; ++i) out[i] += t2[i];
+        }
+        /* m is U_mu(x-nu) of a lower staple: mu = a, x = y + nu */
+        acc3(out, LK(UP(y, a), m), 0, WK(UP(y, m), a), 0, LK(y, m), 1);
+        /* m is U_nu(x-nu+mu) of a lower staple: nu = a, x = y + a - mu */
+        {
+            long z = DN(y, m); /* y - mu */
+            long x = UP(z, a); /* y - mu + a */
+            acc3(out, WK(x, m), 0, LK(z, a), 1, LK(z, m), 0);
+        }
+    }
+#undef LK
+#undef WK
+#undef UP
+#undef DN
+}
+
+int orc_stout_force(const int dims[4], double rho, int n_levels, const double* U_thin, const double* F_top,
+                    double* F_thin)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    long V = t.V, nl = 4 * V;
+    double** lev = (double**)malloc(sizeof(double*) * (n_levels + 1));
+    for (int k = 0; k <= n_levels; ++k) lev[k] = (double*)malloc(sizeof(double) * 72 * V);
+    memcpy(lev[0], U_thin, sizeof(double) * 72 * V);
+    int bad = 0;
+    for (int k = 0; k < n_levels && !bad; ++k) {
+        memcpy(lev[k + 1], lev[k], sizeof(double) * 72 * V);
+        bad = orc_stout(dims, rho, 1, lev[k + 1]);
+    }
+    cx* G = (cx*)malloc(sizeof(cx) * 9 * nl);
+    cx* Gn = (cx*)malloc(sizeof(cx) * 9 * nl);
+    cx* W = (cx*)malloc(sizeof(cx) * 9 * nl);
+    /* top: G = -2i V^dag F */
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < nl; ++l) {
+        cx vd[9], g[9];
+        m_adj((const cx*)(lev[n_levels] + l * 18), vd);
+        m_mul(vd, (const cx*)(F_top + l * 18), g);
+        for (int i = 0; i < 9; ++i) G[l * 9 + i] = -2.0 * I * g[i];
+    }
+    for (int k = n_levels - 1; k >= 0 && !bad; --k) {
+        const double* Uk = lev[k];
+#pragma omp parallel for schedule(static) reduction(| : bad)
+        for (long l = 0; l < nl; ++l) {
+            long s = l / 4;
+            int mu = (int)(l % 4);
+            const cx* u = (const cx*)(Uk + l * 18);
+            cx C[9], om[9], A[9], Q[9], Q2[9], B[9], eq[9];
+            stout_staple(&t, Uk, s, mu, C);
+            m_mul_adj(C, u, om);
+            proj_ah(om, A);
+            for (int i = 0; i < 9; ++i) Q[i] = -I * rho * A[i];
+            cx f[3], d0[3], d1[3];
+            if (expiq_coeffs(Q, f, d0, d1) != ORC_OK) { bad = 1; continue; }
+            m_mul(Q, Q, Q2);
+            for (int i = 0; i < 9; ++i) eq[i] = f[1] * Q[i] + f[2] * Q2[i];
+            eq[0] += f[0]; eq[4] += f[0]; eq[8] += f[0];
+            m_mul(u, G + l * 9, B);
+            cx BQ[9], BQ2[9];
+            m_mul(B, Q, BQ);
+            m_mul(B, Q2, BQ2);
+            cx tr[3] = {m_tr(B), m_tr(BQ), m_tr(BQ2)};
+            cx b0 = 0, b1 = 0;
+            for (int j = 0; j < 3; ++j) { b0 += tr[j] * d0[j]; b1 += tr[j] * d1[j]; }
+            cx QB[9], Lh[9], L[9];
+            m_mul(Q, B, QB);
+            for (int i = 0; i < 9; ++i) Lh[i] = b0 * Q2[i] + b1 * Q[i] + f[1] * B[i] + f[2] * (QB[i] + BQ[i]);
+            m_th(Lh, L);
+            cx K[9], ud[9], w[9], g1[9], cd[9], g2[9];
+            for (int i = 0; i < 9; ++i) K[i] = -I * rho * L[i];
+            m_adj(u, ud);
+            m_mul(ud, K, w);
+            for (int i = 0; i < 9; ++i) W[l * 9 + i] = w[i];
+            m_mul(G + l * 9, eq, g1);
+            m_adj(C, cd);
+            m_mul(cd, K, g2);
+            for (int i = 0; i < 9; ++i) Gn[l * 9 + i] = g1[i] - g2[i];
+        }
+        if (bad) break;
+#pragma omp parallel for schedule(static)
+        for (long l = 0; l < nl; ++l) {
+            cx acc[9];
+            for (int i = 0; i < 9; ++i) acc[i] = 0;
+            stout_gather(&t, Uk, W, l / 4, (int)(l % 4), acc);
+            for (int i = 0; i < 9; ++i) G[l * 9 + i] = Gn[l * 9 + i] + acc[i];
+        }
+    }
+    if (!bad) {
+#pragma omp parallel for schedule(static)
+        for (long l = 0; l < nl; ++l) {
+            cx ug[9], iug[9], f[9];
+            m_mul((const cx*)(lev[0] + l * 18), G + l * 9, ug);
+            for (int i = 0; i < 9; ++i) iug[i] = I * ug[i];
+            m_th(iug, f);
+            for (int i = 0; i < 9; ++i) ((cx*)(F_thin + l * 18))[i] = 0.5 * f[i];
+        }
+    }
+    free(G); free(Gn); free(W);
+    for (int k = 0; k <= n_levels; ++k) free(lev[k]);
+    free(lev);
+    tab_free(&t);
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
 /* HEX, Smearing.cpp:76-311.  Decorated fields are stored as
  * [combo][site][9] with combo = (4 mu + nu) 4 + rho (level 1),
  * 4 mu + nu (level 2), mu (level 3), as in the reference's flat indices

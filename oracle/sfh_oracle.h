@@ -7,8 +7,9 @@
  * baseline leg may load it.  The product library never calls it.
  *
  * Parity pin: the restatement is checked against fixtures produced by the
- * reference's own sources (tests/golden/, generated by oracle/make_golden.py
- * from a build of the unmodified reference files, see oracle/Makefile) and
+ * reference's own sources (tests/golden/, generated by
+ * tests/golden/make_golden.py from binaries that oracle/build_ref.py builds
+ * from the unmodified reference files) and
  * against the reference's analytic known-answer tests (cold-start staples
  * 6I / 18I, cold action, cold plaquette, unitarity).
  *
@@ -114,6 +115,12 @@ int orc_stout(const int dims[4], double rho, int n_levels, double* U);
  * exp(A) evaluated as exp(i * (-iA)), Gamma_3 zero-initialised.
  * alphas = {alpha1, alpha2, alpha3} as in Smearing.h:7-9. */
 int orc_hex(const int dims[4], const double alphas[3], double* U);
+
+/* Thin-link force of an action on n_levels stout-smeared links (rho), given
+ * the force F_top on the smeared links (same convention as
+ * orc_fermion_force).  No counterpart in the reference. */
+int orc_stout_force(const int dims[4], double rho, int n_levels, const double* U_thin, const double* F_top,
+                    double* F_thin);
 
 /* U[i] = exp(i eps H[i]) for n matrices (used to build seeded gauge fields). */
 int orc_exp_field(long n, double eps, const double* H, double* U);

@@ -116,6 +116,8 @@ SIGNATURES = {
     "sfh_fermion_force": (ctypes.c_int, [_VP, _D, _D, _D]),
     "sfh_full_force": (ctypes.c_int, [_VP, _D, _D, _D]),
     "sfh_link_update": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_set_fermion_smearing": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_smeared_fermion_force": (ctypes.c_int, [_VP, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D]),
     "sfh_momentum_kick": (ctypes.c_int, [_VP, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, _D, ctypes.POINTER(ctypes.c_long)]),
     "sfh_trp2": (ctypes.c_int, [_VP, _D]),
@@ -372,6 +374,19 @@ class Lattice:
                                    _dptr(X), ctypes.byref(its))
         self._check(st, "leapfrog")
         return X, its.value
+
+    def set_fermion_smearing(self, rho, n_levels):
+        """Fermion operator on stout^n(U) in the HMC (n_levels = 0: thin links)."""
+        self._check(self.lib.sfh_set_fermion_smearing(self.h, rho, n_levels), "set_fermion_smearing")
+
+    def smeared_fermion_force(self, phi, tol=1e-12, max_iter=50000, precision="f64"):
+        """Thin-link fermion force with stout-smeared fermion links; returns (F, X)."""
+        phi = _f64(phi).reshape(-1)
+        F = np.empty(72 * self.V)
+        X = np.empty_like(phi)
+        self._check(self.lib.sfh_smeared_fermion_force(self.h, _dptr(phi), tol, max_iter, PRECISIONS[precision],
+                                                       _dptr(F), _dptr(X)), "smeared_fermion_force")
+        return F, X
 
     def momentum_kick(self, dt, phi=None, forces="full", tol=1e-12, max_iter=50000, precision="f64"):
         """P -= dt F on the device momenta, F the gauge, fermion or full force

@@ -300,6 +300,22 @@ cudaError_t launch_force(const Geom& g, const void* U, const void* X, const void
     return cudaGetLastError();
 }
 
+// Y += a X over a link field (FP64 18-real)
+__global__ void link_axpy_kernel(Geom g, double2* Y, double a, const double2* X, long n)
+{
+    long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double2 x = X[k], y = Y[k];
+    Y[k] = make_double2(fma(a, x.x, y.x), fma(a, x.y, y.y));
+}
+
+cudaError_t launch_link_axpy(const Geom& g, void* Y, double a, const void* X, cudaStream_t s)
+{
+    long n = (long)g.V * 4 * 9;
+    link_axpy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, (double2*)Y, a, (const double2*)X, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_staples(const Geom& g, const void* U, void* A1, void* A2, cudaStream_t s)
 {
     staple_kernel<<<dim3((g.Vh + kThreads - 1) / kThreads, 8), kThreads, 0, s>>>(g, U, A1, A2);

@@ -78,11 +78,94 @@ int reduce(sfh_ctx* c, int kind, const void* A, const void* B, double* out)
     return cuda_check(c, cudaStreamSynchronize(c->stream), "reduction");
 }
 
+}  // namespace
+
+namespace sfh {
+int ensure_scratch(sfh_ctx* c, int nfields);
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Stout-smeared fermion links (no counterpart in the reference): the fermion
+// operator uses V = stout^n(U), the gauge action the thin U.  Scratch link
+// fields: levels 0..n (level 0 = the thin field), then G, Gn, W of the chain
+// rule.  While a smeared operation runs, U64 holds V (so the solver and the
+// operators use it) and level 0 keeps U; smear_out puts U back.
+// ---------------------------------------------------------------------------
+constexpr int kMaxSmearLevels = 16;
+
+void* scratch_field(sfh_ctx* c, int k) { return (char*)c->smear + (size_t)k * c->g.V * 4 * 9 * 16; }
+
+int smear_in(sfh_ctx* c)
+{
+    int st = ensure_scratch(c, c->fsmear_n + 4);
+    if (st) return st;
+    void* lev[kMaxSmearLevels + 1];
+    for (int k = 0; k <= c->fsmear_n; ++k) lev[k] = scratch_field(c, k);
+    st = cuda_check(c, cudaMemcpyAsync(lev[0], c->U64, link_bytes(c), cudaMemcpyDeviceToDevice, c->stream),
+                    "smearing");
+    if (!st) st = cuda_check(c, launch_stout_levels(c->g, lev, c->fsmear_rho, c->fsmear_n, c->derr, c->stream),
+                             "smearing");
+    if (!st) st = cuda_check(c, cudaMemcpyAsync(c->U64, lev[c->fsmear_n], link_bytes(c), cudaMemcpyDeviceToDevice,
+                                                c->stream), "smearing");
+    c->lowp_valid = false;
+    if (!st) st = take_device_error(c, "fermion-link smearing");
+    return st;
+}
+
+int smear_out(sfh_ctx* c)
+{
+    int st = cuda_check(c, cudaMemcpyAsync(c->U64, scratch_field(c, 0), link_bytes(c), cudaMemcpyDeviceToDevice,
+                                           c->stream), "smearing");
+    c->lowp_valid = false;
+    return st;
+}
+
+// fermion force on the thin links into Fbuf: X = (D D^dag)^-1 phi and
+// Y = D^dag X with the smeared links, their force, then the chain rule
+int smeared_fermion_force(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
+                          long* iters, int* solves)
+{
+    int st = smear_in(c);
+    if (!st) {
+        sfh_cg_info inf;
+        std::memset(&inf, 0, sizeof(inf));
+        st = ctx_solve_device(c, phi, X, tol, maxit, prec, &inf);
+        if (iters) *iters += inf.iters;
+        if (solves) *solves += 1;
+        if (!st) {
+            launch_hop(c->g, GP_F64_18, c->U64, SP_F64, X, SP_F64, Y, X, c->mass, -1.0, 0, 2, c->stream);
+            st = cuda_check(c, launch_force(c->g, c->U64, X, Y, c->beta, c->c11, c->c12, 2, c->Fbuf, nullptr, 0.0,
+                                            c->stream), "smeared-link fermion force");
+        }
+    }
+    int st2 = smear_out(c);
+    if (st) return st;
+    if (st2) return st2;
+    void* lev[kMaxSmearLevels + 1];
+    for (int k = 0; k <= c->fsmear_n; ++k) lev[k] = scratch_field(c, k);
+    const int n = c->fsmear_n;
+    st = cuda_check(c, launch_stout_force(c->g, lev, n, c->fsmear_rho, c->Fbuf, scratch_field(c, n + 1),
+                                          scratch_field(c, n + 2), scratch_field(c, n + 3), c->derr, c->stream),
+                    "stout chain rule");
+    if (!st) st = take_device_error(c, "stout chain rule");
+    return st;
+}
+
 // one force evaluation and momentum kick: X = (D D^dag)^-1 phi, Y = D^dag X,
-// P -= kick (F_g + F_f)  (local_* of Fermions.cpp:967-1028)
+// P -= kick (F_g + F_f)  (local_* of Fermions.cpp:967-1028); with smeared
+// fermion links F_f comes from the chain rule
 int force_and_kick(sfh_ctx* c, const void* phi, void* X, void* Y, double kick, double tol, int maxit, int prec,
                    long* iters, int* solves)
 {
+    if (c->fsmear_n > 0) {
+        int st = smeared_fermion_force(c, phi, X, Y, tol, maxit, prec, iters, solves);
+        if (!st) st = cuda_check(c, launch_link_axpy(c->g, c->Pmom, -kick, c->Fbuf, c->stream), "kick");
+        if (!st) st = cuda_check(c, launch_force(c->g, c->U64, nullptr, nullptr, c->beta, c->c11, c->c12, 1, nullptr,
+                                                 c->Pmom, kick, c->stream), "gauge kick");
+        return st;
+    }
     sfh_cg_info inf;
     int st = ctx_solve_device(c, phi, X, tol, maxit, prec, &inf);
     if (iters) *iters += inf.iters;
@@ -202,6 +285,19 @@ extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, doub
     if (cg_iters) *cg_iters = 0;
     void *X = c->spin[4], *Y = c->spin[2];
     int st = SFH_OK;
+    if (ferm && c->fsmear_n > 0) {  // smeared fermion links: chain-rule force, then the gauge part
+        st = spinor_in(c, phi, c->spin[5]);
+        long its = 0;
+        if (!st) st = smeared_fermion_force(c, c->spin[5], X, Y, tol, maxit, precision, &its, nullptr);
+        if (cg_iters) *cg_iters = its;
+        if (!st) st = cuda_check(c, launch_link_axpy(c->g, c->Pmom, -dt, c->Fbuf, c->stream), "momentum kick");
+        if (!st && (forces & SFH_FORCE_GAUGE))
+            st = cuda_check(c, launch_force(c->g, c->U64, nullptr, nullptr, c->beta, c->c11, c->c12, 1, nullptr,
+                                            c->Pmom, dt, c->stream), "momentum kick");
+        if (st) return st;
+        if (X_out) return spinor_out(c, X, X_out);
+        return cuda_check(c, cudaStreamSynchronize(c->stream), "momentum kick");
+    }
     if (ferm) {
         sfh_cg_info inf;
         std::memset(&inf, 0, sizeof(inf));
@@ -216,6 +312,28 @@ extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, doub
     if (st) return st;
     if (ferm && X_out) return spinor_out(c, X, X_out);
     return cuda_check(c, cudaStreamSynchronize(c->stream), "momentum kick");
+}
+
+extern "C" int sfh_set_fermion_smearing(sfh_ctx* c, double rho, int nlevels)
+{
+    if (!c || nlevels < 0 || nlevels > kMaxSmearLevels || !(rho >= 0.0)) return SFH_ERR_INVALID;
+    c->fsmear_rho = rho;
+    c->fsmear_n = nlevels;
+    return SFH_OK;
+}
+
+extern "C" int sfh_smeared_fermion_force(sfh_ctx* c, const double* phi, double tol, int maxit, int precision,
+                                         double* F, double* X_out)
+{
+    if (!c || !phi || !F || !(tol > 0.0) || maxit <= 0 || c->fsmear_n < 1) return SFH_ERR_INVALID;
+    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    void *X = c->spin[4], *Y = c->spin[2];
+    int st = spinor_in(c, phi, c->spin[5]);
+    if (!st) st = smeared_fermion_force(c, c->spin[5], X, Y, tol, maxit, precision, nullptr, nullptr);
+    if (!st) st = links_out(c, c->Fbuf, F);
+    if (!st && X_out) st = spinor_out(c, X, X_out);
+    return st;
 }
 
 extern "C" int sfh_link_update(sfh_ctx* c, double eps, int check)
@@ -292,14 +410,21 @@ extern "C" int sfh_hmc_trajectory(sfh_ctx* c, double eps, int nsteps, unsigned l
     // phi = D chi, chi complex Gaussian with variance 1/2 per real part
     // (Fermions.cpp:207-212, 302-314)
     if (!st) st = cuda_check(c, launch_random_spinor(c->g, 1.0 / std::sqrt(2.0), seed, chi, c->stream), "chi");
+    const bool smeared = c->fsmear_n > 0;  // the fermion operator on stout links
+    if (!st && smeared) st = smear_in(c);
     if (!st) launch_hop(c->g, GP_F64_18, c->U64, SP_F64, chi, SP_F64, phi, chi, c->mass, 1.0, 0, 2, c->stream);
     if (!st) st = cuda_check(c, launch_random_momenta(c->g, seed + 1, c->Pmom, c->stream), "momenta");
     if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T0);
     sfh_cg_info inf;
+    std::memset(&inf, 0, sizeof(inf));
     if (!st) st = ctx_solve_device(c, phi, X, tol, maxit, precision, &inf);  // Fermions.cpp:819
     info->cg_iters += inf.iters;
     info->solves += 1;
     if (!st) st = reduce(c, RED_DOT, phi, X, &F0);
+    if (smeared) {
+        int st2 = smear_out(c);
+        if (!st) st = st2;
+    }
     if (!st) st = cuda_check(c, cudaMemcpyAsync(c->Utrial, c->U64, (size_t)c->g.V * 4 * 9 * 16,
                                                 cudaMemcpyDeviceToDevice, c->stream), "gauge backup");
     if (!st) st = leapfrog(c, phi, X, Y, eps, nsteps, tol, maxit, precision, 1, &info->cg_iters, &info->solves);

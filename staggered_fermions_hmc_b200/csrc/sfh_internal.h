@@ -42,6 +42,8 @@ struct sfh_ctx {
     void* Utrial = nullptr;        // gauge backup for the Metropolis step
     void* smear = nullptr;         // scratch link fields (smearing, staples)
     size_t smear_bytes = 0;
+    double fsmear_rho = 0.0;       // stout smearing of the fermion links (HMC)
+    int fsmear_n = 0;              // levels; 0 = thin links
 
     std::string last_error;
 };
@@ -89,6 +91,10 @@ cudaError_t launch_link_update(const Geom& g, void* U, const void* P, double eps
 enum { RED_TRP2 = 0, RED_ACTION = 1, RED_PLAQ = 2, RED_DOT = 3 };
 // smear.cu
 cudaError_t launch_stout(const Geom& g, void* U, void* tmp, double rho, int n, int* err, cudaStream_t s);
+cudaError_t launch_stout_levels(const Geom& g, void* const* levels, double rho, int n, int* err, cudaStream_t s);
+cudaError_t launch_stout_force(const Geom& g, void* const* levels, int n, double rho, void* F, void* G, void* Gn,
+                               void* W, int* err, cudaStream_t s);
+cudaError_t launch_link_axpy(const Geom& g, void* Y, double a, const void* X, cudaStream_t s);
 cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double a2, double a3, int n, int* err,
                        cudaStream_t s);
 cudaError_t launch_reduce(const Geom& g, int kind, const void* A, const void* B, double beta, double c11,

@@ -167,6 +167,230 @@ __global__ void __launch_bounds__(kThreads) hex3_kernel(Geom g, void* U, const v
 
 dim3 link_grid(const Geom& g) { return dim3((g.Vh + kThreads - 1) / kThreads, 8); }
 
+// ---------------------------------------------------------------------------
+// Smeared-link force: the chain rule through stout levels (no counterpart in
+// the reference).  Method of Morningstar & Peardon, Phys. Rev. D 69 (2004)
+// 054501.  Per level, with C the staples of U, Q = -i rho TA(C U^dag),
+// V = exp(iQ) U and G = dS/dV (dS = sum Re Tr(G dV)):
+//   L = TH(b0 Q^2 + b1 Q + f1 B + f2 (Q B + B Q)), B = U G,
+//   b0 = sum_j Tr(B Q^j) df_j/dc0, b1 = sum_j Tr(B Q^j) df_j/dc1,
+//   K = -i rho L, W = U^dag K,
+//   dS/dU = G exp(iQ) - C^dag K + staple terms of W (sforce_gather_kernel).
+// The force convention at both ends is the reference's (dS/deps = 2 Tr(F H)
+// under U -> exp(i eps H) U): G = -2i V^dag F on top, F = TH(i U G)/2 below.
+// ---------------------------------------------------------------------------
+typedef Cx<double> Z;
+
+__device__ __forceinline__ Z zm(Z a, Z b) { return cmul(a, b); }
+__device__ __forceinline__ Z zs(Z a, double s) { return {a.re * s, a.im * s}; }
+__device__ __forceinline__ Z za(Z a, Z b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ Z zd(Z a, Z b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ Z zi(Z a) { return {-a.im, a.re}; }  // i a
+__device__ __forceinline__ Z zdiv(Z a, double s) { return {a.re / s, a.im / s}; }
+
+__device__ __forceinline__ double xi1_stable(double w)
+{
+    if (fabs(w) < 0.05) {
+        double w2 = w * w;
+        return -1.0 / 3.0 + w2 / 30.0 - w2 * w2 / 840.0 + w2 * w2 * w2 / 45360.0;
+    }
+    return (cos(w) - sin(w) / w) / (w * w);
+}
+
+// f_j of exp(iQ) = f0 + f1 Q + f2 Q^2 and df_j/dc0, df_j/dc1 (c0 = det Q,
+// c1 = Tr Q^2 / 2); h_j as in expiq, dh_j/dw = w g_j, D = 9u^2 - w^2
+__device__ bool expiq_coeffs(const M3& Q, const M3& Q2, Z (&f)[3], Z (&d0)[3], Z (&d1)[3])
+{
+    M3 Q3 = m3_mul(Q2, Q);
+    double c0 = m3_tr(Q3).re / 3.0;
+    double c1 = 0.5 * m3_tr(Q2).re;
+    if (c1 < 0.0) return false;
+    if (c1 < 1e-12) {
+        f[0] = {1.0, 0.0};
+        f[1] = {0.0, 1.0};
+        f[2] = {-0.5, 0.0};
+        for (int j = 0; j < 3; ++j) d0[j] = d1[j] = {0.0, 0.0};
+        return true;
+    }
+    const bool neg = c0 < 0.0;
+    c0 = fabs(c0);
+    double c0max = 2.0 * sqrt(c1 * c1 * c1 / 27.0);
+    double ratio = c0max > 0.0 ? fmin(c0 / c0max, 1.0) : 1.0;
+    double theta = acos(ratio);
+    double st3, ct3;
+    sincos(theta / 3.0, &st3, &ct3);
+    const double w = sqrt(c1) * st3, u = sqrt(c1 / 3.0) * ct3;
+    const double u2 = u * u, w2 = w * w;
+    const double xi0 = sinc_stable(w), xi1 = xi1_stable(w), cw = cos(w);
+    double s2u, c2u, su, cu;
+    sincos(2.0 * u, &s2u, &c2u);
+    sincos(u, &su, &cu);
+    const Z E = {c2u, s2u}, e = {cu, -su};
+    const Z P0 = {8.0 * u2 * cw, 2.0 * u * (3.0 * u2 + w2) * xi0};
+    const Z P1 = {2.0 * u * cw, -(3.0 * u2 - w2) * xi0};
+    const Z P2 = {cw, 3.0 * u * xi0};
+    Z h[3], hu[3], g[3];
+    h[0] = za(zs(E, u2 - w2), zm(e, P0));
+    h[1] = zd(zs(E, 2.0 * u), zm(e, P1));
+    h[2] = zd(E, zm(e, P2));
+    hu[0] = za(za(zs(E, 2.0 * u), zi(zs(E, 2.0 * (u2 - w2)))),
+               zd(zm(e, Z{16.0 * u * cw, 2.0 * (9.0 * u2 + w2) * xi0}), zi(zm(e, P0))));
+    hu[1] = za(za(zs(E, 2.0), zi(zs(E, 4.0 * u))), zd(zi(zm(e, P1)), zm(e, Z{2.0 * cw, -6.0 * u * xi0})));
+    hu[2] = za(zi(zs(E, 2.0)), zd(zi(zm(e, P2)), zm(e, Z{0.0, 3.0 * xi0})));
+    g[0] = za(zs(E, -2.0), zm(e, Z{-8.0 * u2 * xi0, 2.0 * u * (2.0 * xi0 + (3.0 * u2 + w2) * xi1)}));
+    g[1] = zm(e, Z{2.0 * u * xi0, -2.0 * xi0 + (3.0 * u2 - w2) * xi1});
+    g[2] = zm(e, Z{xi0, -3.0 * u * xi1});
+    const double D = 9.0 * u2 - w2, D2 = D * D;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        Z fu = zdiv(zd(zs(hu[j], D), zs(h[j], 18.0 * u)), D2);
+        Z k = zdiv(za(zs(g[j], D), zs(h[j], 2.0)), D2);
+        f[j] = zdiv(h[j], D);
+        d0[j] = zdiv(zd(fu, zs(k, 3.0 * u)), 2.0 * D);
+        d1[j] = zdiv(za(zs(fu, u), zs(k, 0.5 * (3.0 * u2 - w2))), D);
+    }
+    if (neg) {  // f_j(Q) = (-1)^j conj(f_j(-Q)); c0 changes sign
+        f[0] = cconj(f[0]);
+        f[1] = {-f[1].re, f[1].im};
+        f[2] = cconj(f[2]);
+        d1[0] = cconj(d1[0]);
+        d1[1] = {-d1[1].re, d1[1].im};
+        d1[2] = cconj(d1[2]);
+        d0[0] = {-d0[0].re, d0[0].im};
+        d0[1] = cconj(d0[1]);
+        d0[2] = {-d0[2].re, d0[2].im};
+    }
+    return true;
+}
+
+__device__ __forceinline__ M3 m3_th(const M3& a)  // traceless Hermitian part
+{
+    M3 t;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            Z x = a.e[i * 3 + j], y = cconj(a.e[j * 3 + i]);
+            t.e[i * 3 + j] = {0.5 * (x.re + y.re), 0.5 * (x.im + y.im)};
+        }
+    m3_traceless(t);
+    return t;
+}
+
+__device__ __forceinline__ M3 m3_scale(const M3& a, Z s)
+{
+    M3 o;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) o.e[k] = zm(a.e[k], s);
+    return o;
+}
+
+// G = -2i V^dag F
+__global__ void __launch_bounds__(kThreads) sforce_top_kernel(Geom g, const void* V, const void* F, void* G)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int p = blockIdx.y >> 2, mu = blockIdx.y & 3;
+    if (i >= g.Vh) return;
+    st_link(G, p, mu, i, g.Vh, m3_scale(m3_adj_mul(ld_link(V, p, mu, i, g.Vh), ld_link(F, p, mu, i, g.Vh)), Z{0.0, -2.0}));
+}
+
+// per link of level U: W = U^dag K and Gn = G exp(iQ) - C^dag K
+__global__ void __launch_bounds__(kThreads) sforce_level_kernel(Geom g, const void* U, const void* G, void* W, void* Gn,
+                                                                double rho, int* err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int p = blockIdx.y >> 2, mu = blockIdx.y & 3;
+    if (i >= g.Vh) return;
+    Walker x = link_coords(g, p, i);
+    M3 C = m3_zero();
+#pragma unroll 1
+    for (int nu = 0; nu < 4; ++nu)
+        if (nu != mu) m3_acc(C, staple(U, 0, U, 0, g, x, mu, nu));
+    const M3 u = ld_link(U, p, mu, i, g.Vh);
+    M3 om = m3_mul_adj(C, u), Q;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            Z d = zd(om.e[a * 3 + b], cconj(om.e[b * 3 + a]));  // Q = -i rho TA(om)
+            Q.e[a * 3 + b] = {0.5 * rho * d.im, -0.5 * rho * d.re};
+        }
+    m3_traceless(Q);
+    const M3 Q2 = m3_mul(Q, Q);
+    Z f[3], d0[3], d1[3];
+    if (!expiq_coeffs(Q, Q2, f, d0, d1)) {
+        atomicOr(err, DEV_ERR_DOMAIN);
+        return;
+    }
+    M3 eq;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) eq.e[k] = za(zm(f[1], Q.e[k]), zm(f[2], Q2.e[k]));
+    eq.e[0] = za(eq.e[0], f[0]);
+    eq.e[4] = za(eq.e[4], f[0]);
+    eq.e[8] = za(eq.e[8], f[0]);
+    const M3 Gl = ld_link(G, p, mu, i, g.Vh);
+    const M3 B = m3_mul(u, Gl);
+    const M3 BQ = m3_mul(B, Q), BQ2 = m3_mul(B, Q2), QB = m3_mul(Q, B);
+    const Z t0 = m3_tr(B), t1 = m3_tr(BQ), t2 = m3_tr(BQ2);
+    const Z b0 = za(za(zm(t0, d0[0]), zm(t1, d0[1])), zm(t2, d0[2]));
+    const Z b1 = za(za(zm(t0, d1[0]), zm(t1, d1[1])), zm(t2, d1[2]));
+    M3 Lh;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        Lh.e[k] = za(za(zm(b0, Q2.e[k]), zm(b1, Q.e[k])), za(zm(f[1], B.e[k]), zm(f[2], za(QB.e[k], BQ.e[k]))));
+    const M3 K = m3_scale(m3_th(Lh), Z{0.0, -rho});
+    st_link(W, p, mu, i, g.Vh, m3_adj_mul(u, K));
+    M3 out = m3_mul(Gl, eq);
+    const M3 cK = m3_adj_mul(C, K);
+    m3_axpy(out, -1.0, cK);
+    st_link(Gn, p, mu, i, g.Vh, out);
+}
+
+// dS/dU of link (y, a): Gn + the staple terms Re Tr(W_l dC_l) of the links l
+// whose plaquette staples contain it (six positions, three directions each)
+__global__ void __launch_bounds__(kThreads) sforce_gather_kernel(Geom g, const void* U, const void* W, const void* Gn,
+                                                                 void* G)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int p = blockIdx.y >> 2, a = blockIdx.y & 3;
+    if (i >= g.Vh) return;
+    const Walker y = link_coords(g, p, i);
+    M3 out = ld_link(Gn, p, a, i, g.Vh);
+#pragma unroll 1
+    for (int d = 0; d < 4; ++d) {
+        if (d == a) continue;
+        Walker ya = y, yd = y, ymd = y;
+        walk(g, ya, a, +1);
+        walk(g, yd, d, +1);
+        walk(g, ymd, d, -1);
+        Walker ymda = ymd;
+        walk(g, ymda, a, +1);
+        // U_nu(x) of an upper staple of (x = y, d)
+        m3_acc(out, m3_mul(m3_mul_adj(link_at(U, g, ya, d), link_at(U, g, yd, a)), link_at(W, g, y, d)));
+        // U_mu(x+nu) of an upper staple of (x = y - d, a)
+        m3_acc(out, m3_mul(m3_adj_mul(link_at(U, g, ymda, d), link_at(W, g, ymd, a)), link_at(U, g, ymd, d)));
+        // U_nu(x+mu) of an upper staple of (x = y - d, d): (W U_a(x) U_d(x+a))^dag
+        m3_acc(out, m3_adj(m3_mul(m3_mul(link_at(W, g, ymd, d), link_at(U, g, ymd, a)), link_at(U, g, ymda, d))));
+        // U_nu(x-nu) of a lower staple of (x = y + a, d): (U_d(y) U_a(y+d) W)^dag
+        m3_acc(out, m3_adj(m3_mul(m3_mul(link_at(U, g, y, d), link_at(U, g, yd, a)), link_at(W, g, ya, d))));
+        // U_mu(x-nu) of a lower staple of (x = y + d, a)
+        m3_acc(out, m3_mul_adj(m3_mul(link_at(U, g, ya, d), link_at(W, g, yd, a)), link_at(U, g, y, d)));
+        // U_nu(x-nu+mu) of a lower staple of (x = y - d + a, d)
+        m3_acc(out, m3_mul(m3_mul_adj(link_at(W, g, ymda, d), link_at(U, g, ymd, a)), link_at(U, g, ymd, d)));
+    }
+    st_link(G, p, a, i, g.Vh, out);
+}
+
+// F = TH(i U G) / 2
+__global__ void __launch_bounds__(kThreads) sforce_bottom_kernel(Geom g, const void* U, const void* G, void* F)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int p = blockIdx.y >> 2, mu = blockIdx.y & 3;
+    if (i >= g.Vh) return;
+    M3 t = m3_th(m3_scale(m3_mul(ld_link(U, p, mu, i, g.Vh), ld_link(G, p, mu, i, g.Vh)), Z{0.0, 0.5}));
+    st_link(F, p, mu, i, g.Vh, t);
+}
+
 }  // namespace
 
 // n stout levels; U is updated in place, tmp is one link field of scratch
@@ -190,6 +414,31 @@ cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double 
         hex2_kernel<<<link_grid(g), kThreads, 0, s>>>(g, U, V1, V2, 0.5 * a2, err);
         hex3_kernel<<<link_grid(g), kThreads, 0, s>>>(g, U, V2, 0.5 * a1, err);
     }
+    return cudaGetLastError();
+}
+
+}  // namespace sfh
+
+namespace sfh {
+
+// levels: n + 1 link fields, levels[0] = thin U (in), levels[k] = stout^k(U) (out)
+cudaError_t launch_stout_levels(const Geom& g, void* const* levels, double rho, int n, int* err, cudaStream_t s)
+{
+    for (int k = 0; k < n; ++k)
+        stout_kernel<<<link_grid(g), kThreads, 0, s>>>(g, levels[k], levels[k + 1], rho, err);
+    return cudaGetLastError();
+}
+
+// F (in: force on levels[n]; out: force on levels[0]); G, Gn, W: scratch link fields
+cudaError_t launch_stout_force(const Geom& g, void* const* levels, int n, double rho, void* F, void* G, void* Gn,
+                               void* W, int* err, cudaStream_t s)
+{
+    sforce_top_kernel<<<link_grid(g), kThreads, 0, s>>>(g, levels[n], F, G);
+    for (int k = n - 1; k >= 0; --k) {
+        sforce_level_kernel<<<link_grid(g), kThreads, 0, s>>>(g, levels[k], G, W, Gn, rho, err);
+        sforce_gather_kernel<<<link_grid(g), kThreads, 0, s>>>(g, levels[k], W, Gn, G);
+    }
+    sforce_bottom_kernel<<<link_grid(g), kThreads, 0, s>>>(g, levels[0], G, F);
     return cudaGetLastError();
 }
 

@@ -317,3 +317,64 @@ def test_checkpoint_round_trip_is_byte_exact(sfh, orc, tmp_path):
     with pytest.raises(sfh.SfhError) as e:
         lat2.load_lattice_config(str(tmp_path / "missing.bin"))
     assert e.value.status == sfh.SFH_ERR_IO
+
+
+# --- stout-smeared fermion links (no counterpart in the reference) --------
+@pytest.mark.parametrize("n_levels", [1, 3])
+def test_smeared_fermion_force_vs_oracle(sfh, orc, n_levels):
+    """GPU chain-rule force vs the oracle's (itself checked by finite
+    differences in test_oracle_golden::test_stout_force_finite_difference)."""
+    dims, mass, rho = (4, 4, 6, 8), 0.3, 0.125
+    U = orc.random_gauge(dims, 0.4, 161)
+    phi = orc.random_spinor(dims, 162)
+    lat = sfh.Lattice(dims, mass, 4.2)
+    lat.upload_gauge(U)
+    lat.set_fermion_smearing(rho, n_levels)
+    F, X = lat.smeared_fermion_force(phi, tol=1e-13)
+    Vs = orc.stout(dims, rho, n_levels, U)
+    Xo, _, _, _ = orc.cg(dims, mass, Vs, phi, 1e-13)
+    Yo = orc.dirac(dims, mass, Vs, Xo, dagger=True)
+    Fo = orc.stout_force(dims, rho, n_levels, U, orc.fermion_force(dims, Vs, Xo, Yo))
+    assert rel(X, Xo) < 1e-10
+    assert rel(F, Fo) < 1e-10
+    assert np.array_equal(lat.download_gauge(), U)  # the thin field is left as it was
+
+
+def test_smeared_leapfrog_reversible_and_second_order(sfh, orc):
+    """With smeared fermion links the integrator stays reversible and
+    dH(eps)/dH(eps/2) ~ 4 (force consistent with the action)."""
+    dims, mass, rho, nl = (4, 4, 4, 4), 0.5, 0.125, 2
+    U = orc.random_gauge(dims, 0.15, 171)
+    P = orc.random_momenta(dims, 172)
+    phi = orc.random_spinor(dims, 173)
+    lat = sfh.Lattice(dims, mass, 4.2)
+    lat.set_fermion_smearing(rho, nl)
+    lat.upload_gauge(U)
+    lat.upload_momenta(P)
+    lat.leapfrog(phi, 0.02, 10, tol=1e-14)
+    lat.upload_momenta(-lat.download_momenta())
+    lat.leapfrog(phi, 0.02, 10, tol=1e-14)
+    assert np.abs(lat.download_gauge() - U).max() < 1e-10
+    assert np.abs(lat.download_momenta() + P).max() < 1e-9
+
+    def dH(eps, n):
+        lat.upload_gauge(U)
+        lat.upload_momenta(P)
+        _, X0 = lat.smeared_fermion_force(phi, tol=1e-14)
+        h0 = lat.compute_Tr_P2() + lat.compute_action() + float(np.dot(phi, X0))
+        X, _ = lat.leapfrog(phi, eps, n, tol=1e-14)
+        h1 = lat.compute_Tr_P2() + lat.compute_action() + float(np.dot(phi, X))
+        return h1 - h0
+
+    d1, d2 = dH(0.02, 10), dH(0.01, 20)
+    assert 3.5 < abs(d1) / abs(d2) < 4.5, (d1, d2)
+
+
+def test_smeared_hmc_trajectory_accepts_small_steps(sfh, orc):
+    dims = (4, 4, 4, 4)
+    lat = sfh.Lattice(dims, 0.3, 4.2)
+    lat.upload_gauge(orc.random_gauge(dims, 0.05, 181))
+    lat.set_fermion_smearing(0.125, 4)
+    info = lat.hmc_trajectory(0.01, 10, seed=77, tol=1e-12)
+    assert abs(info["dH"]) < 0.05 and info["accepted"]
+    assert np.isfinite(info["plaquette"])
