@@ -398,6 +398,7 @@ __device__ __forceinline__ void finish_lane(const CgArgs& a, const CgSys& S, int
         }
     } else {  // reliable update: s[3] = |b - M x|^2 in FP64
         const double rt = s[3];
+        const double r_iter = L->rr_next;  // the recurrence's |r|^2 that triggered the update
         L->nru += 1;
         L->rr_next = rt;
         if (rt < L->target) {
@@ -408,8 +409,10 @@ __device__ __forceinline__ void finish_lane(const CgArgs& a, const CgSys& S, int
             lane_stop(a, L, cur, LM_DONE, LM_DONE, SFH_ERR_NOCONV);
         } else {
             // keep the search direction, or restart it (p = r) when the lane
-            // restarts after every update or the last stretch made little progress
-            const bool restart = a.restart || rt > 0.5 * L->rr_old;
+            // restarts after every update, the last stretch made little
+            // progress, or the recurrence drifted from the true residual
+            // (|r_true|^2 > 1.5 |r_iterated|^2: the search directions lost accuracy)
+            const bool restart = a.restart || rt > 0.5 * L->rr_old || rt > 1.5 * r_iter;
             L->rr_old = rt;
             L->rmax = sqrt(rt);
             L->mode[nxt] = restart ? LM_RESTART : LM_ACTIVE;
@@ -1061,7 +1064,7 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.delta = delta;
     a.maxit = maxit;
     a.mixed = w.prec != SFH_PREC_F64;
-    a.restart = w.prec == SFH_PREC_F16;  // FP16: defect correction (restart after each update)
+    a.restart = 0;  // restart only when an update shows little progress (finish_lane)
     a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
     a.tpi = tpi;
     return a;
