@@ -143,6 +143,19 @@ int sfh_full_force(sfh_ctx* ctx, const double* X, const double* Y, double* F);
 #define SFH_FORCE_FERMION 2
 int sfh_momentum_kick(sfh_ctx* ctx, int forces, const double* phi, double dt, double tol, int maxit,
                       int precision, double* X_out, long* cg_iters);
+/* nsweeps heatbath sweeps of the context's gauge field at its beta:
+ * heatbath_update (Lattice.cpp:722-757) with single_link_heatbath's
+ * Cabibbo-Marinari SU(2) subgroups and the sampler of SU3_Sampling.cpp:17-199.
+ * The reference sweeps lexicographically with an unseeded generator; here one
+ * direction and one of eight colours of mutually independent links per launch,
+ * with Philox uniforms from (seed, link, sweep index), sweep indices sweep0..
+ * Every extent must be a multiple of 4.  plaq / action_density (may be NULL)
+ * receive the average plaquette (1 on a cold field, the normalisation
+ * heatbath_update returns) and the Symanzik action per site after the sweeps
+ * (the reference accumulates them during its sweep). */
+int sfh_heatbath(sfh_ctx* ctx, int nsweeps, unsigned long long seed, int sweep0, double* plaq,
+                 double* action_density);
+
 /* Stout-smeared fermion links (no counterpart in the reference, which has no
  * smeared-link HMC): with nlevels > 0 the fermion operator of sfh_leapfrog,
  * sfh_hmc_trajectory and sfh_momentum_kick uses V = stout^nlevels(U) with

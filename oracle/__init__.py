@@ -74,6 +74,8 @@ def lib():
             "orc_stout": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_int, D]),
             "orc_hex": (ctypes.c_int, [dims, D, D]),
             "orc_stout_force": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_int, D, D, D]),
+            "orc_heatbath": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, D]),
             "orc_exp_field": (ctypes.c_int, [ctypes.c_long, ctypes.c_double, D, D]),
         }
         for name, (res, args) in sig.items():
@@ -235,6 +237,15 @@ def stout(dims, rho, n_levels, U):
     st = lib().orc_stout(_dims(dims), rho, n_levels, _d(U))
     if st != ORC_OK:
         raise OracleError(st, "stout")
+    return U
+
+
+def heatbath(dims, beta, U, seed, nsweeps=1, sweep0=0, c11=5.0 / 3.0, c12=-1.0 / 12.0):
+    """nsweeps heatbath sweeps in colour order with seeded uniforms."""
+    U = U.copy()
+    st = lib().orc_heatbath(_dims(dims), beta, c11, c12, seed, sweep0, nsweeps, _d(U))
+    if st != ORC_OK:
+        raise OracleError(st, "heatbath")
     return U
 
 

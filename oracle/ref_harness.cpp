@@ -11,6 +11,7 @@
 // usage:
 //   ref_harness run  <indir> <outdir> <beta> <eps> <nsteps>
 //   ref_harness time <indir> <nsolves>        (prints one JSON line)
+//   ref_harness heatbath <indir> <outdir> <beta> <nsweeps>
 //
 // inputs in <indir>: U.bin (72V), phi.bin (6V), P.bin (72V), H.bin (18n)
 #include <omp.h>
@@ -207,13 +208,31 @@ static int time_cg(const std::string& indir, int nsolves)
     return 0;
 }
 
+// heatbath_update (Lattice.cpp:722-757) nsweeps times from U.bin; writes
+// plaq.bin: compute_avg_plaq after every sweep (the reference's generator is
+// unseeded, so this is one realisation of its Markov chain)
+static int heatbath_run(const std::string& in, const std::string& out, double beta, int nsweeps)
+{
+    Link_array U = read_bin(in + "/U.bin");
+    std::vector<double> plaq;
+    for (int k = 0; k < nsweeps; ++k) {
+        heatbath_update(U, beta);
+        plaq.push_back(compute_avg_plaq(U));
+    }
+    write_vec(out + "/plaq.bin", plaq);
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
+    if (argc >= 6 && std::string(argv[1]) == "heatbath")
+        return heatbath_run(argv[2], argv[3], std::atof(argv[4]), std::atoi(argv[5]));
     if (argc >= 7 && std::string(argv[1]) == "run")
         return run(argv[2], argv[3], std::atof(argv[4]), std::atof(argv[5]), std::atoi(argv[6]));
     if (argc >= 4 && std::string(argv[1]) == "time")
         return time_cg(argv[2], std::atoi(argv[3]));
     std::cerr << "usage: ref_harness run <indir> <outdir> <beta> <eps> <nsteps>\n"
-                 "       ref_harness time <indir> <nsolves>\n";
+                 "       ref_harness time <indir> <nsolves>\n"
+                 "       ref_harness heatbath <indir> <outdir> <beta> <nsweeps>\n";
     return 1;
 }

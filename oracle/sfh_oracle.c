@@ -17,6 +17,7 @@
 
 #include <complex.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1099,6 +1100,170 @@ int orc_stout_force(const int dims[4], double rho, int n_levels, const double* U
     free(lev);
     tab_free(&t);
     return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* heatbath: Cabibbo-Marinari SU(2) subgroups (Lattice.cpp:614-757,          */
+/* SU3_Sampling.cpp:17-199)                                                  */
+/* ------------------------------------------------------------------------ */
+/*
+ * single_link_heatbath restated per link: A = c11 A1 + c12 A2; for the
+ * subgroups R (rows/cols 0,1), S (0,2), T (1,2) in turn: W = the SU(2)
+ * projection of that 2x2 block of U A, a = sqrt(det W); a <= 1e-14: R a
+ * uniform SU(2) element, else X from the sampler with (a, 2 beta / 3) and
+ * R = X (W/a)^dag; U <- R U.
+ * Order: the reference sweeps lexicographically; here (as on the GPU) one
+ * direction mu at a time and, within it, eight colours
+ * (x_mu mod 2) * 4 + (sum_{nu != mu} x_nu mod 4) of links whose staples do not
+ * contain each other (needs every extent divisible by 4).  The uniforms are
+ * Philox-4x32-10 (Salmon et al., SC'11) keyed by the seed, counter
+ * (link, draw, sweep, 0x48420000 + subgroup), 53-bit doubles in [0, 1);
+ * the reference's generator is unseeded, so parity with it is statistical.
+ */
+static void philox_4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n1 = (uint32_t)p1;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1, n3 = (uint32_t)p0;
+        c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+typedef struct {
+    uint32_t k0, k1, link, sweep, tag, draw;
+    double buf[2];
+    int have;
+} hb_rng;
+
+static double hb_u(hb_rng* r)  /* uniform in [0, 1) */
+{
+    if (r->have == 0) {
+        uint32_t c[4] = {r->link, r->draw++, r->sweep, r->tag};
+        philox_4x32_10(c, r->k0, r->k1);
+        uint64_t a = (((uint64_t)c[0] << 21) ^ (uint64_t)(c[1] >> 11)) & ((1ull << 53) - 1);
+        uint64_t b = (((uint64_t)c[2] << 21) ^ (uint64_t)(c[3] >> 11)) & ((1ull << 53) - 1);
+        r->buf[0] = (double)a * (1.0 / 9007199254740992.0);
+        r->buf[1] = (double)b * (1.0 / 9007199254740992.0);
+        r->have = 2;
+    }
+    return r->buf[2 - r->have--];
+}
+
+/* SU3_Sampling.cpp:17-31 (generate_x0) */
+static double hb_x0(hb_rng* r, double a, double beta)
+{
+    for (;;) {
+        double r1 = 1.0 - hb_u(r), r2 = 1.0 - hb_u(r), r3 = 1.0 - hb_u(r);
+        double c = cos(2.0 * 3.14159265358979323846 * r2);
+        double l2 = -1.0 / (2.0 * a * beta) * (log(r1) + c * c * log(r3));
+        double x = 1.0 - l2;
+        double rr = hb_u(r);
+        if (rr * rr <= x && x >= -1.0 && x <= 1.0) return 1.0 - 2.0 * l2;
+    }
+}
+
+/* SU3_Sampling.cpp:42-58 / 152-168: uniform unit vector by rejection */
+static void hb_unit(hb_rng* r, double* v, int n)
+{
+    for (;;) {
+        double len2 = 0.0;
+        for (int k = 0; k < n; ++k) {
+            v[k] = 2.0 * hb_u(r) - 1.0;
+            len2 += v[k] * v[k];
+        }
+        double len = sqrt(len2);
+        if (len <= 1.0 && len > 0.0) {
+            for (int k = 0; k < n; ++k) v[k] /= len;
+            return;
+        }
+    }
+}
+
+/* 2x2 (row-major) from quaternion q: q0 I + i (q1 sx + q2 sy + q3 sz) */
+static void quat_su2(const double q[4], cx m[4])
+{
+    m[0] = q[0] + I * q[3];
+    m[1] = q[2] + I * q[1];
+    m[2] = -q[2] + I * q[1];
+    m[3] = q[0] - I * q[3];
+}
+
+static void hb_subgroup(hb_rng* r, cx* U, const cx* A, int i, int j, double beta)
+{
+    cx UA[9];
+    m_mul(U, A, UA);
+    cx b[4] = {UA[i * 3 + i], UA[i * 3 + j], UA[j * 3 + i], UA[j * 3 + j]};
+    /* SU(2) projection (Lattice.cpp:570-598): w0 = Re tr/2, w_k from the
+     * anti-Hermitian part */
+    double w0 = 0.5 * creal(b[0] + b[3]);
+    double w1 = 0.5 * cimag(b[1] + b[2]);
+    double w2 = 0.5 * creal(b[1] - b[2]);
+    double w3 = 0.5 * cimag(b[0] - b[3]);
+    double a = sqrt(w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3);
+    cx R[4];
+    if (a <= 1e-14) {
+        double q[4];
+        hb_unit(r, q, 4);
+        quat_su2(q, R);
+    } else {
+        double x0 = hb_x0(r, a, 2.0 * beta / 3.0);
+        double v[3];
+        hb_unit(r, v, 3);
+        double nx = sqrt(1.0 - x0 * x0);
+        double qx[4] = {x0, nx * v[0], nx * v[1], nx * v[2]};
+        double qw[4] = {w0 / a, -w1 / a, -w2 / a, -w3 / a};  /* (W/a)^dag */
+        cx X[4], Wd[4];
+        quat_su2(qx, X);
+        quat_su2(qw, Wd);
+        R[0] = X[0] * Wd[0] + X[1] * Wd[2];
+        R[1] = X[0] * Wd[1] + X[1] * Wd[3];
+        R[2] = X[2] * Wd[0] + X[3] * Wd[2];
+        R[3] = X[2] * Wd[1] + X[3] * Wd[3];
+    }
+    cx E[9], out[9];
+    m_id(E);
+    E[i * 3 + i] = R[0]; E[i * 3 + j] = R[1];
+    E[j * 3 + i] = R[2]; E[j * 3 + j] = R[3];
+    m_mul(E, U, out);
+    memcpy(U, out, sizeof(out));
+}
+
+int orc_heatbath(const int dims[4], double beta, double c11, double c12, unsigned long long seed, int sweep0,
+                 int nsweeps, double* U)
+{
+    for (int k = 0; k < 4; ++k)
+        if (dims[k] % 4) return ORC_ERR_DOMAIN;
+    tab_t t;
+    tab_build(&t, dims);
+    long V = t.V;
+    for (int sw = sweep0; sw < sweep0 + nsweeps; ++sw)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int col = 0; col < 8; ++col)
+#pragma omp parallel for schedule(static)
+                for (long s = 0; s < V; ++s) {
+                    int c[4];
+                    coords_of(t.L, s, c);
+                    int sum = 0;
+                    for (int nu = 0; nu < 4; ++nu)
+                        if (nu != mu) sum += c[nu];
+                    if ((c[mu] & 1) * 4 + (sum & 3) != col) continue;
+                    cx A1[9], A2[9], A[9];
+                    staple_plaq(&t, U, s, mu, A1);
+                    staple_rect(&t, U, s, mu, A2);
+                    for (int i = 0; i < 9; ++i) A[i] = c11 * A1[i] + c12 * A2[i];
+                    cx* u = (cx*)(U + (s * 4 + mu) * 18);
+                    const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+                    for (int g = 0; g < 3; ++g) {
+                        hb_rng r = {(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(s * 4 + mu),
+                                    (uint32_t)sw, 0x48420000u + (uint32_t)g, 0, {0, 0}, 0};
+                        hb_subgroup(&r, u, A, sub[g][0], sub[g][1], beta);
+                    }
+                }
+    tab_free(&t);
+    return ORC_OK;
 }
 
 /* HEX, Smearing.cpp:76-311.  Decorated fields are stored as

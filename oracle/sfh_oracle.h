@@ -116,6 +116,11 @@ int orc_stout(const int dims[4], double rho, int n_levels, double* U);
  * alphas = {alpha1, alpha2, alpha3} as in Smearing.h:7-9. */
 int orc_hex(const int dims[4], const double alphas[3], double* U);
 
+/* nsweeps heatbath sweeps (single_link_heatbath, Lattice.cpp:722-757, in
+ * colour order; seeded Philox uniforms), sweep indices sweep0.. */
+int orc_heatbath(const int dims[4], double beta, double c11, double c12, unsigned long long seed, int sweep0,
+                 int nsweeps, double* U);
+
 /* Thin-link force of an action on n_levels stout-smeared links (rho), given
  * the force F_top on the smeared links (same convention as
  * orc_fermion_force).  No counterpart in the reference. */

@@ -117,6 +117,7 @@ SIGNATURES = {
     "sfh_full_force": (ctypes.c_int, [_VP, _D, _D, _D]),
     "sfh_link_update": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_set_fermion_smearing": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
+    "sfh_heatbath": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_int, _D, _D]),
     "sfh_smeared_fermion_force": (ctypes.c_int, [_VP, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D]),
     "sfh_momentum_kick": (ctypes.c_int, [_VP, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, _D, ctypes.POINTER(ctypes.c_long)]),
@@ -374,6 +375,14 @@ class Lattice:
                                    _dptr(X), ctypes.byref(its))
         self._check(st, "leapfrog")
         return X, its.value
+
+    def heatbath_update(self, n_sweeps=1, seed=1, sweep0=0):
+        """heatbath_update (Lattice.cpp:722-757) n_sweeps times at the context's
+        beta; returns (average plaquette, action per site) after the sweeps."""
+        p, a = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        self._check(self.lib.sfh_heatbath(self.h, n_sweeps, seed, sweep0, ctypes.byref(p), ctypes.byref(a)),
+                    "heatbath")
+        return p.value, a.value
 
     def set_fermion_smearing(self, rho, n_levels):
         """Fermion operator on stout^n(U) in the HMC (n_levels = 0: thin links)."""

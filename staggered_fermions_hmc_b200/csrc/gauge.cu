@@ -300,6 +300,161 @@ cudaError_t launch_force(const Geom& g, const void* U, const void* X, const void
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Heatbath (single_link_heatbath, Lattice.cpp:722-757, with the SU(2)
+// sampler of SU3_Sampling.cpp:17-199).  Per link: A = c11 A1 + c12 A2; for
+// the subgroups R (0,1), S (0,2), T (1,2): W = the SU(2) projection of that
+// block of U A, a = sqrt(det W); a <= 1e-14: a uniform SU(2) element, else X
+// drawn with (a, 2 beta / 3) and R = X (W / a)^dag; U <- R U.  One launch
+// updates one direction and one colour (x_mu mod 2) * 4 + (sum_{nu != mu} x_nu
+// mod 4): links whose staples do not contain each other.  Uniforms: Philox-
+// 4x32-10 keyed by the seed, counter (link, draw, sweep, 0x48420000 + subgroup).
+// ---------------------------------------------------------------------------
+struct HbRng {
+    uint2 key;
+    unsigned link, sweep, tag, draw;
+    double buf[2];
+    int have;
+    __device__ double u()  // uniform in [0, 1)
+    {
+        if (have == 0) {
+            uint4 r = Philox::gen(make_uint4(link, draw++, sweep, tag), key);
+            unsigned long long a = (((unsigned long long)r.x << 21) ^ (unsigned long long)(r.y >> 11)) & ((1ull << 53) - 1);
+            unsigned long long b = (((unsigned long long)r.z << 21) ^ (unsigned long long)(r.w >> 11)) & ((1ull << 53) - 1);
+            buf[0] = (double)a * (1.0 / 9007199254740992.0);
+            buf[1] = (double)b * (1.0 / 9007199254740992.0);
+            have = 2;
+        }
+        return buf[2 - have--];
+    }
+};
+
+// generate_x0 (SU3_Sampling.cpp:17-31)
+__device__ double hb_x0(HbRng& r, double a, double beta)
+{
+    for (;;) {
+        double r1 = 1.0 - r.u(), r2 = 1.0 - r.u(), r3 = 1.0 - r.u();
+        double c = cospi(2.0 * r2);
+        double l2 = -1.0 / (2.0 * a * beta) * (log(r1) + c * c * log(r3));
+        double x = 1.0 - l2;
+        double rr = r.u();
+        if (rr * rr <= x && x >= -1.0 && x <= 1.0) return 1.0 - 2.0 * l2;
+    }
+}
+
+template <int N>
+__device__ void hb_unit(HbRng& r, double (&v)[N])
+{
+    for (;;) {
+        double len2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            v[k] = 2.0 * r.u() - 1.0;
+            len2 += v[k] * v[k];
+        }
+        double len = sqrt(len2);
+        if (len <= 1.0 && len > 0.0) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) v[k] /= len;
+            return;
+        }
+    }
+}
+
+// q0 I + i (q1 sx + q2 sy + q3 sz), row-major 2x2
+__device__ __forceinline__ void quat_su2(const double (&q)[4], Cx<double> (&m)[4])
+{
+    m[0] = {q[0], q[3]};
+    m[1] = {q[2], q[1]};
+    m[2] = {-q[2], q[1]};
+    m[3] = {q[0], -q[3]};
+}
+
+__device__ void hb_subgroup(HbRng& r, M3& U, const M3& A, int i, int j, double beta)
+{
+    const M3 UA = m3_mul(U, A);
+    const Cx<double> b0 = UA.e[i * 3 + i], b1 = UA.e[i * 3 + j], b2 = UA.e[j * 3 + i], b3 = UA.e[j * 3 + j];
+    const double w0 = 0.5 * (b0.re + b3.re), w1 = 0.5 * (b1.im + b2.im);
+    const double w2 = 0.5 * (b1.re - b2.re), w3 = 0.5 * (b0.im - b3.im);
+    const double a = sqrt(w0 * w0 + w1 * w1 + w2 * w2 + w3 * w3);
+    Cx<double> R[4];
+    if (a <= 1e-14) {
+        double q[4];
+        hb_unit<4>(r, q);
+        quat_su2(q, R);
+    } else {
+        const double x0 = hb_x0(r, a, 2.0 * beta / 3.0);
+        double v[3];
+        hb_unit<3>(r, v);
+        const double nx = sqrt(1.0 - x0 * x0);
+        const double qx[4] = {x0, nx * v[0], nx * v[1], nx * v[2]};
+        const double qw[4] = {w0 / a, -w1 / a, -w2 / a, -w3 / a};
+        Cx<double> X[4], Wd[4];
+        quat_su2(qx, X);
+        quat_su2(qw, Wd);
+        R[0] = cadd(cmul(X[0], Wd[0]), cmul(X[1], Wd[2]));
+        R[1] = cadd(cmul(X[0], Wd[1]), cmul(X[1], Wd[3]));
+        R[2] = cadd(cmul(X[2], Wd[0]), cmul(X[3], Wd[2]));
+        R[3] = cadd(cmul(X[2], Wd[1]), cmul(X[3], Wd[3]));
+    }
+    M3 E = m3_id();
+    E.e[i * 3 + i] = R[0];
+    E.e[i * 3 + j] = R[1];
+    E.e[j * 3 + i] = R[2];
+    E.e[j * 3 + j] = R[3];
+    U = m3_mul(E, U);
+}
+
+__global__ void __launch_bounds__(128) heatbath_kernel(Geom g, void* U, int mu, int colour, double beta, double c11,
+                                                       double c12, unsigned long long seed, int sweep)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.V) return;
+    Walker x;
+    int rest = s;
+    x.x[3] = rest % g.L[3];
+    rest /= g.L[3];
+    x.x[2] = rest % g.L[2];
+    rest /= g.L[2];
+    x.x[1] = rest % g.L[1];
+    x.x[0] = rest / g.L[1];
+    int sum = 0;
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu)
+        if (nu != mu) sum += x.x[nu];
+    if ((x.x[mu] & 1) * 4 + (sum & 3) != colour) return;
+    M3 A1, A2;
+    staples(U, g, x, mu, A1, A2);
+    M3 A = m3_zero();
+    m3_axpy(A, c11, A1);
+    m3_axpy(A, c12, A2);
+    const int p = (x.x[0] + x.x[1] + x.x[2] + x.x[3]) & 1, i = s >> 1;
+    M3 u = ld_link(U, p, mu, i, g.Vh);
+    const int sub[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+        HbRng r;
+        r.key = make_uint2((unsigned)seed, (unsigned)(seed >> 32));
+        r.link = (unsigned)(s * 4 + mu);
+        r.sweep = (unsigned)sweep;
+        r.tag = 0x48420000u + (unsigned)k;
+        r.draw = 0;
+        r.have = 0;
+        hb_subgroup(r, u, A, sub[k][0], sub[k][1], beta);
+    }
+    st_link(U, p, mu, i, g.Vh, u);
+}
+
+cudaError_t launch_heatbath(const Geom& g, void* U, double beta, double c11, double c12, unsigned long long seed,
+                            int sweep0, int nsweeps, cudaStream_t s)
+{
+    for (int sw = sweep0; sw < sweep0 + nsweeps; ++sw)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int col = 0; col < 8; ++col)
+                heatbath_kernel<<<(g.V + 127) / 128, 128, 0, s>>>(g, U, mu, col, beta, c11, c12, seed, sw);
+    return cudaGetLastError();
+}
+
 // Y += a X over a link field (FP64 18-real)
 __global__ void link_axpy_kernel(Geom g, double2* Y, double a, const double2* X, long n)
 {

@@ -314,6 +314,26 @@ extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, doub
     return cuda_check(c, cudaStreamSynchronize(c->stream), "momentum kick");
 }
 
+extern "C" int sfh_heatbath(sfh_ctx* c, int nsweeps, unsigned long long seed, int sweep0, double* plaq,
+                            double* action_density)
+{
+    if (!c || nsweeps < 0 || sweep0 < 0) return SFH_ERR_INVALID;
+    for (int k = 0; k < 4; ++k)
+        if (c->g.L[k] % 4) return set_error(c, SFH_ERR_INVALID, "heatbath: every extent must be a multiple of 4");
+    cudaSetDevice(c->device);
+    int st = cuda_check(c, launch_heatbath(c->g, c->U64, c->beta, c->c11, c->c12, seed, sweep0, nsweeps, c->stream),
+                        "heatbath");
+    c->lowp_valid = false;
+    double p = 0.0, a = 0.0;
+    if (!st && plaq) st = reduce(c, RED_PLAQ, c->U64, nullptr, &p);
+    if (!st && action_density) st = reduce(c, RED_ACTION, c->U64, nullptr, &a);
+    if (st) return st;
+    const double V = (double)c->g.V;
+    if (plaq) *plaq = p / (4.0 * V) / 6.0;  // conventional normalisation: 1 on a cold field
+    if (action_density) *action_density = a / V;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "heatbath");
+}
+
 extern "C" int sfh_set_fermion_smearing(sfh_ctx* c, double rho, int nlevels)
 {
     if (!c || nlevels < 0 || nlevels > kMaxSmearLevels || !(rho >= 0.0)) return SFH_ERR_INVALID;

@@ -95,6 +95,8 @@ cudaError_t launch_stout_levels(const Geom& g, void* const* levels, double rho, 
 cudaError_t launch_stout_force(const Geom& g, void* const* levels, int n, double rho, void* F, void* G, void* Gn,
                                void* W, int* err, cudaStream_t s);
 cudaError_t launch_link_axpy(const Geom& g, void* Y, double a, const void* X, cudaStream_t s);
+cudaError_t launch_heatbath(const Geom& g, void* U, double beta, double c11, double c12, unsigned long long seed,
+                            int sweep0, int nsweeps, cudaStream_t s);
 cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double a2, double a3, int n, int* err,
                        cudaStream_t s);
 cudaError_t launch_reduce(const Geom& g, int kind, const void* A, const void* B, double beta, double c11,

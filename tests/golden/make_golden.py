@@ -70,9 +70,36 @@ def make(L, T, mass, tol, geps, seed, beta, eps, nsteps):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# heatbath: (beta values, runs per beta, sweeps) on 4^4 from a cold start
+HEATBATH = ((2.0, 4.2), 4, 100)
+
+
+def make_heatbath():
+    """Plaquette histories of the reference's heatbath_update (Lattice.cpp:
+    722-757).  Its generator is unseeded, so these are independent
+    realisations of its Markov chain; the tests compare equilibrium means."""
+    betas, runs, sweeps = HEATBATH
+    exe = build_ref.build(4, 4, 0.1, 1e-12)
+    hist = np.zeros((len(betas), runs, sweeps))
+    with tempfile.TemporaryDirectory() as td:
+        ind = os.path.join(td, "in")
+        os.makedirs(ind)
+        oracle.cold_gauge((4, 4, 4, 4)).astype("<f8").tofile(os.path.join(ind, "U.bin"))
+        for b, beta in enumerate(betas):
+            for r in range(runs):
+                outd = os.path.join(td, f"out{b}_{r}")
+                os.makedirs(outd)
+                subprocess.run([exe, "heatbath", ind, outd, repr(beta), str(sweeps)], check=True)
+                hist[b, r] = np.fromfile(os.path.join(outd, "plaq.bin"))
+    path = os.path.join(HERE, "heatbath_ref_L4T4.npz")  # outside the ref_*.npz operator fixtures
+    np.savez_compressed(path, betas=np.array(betas), plaq=hist)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def main():
     for fx in FIXTURES:
         make(*fx)
+    make_heatbath()
 
 
 if __name__ == "__main__":

@@ -379,3 +379,46 @@ def test_smeared_hmc_trajectory_accepts_small_steps(sfh, orc):
     assert info["status"] == 0
     assert abs(info["dH"]) < 0.1  # the same bound as the thin-link trajectory
     assert np.isfinite(info["plaquette"])
+
+
+# --- heatbath (Lattice.cpp:722-757, SU3_Sampling.cpp) --------------------
+@pytest.mark.parametrize("dims", [(4, 4, 4, 4), (4, 4, 8, 8)])
+def test_heatbath_vs_oracle(sfh, orc, dims):
+    """Same colour order and the same seeded uniforms: the GPU sweeps equal the
+    oracle's to rounding."""
+    U = orc.random_gauge(dims, 0.6, 191)
+    lat = sfh.Lattice(dims, 0.1, 4.2)
+    lat.upload_gauge(U)
+    plaq, act = lat.heatbath_update(n_sweeps=2, seed=17, sweep0=3)
+    ref = orc.heatbath(dims, 4.2, U, seed=17, nsweeps=2, sweep0=3)
+    assert rel(lat.download_gauge(), ref) < 1e-12
+    V = int(np.prod(dims))
+    assert abs(plaq - orc.avg_plaq(dims, ref) / 6.0) < 1e-12
+    assert abs(act - orc.action(dims, 4.2, ref) / V) < 1e-10 * max(1.0, abs(act))
+
+
+def test_heatbath_equilibrium_vs_reference(sfh, orc):
+    """The GPU chain reaches the reference's equilibrium plaquette (its
+    recorded, unseeded chains in tests/golden) at beta 2.0 and 4.2."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "heatbath_ref_L4T4.npz"))
+    dims = (4, 4, 4, 4)
+    nsw = g["plaq"].shape[2]
+    for b, beta in enumerate(g["betas"]):
+        m = g["plaq"][b][:, 30:].mean(axis=1)
+        ref_mean, ref_se = m.mean(), m.std(ddof=1) / np.sqrt(len(m))
+        means = []
+        for seed in range(8):
+            lat = sfh.Lattice(dims, 0.1, beta)
+            lat.upload_gauge(orc.cold_gauge(dims))
+            h = [lat.heatbath_update(1, seed=900 + seed, sweep0=sw)[0] * 6.0 for sw in range(nsw)]
+            means.append(np.mean(h[30:]))
+            lat.close()
+        mean, se = np.mean(means), np.std(means, ddof=1) / np.sqrt(len(means))
+        assert abs(mean - ref_mean) < 4.0 * np.hypot(ref_se, se) + 2e-3, (beta, mean, ref_mean)
+
+
+def test_heatbath_rejects_extents_not_multiple_of_four(sfh, orc):
+    lat = sfh.Lattice((4, 4, 4, 6), 0.1, 4.2)
+    with pytest.raises(sfh.SfhError) as e:
+        lat.heatbath_update(1)
+    assert e.value.status == sfh.SFH_ERR_INVALID

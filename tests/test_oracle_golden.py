@@ -228,3 +228,34 @@ def test_stout_force_finite_difference(orc, n_levels):
 def _xy(orc, dims, mass, U, phi):
     X, _, _, _ = orc.cg(dims, mass, U, phi, 1e-14)
     return X, orc.dirac(dims, mass, U, X, dagger=True)
+
+
+def _hb_equilibrium(hist, start=30):
+    """Mean plaquette over the sweeps after start and its standard error from
+    the spread of independent runs."""
+    m = hist[:, start:].mean(axis=1)
+    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(len(m)))
+
+
+def test_heatbath_oracle_vs_reference_statistics(orc):
+    """heatbath_update (Lattice.cpp:722-757): the reference's generator is
+    unseeded, so tests/golden holds independent plaquette histories of its own
+    chain (4^4 from a cold start).  The oracle's chain (colour order, seeded
+    uniforms) must reach the same equilibrium plaquette at each beta."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "heatbath_ref_L4T4.npz"))
+    dims = (4, 4, 4, 4)
+    for b, beta in enumerate(g["betas"]):
+        ref_mean, ref_se = _hb_equilibrium(g["plaq"][b])
+        hist = []
+        for seed in range(4):
+            U = orc.cold_gauge(dims)
+            h = []
+            for sw in range(g["plaq"].shape[2]):
+                U = orc.heatbath(dims, beta, U, seed=100 + seed, nsweeps=1, sweep0=sw)
+                h.append(orc.avg_plaq(dims, U))
+            hist.append(h)
+        mean, se = _hb_equilibrium(np.array(hist))
+        tol = 4.0 * np.hypot(ref_se, se) + 2e-3
+        assert abs(mean - ref_mean) < tol, (beta, mean, ref_mean, tol)
+    V = U.view(np.complex128).reshape(-1, 3, 3)
+    assert np.abs(np.einsum("lij,lkj->lik", V, V.conj()) - np.eye(3)).max() < 1e-12
