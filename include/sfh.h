@@ -164,6 +164,15 @@ int sfh_heatbath(sfh_ctx* ctx, int nsweeps, unsigned long long seed, int sweep0,
  * levels (Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501).
  * nlevels = 0 (the default) restores thin links.  At most 16 levels. */
 int sfh_set_fermion_smearing(sfh_ctx* ctx, double rho, int nlevels);
+/* Hasenbusch mass splitting (no counterpart in the reference): with
+ * heavy_mass > 0 the fermion action of sfh_leapfrog, sfh_hmc_trajectory and
+ * sfh_momentum_kick is phi_h^dag M(m_h)^{-1} phi_h + phi^dag M(m_h) M(m)^{-1} phi,
+ * M(m) = D(m) D(m)^dag, m the context's mass (both terms on the smeared links
+ * when sfh_set_fermion_smearing is on).  phi is the caller's pseudofermion (or
+ * the trajectory's own); phi_heavy (may be NULL: zero, or what the last
+ * trajectory drew) is the heavy one.  heavy_mass = 0 restores one
+ * pseudofermion. */
+int sfh_set_hasenbusch(sfh_ctx* ctx, double heavy_mass, const double* phi_heavy);
 /* The fermion force on the thin links under that smearing: X = (D D^dag)^{-1}
  * phi and Y = D^dag X with V, compute_fermion_force_at_link (Fermions.cpp:443-515)
  * on V, then the chain rule.  F: link-field layout; X_out may be NULL. */

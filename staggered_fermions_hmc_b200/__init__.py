@@ -118,6 +118,7 @@ SIGNATURES = {
     "sfh_link_update": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_set_fermion_smearing": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_heatbath": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_ulonglong, ctypes.c_int, _D, _D]),
+    "sfh_set_hasenbusch": (ctypes.c_int, [_VP, ctypes.c_double, _D]),
     "sfh_smeared_fermion_force": (ctypes.c_int, [_VP, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D]),
     "sfh_momentum_kick": (ctypes.c_int, [_VP, ctypes.c_int, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, _D, ctypes.POINTER(ctypes.c_long)]),
@@ -383,6 +384,12 @@ class Lattice:
         self._check(self.lib.sfh_heatbath(self.h, n_sweeps, seed, sweep0, ctypes.byref(p), ctypes.byref(a)),
                     "heatbath")
         return p.value, a.value
+
+    def set_hasenbusch(self, heavy_mass, phi_heavy=None):
+        """Hasenbusch pair: heavy pseudofermion at heavy_mass (0 = off)."""
+        ph = None if phi_heavy is None else _f64(phi_heavy).reshape(-1)
+        self._check(self.lib.sfh_set_hasenbusch(self.h, heavy_mass, None if ph is None else _dptr(ph)),
+                    "set_hasenbusch")
 
     def set_fermion_smearing(self, rho, n_levels):
         """Fermion operator on stout^n(U) in the HMC (n_levels = 0: thin links)."""

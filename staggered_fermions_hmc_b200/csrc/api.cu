@@ -118,7 +118,7 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     for (int k = 0; k < 4; ++k)
         if (c->ws[k]) workspace_free(c->ws[k]);
     void* ptrs[] = {c->U64, c->U32, c->U16, c->U32_18, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
-                    c->smear};
+                    c->smear, c->hphi, c->hX};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : c->spin)

@@ -1536,13 +1536,15 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
         launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18);
         c->lowp_valid = true;
     }
-    if (c->ws[prec] && c->ws_mass[prec] != c->mass) {  // mass is baked into the system table
-        workspace_free(c->ws[prec]);
-        c->ws[prec] = nullptr;
-    }
     cudaError_t e;
     CgWorkspace* w = ctx_workspace(c, prec, &e);
     if (!w) return cuda_check(c, e, "cg workspace");
+    if (c->ws_mass[prec] != c->mass) {  // the mass lives in the device system table
+        w->sys[0].m2 = c->mass * c->mass;
+        e = cudaMemcpyAsync(w->d_sys, w->sys.data(), sizeof(CgSys), cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cg mass");
+        c->ws_mass[prec] = c->mass;
+    }
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");

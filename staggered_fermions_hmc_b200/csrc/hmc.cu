@@ -97,6 +97,14 @@ constexpr int kMaxSmearLevels = 16;
 
 void* scratch_field(sfh_ctx* c, int k) { return (char*)c->smear + (size_t)k * c->g.V * 4 * 9 * 16; }
 
+int ensure_hasen(sfh_ctx* c)
+{
+    int st = SFH_OK;
+    if (!c->hphi) st = cuda_check(c, cudaMalloc(&c->hphi, spinor_bytes(c)), "heavy pseudofermion");
+    if (!st && !c->hX) st = cuda_check(c, cudaMalloc(&c->hX, spinor_bytes(c)), "heavy pseudofermion");
+    return st;
+}
+
 int smear_in(sfh_ctx* c)
 {
     int st = ensure_scratch(c, c->fsmear_n + 4);
@@ -122,24 +130,65 @@ int smear_out(sfh_ctx* c)
     return st;
 }
 
-// fermion force on the thin links into Fbuf: X = (D D^dag)^-1 phi and
-// Y = D^dag X with the smeared links, their force, then the chain rule
-int smeared_fermion_force(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
-                          long* iters, int* solves)
+// ---------------------------------------------------------------------------
+// Pseudofermion terms.  One pseudofermion: S_f = phi^dag M(m)^-1 phi with
+// M(m) = D(m) D(m)^dag.  With a Hasenbusch heavy mass m_h (no counterpart in
+// the reference): S_f = phi_h^dag M(m_h)^-1 phi_h + phi^dag M(m_h) M(m)^-1 phi,
+// and since M(m_h) M(m)^-1 = 1 + (m_h^2 - m^2) M(m)^-1 every term is a weight
+// times phi_k^dag M(m_k)^-1 phi_k (plus |phi|^2, constant in the MD).  The
+// fermion force of a term is compute_fermion_force_at_link (Fermions.cpp:
+// 443-515) of X_k = M(m_k)^-1 phi_k, Y_k = D(m_k)^dag X_k, times its weight.
+// ---------------------------------------------------------------------------
+struct PfTerm {
+    const void* phi;
+    void* X;
+    double mass, weight;
+};
+
+int pf_terms(sfh_ctx* c, const void* phi, void* X, PfTerm (&t)[2])
 {
-    int st = smear_in(c);
-    if (!st) {
+    if (c->hasen_mass > 0.0) {
+        t[0] = {c->hphi, c->hX, c->hasen_mass, 1.0};
+        t[1] = {phi, X, c->mass, c->hasen_mass * c->hasen_mass - c->mass * c->mass};
+        return 2;
+    }
+    t[0] = {phi, X, c->mass, 1.0};
+    return 1;
+}
+
+// Fbuf = sum_k w_k F_f(X_k, Y_k) on the links in U64
+int fermion_force_terms(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
+                        long* iters, int* solves)
+{
+    PfTerm t[2];
+    const int n = pf_terms(c, phi, X, t);
+    const double m = c->mass;
+    int st = cuda_check(c, cudaMemsetAsync(c->Fbuf, 0, link_bytes(c), c->stream), "fermion force");
+    for (int k = 0; k < n && !st; ++k) {
+        c->mass = t[k].mass;
         sfh_cg_info inf;
         std::memset(&inf, 0, sizeof(inf));
-        st = ctx_solve_device(c, phi, X, tol, maxit, prec, &inf);
+        st = ctx_solve_device(c, t[k].phi, t[k].X, tol, maxit, prec, &inf);
         if (iters) *iters += inf.iters;
         if (solves) *solves += 1;
-        if (!st) {
-            launch_hop(c->g, GP_F64_18, c->U64, SP_F64, X, SP_F64, Y, X, c->mass, -1.0, 0, 2, c->stream);
-            st = cuda_check(c, launch_force(c->g, c->U64, X, Y, c->beta, c->c11, c->c12, 2, c->Fbuf, nullptr, 0.0,
-                                            c->stream), "smeared-link fermion force");
-        }
+        if (st) break;
+        launch_hop(c->g, GP_F64_18, c->U64, SP_F64, t[k].X, SP_F64, Y, t[k].X, t[k].mass, -1.0, 0, 2, c->stream);
+        // Fbuf -= (-w) F: the kick form of force_kernel accumulates w F
+        st = cuda_check(c, launch_force(c->g, c->U64, t[k].X, Y, c->beta, c->c11, c->c12, 2, nullptr, c->Fbuf,
+                                        -t[k].weight, c->stream), "fermion force");
     }
+    c->mass = m;
+    return st;
+}
+
+// the fermion force on the thin links into Fbuf, through the smearing levels
+// when the fermion links are smeared
+int fermion_force_general(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
+                          long* iters, int* solves)
+{
+    if (c->fsmear_n == 0) return fermion_force_terms(c, phi, X, Y, tol, maxit, prec, iters, solves);
+    int st = smear_in(c);
+    if (!st) st = fermion_force_terms(c, phi, X, Y, tol, maxit, prec, iters, solves);
     int st2 = smear_out(c);
     if (st) return st;
     if (st2) return st2;
@@ -153,14 +202,56 @@ int smeared_fermion_force(sfh_ctx* c, const void* phi, void* X, void* Y, double 
     return st;
 }
 
+int smeared_fermion_force(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
+                          long* iters, int* solves)
+{
+    return fermion_force_general(c, phi, X, Y, tol, maxit, prec, iters, solves);
+}
+
+// S_f = sum_k w_k phi_k . X_k (+ |phi|^2 for a Hasenbusch pair) with solves on
+// the current fermion links (smeared when set)
+int fermion_action(sfh_ctx* c, const void* phi, void* X, double tol, int maxit, int prec, double* S, long* iters,
+                   int* solves)
+{
+    PfTerm t[2];
+    const int n = pf_terms(c, phi, X, t);
+    const double m = c->mass;
+    int st = c->fsmear_n > 0 ? smear_in(c) : SFH_OK;
+    double sum = 0.0;
+    for (int k = 0; k < n && !st; ++k) {
+        c->mass = t[k].mass;
+        sfh_cg_info inf;
+        std::memset(&inf, 0, sizeof(inf));
+        st = ctx_solve_device(c, t[k].phi, t[k].X, tol, maxit, prec, &inf);
+        if (iters) *iters += inf.iters;
+        if (solves) *solves += 1;
+        double d = 0.0;
+        if (!st) st = reduce(c, RED_DOT, t[k].phi, t[k].X, &d);
+        sum += t[k].weight * d;
+    }
+    c->mass = m;
+    if (!st && n == 2) {
+        double pp = 0.0;
+        st = reduce(c, RED_DOT, phi, phi, &pp);
+        sum += pp;
+    }
+    if (c->fsmear_n > 0) {
+        int st2 = smear_out(c);
+        if (!st) st = st2;
+    }
+    *S = sum;
+    return st;
+}
+
 // one force evaluation and momentum kick: X = (D D^dag)^-1 phi, Y = D^dag X,
 // P -= kick (F_g + F_f)  (local_* of Fermions.cpp:967-1028); with smeared
-// fermion links F_f comes from the chain rule
+// fermion links or a Hasenbusch pair F_f is the sum over the pseudofermion
+// terms, through the smearing chain rule
 int force_and_kick(sfh_ctx* c, const void* phi, void* X, void* Y, double kick, double tol, int maxit, int prec,
                    long* iters, int* solves)
 {
-    if (c->fsmear_n > 0) {
-        int st = smeared_fermion_force(c, phi, X, Y, tol, maxit, prec, iters, solves);
+    if (c->fsmear_n > 0 || c->hasen_mass > 0.0) {
+        int st = fermion_force_general(c, phi, X, Y, tol, maxit, prec, iters, solves);
         if (!st) st = cuda_check(c, launch_link_axpy(c->g, c->Pmom, -kick, c->Fbuf, c->stream), "kick");
         if (!st) st = cuda_check(c, launch_force(c->g, c->U64, nullptr, nullptr, c->beta, c->c11, c->c12, 1, nullptr,
                                                  c->Pmom, kick, c->stream), "gauge kick");
@@ -285,7 +376,7 @@ extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, doub
     if (cg_iters) *cg_iters = 0;
     void *X = c->spin[4], *Y = c->spin[2];
     int st = SFH_OK;
-    if (ferm && c->fsmear_n > 0) {  // smeared fermion links: chain-rule force, then the gauge part
+    if (ferm && (c->fsmear_n > 0 || c->hasen_mass > 0.0)) {  // smeared links / Hasenbusch: general path
         st = spinor_in(c, phi, c->spin[5]);
         long its = 0;
         if (!st) st = smeared_fermion_force(c, c->spin[5], X, Y, tol, maxit, precision, &its, nullptr);
@@ -332,6 +423,19 @@ extern "C" int sfh_heatbath(sfh_ctx* c, int nsweeps, unsigned long long seed, in
     if (plaq) *plaq = p / (4.0 * V) / 6.0;  // conventional normalisation: 1 on a cold field
     if (action_density) *action_density = a / V;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "heatbath");
+}
+
+extern "C" int sfh_set_hasenbusch(sfh_ctx* c, double heavy_mass, const double* phi_heavy)
+{
+    if (!c || !(heavy_mass >= 0.0)) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    c->hasen_mass = heavy_mass;
+    if (heavy_mass == 0.0) return SFH_OK;
+    int st = ensure_hasen(c);
+    if (!st && phi_heavy) st = spinor_in(c, phi_heavy, c->hphi);
+    else if (!st) st = cuda_check(c, cudaMemsetAsync(c->hphi, 0, spinor_bytes(c), c->stream), "heavy pseudofermion");
+    if (!st) st = cuda_check(c, cudaStreamSynchronize(c->stream), "heavy pseudofermion");
+    return st;
 }
 
 extern "C" int sfh_set_fermion_smearing(sfh_ctx* c, double rho, int nlevels)
@@ -431,27 +535,43 @@ extern "C" int sfh_hmc_trajectory(sfh_ctx* c, double eps, int nsteps, unsigned l
     // (Fermions.cpp:207-212, 302-314)
     if (!st) st = cuda_check(c, launch_random_spinor(c->g, 1.0 / std::sqrt(2.0), seed, chi, c->stream), "chi");
     const bool smeared = c->fsmear_n > 0;  // the fermion operator on stout links
+    const bool hasen = c->hasen_mass > 0.0;
+    if (!st && hasen) st = ensure_hasen(c);
     if (!st && smeared) st = smear_in(c);
-    if (!st) launch_hop(c->g, GP_F64_18, c->U64, SP_F64, chi, SP_F64, phi, chi, c->mass, 1.0, 0, 2, c->stream);
-    if (!st) st = cuda_check(c, launch_random_momenta(c->g, seed + 1, c->Pmom, c->stream), "momenta");
-    if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T0);
-    sfh_cg_info inf;
-    std::memset(&inf, 0, sizeof(inf));
-    if (!st) st = ctx_solve_device(c, phi, X, tol, maxit, precision, &inf);  // Fermions.cpp:819
-    info->cg_iters += inf.iters;
-    info->solves += 1;
-    if (!st) st = reduce(c, RED_DOT, phi, X, &F0);
+    if (!st && !hasen) {
+        launch_hop(c->g, GP_F64_18, c->U64, SP_F64, chi, SP_F64, phi, chi, c->mass, 1.0, 0, 2, c->stream);
+    } else if (!st) {
+        // heavy: phi_h = D(m_h) chi_h; ratio: phi = D(m) D(m_h)^-1 chi = D(m) D(m_h)^dag M(m_h)^-1 chi
+        const double m = c->mass, mh = c->hasen_mass;
+        st = cuda_check(c, launch_random_spinor(c->g, 1.0 / std::sqrt(2.0), seed + 3, c->hX, c->stream), "chi_h");
+        if (!st) launch_hop(c->g, GP_F64_18, c->U64, SP_F64, c->hX, SP_F64, c->hphi, c->hX, mh, 1.0, 0, 2, c->stream);
+        sfh_cg_info inf;
+        std::memset(&inf, 0, sizeof(inf));
+        c->mass = mh;
+        if (!st) st = ctx_solve_device(c, chi, X, tol, maxit, precision, &inf);
+        c->mass = m;
+        info->cg_iters += inf.iters;
+        info->solves += 1;
+        if (!st) {
+            launch_hop(c->g, GP_F64_18, c->U64, SP_F64, X, SP_F64, Y, X, mh, -1.0, 0, 2, c->stream);
+            launch_hop(c->g, GP_F64_18, c->U64, SP_F64, Y, SP_F64, phi, Y, m, 1.0, 0, 2, c->stream);
+        }
+    }
     if (smeared) {
         int st2 = smear_out(c);
         if (!st) st = st2;
     }
+    if (!st) st = cuda_check(c, launch_random_momenta(c->g, seed + 1, c->Pmom, c->stream), "momenta");
+    if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T0);
+    if (!st) st = fermion_action(c, phi, X, tol, maxit, precision, &F0, &info->cg_iters, &info->solves);
     if (!st) st = cuda_check(c, cudaMemcpyAsync(c->Utrial, c->U64, (size_t)c->g.V * 4 * 9 * 16,
                                                 cudaMemcpyDeviceToDevice, c->stream), "gauge backup");
     if (!st) st = leapfrog(c, phi, X, Y, eps, nsteps, tol, maxit, precision, 1, &info->cg_iters, &info->solves);
     double T1 = 0, Sg1 = 0, F1 = 0;
     if (!st) st = reduce(c, RED_TRP2, c->Pmom, nullptr, &T1);
     if (!st) st = reduce(c, RED_ACTION, c->U64, nullptr, &Sg1);
-    if (!st) st = reduce(c, RED_DOT, phi, X, &F1);
+    if (!st && !hasen) st = reduce(c, RED_DOT, phi, X, &F1);  // X of the last force evaluation
+    if (!st && hasen) st = fermion_action(c, phi, X, tol, maxit, precision, &F1, &info->cg_iters, &info->solves);
     if (st) {  // leave the field as it was before the trajectory
         cudaMemcpyAsync(c->U64, c->Utrial, (size_t)c->g.V * 4 * 9 * 16, cudaMemcpyDeviceToDevice, c->stream);
         cudaStreamSynchronize(c->stream);

@@ -44,6 +44,9 @@ struct sfh_ctx {
     size_t smear_bytes = 0;
     double fsmear_rho = 0.0;       // stout smearing of the fermion links (HMC)
     int fsmear_n = 0;              // levels; 0 = thin links
+    double hasen_mass = 0.0;       // Hasenbusch heavy mass (0 = one pseudofermion)
+    void* hphi = nullptr;          // heavy pseudofermion and its solution (FP64 spinors)
+    void* hX = nullptr;
 
     std::string last_error;
 };

@@ -422,3 +422,42 @@ def test_heatbath_rejects_extents_not_multiple_of_four(sfh, orc):
     with pytest.raises(sfh.SfhError) as e:
         lat.heatbath_update(1)
     assert e.value.status == sfh.SFH_ERR_INVALID
+
+
+# --- Hasenbusch pair (no counterpart in the reference) --------------------
+def test_hasenbusch_force_vs_oracle(sfh, orc):
+    """P -= dt F with F = F_f(X_h, Y_h) + (m_h^2 - m^2) F_f(X, Y), X_h solved at
+    the heavy mass, X at the light one."""
+    dims, m, mh, beta, dt = (4, 4, 4, 8), 0.1, 0.4, 4.2, 0.05
+    U = orc.random_gauge(dims, 0.4, 201)
+    phi = orc.random_spinor(dims, 202)
+    phih = orc.random_spinor(dims, 203)
+    lat = sfh.Lattice(dims, m, beta)
+    lat.upload_gauge(U)
+    lat.upload_momenta(np.zeros(72 * int(np.prod(dims))))
+    lat.set_hasenbusch(mh, phih)
+    lat.momentum_kick(dt, phi, forces="fermion", tol=1e-13)
+    Xh, _, _, _ = orc.cg(dims, mh, U, phih, 1e-13)
+    Xr, _, _, _ = orc.cg(dims, m, U, phi, 1e-13)
+    F = orc.fermion_force(dims, U, Xh, orc.dirac(dims, mh, U, Xh, dagger=True)) + \
+        (mh * mh - m * m) * orc.fermion_force(dims, U, Xr, orc.dirac(dims, m, U, Xr, dagger=True))
+    assert rel(lat.download_momenta(), -dt * F) < 1e-10
+
+
+@pytest.mark.parametrize("smear", [0, 2])
+def test_hasenbusch_trajectory_second_order(sfh, orc, smear):
+    """dH(eps)/dH(eps/2) ~ 4 for the two-pseudofermion action (and on smeared
+    links), from the same field and seed."""
+    dims = (4, 4, 4, 4)
+    U = orc.random_gauge(dims, 0.15, 211)
+    lat = sfh.Lattice(dims, 0.1, 4.2)
+    lat.set_hasenbusch(0.4)
+    if smear:
+        lat.set_fermion_smearing(0.125, smear)
+
+    def dH(eps, n):
+        lat.upload_gauge(U)
+        return lat.hmc_trajectory(eps, n, seed=31, tol=1e-14)["dH"]
+
+    d1, d2 = dH(0.04, 5), dH(0.02, 10)
+    assert 3.5 < abs(d1) / abs(d2) < 4.5, (d1, d2)
