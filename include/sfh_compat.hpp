@@ -23,6 +23,7 @@
 
 #include <array>
 #include <complex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -101,6 +102,10 @@ void local_final_step_gauge(std::vector<double>& P_field, double beta, Link_arra
 // ---- Lattice.h --------------------------------------------------------------
 double compute_action(const Link_array& arr, double beta);
 double compute_avg_plaq(const Link_array& arr);
+// one heatbath sweep (Lattice.cpp:722-757); returns (average plaquette, action
+// per site) after the sweep.  Seeded: the sweeps of a thread draw from the
+// settings' seed and a sweep counter.
+std::pair<double, double> heatbath_update(Link_array& arr, double beta);
 std::vector<std::complex<double>> precompute_polyakov_grid(const Link_array& arr);
 std::complex<double> correlator_over_fixed_distance_fast(const std::vector<std::complex<double>>& P_grid,
                                                          int r_squared);

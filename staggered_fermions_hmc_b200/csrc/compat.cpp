@@ -17,6 +17,7 @@ struct ThreadState {
     Settings s;
     sfh_ctx* ctx = nullptr;
     unsigned long long draws = 0;
+    int sweeps = 0;  // heatbath sweeps so far (the sweep index of the uniforms)
 };
 
 thread_local ThreadState T;
@@ -132,6 +133,7 @@ void configure(const Settings& s)
     shutdown();
     T.s = s;
     T.draws = 0;
+    T.sweeps = 0;
 }
 
 const Settings& settings() { return T.s; }
@@ -422,6 +424,16 @@ double compute_avg_plaq(const Link_array& arr)
     double s = 0.0;
     check(sfh_plaquette(ctx(), &s));
     return s;
+}
+
+std::pair<double, double> heatbath_update(Link_array& arr, double beta)
+{
+    gauge_in(arr);
+    check(sfh_set_beta(ctx(), beta));
+    double plaq = 0.0, act = 0.0;
+    check(sfh_heatbath(ctx(), 1, T.s.seed, T.sweeps++, &plaq, &act));
+    gauge_out(arr);
+    return {plaq, act};
 }
 
 std::vector<std::complex<double>> precompute_polyakov_grid(const Link_array& arr)

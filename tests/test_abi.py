@@ -71,7 +71,7 @@ COMPAT_FUNCTIONS = [
     "local_leapfrog_steps_fermion", "local_final_step_fermion", "local_initial_half_step_gauge",
     "local_leapfrog_steps_gauge", "local_final_step_gauge", "compute_action", "compute_avg_plaq",
     "precompute_polyakov_grid", "correlator_over_fixed_distance_fast", "save_lattice_configs",
-    "load_lattice_configs", "Apply_HEX_smearing", "Apply_4HEX_smearing",
+    "load_lattice_configs", "Apply_HEX_smearing", "Apply_4HEX_smearing", "heatbath_update",
 ]
 
 
