@@ -164,12 +164,13 @@ def solve_bytes(spec, infos, precision):
 
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
-# algorithmic byte of cg_hop2, f32, RHS groups of 2, 4 tiles per block: one
-# launch of the first 8 systems of the batch with every lane active (553.2 MB
-# of DRAM traffic for 491.0 MB of algorithmic bytes), the capture summarised
-# in profiles/cg_iteration_kernels_f32_batch8_ncu.md.  The bench scales it to
-# its own launches by their algorithmic bytes.
-HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0}
+# algorithmic byte of cg_hop2 for one launch of the first 8 systems of the
+# batch with every lane active, RHS groups of 2, 4 tiles per block: f32 553.2
+# MB for 491.0 MB (profiles/cg_iteration_kernels_f32_batch8_ncu.md), f16 with
+# staged links 242.8 MB for 291.9 MB (profiles/cg_iteration_kernels_f16_
+# batch8_ncu.md).  The bench scales it to its own launches by their
+# algorithmic bytes.
+HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 242.8 / 291.9}
 
 
 def build_batch(sfh, spec, precision, device):
