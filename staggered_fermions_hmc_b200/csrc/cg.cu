@@ -191,9 +191,9 @@ __device__ __forceinline__ void vfma(Vec3<R>& acc, R s, const Vec3<R>& w)
 }
 
 template <typename R>
-__device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg)
+__device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg, R scale = R(1))
 {
-    const R s = neg ? R(-1) : R(1);
+    const R s = neg ? -scale : scale;
     Vec3<R> o;
 #pragma unroll
     for (int k = 0; k < 3; ++k) o.c[k] = {s * v.c[k].re, s * v.c[k].im};
@@ -266,17 +266,26 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
 {
     typedef typename GaugeFmt<GP>::R R;
     const int nq = 1 - q;
+    // 18-element links (FP64, FP32-18) leave fewer registers: the signs go
+    // onto the input vectors and both hops accumulate into acc directly;
+    // otherwise the two hops of a direction are summed first and take eta/2 once
+    constexpr bool direct = GaugeFmt<GP>::K == 9;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
-        Vec3<R> w[NB];
+        const R s = ((n.eta >> mu) & 1u) ? R(-0.5) : R(0.5);
+        Vec3<R> w[direct ? 1 : NB];
         {
             const Mat3<R> U = hop_link<GP, STG>(sl, Ulo, 2 * mu, q, mu, i, Vh);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
                     Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh));
-                    if (mu == 3) v = vneg_if(v, n.wu);
-                    mv_add<true>(w[l], U, v);
+                    if constexpr (direct) {
+                        mv_add<false>(acc[l], U, vneg_if(v, n.wu && mu == 3, s));
+                    } else {
+                        if (mu == 3) v = vneg_if(v, n.wu);
+                        mv_add<true>(w[l], U, v);
+                    }
                 }
         }
         {
@@ -285,14 +294,19 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
                     Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh));
-                    if (mu == 3) v = vneg_if(v, n.wd);
-                    mdv_sub(w[l], U, v);
+                    if constexpr (direct) {
+                        mdv_sub(acc[l], U, vneg_if(v, n.wd && mu == 3, s));
+                    } else {
+                        if (mu == 3) v = vneg_if(v, n.wd);
+                        mdv_sub(w[l], U, v);
+                    }
                 }
         }
-        const R s = ((n.eta >> mu) & 1u) ? R(-0.5) : R(0.5);
+        if constexpr (!direct) {
 #pragma unroll
-        for (int l = 0; l < NB; ++l)
-            if (on[l]) vfma(acc[l], s, w[l]);
+            for (int l = 0; l < NB; ++l)
+                if (on[l]) vfma(acc[l], s, w[l]);
+        }
     }
 }
 
@@ -553,8 +567,12 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
+    // the FP64 hop of lanes in a reliable update: here for the reduced
+    // precisions, in cg_ru1 for FP64 lanes (keeps the FP64 hop's registers
+    // free; measured faster both ways)
+    constexpr bool ru_here = SP != SP_F64;
     gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
-    if (!(P.anyA || P.anyR)) return;
+    if (!(P.anyA || (ru_here && P.anyR))) return;
     const void* pin[NB];
     const void* tout[NB];
     bool on[NB];
@@ -584,17 +602,43 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
             }
         }
     }
-    // reliable updates in a loop of their own: no call inside the hop loop
-    // (a call there makes the compiler keep the hop's registers on the stack)
-    if (P.anyR) {
-        for (int t = ir.first; t < ir.end; ++t) {
-            const TileInfo ti = decode_tile(S, t);
-            if (!ti.valid) break;
-            const Coord c = eo_coords(S.g, q, ti.i);
+    if constexpr (ru_here) {
+        // in a loop of its own: no call inside the hop loop
+        if (P.anyR) {
+            for (int t = ir.first; t < ir.end; ++t) {
+                const TileInfo ti = decode_tile(S, t);
+                if (!ti.valid) break;
+                const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll 1
-            for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
+                for (int l = 0; l < NB; ++l)
+                    if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
+            }
         }
+    }
+}
+
+// the FP64 hop of the lanes of a work item that are in a reliable update
+// (a kernel of its own: the FP64 registers stay out of the hop kernels)
+template <int SP, int NB>
+__global__ void __launch_bounds__(kTile) cg_ru1(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const ItemRange ir = item_range(a, S, it.x);
+    const int q = ir.q;
+    LanePass<NB> P;
+    gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
+    if (!P.anyR) return;
+    for (int t = ir.first; t < ir.end; ++t) {
+        const TileInfo ti = decode_tile(S, t);
+        if (!ti.valid) break;
+        const Coord c = eo_coords(S.g, q, ti.i);
+#pragma unroll 1
+        for (int l = 0; l < NB; ++l)
+            if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
     }
 }
 
@@ -658,15 +702,19 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
+    // the reliable-update residuals stay in this kernel: measured faster than
+    // a kernel of their own, and the compiler keeps the FP64 hop's registers
+    // better with them here
+    constexpr bool ru_here = true;
     gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
-    if (!(P.anyA || P.anyR)) return;  // uniform across the block
+    if (!(P.anyA || (ru_here && P.anyR))) return;  // uniform across the block
     bool part[NB], on[NB];
     double sums[NB * kSums];
     const void* tin[NB];
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
-        part[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART || P.mode[l] == LM_RU;
         on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+        part[l] = on[l] || (ru_here && P.mode[l] == LM_RU);
         tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
 #pragma unroll
         for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
@@ -709,16 +757,61 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
             }
         }
     }
-    // reliable updates in a loop of their own (no call inside the hop loop)
-    if (P.anyR) {
-        for (int t = ir.first; t < ir.end; ++t) {
-            const TileInfo ti = decode_tile(S, t);
-            if (!ti.valid) break;
-            const Coord c = eo_coords(S.g, q, ti.i);
+    if constexpr (ru_here) {
+        if (P.anyR) {
+            for (int t = ir.first; t < ir.end; ++t) {
+                const TileInfo ti = decode_tile(S, t);
+                if (!ti.valid) break;
+                const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+                for (int l = 0; l < NB; ++l)
+                    if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+            }
         }
+    }
+    block_sum<NB * kSums>(sums, smem);
+    const unsigned nsq = (unsigned)item_groups(a, S);
+    unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ir.slot, S.both ? 2u * nsq : nsq, &s_mask);
+    if (mask && threadIdx.x < 32) {
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+            if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
+    }
+}
+
+// the reliable-update residuals of the lanes of a work item that are in a
+// reliable update: |b - M x|^2 in FP64 as the lane's sum, then the lane's
+// scalars (finish_lane) once its last item has arrived
+template <int SP, int NB>
+__global__ void __launch_bounds__(kTile) cg_ru2(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    __shared__ double smem[32 * NB * kSums];
+    __shared__ unsigned s_mask;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const ItemRange ir = item_range(a, S, it.x);
+    const int q = ir.q;
+    LanePass<NB> P;
+    gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
+    if (!P.anyR) return;  // uniform across the block
+    bool part[NB];
+    double sums[NB * kSums];
+#pragma unroll
+    for (int l = 0; l < NB; ++l) {
+        part[l] = P.mode[l] == LM_RU;
+#pragma unroll
+        for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
+    }
+    for (int t = ir.first; t < ir.end; ++t) {
+        const TileInfo ti = decode_tile(S, t);
+        if (!ti.valid) break;
+        const Coord c = eo_coords(S.g, q, ti.i);
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+            if (part[l]) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
     }
     block_sum<NB * kSums>(sums, smem);
     const unsigned nsq = (unsigned)item_groups(a, S);
@@ -787,6 +880,7 @@ typedef void (*HopKernel)(CgArgs, const int2*, int);
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
+    HopKernel ru1, ru2;  // the reliable-update parts of the two hops
     int nb1, nb2;   // RHS-group widths the hop kernels are compiled for
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
 };
@@ -822,6 +916,9 @@ static CgKernels pick_typed(int nb1, int nb2)
     k.hop1 = pick_hop1<GP, SP, STG>(nb1, &k.nb1);
     pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
+    k.ru1 = k.nb1 == 8 ? cg_ru1<SP, 8> : (k.nb1 == 4 ? cg_ru1<SP, 4> : (k.nb1 == 2 ? cg_ru1<SP, 2> : cg_ru1<SP, 1>));
+    k.ru2 = nullptr;  // cg_hop2 does the reliable-update residuals itself
+    if constexpr (SP != SP_F64) k.ru1 = nullptr;  // cg_hop1 does them itself
     k.smem = STG ? StageBytes<GP>::v : 0;
     return k;
 }
@@ -1019,6 +1116,9 @@ static int default_nb(int max_nrhs, int cap)
 }
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
+// kernels per CG iteration: hop1, its reliable-update part, hop2, its
+// reliable-update part, update
+constexpr int kPhases = 5;
 
 // Work items (first tile, first RHS): tpi tiles of one parity of a system and
 // one RHS group of width nb; one block each.  The groups of a tile range are
@@ -1074,30 +1174,33 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
 static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, double tol, int maxit,
                                 double delta)
 {
-    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.g_tol == tol &&
+    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.gk.ru1 == k.ru1 &&
+        w.gk.ru2 == k.ru2 && w.g_tol == tol &&
         w.g_tpi == a.tpi &&
         w.g_maxit == maxit &&
         w.g_delta == delta)
         return cudaSuccess;
     w.release_graph();
-    const int2* items[3];
-    int nitems[3];
-    const int widths[3] = {k.nb1, k.nb2, 1};
+    const int2* items[kPhases];
+    int nitems[kPhases];
+    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, k.nb2, 1};
+    const HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.ru2, k.update};
     cudaError_t e;
-    for (int ph = 0; ph < 3; ++ph)
+    for (int ph = 0; ph < kPhases; ++ph)
         if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
     e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
     cudaGraphNode_t prev = nullptr;
     for (int it = 0; it < kChunk; ++it) {
         int cur = it & 1;
-        for (int ph = 0; ph < 3; ++ph) {
+        for (int ph = 0; ph < kPhases; ++ph) {
+            if (!fn[ph]) continue;
             cudaKernelNodeParams p;
             std::memset(&p, 0, sizeof(p));
-            p.func = (void*)(ph == 0 ? k.hop1 : (ph == 1 ? k.hop2 : k.update));
+            p.func = (void*)fn[ph];
             p.gridDim = dim3(nitems[ph]);
             p.blockDim = dim3(kTile);
-            p.sharedMemBytes = ph < 2 ? (unsigned)k.smem : 0u;
+            p.sharedMemBytes = (ph == 0 || ph == 2) ? (unsigned)k.smem : 0u;
             void* args[] = {&a, (void*)&items[ph], &cur};
             p.kernelParams = args;
             cudaGraphNode_t node;
@@ -1123,7 +1226,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
 // Device time of each iteration kernel over one solve (timed solves launch
 // the kernels one by one between CUDA events instead of replaying the graph).
 struct PhaseTimes {
-    double ms[3];  // hop1, hop2, update
+    double ms[3];  // hop1, hop2, update (each with its reliable-update kernel)
     long n[3];
 };
 
@@ -1157,18 +1260,20 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (!timing && (e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
     // timed solves: the same kernels and work items, launched one by one
-    const int2* items[3];
-    int nitems[3];
-    const int widths[3] = {k.nb1, k.nb2, 1};
-    HopKernel fn[3] = {k.hop1, k.hop2, k.update};
+    const int2* items[kPhases];
+    int nitems[kPhases];
+    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, k.nb2, 1};
+    HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.ru2, k.update};
+    const int report[kPhases] = {0, 0, 1, 1, 2};  // the reliable-update kernels count with their hop
     std::vector<cudaEvent_t> tev;
     if (timing) {
-        for (int ph = 0; ph < 3; ++ph) {
+        for (int ph = 0; ph < kPhases; ++ph)
             if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
-            timing->ms[ph] = 0.0;
-            timing->n[ph] = 0;
+        for (int r = 0; r < 3; ++r) {
+            timing->ms[r] = 0.0;
+            timing->n[r] = 0;
         }
-        tev.resize(2 * (3 * kChunk + 1));
+        tev.resize(2 * (kPhases * kChunk + 1));
         for (cudaEvent_t& ev : tev)
             if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
     }
@@ -1178,24 +1283,27 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         tev.clear();
     };
     auto accumulate = [&](int pool) {  // a finished chunk's per-kernel times
-        cudaEvent_t* ev = tev.data() + pool * (3 * kChunk + 1);
-        for (int j = 0; j < 3 * kChunk; ++j) {
+        cudaEvent_t* ev = tev.data() + pool * (kPhases * kChunk + 1);
+        for (int j = 0; j < kPhases * kChunk; ++j) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
-            timing->ms[j % 3] += ms;
-            timing->n[j % 3] += 1;
+            const int r = report[j % kPhases];
+            timing->ms[r] += ms;
+            if (j % kPhases != 1 && j % kPhases != 3) timing->n[r] += 1;
         }
     };
     const int max_chunks = a.maxloop / kChunk + 2;
     // keep one chunk queued ahead of the convergence check
     for (int c = 0; c < max_chunks; ++c) {
         if (timing) {
-            cudaEvent_t* ev = tev.data() + (c & 1) * (3 * kChunk + 1);
+            cudaEvent_t* ev = tev.data() + (c & 1) * (kPhases * kChunk + 1);
             if ((e = cudaEventRecord(ev[0], stream)) != cudaSuccess) { destroy_events(); return e; }
             for (int it = 0; it < kChunk; ++it)
-                for (int ph = 0; ph < 3; ++ph) {
-                    fn[ph]<<<nitems[ph], kTile, ph < 2 ? k.smem : 0, stream>>>(a, items[ph], it & 1);
-                    if ((e = cudaEventRecord(ev[3 * it + ph + 1], stream)) != cudaSuccess) {
+                for (int ph = 0; ph < kPhases; ++ph) {
+                    if (fn[ph])
+                        fn[ph]<<<nitems[ph], kTile, (ph == 0 || ph == 2) ? k.smem : 0, stream>>>(a, items[ph],
+                                                                                               it & 1);
+                    if ((e = cudaEventRecord(ev[kPhases * it + ph + 1], stream)) != cudaSuccess) {
                         destroy_events();
                         return e;
                     }
@@ -1203,7 +1311,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         } else if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) {
             return e;
         }
-        w.launches += 3 * kChunk;
+        w.launches += (kPhases - (k.ru1 ? 0 : 1) - (k.ru2 ? 0 : 1)) * kChunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
