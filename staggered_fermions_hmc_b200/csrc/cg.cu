@@ -259,6 +259,20 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
+// a neighbour spinor with the hop's scalar factor applied: the eta / 2 and
+// time-wrap sign, and for FP16 storage the per-site scale (one multiply)
+template <int SP, typename R>
+__device__ __forceinline__ Vec3<R> hop_input(const void* in, int nq, int j, int Vh, bool neg, R s)
+{
+    if constexpr (SP == SP_F16) {
+        float sc;
+        Vec3<R> v = SpinorFmt<SP>::load_unscaled(in, nq, j, Vh, &sc);
+        return vneg_if(v, neg, s * sc);
+    } else {
+        return vneg_if(vcvt<R>(SpinorFmt<SP>::load(in, nq, j, Vh)), neg, s);
+    }
+}
+
 template <int GP, int SP, int NB, bool STG>
 __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeFmt<GP>::E* sl, const Nbr& n, int q,
                                           int i, int Vh, const void* const (&in)[NB], const bool (&on)[NB],
@@ -266,10 +280,11 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
 {
     typedef typename GaugeFmt<GP>::R R;
     const int nq = 1 - q;
-    // 18-element links (FP64, FP32-18) leave fewer registers: the signs go
-    // onto the input vectors and both hops accumulate into acc directly;
-    // otherwise the two hops of a direction are summed first and take eta/2 once
-    constexpr bool direct = GaugeFmt<GP>::K == 9;
+    // Both hops of a direction accumulate into acc directly, the scalar
+    // factor (eta/2, the anti-periodic time sign, the FP16 site scale) going
+    // onto the input vector; FP32-12 sums the two hops of a direction first
+    // and applies eta/2 once (measured faster there)
+    constexpr bool direct = GaugeFmt<GP>::K == 9 || SP == SP_F16;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
         const R s = ((n.eta >> mu) & 1u) ? R(-0.5) : R(0.5);
@@ -279,10 +294,10 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
-                    Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh));
                     if constexpr (direct) {
-                        mv_add<false>(acc[l], U, vneg_if(v, n.wu && mu == 3, s));
+                        mv_add<false>(acc[l], U, hop_input<SP>(in[l], nq, n.up[mu], Vh, n.wu && mu == 3, s));
                     } else {
+                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh));
                         if (mu == 3) v = vneg_if(v, n.wu);
                         mv_add<true>(w[l], U, v);
                     }
@@ -293,10 +308,10 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
-                    Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh));
                     if constexpr (direct) {
-                        mdv_sub(acc[l], U, vneg_if(v, n.wd && mu == 3, s));
+                        mdv_sub(acc[l], U, hop_input<SP>(in[l], nq, n.dn[mu], Vh, n.wd && mu == 3, s));
                     } else {
+                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh));
                         if (mu == 3) v = vneg_if(v, n.wd);
                         mdv_sub(w[l], U, v);
                     }

@@ -314,6 +314,22 @@ template <> struct SpinorFmt<SP_F16> {
         return unpack(__ldcg((const uint4*)base + (size_t)p * Vh + i));
     }
     __device__ static __forceinline__ Vec3<R> quantize(const Vec3<R>& v) { return unpack(pack(v)); }
+    // the halves converted, without the scale (returned in *scale)
+    __device__ static __forceinline__ Vec3<R> load_unscaled(const void* base, int p, int i, int Vh, float* scale)
+    {
+        const uint4* b = (const uint4*)base + (size_t)p * Vh;
+        uint4 w = __ldg(b + i);
+        *scale = __uint_as_float(w.w);
+        Vec3<R> v;
+        uint32_t words[3] = {w.x, w.y, w.z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            __half2 h = *reinterpret_cast<__half2*>(&words[c]);
+            float2 f = __half22float2(h);
+            v.c[c] = {f.x, f.y};
+        }
+        return v;
+    }
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
