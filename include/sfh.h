@@ -274,6 +274,12 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * their links in shared memory with asynchronous copies (reduced precisions
  * only); and its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
+/* Reliable-update threshold of the mixed precisions (default 0.1 for
+ * SFH_PREC_F16, 0.01 for the FP32 storages): an FP64
+ * update (x_hi += x_lo, r = b - M x_hi) when the iterated residual has dropped
+ * by this factor below its largest value since the last update.  No
+ * counterpart in the reference (its CG is FP64 only). */
+int sfh_batch_set_reliable_delta(sfh_batch* batch, double delta);
 int sfh_batch_get_schedule(sfh_batch* batch, int* width, int* tiles_per_block, int* stage_links);
 int sfh_batch_set_gauge(sfh_batch* batch, int sys, const double* links);
 int sfh_batch_set_rhs(sfh_batch* batch, int sys, int rhs, const double* phi);

@@ -147,6 +147,7 @@ SIGNATURES = {
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_set_reliable_delta": (ctypes.c_int, [_VP, ctypes.c_double]),
     "sfh_batch_solve_timed": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, _D,
                                              ctypes.POINTER(ctypes.c_long)]),
     "sfh_batch_get_schedule": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
@@ -529,6 +530,10 @@ class Batch:
     def set_schedule(self, width, tiles_per_block, stage_links=False):
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, 1 if stage_links else 0),
                     "set_schedule")
+
+    def set_reliable_delta(self, delta):
+        """Reliable-update threshold of the mixed precisions (default 0.1)."""
+        self._check(self.lib.sfh_batch_set_reliable_delta(self.h, delta), "set_reliable_delta")
 
     def schedule(self):
         """(RHS-block width, tiles per block, links staged) the next solve uses."""
