@@ -591,7 +591,7 @@ def main():
             B.solve(tol=TOL, max_iter=MAXIT)
             for k, s in enumerate(spec):
                 for j in range(s["nrhs"]):
-                    host_x[k][j][:] = B.solution(k, j)
+                    B.solution(k, j, out=host_x[k][j])
 
         te = time_steps(torch, B.stream, e2e_step, max(2, args.steps // 2), 1)
         mse = max_over_ranks(statistics.mean(te), world)

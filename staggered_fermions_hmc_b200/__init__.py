@@ -532,7 +532,8 @@ class Batch:
                     "set_schedule")
 
     def set_reliable_delta(self, delta):
-        """Reliable-update threshold of the mixed precisions (default 0.1)."""
+        """Reliable-update threshold of the mixed precisions (default 0.1 for
+        "f16", 0.01 for the FP32 storages)."""
         self._check(self.lib.sfh_batch_set_reliable_delta(self.h, delta), "set_reliable_delta")
 
     def schedule(self):
@@ -572,8 +573,14 @@ class Batch:
             self._check(st, "batch solve")
         return st
 
-    def solution(self, k, j):
-        X = np.empty(6 * volume(self.systems[k][0]))
+    def solution(self, k, j, out=None):
+        """X of system k, right-hand side j (reference layout).  With ``out``
+        (a C-contiguous float64 array of 6 V, e.g. in pinned memory) the
+        solution is copied straight into it."""
+        n = 6 * volume(self.systems[k][0])
+        X = np.empty(n) if out is None else out
+        if X.size != n:
+            raise ValueError(f"out has {X.size} elements, expected {n}")
         self._check(self.lib.sfh_batch_get_solution(self.h, k, j, _dptr(X)), "get_solution")
         return X
 

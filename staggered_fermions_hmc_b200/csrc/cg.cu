@@ -29,8 +29,9 @@
 // x is accumulated in FP32 between reliable updates.  When |r| has dropped by
 // delta since the last update, or the recurrence meets the target, the lane
 // spends its next iteration on an FP64 reliable update: x_hi += x_lo and
-// r = b - M x_hi with FP64 links and vectors, keeping p.  Mixed lanes
-// converge only on that FP64 true residual.
+// r = b - M x_hi with FP64 links and vectors, keeping p (rebuilt on the
+// true residual: p += r_true - r_iter).  Mixed lanes converge only on that
+// FP64 true residual.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -660,7 +661,7 @@ __global__ void __launch_bounds__(kTile) cg_ru1(CgArgs a, const int2* __restrict
 // reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
 // r = b - M x_hi; returns the |r|^2 contribution (FP64)
 template <int SP, int XP>
-__device__ __forceinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
+__device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     typedef typename SpinorFmt<SP>::R RS;
     const int nq = 1 - q, Vh = S.g.Vh;
@@ -693,7 +694,23 @@ __device__ __forceinline__ double ru_hop2(const CgArgs& a, const CgSys& S, const
         res.c[k].re = b.c[k].re - (S.m2 * xn.c[k].re - 0.5 * acc.c[k].re);
         res.c[k].im = b.c[k].im - (S.m2 * xn.c[k].im - 0.5 * acc.c[k].im);
     }
-    SpinorFmt<SP>::store(rhs_ptr(a, rid, F_R), q, i, Vh, vcvt<RS>(res));
+    // The search direction of the previous update, p = r_iter + beta p_old,
+    // was built from the iterated residual; give it the true one instead,
+    // p = r_true + beta p_old, by adding the correction r_true - r_iter.
+    // Without it the low-precision lanes of ill-conditioned systems lose
+    // their Krylov progress at every update (FP16 storage, eps = 1 links,
+    // m = 0.02 on 16^4: 7648 iterations against FP64's 1564; 1750 with it).
+    void* rp = rhs_ptr(a, rid, F_R);
+    void* pp = rhs_ptr(a, rid, F_P);
+    const Vec3<RS> r_iter = SpinorFmt<SP>::load_cg(rp, q, i, Vh);
+    Vec3<RS> p = SpinorFmt<SP>::load_cg(pp, q, i, Vh);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        p.c[k].re += (RS)res.c[k].re - r_iter.c[k].re;
+        p.c[k].im += (RS)res.c[k].im - r_iter.c[k].im;
+    }
+    SpinorFmt<SP>::store(pp, q, i, Vh, p);
+    SpinorFmt<SP>::store(rp, q, i, Vh, vcvt<RS>(res));
     return vdot_re(res, res);
 }
 
@@ -780,7 +797,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
                 const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
                 for (int l = 0; l < NB; ++l)
-                    if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+                    if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
             }
         }
     }
@@ -826,7 +843,7 @@ __global__ void __launch_bounds__(kTile) cg_ru2(CgArgs a, const int2* __restrict
         const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
         for (int l = 0; l < NB; ++l)
-            if (part[l]) sums[l * kSums + 3] += ru_hop2<SP, XP>(a, S, c, q, ti.i, P.rid[l]);
+            if (part[l]) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
     }
     block_sum<NB * kSums>(sums, smem);
     const unsigned nsq = (unsigned)item_groups(a, S);
@@ -1245,6 +1262,12 @@ struct PhaseTimes {
     long n[3];
 };
 
+// Reliable-update threshold (|r| drop between FP64 updates) of the mixed
+// precisions: FP16 storage needs the tighter 0.1 (at 0.02 its recurrence
+// drifts too far to converge); FP32 keeps its recurrence to 0.01, half the
+// updates of 0.1 at the same iteration count.
+static double default_reliable_delta(int prec) { return prec == SFH_PREC_F16 ? 0.1 : 0.01; }
+
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
                                    int tpi, bool stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
 {
@@ -1429,7 +1452,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
     b->flags = flags;
     // FP16 vectors track a drop of about 10x before they lose accuracy; FP32
     // ones a drop of 100x (fewer FP64 updates, same iterations: measured)
-    b->delta = precision == SFH_PREC_F16 ? 0.1 : 0.01;
+    b->delta = sfh::default_reliable_delta(precision);
     b->desc.assign(systems, systems + nsys);
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -1675,7 +1698,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");
-    e = workspace_solve(*w, tol, maxit, 0.1, 0, 0, 0, false, c->stream);
+    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), 0, 0, 0, false, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
     e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solution");

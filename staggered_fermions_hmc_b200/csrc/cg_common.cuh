@@ -193,11 +193,13 @@ __device__ __forceinline__ int lane_nslots(const CgSys& S) { return S.both ? 2 *
 
 // pointer fields of the per-RHS vector table (read-only during the kernel)
 enum RhsField { F_B = 0, F_XHI, F_THI, F_R, F_P, F_V, F_T, F_XLO };
-__device__ __forceinline__ void* rhs_ptr(const CgArgs& a, int rid, int f)
+__device__ __forceinline__ void* rhs_ptr(const CgRhs* rhs, int rid, int f)
 {
-    const unsigned long long* base = reinterpret_cast<const unsigned long long*>(a.rhs + rid);
+    const unsigned long long* base = reinterpret_cast<const unsigned long long*>(rhs + rid);
     return reinterpret_cast<void*>(__ldg(base + f));
 }
+
+__device__ __forceinline__ void* rhs_ptr(const CgArgs& a, int rid, int f) { return rhs_ptr(a.rhs, rid, f); }
 
 }  // namespace
 }  // namespace sfh

@@ -145,6 +145,9 @@ def test_batch_uneven_systems(sfh, orc, precision):
             r = true_resid(orc, dims, mass, U, bs[j], X)
             assert r < 1.5 * tol, (k, j, r, info)
             assert abs(B.true_residual(k, j) - r) < 1e-3 * tol + 1e-3 * r
+            out = np.full(X.size, np.nan)
+            assert B.solution(k, j, out=out) is out
+            assert np.array_equal(out, X)
 
 
 def test_batch_full_lattice_matches_single(sfh, orc):
@@ -216,3 +219,23 @@ def test_batch_timed_solve_matches_graph_solve(sfh, orc):
     n = [times[k][1] for k in ("cg_hop1", "cg_hop2", "cg_update")]
     assert n[0] == n[1] == n[2] > 0
     assert all(times[k][0] > 0 for k in times)
+
+
+@pytest.mark.parametrize("precision", ["f16", "f32"])
+def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, precision):
+    """eps = 1 links at m = 0.02 on 16^4: the mixed-precision CG needs at most
+    a quarter more iterations than FP64 (the reliable update rebuilds the
+    search direction on the true residual; without it FP16 took 4.9 times
+    FP64's count here), and reaches the FP64 true residual."""
+    tol = 1e-10
+    lat = sfh.Lattice((16, 16, 16, 16), 0.02, 4.2)
+    try:
+        lat.random_gauge(1.0, 21)
+        phi = lat.gaussian_spinor(22)
+        X64, i64 = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision="f64", info=True)
+        X, inf = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision=precision, info=True)
+        assert inf["status"] == 0
+        assert inf["iters"] <= 1.25 * i64["iters"], (inf, i64)
+        assert rel(X, X64) < 1e-6
+    finally:
+        lat.close()
