@@ -124,8 +124,8 @@ class ClockSampler:
 # update (mixed precision) adds an FP64 hop in each hop kernel (8 FP64 links,
 # the FP64 solution or temporary) and the FP64 residual in cg_hop2.
 # ---------------------------------------------------------------------------
-SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24}
-LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72}
+SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24, "bf16": 16}
+LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72, "bf16": 24}
 KERNELS = ("cg_hop1", "cg_hop2", "cg_update")
 
 
@@ -165,11 +165,10 @@ def solve_bytes(spec, infos, precision):
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
 # algorithmic byte of cg_hop2 for one launch of the first 8 systems of the
-# batch with every lane active, RHS groups of 2, 4 tiles per block: f32 553.2
-# MB for 491.0 MB (profiles/cg_iteration_kernels_f32_batch8_ncu.md), f16 with
-# staged links 242.8 MB for 291.9 MB (profiles/cg_iteration_kernels_f16_
-# batch8_ncu.md).  The bench scales it to its own launches by their
-# algorithmic bytes.
+# batch with every lane active, RHS groups of 2, 4 tiles per block (the ncu
+# captures of the three iteration kernels kept under profiles/): f32 553.2 MB
+# for 491.0 MB, f16 with staged links 242.8 MB for 291.9 MB.  The bench
+# scales it to its own launches by their algorithmic bytes.
 HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 242.8 / 291.9}
 
 
@@ -320,8 +319,11 @@ def make_host_fields(spec, device):
     return fields
 
 
-DSLASH_BYTES = {0: 1248, 1: 432, 2: 224, 3: 624}   # per output site, see DESIGN.md
-DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18"}
+# algorithmic bytes per output site of one hop: its 8 links (144 / 48 / 24 /
+# 72 / 24 B), one input vector (each is the neighbour of 8 sites but leaves
+# DRAM once) and one output vector (48 / 24 / 16 / 24 / 16 B)
+DSLASH_BYTES = {0: 1248, 1: 432, 2: 224, 3: 624, 4: 224}
+DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18", 4: "bf16_12"}
 
 
 def run_extras(sfh, hbm, quick=False):
@@ -336,7 +338,7 @@ def run_extras(sfh, hbm, quick=False):
     lat.random_gauge(1.0, 3)
     Vh = int(np.prod(dims)) // 2
     ds = {}
-    for st in (0, 3, 1, 2):
+    for st in (0, 3, 1, 2, 4):
         ms = lat.dslash_timing(st, nrep=20)
         gbs = DSLASH_BYTES[st] * Vh / (ms * 1e-3) / 1e9
         ds[DSLASH_NAMES[st]] = {"ms_per_hop": ms, "GB/s": gbs, "frac": gbs / hbm,
@@ -349,7 +351,7 @@ def run_extras(sfh, hbm, quick=False):
     X64, i64 = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision="f64", info=True)
     t64 = time.perf_counter() - t0
     sol["f64"] = {"iters": i64["iters"], "seconds": t64}
-    for prec in ("f16", "f32"):
+    for prec in ("f16", "bf16", "f32"):
         t0 = time.perf_counter()
         try:
             Xm, im = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
@@ -373,7 +375,7 @@ def run_extras(sfh, hbm, quick=False):
         for m in (0.1, 0.02):
             lat.set_mass(m)
             row = {}
-            for prec in ("f64", "f32_18", "f32", "f16"):
+            for prec in ("f64", "f32_18", "f32", "f16", "bf16"):
                 t0 = time.perf_counter()
                 _, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
                 row[prec] = {"iters": inf["iters"], "ms": 1e3 * (time.perf_counter() - t0)}
@@ -413,9 +415,19 @@ def run_extras(sfh, hbm, quick=False):
     lat.set_hasenbusch(0.2)
     trajs = []
     for k in range(2):
+        # the mixed-precision trajectory, then the FP64 path from the same
+        # start with the same draws; the chain continues from the mixed one
+        U0 = lat.download_gauge()
         info = lat.hmc_trajectory(1.0 / 20, 20, seed=100 + 10 * k, tol=TOL, precision="f32")
+        U1 = lat.download_gauge()
+        lat.upload_gauge(U0)
+        i64 = lat.hmc_trajectory(1.0 / 20, 20, seed=100 + 10 * k, tol=TOL, precision="f64")
+        lat.upload_gauge(U1)
         trajs.append({"dH": info["dH"], "accepted": info["accepted"], "plaquette": info["plaquette"],
-                      "seconds": info["seconds"], "cg_iters": info["cg_iters"], "solves": info["solves"]})
+                      "seconds": info["seconds"], "cg_iters": info["cg_iters"], "solves": info["solves"],
+                      "fp64_path": {"dH": i64["dH"], "accepted": i64["accepted"], "plaquette": i64["plaquette"],
+                                    "seconds": i64["seconds"], "cg_iters": i64["cg_iters"]},
+                      "dH_minus_fp64": info["dH"] - i64["dH"]})
     poly = lat.precompute_polyakov_grid()
     ex["c5_24^4_trajectory"] = {"heatbath_20_sweeps": {"seconds": hb_s, "plaquette": hb_plaq},
                                 "trajectories": trajs, "polyakov_mean": [float(poly.mean().real),
@@ -446,7 +458,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="sfh", choices=["sfh", "reference"])
-    ap.add_argument("--precision", default="f16", choices=["f32", "f16", "f32_18"],
+    ap.add_argument("--precision", default="f16", choices=["f32", "f16", "f32_18", "bf16"],
                     help="storage of the iterated vectors and links: f16 (half precision with a per-site "
                          "scale), f32 (12-real links) or f32_18; arithmetic is f32, reliable updates f64")
     ap.add_argument("--nsys", type=int, default=64)
@@ -548,7 +560,7 @@ def main():
     # the other mixed precisions on the same batch, autotuned (secondary)
     other = {}
     if not args.no_extras:
-        for prec in [p for p in ("f32", "f16") if p != args.precision]:
+        for prec in [p for p in ("f32", "f16", "bf16") if p != args.precision]:
             try:
                 Bo = build_batch(sfh, spec, prec, local)
                 Bo.autotune()
@@ -632,7 +644,8 @@ def main():
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
                    "arithmetic": {"f16": "f16 storage with a per-site scale, f32 arithmetic, f64 reliable updates",
                                   "f32": "f32 storage (12-real links), f32 arithmetic, f64 reliable updates",
-                                  "f32_18": "f32 storage (18-real links), f32 arithmetic, f64 reliable updates"
+                                  "f32_18": "f32 storage (18-real links), f32 arithmetic, f64 reliable updates",
+                                  "bf16": "bf16 storage with a per-site scale, f32 arithmetic, f64 reliable updates"
                                   }[args.precision],
                    "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
                                                                       "staged_links": schedule[2]},

@@ -41,6 +41,8 @@ extern "C" {
                             FP64 reliable updates                                      */
 #define SFH_PREC_F32_18 3 /* FP32 18-real links (no reconstruction), FP32 vectors,
                              FP64 reliable updates                                     */
+#define SFH_PREC_BF16 4  /* BF16 12-real links, BF16+per-site-scale vectors, FP32 math,
+                            FP64 reliable updates                                      */
 
 typedef struct sfh_ctx sfh_ctx;
 typedef struct sfh_batch sfh_batch;
@@ -105,7 +107,8 @@ int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
 
 /* Device time of one even-odd hop (V/2 output sites, the hopping part of
  * Fermions.cpp:218-283) in a storage format: 0 FP64 18-real, 1 FP32 12-real,
- * 2 FP16 12-real with per-site spinor scale, 3 FP32 18-real.  Benchmark aid;
+ * 2 FP16 12-real with per-site spinor scale, 3 FP32 18-real, 4 BF16 12-real
+ * with per-site spinor scale.  Benchmark aid;
  * the input is all zeros, so the value of the output is meaningless. */
 int sfh_dslash_timing(sfh_ctx* ctx, int storage, int nrep, double* ms_per_hop);
 
@@ -275,7 +278,7 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * only); and its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Reliable-update threshold of the mixed precisions (default 0.1 for
- * SFH_PREC_F16, 0.01 for the FP32 storages): an FP64
+ * the 16-bit storages, 0.01 for the FP32 ones): an FP64
  * update (x_hi += x_lo, r = b - M x_hi) when the iterated residual has dropped
  * by this factor below its largest value since the last update.  No
  * counterpart in the reference (its CG is FP64 only). */

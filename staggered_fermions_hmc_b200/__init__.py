@@ -36,8 +36,8 @@ SFH_ERR_IO = 9
 FORCE_GAUGE = 1
 FORCE_FERMION = 2
 
-PREC_F64, PREC_F32, PREC_F16, PREC_F32_18 = 0, 1, 2, 3
-PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "f32_18": PREC_F32_18}
+PREC_F64, PREC_F32, PREC_F16, PREC_F32_18, PREC_BF16 = 0, 1, 2, 3, 4
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16": PREC_F16, "f32_18": PREC_F32_18, "bf16": PREC_BF16}
 BATCH_FULL_LATTICE = 1
 
 
@@ -294,7 +294,7 @@ class Lattice:
 
     def dslash_timing(self, storage, nrep=20):
         """ms per even-odd hop (V/2 output sites); storage 0 FP64-18, 1 FP32-12,
-        2 FP16-12, 3 FP32-18."""
+        2 FP16-12, 3 FP32-18, 4 BF16-12."""
         ms = ctypes.c_double(0.0)
         self._check(self.lib.sfh_dslash_timing(self.h, storage, nrep, ctypes.byref(ms)), "dslash timing")
         return ms.value
@@ -533,7 +533,7 @@ class Batch:
 
     def set_reliable_delta(self, delta):
         """Reliable-update threshold of the mixed precisions (default 0.1 for
-        "f16", 0.01 for the FP32 storages)."""
+        "f16" and "bf16", 0.01 for the FP32 storages)."""
         self._check(self.lib.sfh_batch_set_reliable_delta(self.h, delta), "set_reliable_delta")
 
     def schedule(self):

@@ -92,6 +92,7 @@ extern "C" int sfh_create(const sfh_params* p, sfh_ctx** out)
     e = cudaMalloc(&c->U64, links64);
     if (e == cudaSuccess) e = cudaMalloc(&c->U32, V * 4 * 3 * 16);
     if (e == cudaSuccess) e = cudaMalloc(&c->U16, V * 4 * 3 * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&c->Ubf16, V * 4 * 3 * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->U32_18, V * 4 * 9 * 8);
     if (e == cudaSuccess) e = cudaMalloc(&c->Pmom, links64);
     if (e == cudaSuccess) e = cudaMalloc(&c->Fbuf, links64);
@@ -115,9 +116,9 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     if (!c) return SFH_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kNumPrecisions; ++k)
         if (c->ws[k]) workspace_free(c->ws[k]);
-    void* ptrs[] = {c->U64, c->U32, c->U16, c->U32_18, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
+    void* ptrs[] = {c->U64, c->U32, c->U16, c->Ubf16, c->U32_18, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
                     c->smear, c->hphi, c->hX};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -233,7 +234,7 @@ extern "C" int sfh_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol
                             int precision, sfh_cg_info* info)
 {
     if (!c || !phi || !X || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!valid_precision(precision)) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     return ctx_cg_solve(c, phi, X, tol, maxit, precision, info);
 }
@@ -304,21 +305,23 @@ extern "C" int sfh_download_momenta(sfh_ctx* c, double* P)
 }
 
 // Device time of one even-odd hop (V/2 output sites) in a storage format:
-// 0 FP64 18-real, 1 FP32 12-real, 2 FP16 12-real + scale, 3 FP32 18-real.
+// 0 FP64 18-real, 1 FP32 12-real, 2 FP16 12-real + scale, 3 FP32 18-real,
+// 4 BF16 12-real + scale.
 // Uses the context's gauge field and a zero input (the memory traffic and
 // arithmetic do not depend on the values); nrep timed hops after three
 // untimed ones, measured with CUDA events on the context's stream.
 extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_per_hop)
 {
-    if (!c || !ms_per_hop || storage < 0 || storage > 3 || nrep < 1) return SFH_ERR_INVALID;
+    if (!c || !ms_per_hop || storage < 0 || storage > 4 || nrep < 1) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     if (!c->lowp_valid) {
-        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18);
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18, c->Ubf16);
         c->lowp_valid = true;
     }
-    static const int gp[4] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18};
-    static const int sp[4] = {SP_F64, SP_F32, SP_F16, SP_F32};
-    const void* U = storage == 0 ? c->U64 : (storage == 1 ? c->U32 : (storage == 2 ? c->U16 : c->U32_18));
+    static const int gp[5] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18, GP_BF16_12};
+    static const int sp[5] = {SP_F64, SP_F32, SP_F16, SP_F32, SP_BF16};
+    const void* const Us[5] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16};
+    const void* U = Us[storage];
     int st = SFH_OK;
     void* in = c->spin[0];
     void* out = c->spin[1];

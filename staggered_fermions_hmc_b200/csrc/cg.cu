@@ -261,11 +261,11 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
 // a neighbour spinor with the hop's scalar factor applied: the eta / 2 and
-// time-wrap sign, and for FP16 storage the per-site scale (one multiply)
+// time-wrap sign, and for the 16-bit storages the per-site scale (one multiply)
 template <int SP, typename R>
 __device__ __forceinline__ Vec3<R> hop_input(const void* in, int nq, int j, int Vh, bool neg, R s)
 {
-    if constexpr (SP == SP_F16) {
+    if constexpr (SpinorFmt<SP>::scaled) {
         float sc;
         Vec3<R> v = SpinorFmt<SP>::load_unscaled(in, nq, j, Vh, &sc);
         return vneg_if(v, neg, s * sc);
@@ -285,7 +285,7 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
     // factor (eta/2, the anti-periodic time sign, the FP16 site scale) going
     // onto the input vector; FP32-12 sums the two hops of a direction first
     // and applies eta/2 once (measured faster there)
-    constexpr bool direct = GaugeFmt<GP>::K == 9 || SP == SP_F16;
+    constexpr bool direct = GaugeFmt<GP>::K == 9 || SpinorFmt<SP>::scaled;
 #pragma unroll
     for (int mu = 0; mu < 4; ++mu) {
         const R s = ((n.eta >> mu) & 1u) ? R(-0.5) : R(0.5);
@@ -971,6 +971,7 @@ static CgKernels pick_kernels(int prec, int nb1, int nb2, bool stage)
     if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false);
     else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage);
     else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage);
+    else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stage);
     else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stage);
     if (k.smem) {  // opt in to the staged kernels' shared memory (idempotent)
         cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
@@ -1064,7 +1065,7 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
     w.both = both;
     w.nsys = (int)systems.size();
     w.sys.clear(); w.rhs.clear(); w.rhs0.clear(); w.lanes_h.clear();
-    const int sp = prec == SFH_PREC_F64 ? SP_F64 : (prec == SFH_PREC_F16 ? SP_F16 : SP_F32);
+    const int sp = prec == SFH_PREC_F64 ? SP_F64 : (prec == SFH_PREC_F16 ? SP_F16 : (prec == SFH_PREC_BF16 ? SP_BF16 : SP_F32));
     int tile = 0, lane = 0, poff = 0;
     std::vector<int> tile_sys;
     for (int k = 0; k < w.nsys; ++k) {
@@ -1266,7 +1267,10 @@ struct PhaseTimes {
 // precisions: FP16 storage needs the tighter 0.1 (at 0.02 its recurrence
 // drifts too far to converge); FP32 keeps its recurrence to 0.01, half the
 // updates of 0.1 at the same iteration count.
-static double default_reliable_delta(int prec) { return prec == SFH_PREC_F16 ? 0.1 : 0.01; }
+static double default_reliable_delta(int prec)
+{
+    return (prec == SFH_PREC_F16 || prec == SFH_PREC_BF16) ? 0.1 : 0.01;
+}
 
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
                                    int tpi, bool stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
@@ -1396,7 +1400,7 @@ struct sfh_batch {
     double delta = 0.1;  // reliable-update threshold of the mixed precisions (set at creation)
     std::vector<sfh_system_desc> desc;
     std::vector<sfh::Geom> geoms;
-    std::vector<void*> U64, U32, U16;
+    std::vector<void*> U64, U32, U16;  // U16: the FP16 or BF16 links of a 16-bit batch
     std::vector<bool> lowp_valid;
     void* stage = nullptr;   // device staging (largest 72V doubles)
     size_t stage_bytes = 0;
@@ -1419,6 +1423,8 @@ static void batch_make_lowp(sfh_batch* b, int k)
     if (b->prec == SFH_PREC_F64) return;
     if (b->prec == SFH_PREC_F32_18)
         sfh::launch_make_lowp_gauge(b->geoms[k], b->U64[k], nullptr, nullptr, b->stream, b->U32[k]);
+    else if (b->prec == SFH_PREC_BF16)
+        sfh::launch_make_lowp_gauge(b->geoms[k], b->U64[k], nullptr, nullptr, b->stream, nullptr, b->U16[k]);
     else
         sfh::launch_make_lowp_gauge(b->geoms[k], b->U64[k], b->U32[k], b->U16[k], b->stream);
 }
@@ -1440,7 +1446,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
                                 int flags, sfh_batch** out)
 {
     if (!out || nsys <= 0 || !systems) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!sfh::valid_precision(precision)) return SFH_ERR_INVALID;
     if ((flags & SFH_BATCH_FULL_LATTICE) && precision != SFH_PREC_F64) return SFH_ERR_INVALID;
     for (int k = 0; k < nsys; ++k)
         if (!sfh::dims_ok(systems[k].dims) || systems[k].nrhs <= 0 || systems[k].nrhs > 64)
@@ -1468,7 +1474,8 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
         size_t n64 = (size_t)g.V * 4 * 9 * 16;
         e = cudaMalloc(&u64, n64);
         if (e == cudaSuccess && precision == SFH_PREC_F32) e = cudaMalloc(&u32, (size_t)g.V * 4 * 3 * 16);
-        if (e == cudaSuccess && precision == SFH_PREC_F16) e = cudaMalloc(&u16, (size_t)g.V * 4 * 3 * 8);
+        if (e == cudaSuccess && (precision == SFH_PREC_F16 || precision == SFH_PREC_BF16))
+            e = cudaMalloc(&u16, (size_t)g.V * 4 * 3 * 8);
         if (e == cudaSuccess && precision == SFH_PREC_F32_18) e = cudaMalloc(&u32, (size_t)g.V * 4 * 9 * 8);
         b->U64.push_back(u64);
         b->U32.push_back(u32);
@@ -1491,7 +1498,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
         h.U64 = b->U64[k];
         h.Ulo = (precision == SFH_PREC_F32 || precision == SFH_PREC_F32_18)
                     ? b->U32[k]
-                    : (precision == SFH_PREC_F16 ? b->U16[k] : b->U64[k]);
+                    : ((precision == SFH_PREC_F16 || precision == SFH_PREC_BF16) ? b->U16[k] : b->U64[k]);
         hs.push_back(h);
     }
     e = sfh::workspace_build(b->ws, hs, precision, (flags & SFH_BATCH_FULL_LATTICE) ? 1 : 0);
@@ -1660,6 +1667,10 @@ void workspace_free(CgWorkspace* w) { delete w; }
 static CgWorkspace* ctx_workspace(sfh_ctx* c, int prec, cudaError_t* err)
 {
     *err = cudaSuccess;
+    if (!valid_precision(prec)) {
+        *err = cudaErrorInvalidValue;
+        return nullptr;
+    }
     if (c->ws[prec]) return c->ws[prec];
     CgWorkspace* w = new CgWorkspace();
     SolverSystemHost h;
@@ -1667,7 +1678,8 @@ static CgWorkspace* ctx_workspace(sfh_ctx* c, int prec, cudaError_t* err)
     h.mass = c->mass;
     h.nrhs = 1;
     h.U64 = c->U64;
-    h.Ulo = prec == SFH_PREC_F32 ? c->U32 : (prec == SFH_PREC_F16 ? c->U16 : (prec == SFH_PREC_F32_18 ? c->U32_18 : c->U64));
+    const void* const lo[5] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16};
+    h.Ulo = lo[prec];
     std::vector<SolverSystemHost> hs(1, h);
     *err = workspace_build(*w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
     if (*err != cudaSuccess) {
@@ -1683,7 +1695,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
                      sfh_cg_info* info)
 {
     if (prec != SFH_PREC_F64 && !c->lowp_valid) {
-        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18);
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18, c->Ubf16);
         c->lowp_valid = true;
     }
     cudaError_t e;

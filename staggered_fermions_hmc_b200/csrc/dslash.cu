@@ -123,6 +123,8 @@ void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, c
         launch_typed<GP_F16_12, SP_F16>(g, gauge, in, out, self, a, b, q0, nq, s);
     else if (gauge_prec == GP_F32_18 && in_prec == SP_F32)
         launch_typed<GP_F32_18, SP_F32>(g, gauge, in, out, self, a, b, q0, nq, s);
+    else if (gauge_prec == GP_BF16_12 && in_prec == SP_BF16)
+        launch_typed<GP_BF16_12, SP_BF16>(g, gauge, in, out, self, a, b, q0, nq, s);
 }
 
 }  // namespace sfh

@@ -371,7 +371,7 @@ extern "C" int sfh_momentum_kick(sfh_ctx* c, int forces, const double* phi, doub
     if (!c || forces < SFH_FORCE_GAUGE || forces > (SFH_FORCE_GAUGE | SFH_FORCE_FERMION)) return SFH_ERR_INVALID;
     const bool ferm = (forces & SFH_FORCE_FERMION) != 0;
     if (ferm && (!phi || !(tol > 0.0) || maxit <= 0)) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!valid_precision(precision)) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     if (cg_iters) *cg_iters = 0;
     void *X = c->spin[4], *Y = c->spin[2];
@@ -450,7 +450,7 @@ extern "C" int sfh_smeared_fermion_force(sfh_ctx* c, const double* phi, double t
                                          double* F, double* X_out)
 {
     if (!c || !phi || !F || !(tol > 0.0) || maxit <= 0 || c->fsmear_n < 1) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!valid_precision(precision)) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     void *X = c->spin[4], *Y = c->spin[2];
     int st = spinor_in(c, phi, c->spin[5]);
@@ -505,7 +505,7 @@ extern "C" int sfh_leapfrog(sfh_ctx* c, const double* phi, double eps, int nstep
                             int precision, double* X_out, long* cg_iters)
 {
     if (!c || !phi || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!valid_precision(precision)) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     int st = spinor_in(c, phi, c->spin[5]);
     if (st) return st;
@@ -521,7 +521,7 @@ extern "C" int sfh_hmc_trajectory(sfh_ctx* c, double eps, int nsteps, unsigned l
                                   int maxit, int precision, sfh_traj_info* info)
 {
     if (!c || !info || nsteps < 1 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
-    if (precision < SFH_PREC_F64 || precision > SFH_PREC_F32_18) return SFH_ERR_INVALID;
+    if (!valid_precision(precision)) return SFH_ERR_INVALID;
     cudaSetDevice(c->device);
     std::memset(info, 0, sizeof(*info));
     auto t0 = std::chrono::steady_clock::now();

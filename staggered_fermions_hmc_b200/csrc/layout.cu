@@ -65,9 +65,10 @@ __global__ void links_eo_to_aos(Geom g, const double2* __restrict__ eo, double* 
     for (int k = 0; k < 9; ++k) dst[k] = src[(size_t)k * g.Vh];
 }
 
-// FP64 18-real -> FP32 12-real (float4 x3) and FP16 12-real (uint2 x3)
+// FP64 18-real -> FP32 12-real (float4 x3), FP16 / BF16 12-real (uint2 x3)
+// and FP32 18-real, each where its output is given
 __global__ void make_lowp(Geom g, const double2* __restrict__ U64, float4* __restrict__ U32,
-                          uint2* __restrict__ U16, float2* __restrict__ U32_18)
+                          uint2* __restrict__ U16, float2* __restrict__ U32_18, uint2* __restrict__ Ubf16)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int pm = blockIdx.y;  // p*4+mu
@@ -88,14 +89,14 @@ __global__ void make_lowp(Geom g, const double2* __restrict__ U64, float4* __res
         if (U32)
             U32[((size_t)pm * 3 + k) * g.Vh + i] =
                 make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
-        if (U16) {
-            __half2 h0 = __floats2half2_rn((float)a.x, (float)a.y);
-            __half2 h1 = __floats2half2_rn((float)b.x, (float)b.y);
-            uint2 w;
-            w.x = *reinterpret_cast<uint32_t*>(&h0);
-            w.y = *reinterpret_cast<uint32_t*>(&h1);
-            U16[((size_t)pm * 3 + k) * g.Vh + i] = w;
-        }
+        if (U16)
+            U16[((size_t)pm * 3 + k) * g.Vh + i] =
+                make_uint2(Pair16<SP_F16>::from_floats((float)a.x, (float)a.y),
+                           Pair16<SP_F16>::from_floats((float)b.x, (float)b.y));
+        if (Ubf16)
+            Ubf16[((size_t)pm * 3 + k) * g.Vh + i] =
+                make_uint2(Pair16<SP_BF16>::from_floats((float)a.x, (float)a.y),
+                           Pair16<SP_BF16>::from_floats((float)b.x, (float)b.y));
     }
 }
 
@@ -121,10 +122,11 @@ void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStre
     links_eo_to_aos<<<dim3(blocks_for(g.Vh), 8), kThreads, 0, s>>>(g, (const double2*)eo, aos);
 }
 
-void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s, void* U32_18)
+void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s, void* U32_18,
+                            void* Ubf16)
 {
     make_lowp<<<dim3(blocks_for(g.Vh), 8), kThreads, 0, s>>>(g, (const double2*)U64, (float4*)U32,
-                                                              (uint2*)U16, (float2*)U32_18);
+                                                              (uint2*)U16, (float2*)U32_18, (uint2*)Ubf16);
 }
 
 }  // namespace sfh

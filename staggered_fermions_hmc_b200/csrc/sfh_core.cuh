@@ -17,6 +17,7 @@
 //   momentum / force : double2 [p][mu][entry 9][i]        (FP64, 18-real)
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -204,14 +205,15 @@ __device__ __forceinline__ void reconstruct_row2(Mat3<R>& U)
 // ---------------------------------------------------------------------------
 // storage formats
 // ---------------------------------------------------------------------------
-enum SpinorPrec { SP_F64 = 0, SP_F32 = 1, SP_F16 = 2 };
-enum GaugePrec { GP_F64_18 = 0, GP_F32_12 = 1, GP_F16_12 = 2, GP_F32_18 = 3 };
+enum SpinorPrec { SP_F64 = 0, SP_F32 = 1, SP_F16 = 2, SP_BF16 = 3 };
+enum GaugePrec { GP_F64_18 = 0, GP_F32_12 = 1, GP_F16_12 = 2, GP_F32_18 = 3, GP_BF16_12 = 4 };
 
 template <int SP> struct SpinorFmt;
 
 template <> struct SpinorFmt<SP_F64> {
     typedef double R;
     static constexpr size_t site_bytes = 48;
+    static constexpr bool scaled = false;
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const double2* b = (const double2*)base + (size_t)p * 3 * Vh;
@@ -246,6 +248,7 @@ template <> struct SpinorFmt<SP_F64> {
 template <> struct SpinorFmt<SP_F32> {
     typedef float R;
     static constexpr size_t site_bytes = 24;
+    static constexpr bool scaled = false;
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const float2* b = (const float2*)base + (size_t)p * 3 * Vh;
@@ -277,9 +280,39 @@ template <> struct SpinorFmt<SP_F32> {
     }
 };
 
-template <> struct SpinorFmt<SP_F16> {
+// 16-bit complex pairs (re, im) in one 32-bit word: FP16 or BF16
+template <int SP> struct Pair16;
+template <> struct Pair16<SP_F16> {
+    __device__ static __forceinline__ float2 to_float2(uint32_t w)
+    {
+        return __half22float2(*reinterpret_cast<__half2*>(&w));
+    }
+    __device__ static __forceinline__ uint32_t from_floats(float a, float b)
+    {
+        __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+};
+template <> struct Pair16<SP_BF16> {
+    __device__ static __forceinline__ float2 to_float2(uint32_t w)
+    {
+        return __bfloat1622float2(*reinterpret_cast<__nv_bfloat162*>(&w));
+    }
+    __device__ static __forceinline__ uint32_t from_floats(float a, float b)
+    {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+};
+
+// 16-bit vectors with a per-site scale: one uint4 per site, three (re, im)
+// pairs of the colour components divided by their largest magnitude, and
+// that magnitude as an FP32 in the last word
+template <int SP> struct ScaledSpinorFmt {
     typedef float R;
+    typedef Pair16<SP> P;
     static constexpr size_t site_bytes = 16;
+    static constexpr bool scaled = true;
     __device__ static __forceinline__ Vec3<R> unpack(uint4 w)
     {
         float s = __uint_as_float(w.w);
@@ -287,8 +320,7 @@ template <> struct SpinorFmt<SP_F16> {
         uint32_t words[3] = {w.x, w.y, w.z};
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            __half2 h = *reinterpret_cast<__half2*>(&words[c]);
-            float2 f = __half22float2(h);
+            float2 f = P::to_float2(words[c]);
             v.c[c] = {f.x * s, f.y * s};
         }
         return v;
@@ -301,10 +333,7 @@ template <> struct SpinorFmt<SP_F16> {
         float inv = m > 0.f ? 1.0f / m : 0.f;
         uint32_t words[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            __half2 h = __floats2half2_rn(v.c[c].re * inv, v.c[c].im * inv);
-            words[c] = *reinterpret_cast<uint32_t*>(&h);
-        }
+        for (int c = 0; c < 3; ++c) words[c] = P::from_floats(v.c[c].re * inv, v.c[c].im * inv);
         uint4 w;
         w.x = words[0]; w.y = words[1]; w.z = words[2]; w.w = __float_as_uint(m);
         return w;
@@ -314,7 +343,7 @@ template <> struct SpinorFmt<SP_F16> {
         return unpack(__ldcg((const uint4*)base + (size_t)p * Vh + i));
     }
     __device__ static __forceinline__ Vec3<R> quantize(const Vec3<R>& v) { return unpack(pack(v)); }
-    // the halves converted, without the scale (returned in *scale)
+    // the pairs converted, without the scale (returned in *scale)
     __device__ static __forceinline__ Vec3<R> load_unscaled(const void* base, int p, int i, int Vh, float* scale)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
@@ -324,8 +353,7 @@ template <> struct SpinorFmt<SP_F16> {
         uint32_t words[3] = {w.x, w.y, w.z};
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            __half2 h = *reinterpret_cast<__half2*>(&words[c]);
-            float2 f = __half22float2(h);
+            float2 f = P::to_float2(words[c]);
             v.c[c] = {f.x, f.y};
         }
         return v;
@@ -333,17 +361,7 @@ template <> struct SpinorFmt<SP_F16> {
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
-        uint4 w = __ldg(b + i);
-        float s = __uint_as_float(w.w);
-        Vec3<R> v;
-        uint32_t words[3] = {w.x, w.y, w.z};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            __half2 h = *reinterpret_cast<__half2*>(&words[c]);
-            float2 f = __half22float2(h);
-            v.c[c] = {f.x * s, f.y * s};
-        }
-        return v;
+        return unpack(__ldg(b + i));
     }
     __device__ static __forceinline__ void store(void* base, int p, int i, int Vh, const Vec3<R>& v)
     {
@@ -351,6 +369,9 @@ template <> struct SpinorFmt<SP_F16> {
         b[i] = pack(v);
     }
 };
+
+template <> struct SpinorFmt<SP_F16> : ScaledSpinorFmt<SP_F16> {};
+template <> struct SpinorFmt<SP_BF16> : ScaledSpinorFmt<SP_BF16> {};
 
 template <int GP> struct GaugeFmt;
 
@@ -420,7 +441,9 @@ template <> struct GaugeFmt<GP_F32_12> {
     }
 };
 
-template <> struct GaugeFmt<GP_F16_12> {
+// 16-bit 12-real links (the first two rows; the third reconstructed):
+// three uint2 per link, each two (re, im) pairs
+template <int SPAIR> struct Gauge16Fmt {
     typedef float R;
     typedef uint2 E;
     static constexpr int K = 3;
@@ -430,9 +453,8 @@ template <> struct GaugeFmt<GP_F16_12> {
         Mat3<R> U;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            uint2 x = w[k];
-            float2 f0 = __half22float2(*reinterpret_cast<__half2*>(&x.x));
-            float2 f1 = __half22float2(*reinterpret_cast<__half2*>(&x.y));
+            float2 f0 = Pair16<SPAIR>::to_float2(w[k].x);
+            float2 f1 = Pair16<SPAIR>::to_float2(w[k].y);
             U.e[2 * k] = {f0.x, f0.y};
             U.e[2 * k + 1] = {f1.x, f1.y};
         }
@@ -448,6 +470,9 @@ template <> struct GaugeFmt<GP_F16_12> {
         return unpack(w);
     }
 };
+
+template <> struct GaugeFmt<GP_F16_12> : Gauge16Fmt<SP_F16> {};
+template <> struct GaugeFmt<GP_BF16_12> : Gauge16Fmt<SP_BF16> {};
 
 // ---------------------------------------------------------------------------
 // error flags written by kernels (never traps)

@@ -12,6 +12,7 @@
 
 namespace sfh {
 struct CgWorkspace;
+constexpr int kNumPrecisions = SFH_PREC_BF16 + 1;  // the solver precisions of include/sfh.h
 }
 
 struct sfh_ctx {
@@ -26,6 +27,7 @@ struct sfh_ctx {
     void* U64 = nullptr;       // gauge FP64 18-real
     void* U32 = nullptr;       // gauge FP32 12-real (derived)
     void* U16 = nullptr;       // gauge FP16 12-real (derived)
+    void* Ubf16 = nullptr;     // gauge BF16 12-real (derived)
     void* U32_18 = nullptr;    // gauge FP32 18-real (derived)
     bool lowp_valid = false;   // derived copies match U64
     void* Pmom = nullptr;      // momenta FP64 18-real
@@ -37,8 +39,8 @@ struct sfh_ctx {
     void* pinned = nullptr;    // pinned host staging (72V doubles)
     size_t pinned_bytes = 0;
 
-    sfh::CgWorkspace* ws[4] = {};  // cached solver workspaces per precision
-    double ws_mass[4] = {};
+    sfh::CgWorkspace* ws[sfh::kNumPrecisions] = {};  // cached solver workspaces per precision
+    double ws_mass[sfh::kNumPrecisions] = {};
     void* Utrial = nullptr;        // gauge backup for the Metropolis step
     void* smear = nullptr;         // scratch link fields (smearing, staples)
     size_t smear_bytes = 0;
@@ -63,7 +65,10 @@ void launch_spinor_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStr
 void launch_links_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
 void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
 void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s,
-                            void* U32_18 = nullptr);
+                            void* U32_18 = nullptr, void* Ubf16 = nullptr);
+
+// the solver precisions of include/sfh.h
+inline bool valid_precision(int p) { return p >= SFH_PREC_F64 && p <= SFH_PREC_BF16; }
 
 // out_q = a*self_q + b*K_{q,1-q} in  for q in [q0, q0+nq); precisions by enum
 void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,

@@ -76,7 +76,7 @@ def true_resid(orc, dims, mass, U, b, x):
     return float(np.linalg.norm(r) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18"])
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18", "bf16"])
 def test_cg_precisions_true_residual(sfh, orc, precision):
     dims, mass = (8, 8, 8, 8), 0.1
     U = orc.random_gauge(dims, 0.3, 41)
@@ -121,7 +121,7 @@ def test_invalid_dims_rejected(sfh):
     assert e.value.status == sfh.SFH_ERR_INVALID
 
 
-@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18"])
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "f32_18", "bf16"])
 def test_batch_uneven_systems(sfh, orc, precision):
     systems = [((4, 4, 4, 4), 0.2, 2), ((6, 6, 6, 8), 0.05, 3), ((8, 8, 8, 4), 0.1, 1),
                ((4, 4, 8, 8), 0.1, 5)]
@@ -221,12 +221,12 @@ def test_batch_timed_solve_matches_graph_solve(sfh, orc):
     assert all(times[k][0] > 0 for k in times)
 
 
-@pytest.mark.parametrize("precision", ["f16", "f32"])
-def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, precision):
+@pytest.mark.parametrize("precision,bound", [("f16", 1.25), ("f32", 1.25), ("bf16", 1.35)])
+def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, precision, bound):
     """eps = 1 links at m = 0.02 on 16^4: the mixed-precision CG needs at most
-    a quarter more iterations than FP64 (the reliable update rebuilds the
-    search direction on the true residual; without it FP16 took 4.9 times
-    FP64's count here), and reaches the FP64 true residual."""
+    `bound` times FP64's iterations (the reliable update rebuilds the search
+    direction on the true residual; without it FP16 took 4.9 times FP64's
+    count here), and reaches the FP64 true residual."""
     tol = 1e-10
     lat = sfh.Lattice((16, 16, 16, 16), 0.02, 4.2)
     try:
@@ -235,7 +235,7 @@ def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, precision):
         X64, i64 = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision="f64", info=True)
         X, inf = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision=precision, info=True)
         assert inf["status"] == 0
-        assert inf["iters"] <= 1.25 * i64["iters"], (inf, i64)
+        assert inf["iters"] <= bound * i64["iters"], (inf, i64)
         assert rel(X, X64) < 1e-6
     finally:
         lat.close()
