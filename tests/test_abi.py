@@ -95,3 +95,17 @@ def test_compat_header_declares_and_library_defines():
         out = subprocess.run([nm, "-DC", "--defined-only", sfh.LIB_PATH], capture_output=True, text=True).stdout
         missing = [n for n in COMPAT_FUNCTIONS if "sfh_compat::" + n + "(" not in out]
         assert not missing, missing
+
+
+def test_python_constants_match_header():
+    """Every #define of include/sfh.h with a number has the same value in the
+    binding (SFH_ERR_* by name, SFH_PREC_* as PREC_*, the others without the
+    SFH_ prefix)."""
+    import staggered_fermions_hmc_b200 as sfh
+    text = open(os.path.join(ROOT, "include", "sfh.h")).read()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (SFH_[A-Z0-9_]+) (\d+)", text)}
+    assert "SFH_PREC_BF16" in defines
+    for name, value in defines.items():
+        py = name if name.startswith(("SFH_OK", "SFH_ERR_")) else name[len("SFH_"):]
+        assert getattr(sfh, py) == value, (name, py)
+    assert sorted(sfh.PRECISIONS.values()) == sorted(v for k, v in defines.items() if k.startswith("SFH_PREC_"))
