@@ -108,9 +108,15 @@ int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
 /* Device time of one even-odd hop (V/2 output sites, the hopping part of
  * Fermions.cpp:218-283) in a storage format: 0 FP64 18-real, 1 FP32 12-real,
  * 2 FP16 12-real with per-site spinor scale, 3 FP32 18-real, 4 BF16 12-real
- * with per-site spinor scale.  Benchmark aid;
+ * with per-site spinor scale, 5 FP64 12-real.  Benchmark aid;
  * the input is all zeros, so the value of the output is meaningless. */
 int sfh_dslash_timing(sfh_ctx* ctx, int storage, int nrep, double* ms_per_hop);
+/* out = K in (the hopping term of D = m + K, Fermions.cpp:218-247, both
+ * parities, reference AoS layout) computed by the same Dslash kernel in a
+ * storage format (0..5 as above): the input rounded to the format's vectors
+ * and the links to its links; the result returned in FP64.  The numerical
+ * check of the kernels sfh_dslash_timing times. */
+int sfh_dslash_storage(sfh_ctx* ctx, int storage, const double* in, double* out);
 
 /* ---- solver --------------------------------------------------------------- */
 /* X = (D D^dag)^{-1} phi to |r| < tol |phi|: solve_CG_DDdagger / solve_X_field

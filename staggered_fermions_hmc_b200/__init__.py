@@ -109,6 +109,7 @@ SIGNATURES = {
     "sfh_dirac": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_ddag": (ctypes.c_int, [_VP, _D, _D]),
     "sfh_dslash_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_dslash_storage": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_cg_solve": (ctypes.c_int, [_VP, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(CgInfo)]),
     "sfh_staples": (ctypes.c_int, [_VP, _D, _D]),
@@ -292,9 +293,18 @@ class Lattice:
         self._check(self.lib.sfh_dirac(self.h, 1, _dptr(psi), _dptr(out)), "dirac_dagger")
         return out
 
+    def dslash_storage(self, storage, psi):
+        """K psi (the hopping term, both parities) by the standalone Dslash in
+        a storage format (0 FP64-18, 1 FP32-12, 2 FP16-12, 3 FP32-18,
+        4 BF16-12, 5 FP64-12), returned in FP64."""
+        psi = _f64(psi).reshape(-1)
+        out = np.empty_like(psi)
+        self._check(self.lib.sfh_dslash_storage(self.h, storage, _dptr(psi), _dptr(out)), "dslash storage")
+        return out
+
     def dslash_timing(self, storage, nrep=20):
         """ms per even-odd hop (V/2 output sites); storage 0 FP64-18, 1 FP32-12,
-        2 FP16-12, 3 FP32-18, 4 BF16-12."""
+        2 FP16-12, 3 FP32-18, 4 BF16-12, 5 FP64-12."""
         ms = ctypes.c_double(0.0)
         self._check(self.lib.sfh_dslash_timing(self.h, storage, nrep, ctypes.byref(ms)), "dslash timing")
         return ms.value

@@ -118,7 +118,7 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int k = 0; k < kNumPrecisions; ++k)
         if (c->ws[k]) workspace_free(c->ws[k]);
-    void* ptrs[] = {c->U64, c->U32, c->U16, c->Ubf16, c->U32_18, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
+    void* ptrs[] = {c->U64, c->U32, c->U16, c->Ubf16, c->U32_18, c->U64_12, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
                     c->smear, c->hphi, c->hX};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -304,25 +304,79 @@ extern "C" int sfh_download_momenta(sfh_ctx* c, double* P)
     return cuda_check(c, cudaStreamSynchronize(c->stream), "momenta download");
 }
 
-// Device time of one even-odd hop (V/2 output sites) in a storage format:
+// The links, gauge format and vector format of a standalone-Dslash storage:
 // 0 FP64 18-real, 1 FP32 12-real, 2 FP16 12-real + scale, 3 FP32 18-real,
-// 4 BF16 12-real + scale.
-// Uses the context's gauge field and a zero input (the memory traffic and
-// arithmetic do not depend on the values); nrep timed hops after three
-// untimed ones, measured with CUDA events on the context's stream.
-extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_per_hop)
+// 4 BF16 12-real + scale, 5 FP64 12-real (derived from U64 on each call,
+// in a buffer allocated on first use).
+static int storage_links(sfh_ctx* c, int storage, const void** U, int* gp, int* sp)
 {
-    if (!c || !ms_per_hop || storage < 0 || storage > 4 || nrep < 1) return SFH_ERR_INVALID;
-    cudaSetDevice(c->device);
+    static const int gps[6] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18, GP_BF16_12, GP_F64_12};
+    static const int sps[6] = {SP_F64, SP_F32, SP_F16, SP_F32, SP_BF16, SP_F64};
+    if (storage < 0 || storage > 5) return SFH_ERR_INVALID;
     if (!c->lowp_valid) {
         launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18, c->Ubf16);
         c->lowp_valid = true;
     }
-    static const int gp[5] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18, GP_BF16_12};
-    static const int sp[5] = {SP_F64, SP_F32, SP_F16, SP_F32, SP_BF16};
-    const void* const Us[5] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16};
-    const void* U = Us[storage];
-    int st = SFH_OK;
+    if (storage == 5) {
+        const size_t Vh = (size_t)c->g.Vh;
+        if (!c->U64_12) {
+            int st = cuda_check(c, cudaMalloc(&c->U64_12, (size_t)c->g.V * 4 * 6 * 16), "FP64 12-real links");
+            if (st) return st;
+        }
+        for (int pm = 0; pm < 8; ++pm) {  // rows 0 and 1: the first 6 of the 9 elements of each (p, mu)
+            int st = cuda_check(c,
+                                cudaMemcpyAsync((char*)c->U64_12 + pm * 6 * Vh * 16, (const char*)c->U64 + pm * 9 * Vh * 16,
+                                                6 * Vh * 16, cudaMemcpyDeviceToDevice, c->stream),
+                                "FP64 12-real links");
+            if (st) return st;
+        }
+    }
+    const void* const Us[6] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16, c->U64_12};
+    *U = Us[storage];
+    *gp = gps[storage];
+    *sp = sps[storage];
+    return SFH_OK;
+}
+
+// out = K in (the hopping term of D = m + K, Fermions.cpp:218-247, both
+// parities) computed by the standalone Dslash kernel in a storage format
+// (0..5 as storage_links): the input rounded to the format's vectors, the
+// links to its links, the result returned in FP64.  The check of the
+// kernels that sfh_dslash_timing times.
+extern "C" int sfh_dslash_storage(sfh_ctx* c, int storage, const double* in, double* out)
+{
+    if (!c || !in || !out) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const void* U = nullptr;
+    int gp = 0, sp = 0;
+    int st = storage_links(c, storage, &U, &gp, &sp);
+    if (st) return st;
+    const size_t n = (size_t)c->g.V * 6 * sizeof(double);
+    st = cuda_check(c, cudaMemcpyAsync(c->stage, in, n, cudaMemcpyHostToDevice, c->stream), "dslash input");
+    if (st) return st;
+    launch_spinor_aos_to_eo(c->g, (const double*)c->stage, c->spin[0], c->stream);
+    launch_spinor_convert(c->g, sp, true, c->spin[0], c->spin[1], c->stream);
+    launch_hop(c->g, gp, U, sp, c->spin[1], sp, c->spin[2], nullptr, 0.0, 1.0, 0, 2, c->stream);
+    launch_spinor_convert(c->g, sp, false, c->spin[2], c->spin[3], c->stream);
+    launch_spinor_eo_to_aos(c->g, c->spin[3], (double*)c->stage, c->stream);
+    st = cuda_check(c, cudaMemcpyAsync(out, c->stage, n, cudaMemcpyDeviceToHost, c->stream), "dslash output");
+    if (st) return st;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "dslash storage");
+}
+
+// Device time of one even-odd hop (V/2 output sites) in a storage format
+// (0..5 as storage_links).  Uses the context's gauge field and a zero input
+// (the memory traffic and arithmetic do not depend on the values); nrep
+// timed hops after three untimed ones, measured with CUDA events on the
+// context's stream.
+extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_per_hop)
+{
+    if (!c || !ms_per_hop || nrep < 1) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const void* U = nullptr;
+    int gp = 0, sp = 0;
+    int st = storage_links(c, storage, &U, &gp, &sp);
+    if (st) return st;
     void* in = c->spin[0];
     void* out = c->spin[1];
     cudaMemsetAsync(in, 0, (size_t)c->g.V * 48, c->stream);
@@ -330,10 +384,9 @@ extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_p
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int k = 0; k < 3; ++k) launch_hop(c->g, gp[storage], U, sp[storage], in, sp[storage], out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    for (int k = 0; k < 3; ++k) launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, 0, 1, c->stream);
     cudaEventRecord(e0, c->stream);
-    for (int k = 0; k < nrep; ++k)
-        launch_hop(c->g, gp[storage], U, sp[storage], in, sp[storage], out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    for (int k = 0; k < nrep; ++k) launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, 0, 1, c->stream);
     cudaEventRecord(e1, c->stream);
     st = cuda_check(c, cudaEventSynchronize(e1), "dslash timing");
     float ms = 0.f;

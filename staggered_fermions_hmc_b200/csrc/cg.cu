@@ -142,65 +142,6 @@ __device__ __forceinline__ Nbr neighbours(const Geom& g, const Coord& c)
     return n;
 }
 
-// w = U v (FIRST) or w += U v, as FMA chains
-template <bool FIRST, typename R>
-__device__ __forceinline__ void mv_add(Vec3<R>& w, const Mat3<R>& U, const Vec3<R>& v)
-{
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const Cx<R>* u = &U.e[3 * i];
-        R re = FIRST ? u[0].re * v.c[0].re : fma(u[0].re, v.c[0].re, w.c[i].re);
-        R im = FIRST ? u[0].re * v.c[0].im : fma(u[0].re, v.c[0].im, w.c[i].im);
-        re = fma(-u[0].im, v.c[0].im, re);
-        im = fma(u[0].im, v.c[0].re, im);
-#pragma unroll
-        for (int k = 1; k < 3; ++k) {
-            re = fma(u[k].re, v.c[k].re, re);
-            re = fma(-u[k].im, v.c[k].im, re);
-            im = fma(u[k].re, v.c[k].im, im);
-            im = fma(u[k].im, v.c[k].re, im);
-        }
-        w.c[i] = {re, im};
-    }
-}
-
-// w -= U^dag v, as FMA chains: (U^dag v)_i = sum_k conj(U_ki) v_k
-template <typename R>
-__device__ __forceinline__ void mdv_sub(Vec3<R>& w, const Mat3<R>& U, const Vec3<R>& v)
-{
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        R re = w.c[i].re, im = w.c[i].im;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const Cx<R> u = U.e[3 * k + i];
-            re = fma(-u.re, v.c[k].re, re);
-            re = fma(-u.im, v.c[k].im, re);
-            im = fma(-u.re, v.c[k].im, im);
-            im = fma(u.im, v.c[k].re, im);
-        }
-        w.c[i] = {re, im};
-    }
-}
-
-// acc += s w
-template <typename R>
-__device__ __forceinline__ void vfma(Vec3<R>& acc, R s, const Vec3<R>& w)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) acc.c[k] = {fma(s, w.c[k].re, acc.c[k].re), fma(s, w.c[k].im, acc.c[k].im)};
-}
-
-template <typename R>
-__device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg, R scale = R(1))
-{
-    const R s = neg ? -scale : scale;
-    Vec3<R> o;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[k] = {s * v.c[k].re, s * v.c[k].im};
-    return o;
-}
-
 // Link staging: every thread copies the 8 links of its site (4 forward at
 // the site, 4 backward at its neighbours) into its own columns of shared
 // memory with asynchronous copies, [direction][element][thread], so that all
@@ -260,20 +201,6 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
-// a neighbour spinor with the hop's scalar factor applied: the eta / 2 and
-// time-wrap sign, and for the 16-bit storages the per-site scale (one multiply)
-template <int SP, typename R>
-__device__ __forceinline__ Vec3<R> hop_input(const void* in, int nq, int j, int Vh, bool neg, R s)
-{
-    if constexpr (SpinorFmt<SP>::scaled) {
-        float sc;
-        Vec3<R> v = SpinorFmt<SP>::load_unscaled(in, nq, j, Vh, &sc);
-        return vneg_if(v, neg, s * sc);
-    } else {
-        return vneg_if(vcvt<R>(SpinorFmt<SP>::load(in, nq, j, Vh)), neg, s);
-    }
-}
-
 template <int GP, int SP, int NB, bool STG>
 __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeFmt<GP>::E* sl, const Nbr& n, int q,
                                           int i, int Vh, const void* const (&in)[NB], const bool (&on)[NB],

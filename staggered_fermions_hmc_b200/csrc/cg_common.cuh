@@ -5,6 +5,7 @@
 
 #include <cooperative_groups.h>
 
+#include "hop.cuh"
 #include "sfh_internal.h"
 
 namespace sfh {
@@ -89,14 +90,6 @@ __device__ __forceinline__ void vacc(Vec3<R>& acc, const Vec3<R>& w, bool neg)
     }
 }
 
-template <typename To, typename From>
-__device__ __forceinline__ Vec3<To> vcvt(const Vec3<From>& v)
-{
-    Vec3<To> o;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) o.c[k] = {(To)v.c[k].re, (To)v.c[k].im};
-    return o;
-}
 
 // a + s*b with explicit fused multiply-add (identical rounding in every phase)
 __device__ __forceinline__ Vec3<float> vaxpy(const Vec3<float>& a, float s, const Vec3<float>& b)

@@ -12,7 +12,11 @@
 // are read with coalesced SoA loads (neighbour spinors are re-read by up to
 // eight threads and are served from L1/L2).  The staggered phases and the
 // boundary signs are computed from the coordinates, so links stay pure SU(3)
-// and can be stored with 12 reals.
+// and can be stored with 12 reals.  The reduced-precision storages use the
+// solver's FMA-chain hop (hop.cuh): eta_mu / 2, the time-wrap sign and the
+// 16-bit per-site scale go onto the input vector, the products accumulate
+// in place.
+#include "hop.cuh"
 #include "sfh_internal.h"
 
 namespace sfh {
@@ -40,7 +44,13 @@ __device__ __forceinline__ void acc_add(Vec3<R>& acc, const Vec3<R>& w, bool neg
 
 }  // namespace
 
-// Hopping sum for one output site, shared with the solver kernels.
+// Hopping sum for one output site: sum_mu eta_mu [bc U in(x+mu) - bc U^dag
+// in(x-mu)], times 1/2 in the FMA-chain form (every format but FP64-18),
+// without it in FP64-18's own form (halved by the caller).
+template <int GP> struct HopHalfInside {
+    static constexpr bool v = GP != GP_F64_18;
+};
+
 template <int GP, int SPI>
 __device__ __forceinline__ Vec3<typename GaugeFmt<GP>::R> hop_site(const Geom& g, const Coord& c,
                                                                    int q, int i, const void* gauge,
@@ -51,27 +61,48 @@ __device__ __forceinline__ Vec3<typename GaugeFmt<GP>::R> hop_site(const Geom& g
     Vec3<R> acc;
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc.c[k] = {R(0), R(0)};
+    if constexpr (HopHalfInside<GP>::v) {
 #pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        bool eta_neg = eta_sign(c, mu) < 0;
-        int lu = lex_up(g, c, mu) >> 1;
-        int ld = lex_dn(g, c, mu) >> 1;
-        bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
-        bool wrap_dn = (mu == 3) && (c.x[3] == 0);
-        Mat3<R> U = GaugeFmt<GP>::load(gauge, q, mu, i, g.Vh);
-        Vec3<R> v = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, lu, g.Vh));
-        acc_add(acc, mul_mv(U, v), eta_neg != wrap_up);
-        Mat3<R> Ud = GaugeFmt<GP>::load(gauge, 1 - q, mu, ld, g.Vh);
-        Vec3<R> w = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, ld, g.Vh));
-        acc_add(acc, mul_adj_mv(Ud, w), !(eta_neg != wrap_dn));
+        for (int mu = 0; mu < 4; ++mu) {
+            const R s = eta_sign(c, mu) < 0 ? R(-0.5) : R(0.5);
+            const int lu = lex_up(g, c, mu) >> 1;
+            const int ld = lex_dn(g, c, mu) >> 1;
+            const bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
+            const bool wrap_dn = (mu == 3) && (c.x[3] == 0);
+            mv_add<false>(acc, GaugeFmt<GP>::load(gauge, q, mu, i, g.Vh),
+                          hop_input<SPI>(in, 1 - q, lu, g.Vh, wrap_up, s));
+            mdv_sub(acc, GaugeFmt<GP>::load(gauge, 1 - q, mu, ld, g.Vh),
+                    hop_input<SPI>(in, 1 - q, ld, g.Vh, wrap_dn, s));
+        }
+    } else {
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            bool eta_neg = eta_sign(c, mu) < 0;
+            int lu = lex_up(g, c, mu) >> 1;
+            int ld = lex_dn(g, c, mu) >> 1;
+            bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
+            bool wrap_dn = (mu == 3) && (c.x[3] == 0);
+            Mat3<R> U = GaugeFmt<GP>::load(gauge, q, mu, i, g.Vh);
+            Vec3<R> v = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, lu, g.Vh));
+            acc_add(acc, mul_mv(U, v), eta_neg != wrap_up);
+            Mat3<R> Ud = GaugeFmt<GP>::load(gauge, 1 - q, mu, ld, g.Vh);
+            Vec3<R> w = cvt<R, RI>(SpinorFmt<SPI>::load(in, 1 - q, ld, g.Vh));
+            acc_add(acc, mul_adj_mv(Ud, w), !(eta_neg != wrap_dn));
+        }
     }
     return acc;
 }
 
 namespace {
 
+// five resident blocks for the FP32 arithmetic formats (at most 51
+// registers; they fit in 48 without spills), the compiler's choice for FP64
+template <int GP> struct HopMinBlocks {
+    static constexpr int v = sizeof(typename GaugeFmt<GP>::R) == 4 ? 5 : 0;
+};
+
 template <int GP, int SPI, int SPO, bool SELF>
-__global__ void __launch_bounds__(256) hop_kernel(Geom g, const void* __restrict__ gauge,
+__global__ void __launch_bounds__(256, HopMinBlocks<GP>::v) hop_kernel(Geom g, const void* __restrict__ gauge,
                                                   const void* __restrict__ in, const void* self,
                                                   void* out, double a, double b, int q0)
 {
@@ -81,7 +112,7 @@ __global__ void __launch_bounds__(256) hop_kernel(Geom g, const void* __restrict
     if (i >= g.Vh) return;
     Coord c = eo_coords(g, q, i);
     Vec3<R> acc = hop_site<GP, SPI>(g, c, q, i, gauge, in);
-    R hb = (R)(0.5 * b);
+    R hb = (R)(HopHalfInside<GP>::v ? b : 0.5 * b);
     Vec3<R> res;
 #pragma unroll
     for (int k = 0; k < 3; ++k) res.c[k] = {hb * acc.c[k].re, hb * acc.c[k].im};
@@ -108,7 +139,39 @@ void launch_typed(const Geom& g, const void* gauge, const void* in, void* out, c
         hop_kernel<GP, SP, SP, false><<<grid, 256, 0, s>>>(g, gauge, in, self, out, a, b, q0);
 }
 
+// even-odd FP64 vectors (both parities) to storage format SP, or back
+template <int SP, bool TO_FMT>
+__global__ void __launch_bounds__(256) convert_spinor(Geom g, const void* __restrict__ src, void* __restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int p = blockIdx.y;
+    if (i >= g.Vh) return;
+    typedef typename SpinorFmt<SP>::R R;
+    if (TO_FMT)
+        SpinorFmt<SP>::store(dst, p, i, g.Vh, cvt<R, double>(SpinorFmt<SP_F64>::load(src, p, i, g.Vh)));
+    else
+        SpinorFmt<SP_F64>::store(dst, p, i, g.Vh, cvt<double, R>(SpinorFmt<SP>::load(src, p, i, g.Vh)));
+}
+
+template <int SP>
+void launch_convert(const Geom& g, bool to_fmt, const void* src, void* dst, cudaStream_t s)
+{
+    dim3 grid((g.Vh + 255) / 256, 2);
+    if (to_fmt)
+        convert_spinor<SP, true><<<grid, 256, 0, s>>>(g, src, dst);
+    else
+        convert_spinor<SP, false><<<grid, 256, 0, s>>>(g, src, dst);
+}
+
 }  // namespace
+
+void launch_spinor_convert(const Geom& g, int sp, bool to_fmt, const void* src, void* dst, cudaStream_t s)
+{
+    if (sp == SP_F32) launch_convert<SP_F32>(g, to_fmt, src, dst, s);
+    else if (sp == SP_F16) launch_convert<SP_F16>(g, to_fmt, src, dst, s);
+    else if (sp == SP_BF16) launch_convert<SP_BF16>(g, to_fmt, src, dst, s);
+    else launch_convert<SP_F64>(g, to_fmt, src, dst, s);
+}
 
 void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,
                 int out_prec, void* out, const void* self, double a, double b, int q0, int nq,
@@ -125,6 +188,8 @@ void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, c
         launch_typed<GP_F32_18, SP_F32>(g, gauge, in, out, self, a, b, q0, nq, s);
     else if (gauge_prec == GP_BF16_12 && in_prec == SP_BF16)
         launch_typed<GP_BF16_12, SP_BF16>(g, gauge, in, out, self, a, b, q0, nq, s);
+    else if (gauge_prec == GP_F64_12 && in_prec == SP_F64)
+        launch_typed<GP_F64_12, SP_F64>(g, gauge, in, out, self, a, b, q0, nq, s);
 }
 
 }  // namespace sfh

@@ -206,7 +206,7 @@ __device__ __forceinline__ void reconstruct_row2(Mat3<R>& U)
 // storage formats
 // ---------------------------------------------------------------------------
 enum SpinorPrec { SP_F64 = 0, SP_F32 = 1, SP_F16 = 2, SP_BF16 = 3 };
-enum GaugePrec { GP_F64_18 = 0, GP_F32_12 = 1, GP_F16_12 = 2, GP_F32_18 = 3, GP_BF16_12 = 4 };
+enum GaugePrec { GP_F64_18 = 0, GP_F32_12 = 1, GP_F16_12 = 2, GP_F32_18 = 3, GP_BF16_12 = 4, GP_F64_12 = 5 };
 
 template <int SP> struct SpinorFmt;
 
@@ -389,6 +389,27 @@ template <> struct GaugeFmt<GP_F64_18> {
             double2 w = __ldg(b + (size_t)k * Vh);
             U.e[k] = {w.x, w.y};
         }
+        return U;
+    }
+};
+
+// FP64 12-real links (rows 0 and 1; row 2 reconstructed): six double2 per
+// link, [p][mu][6][i]
+template <> struct GaugeFmt<GP_F64_12> {
+    typedef double R;
+    typedef double2 E;
+    static constexpr int K = 6;
+    static constexpr size_t link_bytes = 96;
+    __device__ static __forceinline__ Mat3<R> load(const void* base, int p, int mu, int i, int Vh)
+    {
+        const double2* b = (const double2*)base + ((size_t)(p * 4 + mu) * 6) * Vh + i;
+        Mat3<R> U;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            double2 w = __ldg(b + (size_t)k * Vh);
+            U.e[k] = {w.x, w.y};
+        }
+        reconstruct_row2(U);
         return U;
     }
 };

@@ -28,6 +28,7 @@ struct sfh_ctx {
     void* U32 = nullptr;       // gauge FP32 12-real (derived)
     void* U16 = nullptr;       // gauge FP16 12-real (derived)
     void* Ubf16 = nullptr;     // gauge BF16 12-real (derived)
+    void* U64_12 = nullptr;    // gauge FP64 12-real (derived on use by the standalone Dslash)
     void* U32_18 = nullptr;    // gauge FP32 18-real (derived)
     bool lowp_valid = false;   // derived copies match U64
     void* Pmom = nullptr;      // momenta FP64 18-real
@@ -62,6 +63,8 @@ int cuda_check(sfh_ctx* c, cudaError_t e, const char* what);
 // launch helpers implemented in layout.cu / dslash.cu
 void launch_spinor_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
 void launch_spinor_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
+// even-odd FP64 vectors to storage format sp (to_fmt) or back, both parities
+void launch_spinor_convert(const Geom& g, int sp, bool to_fmt, const void* src, void* dst, cudaStream_t s);
 void launch_links_aos_to_eo(const Geom& g, const double* aos, void* eo, cudaStream_t s);
 void launch_links_eo_to_aos(const Geom& g, const void* eo, double* aos, cudaStream_t s);
 void launch_make_lowp_gauge(const Geom& g, const void* U64, void* U32, void* U16, cudaStream_t s,
