@@ -1,6 +1,6 @@
 // cg_noalloc.cu — single-launch CG solver (one cooperative kernel per solve,
 // phases separated by grid.sync) and the allocation-free entry point built on
-// it.  The kernel runs the reference's CG (solve_CG_DDdagger,
+// it.  The kernel runs the reference's FP64 CG (solve_CG_DDdagger,
 // Fermions.cpp:553-617) with the three-phase iteration
 //   P1  t = K p_new,     p_new = r + beta p computed at the neighbours
 //   P2  p = p_new, v = m^2 p - K t, partial <p, v>      -> alpha
@@ -76,37 +76,19 @@ __device__ __noinline__ void finish_init(const CgArgs& a, const CgSys& S, int la
     }
 }
 
-__device__ __noinline__ void finish_hop2(const CgArgs& a, const CgSys& S, int lane, int mode, int cur)
+__device__ __noinline__ void finish_hop2(const CgArgs& a, const CgSys& S, int lane, int cur)
 {
     CgLane* L = a.lanes + lane;
     double s = warp_sum_slots(a.partial + L->poff + lane_slot0(S, L->parity), lane_nslots(S));
     if (threadIdx.x != 0) return;
-    const int nxt = cur ^ 1;
-    if (mode == LM_ACTIVE) {  // s = <p, M p>; Fermions.cpp:573-586
-        L->pAp = s;
-        double alpha = L->rr / s;
-        if (!isfinite(s) || fabs(s) < 1e-30 || !isfinite(alpha)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else {
-            L->alpha = alpha;
-            L->mode[nxt] = LM_ACTIVE;
-        }
-    } else {  // reliable update finished: s = |b - M x|^2 in FP64
-        L->nru += 1;
-        if (s < L->target) {
-            L->rr = s;
-            set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
-        } else if (!isfinite(s)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else if (L->iters >= a.maxit) {
-            L->rr = s;
-            set_mode_final(L, LM_FAILED, SFH_ERR_NOCONV, a.n_active);
-        } else {
-            L->beta = s / L->rr_old;
-            L->rr = s;
-            L->rmax = sqrt(s);
-            L->mode[nxt] = LM_ACTIVE;
-        }
+    // s = <p, M p>; Fermions.cpp:573-586
+    L->pAp = s;
+    double alpha = L->rr / s;
+    if (!isfinite(s) || fabs(s) < 1e-30 || !isfinite(alpha)) {
+        set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
+    } else {
+        L->alpha = alpha;
+        L->mode[cur ^ 1] = LM_ACTIVE;
     }
 }
 
@@ -117,106 +99,19 @@ __device__ __noinline__ void finish_update(const CgArgs& a, const CgSys& S, int 
     if (threadIdx.x != 0) return;
     const int nxt = cur ^ 1;
     L->iters += 1;
-    if (!isfinite(rn)) {
+    const double beta = rn / L->rr;  // Fermions.cpp:594-601
+    if (!isfinite(rn) || !isfinite(beta)) {
         set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-    } else if (!a.mixed) {
-        double beta = rn / L->rr;  // Fermions.cpp:594-601
-        if (!isfinite(beta)) {
-            set_mode_final(L, LM_FAILED, SFH_ERR_BREAKDOWN, a.n_active);
-        } else {
-            L->beta = beta;
-            L->rr = rn;
-            if (rn < L->target)  // Fermions.cpp:569
-                set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
-            else if (L->iters >= a.maxit)  // Fermions.cpp:609-614
-                set_mode_final(L, LM_FAILED, SFH_ERR_NOCONV, a.n_active);
-            else
-                L->mode[nxt] = LM_ACTIVE;
-        }
     } else {
-        double r = sqrt(rn);
-        if (rn < L->target || r < a.delta * L->rmax || L->iters >= a.maxit) {
-            L->rr_old = L->rr;
-            L->rr = rn;
-            L->mode[nxt] = LM_RU;
-        } else {
-            L->beta = rn / L->rr;
-            L->rr = rn;
-            L->rmax = fmax(L->rmax, r);
+        L->beta = beta;
+        L->rr = rn;
+        if (rn < L->target)  // Fermions.cpp:569
+            set_mode_final(L, LM_DONE, SFH_OK, a.n_active);
+        else if (L->iters >= a.maxit)  // Fermions.cpp:609-614
+            set_mode_final(L, LM_FAILED, SFH_ERR_NOCONV, a.n_active);
+        else
             L->mode[nxt] = LM_ACTIVE;
-        }
     }
-}
-
-// ---------------------------------------------------------------------------
-// reliable-update site kernels (FP64 links and vectors), rare
-// ---------------------------------------------------------------------------
-template <int XP>
-__device__ __noinline__ void ru_hop1_site(const CgArgs& a, const CgSys& S, const Coord& c, int q,
-                                          int i, int rid)
-{
-    const int nq = 1 - q, Vh = S.g.Vh;
-    const void* xhi = rhs_ptr(a, rid, F_XHI);
-    const void* xlo = rhs_ptr(a, rid, F_XLO);
-    Vec3<double> acc;
-    vzero(acc);
-#pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        const bool eta_neg = eta_sign(c, mu) < 0;
-        const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-        const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-        const bool wd = (mu == 3) && (c.x[3] == 0);
-        Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-        Vec3<double> xu = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, nq, lu, Vh), 1.0,
-                                vcvt<double>(SpinorFmt<XP>::load_cg(xlo, nq, lu, Vh)));
-        vacc(acc, mul_mv(U, xu), eta_neg != wu);
-        Mat3<double> Ud = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-        Vec3<double> xd = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, nq, ld, Vh), 1.0,
-                                vcvt<double>(SpinorFmt<XP>::load_cg(xlo, nq, ld, Vh)));
-        vacc(acc, mul_adj_mv(Ud, xd), !(eta_neg != wd));
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) acc.c[k] = {0.5 * acc.c[k].re, 0.5 * acc.c[k].im};
-    SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
-}
-
-template <int SP, int XP>
-__device__ __noinline__ double ru_hop2_site(const CgArgs& a, const CgSys& S, const Coord& c, int q,
-                                            int i, int rid)
-{
-    typedef typename SpinorFmt<SP>::R RS;
-    const int nq = 1 - q, Vh = S.g.Vh;
-    const void* thi = rhs_ptr(a, rid, F_THI);
-    Vec3<double> acc;
-    vzero(acc);
-#pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        const bool eta_neg = eta_sign(c, mu) < 0;
-        const int lu = lex_up(S.g, c, mu) >> 1, ld = lex_dn(S.g, c, mu) >> 1;
-        const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
-        const bool wd = (mu == 3) && (c.x[3] == 0);
-        Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-        vacc(acc, mul_mv(U, SpinorFmt<SP_F64>::load_cg(thi, nq, lu, Vh)), eta_neg != wu);
-        Mat3<double> Ud = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-        vacc(acc, mul_adj_mv(Ud, SpinorFmt<SP_F64>::load_cg(thi, nq, ld, Vh)), !(eta_neg != wd));
-    }
-    void* xhi = rhs_ptr(a, rid, F_XHI);
-    void* xlo = rhs_ptr(a, rid, F_XLO);
-    Vec3<double> xn = vaxpy(SpinorFmt<SP_F64>::load_cg(xhi, q, i, Vh), 1.0,
-                            vcvt<double>(SpinorFmt<XP>::load_cg(xlo, q, i, Vh)));
-    SpinorFmt<SP_F64>::store(xhi, q, i, Vh, xn);
-    Vec3<typename SpinorFmt<XP>::R> z;
-    vzero(z);
-    SpinorFmt<XP>::store(xlo, q, i, Vh, z);
-    Vec3<double> b = SpinorFmt<SP_F64>::load_cg(rhs_ptr(a, rid, F_B), q, i, Vh);
-    Vec3<double> res;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        res.c[k].re = b.c[k].re - (S.m2 * xn.c[k].re - 0.5 * acc.c[k].re);
-        res.c[k].im = b.c[k].im - (S.m2 * xn.c[k].im - 0.5 * acc.c[k].im);
-    }
-    SpinorFmt<SP>::store(rhs_ptr(a, rid, F_R), q, i, Vh, vcvt<RS>(res));
-    return vdot_re(res, res);
 }
 
 // gather the lanes of one RHS pass
@@ -246,7 +141,6 @@ template <int GP, int SP, int NB>
 __device__ void phase_init(const CgArgs& a, const CgSys& S, int t, double* smem, unsigned* s_mask)
 {
     typedef typename SpinorFmt<SP>::R R;
-    constexpr int XP = XFmt<SP>::v;
     const TileInfo ti = decode_tile(S, t);
     const int Vh = S.g.Vh;
     for (int base = 0; base < S.nrhs; base += NB) {
@@ -264,9 +158,6 @@ __device__ void phase_init(const CgArgs& a, const CgSys& S, int t, double* smem,
             Vec3<double> z;
             vzero(z);
             SpinorFmt<SP_F64>::store(rhs_ptr(a, rid[l], F_XHI), ti.q, ti.i, Vh, z);
-            if (a.mixed)
-                SpinorFmt<XP>::store(rhs_ptr(a, rid[l], F_XLO), ti.q, ti.i, Vh,
-                                     vcvt<typename SpinorFmt<XP>::R>(z));
             SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_R), ti.q, ti.i, Vh, vcvt<R>(b));
             SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_P), ti.q, ti.i, Vh, vcvt<R>(z));
             sums[l] = vdot_re(b, b);
@@ -283,15 +174,13 @@ __device__ void phase_init(const CgArgs& a, const CgSys& S, int t, double* smem,
 }
 
 // ---------------------------------------------------------------------------
-// P1: t = K (r + beta p) for normal lanes; thi = K (x_hi + x_lo) for lanes in
-// a reliable update.  Output parity q, inputs on parity 1-q.
+// P1: t = K (r + beta p).  Output parity q, inputs on parity 1-q.
 // ---------------------------------------------------------------------------
 template <int GP, int SP, int NB>
 __device__ void phase_hop1(const CgArgs& a, const CgSys& S, int t, int cur)
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
-    constexpr int XP = XFmt<SP>::v;
     const TileInfo ti = decode_tile(S, t);
     if (!ti.valid) return;
     const Coord c = eo_coords(S.g, ti.q, ti.i);
@@ -301,11 +190,10 @@ __device__ void phase_hop1(const CgArgs& a, const CgSys& S, int t, int cur)
         int lanes[NB], rid[NB], mode[NB];
         RS beta[NB];
         gather<NB>(a, S, base, cnt, q, true, cur, lanes, mode, rid);
-        bool anyA = false, anyR = false;
+        bool anyA = false;
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
             anyA |= mode[l] == LM_ACTIVE;
-            anyR |= mode[l] == LM_RU;
             beta[l] = mode[l] == LM_ACTIVE ? (RS)ld_dbl(&a.lanes[lanes[l]].beta) : RS(0);
         }
         if (anyA) {
@@ -350,17 +238,11 @@ __device__ void phase_hop1(const CgArgs& a, const CgSys& S, int t, int cur)
                 SpinorFmt<SP>::store(rhs_ptr(a, rid[l], F_T), q, ti.i, Vh, vcvt<RS>(o));
             }
         }
-        if (anyR) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mode[l] == LM_RU) ru_hop1_site<XP>(a, S, c, q, ti.i, rid[l]);
-        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// P2: p = r + beta p, v = m^2 p - K t, <p,v> (normal lanes);
-//     x_hi += x_lo, x_lo = 0, r = b - (m^2 x_hi - K thi), |r|^2 (reliable update)
+// P2: p = r + beta p, v = m^2 p - K t, <p,v>
 // ---------------------------------------------------------------------------
 template <int GP, int SP, int NB>
 __device__ void phase_hop2(const CgArgs& a, const CgSys& S, int t, int cur, double* smem,
@@ -368,7 +250,6 @@ __device__ void phase_hop2(const CgArgs& a, const CgSys& S, int t, int cur, doub
 {
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
-    constexpr int XP = XFmt<SP>::v;
     const TileInfo ti = decode_tile(S, t);
     const int q = ti.q, nq = 1 - ti.q, Vh = S.g.Vh;
     Coord c;
@@ -380,16 +261,15 @@ __device__ void phase_hop2(const CgArgs& a, const CgSys& S, int t, int cur, doub
         bool part[NB];
         double sums[NB];
         gather<NB>(a, S, base, cnt, q, false, cur, lanes, mode, rid);
-        bool anyA = false, anyR = false;
+        bool anyA = false;
 #pragma unroll
         for (int l = 0; l < NB; ++l) {
             anyA |= mode[l] == LM_ACTIVE;
-            anyR |= mode[l] == LM_RU;
-            part[l] = mode[l] == LM_ACTIVE || mode[l] == LM_RU;
+            part[l] = mode[l] == LM_ACTIVE;
             sums[l] = 0.0;
             beta[l] = mode[l] == LM_ACTIVE ? (RS)ld_dbl(&a.lanes[lanes[l]].beta) : RS(0);
         }
-        if (!anyA && !anyR) continue;  // uniform across the block
+        if (!anyA) continue;  // uniform across the block
         if (anyA && ti.valid) {
             Vec3<R> acc[NB];
 #pragma unroll
@@ -439,24 +319,19 @@ __device__ void phase_hop2(const CgArgs& a, const CgSys& S, int t, int cur, doub
                 sums[l] = vdot_re(pn, vq);
             }
         }
-        if (anyR && ti.valid) {
-#pragma unroll
-            for (int l = 0; l < NB; ++l)
-                if (mode[l] == LM_RU) sums[l] = ru_hop2_site<SP, XP>(a, S, c, q, ti.i, rid[l]);
-        }
         block_sum<NB>(sums, smem);
         unsigned mask = arrive<NB>(a, S, lanes, part, sums, ti.slot, s_mask);
         if (mask && threadIdx.x < 32) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (mask & (1u << l)) finish_hop2(a, S, lanes[l], mode[l], cur);
+                if (mask & (1u << l)) finish_hop2(a, S, lanes[l], cur);
         }
         __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
-// P3: x += alpha p, r -= alpha v, |r|^2 -> beta, convergence, reliable update
+// P3: x += alpha p, r -= alpha v, |r|^2 -> beta, convergence
 // ---------------------------------------------------------------------------
 template <int GP, int SP, int NB>
 __device__ void phase_update(const CgArgs& a, const CgSys& S, int t, int cur, double* smem,
@@ -514,8 +389,9 @@ __device__ __forceinline__ void load_sys(const CgArgs& a, int t, CgSys* s_sys)
 }
 
 template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (SP == SP_F64 ? 1 : 2)) cg_persistent(CgArgs a)
+__global__ void __launch_bounds__(kTile, 1) cg_persistent(CgArgs a)
 {
+    static_assert(GP == GP_F64_18 && SP == SP_F64, "the single-launch solver runs the FP64 CG only");
     cgrp::grid_group grid = cgrp::this_grid();
     __shared__ double smem[32 * NB];
     __shared__ unsigned s_mask;
@@ -706,7 +582,7 @@ extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* 
         return SFH_ERR_CUDA;
     if (cudaStreamSynchronize(stream) != cudaSuccess) return SFH_ERR_CUDA;
     int status = L.status;
-    if (L.mode[0] == LM_ACTIVE || L.mode[0] == LM_RU) status = SFH_ERR_NOCONV;
+    if (L.mode[0] == LM_ACTIVE) status = SFH_ERR_NOCONV;
     if (info) {
         std::memset(info, 0, sizeof(*info));
         info->status = status;

@@ -30,7 +30,7 @@ namespace sfh {
 // ---------------------------------------------------------------------------
 struct FastDiv {
     uint32_t d, m, l;
-    FastDiv() : d(1), m(0), l(0) {}
+    FastDiv() = default;  // trivial, so that structs holding one can live in __shared__
     explicit FastDiv(uint32_t div) : d(div)
     {
         l = 0;
