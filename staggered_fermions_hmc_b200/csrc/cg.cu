@@ -200,96 +200,6 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
     }
 }
 
-// ---------------------------------------------------------------------------
-// FP16 links and vectors: the products in packed half2 arithmetic
-// ---------------------------------------------------------------------------
-// Complex numbers are half2 pairs (re, im).  With b_perp = (-b.im, b.re),
-// a b = a.re (b.re, b.im) + a.im b_perp: two packed FMAs whose first
-// operand is one half of a broadcast to both (free in the instruction), so
-// a 3x3 complex matrix-vector product is 18 packed FMAs and the links and
-// vectors are used as stored.  Each neighbour's product (|entries| <= 3:
-// link entries and the site-normalised vector entries are at most 1) is
-// converted to FP32 and accumulated there with its scalar factor (eta / 2,
-// the time-wrap sign, the neighbour's site scale).
-
-__device__ __forceinline__ __half2 h2_bits(uint32_t w) { return *reinterpret_cast<__half2*>(&w); }
-
-__device__ __forceinline__ __half2 h2_perp(__half2 b)  // (-b.im, b.re)
-{
-    return __hmul2(__lowhigh2highlow(b), __halves2half2(__ushort_as_half(0xBC00u), __ushort_as_half(0x3C00u)));
-}
-
-// 12-real FP16 link -> nine half2, row 2 = conj(row0 x row1)
-__device__ __forceinline__ void hlink_unpack(const uint2 (&w)[3], __half2 (&e)[9])
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        e[2 * k] = h2_bits(w[k].x);
-        e[2 * k + 1] = h2_bits(w[k].y);
-    }
-    const __half2* a = &e[0];
-    const __half2* b = &e[3];
-    __half2 bp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) bp[k] = h2_perp(b[k]);
-    const __half2 conj = __halves2half2(__ushort_as_half(0x3C00u), __ushort_as_half(0xBC00u));  // (1, -1)
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        const int j = (m + 1) % 3, k = (m + 2) % 3;
-        // a_j b_k - a_k b_j
-        __half2 d = __hmul2(__low2half2(a[j]), b[k]);
-        d = __hfma2(__high2half2(a[j]), bp[k], d);
-        d = __hfma2(__hneg2(__low2half2(a[k])), b[j], d);
-        d = __hfma2(__hneg2(__high2half2(a[k])), bp[j], d);
-        e[6 + m] = __hmul2(d, conj);
-    }
-}
-
-template <bool STG>
-__device__ __forceinline__ void hlink_load(const uint2* s, const void* Ulo, int d, int p, int mu, int i, int Vh,
-                                           __half2 (&e)[9])
-{
-    uint2 w[3];
-    if constexpr (STG) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) w[k] = s[(d * 3 + k) * kTile + threadIdx.x];
-    } else {
-        const uint2* b = (const uint2*)Ulo + ((size_t)(p * 4 + mu) * 3) * Vh + i;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) w[k] = __ldg(b + (size_t)k * Vh);
-    }
-    hlink_unpack(w, e);
-}
-
-// acc += f (U v) (ADJ false) or acc += f (U^dag v) (ADJ true) for a stored
-// FP16 vector v with site scale sc: f = s sc, products in half2
-template <bool ADJ>
-__device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9], const void* in, int nq, int j,
-                                         int Vh, float f)
-{
-    const uint4 w = __ldg((const uint4*)in + (size_t)nq * Vh + j);
-    const __half2 v[3] = {h2_bits(w.x), h2_bits(w.y), h2_bits(w.z)};
-    f *= __uint_as_float(w.w);
-    __half2 vp[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) vp[k] = ADJ ? __hneg2(h2_perp(v[k])) : h2_perp(v[k]);
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        // row r of U (U_rk) or column r (conj(U_kr)); conj(u) v = u.re v - u.im v_perp
-        __half2 y = __hmul2(__low2half2(U[ADJ ? r : 3 * r]), v[0]);
-        y = __hfma2(__high2half2(U[ADJ ? r : 3 * r]), vp[0], y);
-#pragma unroll
-        for (int k = 1; k < 3; ++k) {
-            const __half2 u = U[ADJ ? 3 * k + r : 3 * r + k];
-            y = __hfma2(__low2half2(u), v[k], y);
-            y = __hfma2(__high2half2(u), vp[k], y);
-        }
-        const float2 yf = __half22float2(y);
-        acc.c[r].re = fmaf(f, yf.x, acc.c[r].re);
-        acc.c[r].im = fmaf(f, yf.y, acc.c[r].im);
-    }
-}
-
 // acc[l] += 1/2 sum_mu eta_mu(x) [bc U_mu(x) in_l(x+mu) - bc U_mu(x-mu)^dag in_l(x-mu)]
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
@@ -313,11 +223,11 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
         for (int mu = 0; mu < 4; ++mu) {
             const float s = ((n.eta >> mu) & 1u) ? -0.5f : 0.5f;
             __half2 U[9];
-            hlink_load<STG>(sl, Ulo, 2 * mu, q, mu, i, Vh, U);
+            hlink_load<STG>(sl, kTile, Ulo, 2 * mu, q, mu, i, Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) hop_half<false>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
-            hlink_load<STG>(sl, Ulo, 2 * mu + 1, nq, mu, n.dn[mu], Vh, U);
+            hlink_load<STG>(sl, kTile, Ulo, 2 * mu + 1, nq, mu, n.dn[mu], Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
                 if (on[l]) hop_half<true>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);

@@ -13,9 +13,10 @@
 // eight threads and are served from L1/L2).  The staggered phases and the
 // boundary signs are computed from the coordinates, so links stay pure SU(3)
 // and can be stored with 12 reals.  The reduced-precision storages use the
-// solver's FMA-chain hop (hop.cuh): eta_mu / 2, the time-wrap sign and the
-// 16-bit per-site scale go onto the input vector, the products accumulate
-// in place.
+// solver's hop arithmetic (hop.cuh): for FP16 links and vectors packed-half
+// products accumulated in FP32 with eta_mu / 2, the time-wrap sign and the
+// site scale; for the others FMA chains with that factor on the input
+// vector.
 #include "hop.cuh"
 #include "sfh_internal.h"
 
@@ -61,7 +62,22 @@ __device__ __forceinline__ Vec3<typename GaugeFmt<GP>::R> hop_site(const Geom& g
     Vec3<R> acc;
 #pragma unroll
     for (int k = 0; k < 3; ++k) acc.c[k] = {R(0), R(0)};
-    if constexpr (HopHalfInside<GP>::v) {
+    if constexpr (GP == GP_F16_12 && SPI == SP_F16) {
+        // FP16 links and vectors: packed-half products, FP32 accumulation
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            const float s = eta_sign(c, mu) < 0 ? -0.5f : 0.5f;
+            const int lu = lex_up(g, c, mu) >> 1;
+            const int ld = lex_dn(g, c, mu) >> 1;
+            const bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
+            const bool wrap_dn = (mu == 3) && (c.x[3] == 0);
+            __half2 U[9];
+            hlink_load<false>(nullptr, 0, gauge, 0, q, mu, i, g.Vh, U);
+            hop_half<false>(acc, U, in, 1 - q, lu, g.Vh, wrap_up ? -s : s);
+            hlink_load<false>(nullptr, 0, gauge, 0, 1 - q, mu, ld, g.Vh, U);
+            hop_half<true>(acc, U, in, 1 - q, ld, g.Vh, wrap_dn ? s : -s);
+        }
+    } else if constexpr (HopHalfInside<GP>::v) {
 #pragma unroll
         for (int mu = 0; mu < 4; ++mu) {
             const R s = eta_sign(c, mu) < 0 ? R(-0.5) : R(0.5);
