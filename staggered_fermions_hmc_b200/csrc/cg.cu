@@ -701,12 +701,11 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
-    // the reliable-update residuals stay in this kernel: measured faster than
-    // a kernel of their own, and the compiler keeps the FP64 hop's registers
-    // better with them here
-    constexpr bool ru_here = true;
+    // the reliable-update residuals are computed here too: measured faster
+    // than a kernel of their own, and the compiler keeps the FP64 hop's
+    // registers better with them here
     gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
-    if (!(P.anyA || (ru_here && P.anyR))) return;  // uniform across the block
+    if (!(P.anyA || P.anyR)) return;  // uniform across the block
     bool part[NB], on[NB];
     double sums[NB * kSums];
     // this thread's partial sums across the item's tiles, in shared memory
@@ -717,7 +716,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
         on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
-        part[l] = on[l] || (ru_here && P.mode[l] == LM_RU);
+        part[l] = on[l] || P.mode[l] == LM_RU;
         tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
 #pragma unroll
         for (int f = 0; f < kSums; ++f) s_part[l * kSums + f][threadIdx.x] = 0.0;
@@ -762,61 +761,15 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     }
 #pragma unroll
     for (int f = 0; f < NB * kSums; ++f) sums[f] = s_part[f][threadIdx.x];
-    if constexpr (ru_here) {
-        if (P.anyR) {
-            for (int t = ir.first; t < ir.end; ++t) {
-                const TileInfo ti = decode_tile(S, t);
-                if (!ti.valid) break;
-                const Coord c = eo_coords(S.g, q, ti.i);
+    if (P.anyR) {
+        for (int t = ir.first; t < ir.end; ++t) {
+            const TileInfo ti = decode_tile(S, t);
+            if (!ti.valid) break;
+            const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
-                for (int l = 0; l < NB; ++l)
-                    if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
-            }
+            for (int l = 0; l < NB; ++l)
+                if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
         }
-    }
-    block_sum<NB * kSums>(sums, smem);
-    const unsigned nsq = (unsigned)item_groups(a, S);
-    unsigned mask = arrive_sums<NB>(a, S, P, part, sums, ir.slot, S.both ? 2u * nsq : nsq, &s_mask);
-    if (mask && threadIdx.x < 32) {
-#pragma unroll
-        for (int l = 0; l < NB; ++l)
-            if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
-    }
-}
-
-// the reliable-update residuals of the lanes of a work item that are in a
-// reliable update: |b - M x|^2 in FP64 as the lane's sum, then the lane's
-// scalars (finish_lane) once its last item has arrived
-template <int SP, int NB>
-__global__ void __launch_bounds__(kTile) cg_ru2(CgArgs a, const int2* __restrict__ items, int cur)
-{
-    constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    __shared__ double smem[32 * NB * kSums];
-    __shared__ unsigned s_mask;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const ItemRange ir = item_range(a, S, it.x);
-    const int q = ir.q;
-    LanePass<NB> P;
-    gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
-    if (!P.anyR) return;  // uniform across the block
-    bool part[NB];
-    double sums[NB * kSums];
-#pragma unroll
-    for (int l = 0; l < NB; ++l) {
-        part[l] = P.mode[l] == LM_RU;
-#pragma unroll
-        for (int f = 0; f < kSums; ++f) sums[l * kSums + f] = 0.0;
-    }
-    for (int t = ir.first; t < ir.end; ++t) {
-        const TileInfo ti = decode_tile(S, t);
-        if (!ti.valid) break;
-        const Coord c = eo_coords(S.g, q, ti.i);
-#pragma unroll
-        for (int l = 0; l < NB; ++l)
-            if (part[l]) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
     }
     block_sum<NB * kSums>(sums, smem);
     const unsigned nsq = (unsigned)item_groups(a, S);
@@ -885,7 +838,7 @@ typedef void (*HopKernel)(CgArgs, const int2*, int);
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
-    HopKernel ru1, ru2;  // the reliable-update parts of the two hops
+    HopKernel ru1;  // the FP64 lanes' reliable-update hop (null: cg_hop1 does it)
     int nb1, nb2;   // RHS-group widths the hop kernels are compiled for
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
 };
@@ -922,7 +875,6 @@ static CgKernels pick_typed(int nb1, int nb2)
     pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
     k.ru1 = k.nb1 == 8 ? cg_ru1<SP, 8> : (k.nb1 == 4 ? cg_ru1<SP, 4> : (k.nb1 == 2 ? cg_ru1<SP, 2> : cg_ru1<SP, 1>));
-    k.ru2 = nullptr;  // cg_hop2 does the reliable-update residuals itself
     if constexpr (SP != SP_F64) k.ru1 = nullptr;  // cg_hop1 does them itself
     k.smem = STG ? StageBytes<GP>::v : 0;
     return k;
@@ -1122,9 +1074,10 @@ static int default_nb(int max_nrhs, int cap)
 }
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
-// kernels per CG iteration: hop1, its reliable-update part, hop2, its
-// reliable-update part, update
-constexpr int kPhases = 5;
+// kernels per CG iteration: hop1, its reliable-update part (FP64 lanes
+// only; null otherwise), hop2 (which also computes the reliable-update
+// residuals), update
+constexpr int kPhases = 4;
 
 // Work items (first tile, first RHS): tpi tiles of one parity of a system and
 // one RHS group of width nb; one block each.  The groups of a tile range are
@@ -1181,7 +1134,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
                                 double delta)
 {
     if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.gk.ru1 == k.ru1 &&
-        w.gk.ru2 == k.ru2 && w.g_tol == tol &&
+        w.g_tol == tol &&
         w.g_tpi == a.tpi &&
         w.g_maxit == maxit &&
         w.g_delta == delta)
@@ -1189,8 +1142,8 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     w.release_graph();
     const int2* items[kPhases];
     int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, k.nb2, 1};
-    const HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.ru2, k.update};
+    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, 1};
+    const HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.update};
     cudaError_t e;
     for (int ph = 0; ph < kPhases; ++ph)
         if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
@@ -1225,10 +1178,6 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     return cudaSuccess;
 }
 
-// Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
-// two hop kernels (0 = from the largest RHS count); tpi: tiles per block of
-// the iteration kernels (0 = 2); stage: hop kernels stage their links in
-// shared memory (reduced precisions only).  Returns a cudaError.
 // Device time of each iteration kernel over one solve (timed solves launch
 // the kernels one by one between CUDA events instead of replaying the graph).
 struct PhaseTimes {
@@ -1245,6 +1194,10 @@ static double default_reliable_delta(int prec)
     return (prec == SFH_PREC_F16 || prec == SFH_PREC_BF16) ? 0.1 : 0.01;
 }
 
+// Solve every lane of a built workspace.  nb1 / nb2: RHS-block widths of the
+// two hop kernels (0 = from the largest RHS count); tpi: tiles per block of
+// the iteration kernels (0 = 2); stage: hop kernels stage their links in
+// shared memory (reduced precisions only).  Returns a cudaError.
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
                                    int tpi, bool stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
 {
@@ -1277,9 +1230,9 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     // timed solves: the same kernels and work items, launched one by one
     const int2* items[kPhases];
     int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, k.nb2, 1};
-    HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.ru2, k.update};
-    const int report[kPhases] = {0, 0, 1, 1, 2};  // the reliable-update kernels count with their hop
+    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, 1};
+    HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.update};
+    const int report[kPhases] = {0, 0, 1, 2};  // the reliable-update kernel counts with its hop
     std::vector<cudaEvent_t> tev;
     if (timing) {
         for (int ph = 0; ph < kPhases; ++ph)
@@ -1304,7 +1257,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
             cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
             const int r = report[j % kPhases];
             timing->ms[r] += ms;
-            if (j % kPhases != 1 && j % kPhases != 3) timing->n[r] += 1;
+            if (j % kPhases != 1) timing->n[r] += 1;
         }
     };
     const int max_chunks = a.maxloop / kChunk + 2;
@@ -1326,7 +1279,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         } else if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) {
             return e;
         }
-        w.launches += (kPhases - (k.ru1 ? 0 : 1) - (k.ru2 ? 0 : 1)) * kChunk;
+        w.launches += (kPhases - (k.ru1 ? 0 : 1)) * kChunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
