@@ -531,9 +531,8 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
-    // the FP64 hop of lanes in a reliable update: here for the reduced
-    // precisions, in cg_ru1 for FP64 lanes (keeps the FP64 hop's registers
-    // free; measured faster both ways)
+    // the FP64 hop of lanes in a reliable update (mixed precisions only: FP64
+    // vectors belong to the plain FP64 CG, which has no reliable updates)
     constexpr bool ru_here = SP != SP_F64;
     gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
     if (!(P.anyA || (ru_here && P.anyR))) return;
@@ -578,31 +577,6 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
                     if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
             }
         }
-    }
-}
-
-// the FP64 hop of the lanes of a work item that are in a reliable update
-// (a kernel of its own: the FP64 registers stay out of the hop kernels)
-template <int SP, int NB>
-__global__ void __launch_bounds__(kTile) cg_ru1(CgArgs a, const int2* __restrict__ items, int cur)
-{
-    constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const ItemRange ir = item_range(a, S, it.x);
-    const int q = ir.q;
-    LanePass<NB> P;
-    gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
-    if (!P.anyR) return;
-    for (int t = ir.first; t < ir.end; ++t) {
-        const TileInfo ti = decode_tile(S, t);
-        if (!ti.valid) break;
-        const Coord c = eo_coords(S.g, q, ti.i);
-#pragma unroll 1
-        for (int l = 0; l < NB; ++l)
-            if (P.mode[l] == LM_RU) ru_hop1<XP>(a, S, c, q, ti.i, P.rid[l]);
     }
 }
 
@@ -838,7 +812,6 @@ typedef void (*HopKernel)(CgArgs, const int2*, int);
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
-    HopKernel ru1;  // the FP64 lanes' reliable-update hop (null: cg_hop1 does it)
     int nb1, nb2;   // RHS-group widths the hop kernels are compiled for
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
 };
@@ -874,8 +847,6 @@ static CgKernels pick_typed(int nb1, int nb2)
     k.hop1 = pick_hop1<GP, SP, STG>(nb1, &k.nb1);
     pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
-    k.ru1 = k.nb1 == 8 ? cg_ru1<SP, 8> : (k.nb1 == 4 ? cg_ru1<SP, 4> : (k.nb1 == 2 ? cg_ru1<SP, 2> : cg_ru1<SP, 1>));
-    if constexpr (SP != SP_F64) k.ru1 = nullptr;  // cg_hop1 does them itself
     k.smem = STG ? StageBytes<GP>::v : 0;
     return k;
 }
@@ -1074,10 +1045,9 @@ static int default_nb(int max_nrhs, int cap)
 }
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
-// kernels per CG iteration: hop1, its reliable-update part (FP64 lanes
-// only; null otherwise), hop2 (which also computes the reliable-update
-// residuals), update
-constexpr int kPhases = 4;
+// kernels per CG iteration: hop1, hop2, update (the hop kernels also do the
+// FP64 hops of lanes in a reliable update)
+constexpr int kPhases = 3;
 
 // Work items (first tile, first RHS): tpi tiles of one parity of a system and
 // one RHS group of width nb; one block each.  The groups of a tile range are
@@ -1133,8 +1103,7 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
 static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, double tol, int maxit,
                                 double delta)
 {
-    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.gk.ru1 == k.ru1 &&
-        w.g_tol == tol &&
+    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.g_tol == tol &&
         w.g_tpi == a.tpi &&
         w.g_maxit == maxit &&
         w.g_delta == delta)
@@ -1142,8 +1111,8 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     w.release_graph();
     const int2* items[kPhases];
     int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, 1};
-    const HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.update};
+    const int widths[kPhases] = {k.nb1, k.nb2, 1};
+    const HopKernel fn[kPhases] = {k.hop1, k.hop2, k.update};
     cudaError_t e;
     for (int ph = 0; ph < kPhases; ++ph)
         if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
@@ -1159,7 +1128,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
             p.func = (void*)fn[ph];
             p.gridDim = dim3(nitems[ph]);
             p.blockDim = dim3(kTile);
-            p.sharedMemBytes = (ph == 0 || ph == 2) ? (unsigned)k.smem : 0u;
+            p.sharedMemBytes = ph < 2 ? (unsigned)k.smem : 0u;  // the hop kernels
             void* args[] = {&a, (void*)&items[ph], &cur};
             p.kernelParams = args;
             cudaGraphNode_t node;
@@ -1181,7 +1150,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
 // Device time of each iteration kernel over one solve (timed solves launch
 // the kernels one by one between CUDA events instead of replaying the graph).
 struct PhaseTimes {
-    double ms[3];  // hop1, hop2, update (each with its reliable-update kernel)
+    double ms[3];  // hop1, hop2, update
     long n[3];
 };
 
@@ -1230,9 +1199,8 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     // timed solves: the same kernels and work items, launched one by one
     const int2* items[kPhases];
     int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb1, k.nb2, 1};
-    HopKernel fn[kPhases] = {k.hop1, k.ru1, k.hop2, k.update};
-    const int report[kPhases] = {0, 0, 1, 2};  // the reliable-update kernel counts with its hop
+    const int widths[kPhases] = {k.nb1, k.nb2, 1};
+    HopKernel fn[kPhases] = {k.hop1, k.hop2, k.update};
     std::vector<cudaEvent_t> tev;
     if (timing) {
         for (int ph = 0; ph < kPhases; ++ph)
@@ -1255,9 +1223,9 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         for (int j = 0; j < kPhases * kChunk; ++j) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
-            const int r = report[j % kPhases];
+            const int r = j % kPhases;
             timing->ms[r] += ms;
-            if (j % kPhases != 1) timing->n[r] += 1;
+            timing->n[r] += 1;
         }
     };
     const int max_chunks = a.maxloop / kChunk + 2;
@@ -1269,7 +1237,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
             for (int it = 0; it < kChunk; ++it)
                 for (int ph = 0; ph < kPhases; ++ph) {
                     if (fn[ph])
-                        fn[ph]<<<nitems[ph], kTile, (ph == 0 || ph == 2) ? k.smem : 0, stream>>>(a, items[ph],
+                        fn[ph]<<<nitems[ph], kTile, ph < 2 ? k.smem : 0, stream>>>(a, items[ph],
                                                                                                it & 1);
                     if ((e = cudaEventRecord(ev[kPhases * it + ph + 1], stream)) != cudaSuccess) {
                         destroy_events();
@@ -1279,7 +1247,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         } else if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) {
             return e;
         }
-        w.launches += (kPhases - (k.ru1 ? 0 : 1)) * kChunk;
+        w.launches += kPhases * kChunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
