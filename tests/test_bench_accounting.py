@@ -1,0 +1,72 @@
+"""The bench's algorithmic-byte accounting (the basis of every roofline
+figure it reports), checked on CPU against hand counts for small specs."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+
+def _info(iters, nru):
+    return {"iters_parity": [iters, iters], "reliable_updates": nru}
+
+
+def test_kernel_bytes_fp64_one_rhs():
+    """FP64, one system with one RHS: per parity and iteration hop1 reads p and
+    writes t (2 spinors), hop2 reads t, p, r and writes v (4), update moves 5
+    spinors and 2 solution vectors; both hops read the 8 links of every output
+    site once."""
+    import bench
+    dims = (4, 4, 4, 4)
+    Vh = 128
+    spec = [{"dims": dims, "nrhs": 1}]
+    out = bench.kernel_bytes(spec, [[_info(10, 0)]], "f64")
+    s, sx, lb = 48, 48, 144
+    per_parity = {"cg_hop1": 10 * Vh * (2 * s + 8 * lb),
+                  "cg_hop2": 10 * Vh * (4 * s + 8 * lb),
+                  "cg_update": 10 * Vh * (5 * s + 2 * sx)}
+    for k, v in per_parity.items():
+        assert out[k] == pytest.approx(2 * v), k
+
+
+def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
+    """FP16, two RHS of one system: links are counted once per (system,
+    parity, iteration) with the longer lane's count, spinors per RHS; each
+    reliable update adds an FP64 hop to both hop kernels."""
+    import bench
+    dims = (4, 4, 4, 8)
+    Vh = 256
+    spec = [{"dims": dims, "nrhs": 2}]
+    infos = [[_info(12, 2), _info(20, 4)]]
+    out = bench.kernel_bytes(spec, infos, "f16")
+    s, sx, lb = 16, 24, 24
+    its = 12 + 20
+    nru = (2 + 4) / 2.0  # per parity
+    hop1 = its * Vh * 2 * s + nru * Vh * (8 * 144 + 48 + 24 + 48) + 20 * 8 * lb * Vh
+    hop2 = its * Vh * 4 * s + nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s) + 20 * 8 * lb * Vh
+    upd = its * Vh * (5 * s + 2 * sx)
+    assert out["cg_hop1"] == pytest.approx(2 * hop1)
+    assert out["cg_hop2"] == pytest.approx(2 * hop2)
+    assert out["cg_update"] == pytest.approx(2 * upd)
+    assert bench.solve_bytes(spec, infos, "f16") == pytest.approx(2 * (hop1 + hop2 + upd))
+
+
+def test_dslash_bytes_table():
+    """Per output site of one hop: 8 links, one input and one output vector."""
+    import bench
+    link = {0: 144, 1: 48, 2: 24, 3: 72, 4: 24, 5: 96}
+    vec = {0: 48, 1: 24, 2: 16, 3: 24, 4: 16, 5: 48}
+    for st in link:
+        assert bench.DSLASH_BYTES[st] == 8 * link[st] + 2 * vec[st], bench.DSLASH_NAMES[st]
+
+
+def test_batch_spec_is_the_seeded_workload():
+    """64 systems from the stated sets, 1-8 RHS each, reproducible."""
+    import bench
+    a, b = bench.batch_spec(), bench.batch_spec()
+    assert a == b and len(a) == 64
+    assert all(s["dims"] in bench.LATTICES and s["mass"] in bench.MASSES and s["eps"] in bench.EPSES
+               and 1 <= s["nrhs"] <= 8 for s in a)
+    assert sum(s["nrhs"] for s in a) == 296
