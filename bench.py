@@ -124,6 +124,16 @@ class ClockSampler:
 # update (mixed precision) adds an FP64 hop in each hop kernel (8 FP64 links,
 # the FP64 solution or temporary) and the FP64 residual in cg_hop2.
 # ---------------------------------------------------------------------------
+# the arithmetic each solver precision computes in (dtype of the bench line)
+DTYPE = {"f16": "f16", "bf16": "f32", "f32": "f32", "f32_18": "f32", "f64": "f64"}
+ARITHMETIC = {
+    "f16": "f16 storage with a per-site scale; hop products in packed f16 (half2), each neighbour's product "
+           "accumulated in f32; f64 reliable updates",
+    "bf16": "bf16 storage with a per-site scale; f32 products and accumulation; f64 reliable updates",
+    "f32": "f32 storage (12-real links); f32 products and accumulation; f64 reliable updates",
+    "f32_18": "f32 storage (18-real links); f32 products and accumulation; f64 reliable updates",
+    "f64": "f64 storage and arithmetic (plain CG)",
+}
 SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24, "bf16": 16}
 LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72, "bf16": 24}
 KERNELS = ("cg_hop1", "cg_hop2", "cg_update")
@@ -461,7 +471,8 @@ def main():
     ap.add_argument("--impl", default="sfh", choices=["sfh", "reference"])
     ap.add_argument("--precision", default="f16", choices=["f32", "f16", "f32_18", "bf16"],
                     help="storage of the iterated vectors and links: f16 (half precision with a per-site "
-                         "scale), f32 (12-real links) or f32_18; arithmetic is f32, reliable updates f64")
+                         "scale; packed-half products, f32 accumulation), bf16 (per-site scale; f32 products), "
+                         "f32 (12-real links) or f32_18; reliable updates f64")
     ap.add_argument("--nsys", type=int, default=64)
     ap.add_argument("--ref-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -638,16 +649,12 @@ def main():
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": DTYPE[args.precision],
         "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
         "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
                                " x eps{0.3,1.0}, 1-8 RHS, seed 7",
                    "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
-                   "arithmetic": {"f16": "f16 storage with a per-site scale, f32 arithmetic, f64 reliable updates",
-                                  "f32": "f32 storage (12-real links), f32 arithmetic, f64 reliable updates",
-                                  "f32_18": "f32 storage (18-real links), f32 arithmetic, f64 reliable updates",
-                                  "bf16": "bf16 storage with a per-site scale, f32 arithmetic, f64 reliable updates"
-                                  }[args.precision],
+                   "arithmetic": ARITHMETIC[args.precision],
                    "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
                                                                       "staged_links": schedule[2]},
                    "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},

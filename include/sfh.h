@@ -37,8 +37,9 @@ extern "C" {
 /* solver precisions */
 #define SFH_PREC_F64 0   /* plain FP64 CG, FP64 links and vectors                     */
 #define SFH_PREC_F32 1   /* FP32 12-real links, FP32 vectors, FP64 reliable updates   */
-#define SFH_PREC_F16 2   /* FP16 12-real links, FP16+per-site-scale vectors, FP32 math,
-                            FP64 reliable updates                                      */
+#define SFH_PREC_F16 2   /* FP16 12-real links, FP16+per-site-scale vectors; hop
+                            products in packed FP16 (half2), each neighbour's product
+                            accumulated in FP32; FP64 reliable updates                */
 #define SFH_PREC_F32_18 3 /* FP32 18-real links (no reconstruction), FP32 vectors,
                              FP64 reliable updates                                     */
 #define SFH_PREC_BF16 4  /* BF16 12-real links, BF16+per-site-scale vectors, FP32 math,
@@ -263,7 +264,10 @@ typedef struct {
                                      reference's solve_CG_DDdagger               */
 
 /* No reference counterpart: the reference solves one system at a time
- * (Fermions.cpp:553).  All systems are solved by one persistent launch. */
+ * (Fermions.cpp:553).  All systems of a batch advance together: every CG
+ * iteration of every lane is the same three grid-wide kernels (t = K p;
+ * v = m^2 p - K t with the CG sums; the x, r, p update), replayed as CUDA
+ * graphs of 16 iterations, with the lanes' scalars advanced on the device. */
 int sfh_batch_create(int device, int nsys, const sfh_system_desc* systems, int precision,
                      int flags, sfh_batch** batch);
 int sfh_batch_destroy(sfh_batch* batch);
@@ -313,26 +317,29 @@ int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
 
 /* ---- allocation-free solve ------------------------------------------------ */
 /* No counterpart in the reference.  An FP64 CG solve of D D^dag X = phi (the
- * reference's full-lattice algorithm, as sfh_cg_solve with SFH_PREC_F64) that
- * allocates no device or host memory, for callers that cannot call cudaMalloc:
- * code running while a stream is captured into a CUDA graph, runtimes that own
- * all device memory through their own pool, and loops that must not allocate
- * after start-up.  The solver's work vectors live in a fixed array inside the
- * library (about 12.6 MB, reserved on every GPU that loads the library until
- * the process exits), so the lattice may have at most SFH_NOALLOC_MAX_SITES
- * sites; larger lattices return SFH_ERR_INVALID.
+ * reference's full-lattice algorithm, as sfh_cg_solve with SFH_PREC_F64; there
+ * is no mixed-precision variant) that allocates no device or host memory, for
+ * callers that cannot call cudaMalloc: host runtimes that own all device
+ * memory through their own pool and forbid allocations outside it, and
+ * trajectory loops that must not allocate after start-up.  The solver's work
+ * vectors live in a fixed array inside the library (about 12.6 MB, reserved
+ * on every GPU that loads the library until the process exits), so the
+ * lattice may have at most SFH_NOALLOC_MAX_SITES sites; larger lattices return
+ * SFH_ERR_INVALID.
  *
  * All pointers are device pointers in the library's even-odd layout (site
  * index i = s >> 1 within parity p = (x+y+z+t) & 1, s as above):
  *   links_eo: double2 [p][mu][row*3+col][i]   (4*V*9 double2 = 72*V doubles)
  *   phi_eo, x_eo: double2 [p][color][i]       (6*V doubles)
  * The call runs on cuda_stream (0 = legacy default stream) of the current
- * device and waits for it before returning; info may be NULL.  The first call
- * on a device looks up the array's device address, which can load the
- * library's device code on that device: make that first call before any
- * stream capture.  Every call uses the same array, so calls whose work
- * overlaps on the GPU (other threads, other streams) race and must be
- * serialised by the caller. */
+ * device, copies the solver's status back to the host and waits for the
+ * stream before returning; info may be NULL.  info->true_resid is -1 (not
+ * computed: no array is spare for the extra operator application);
+ * info->rsq_rel is the recurrence's |r|^2 / |b|^2.  The first call on a device
+ * looks up the array's device address, which can load the library's device
+ * code on that device: make that first call before any stream capture.  Every
+ * call uses the same array, so calls whose work overlaps on the GPU (other
+ * threads, other streams) race and must be serialised by the caller. */
 #define SFH_NOALLOC_MAX_SITES 65536
 int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* links_eo, const void* phi_eo,
                          void* x_eo, double tol, int maxit, void* cuda_stream, sfh_cg_info* info);

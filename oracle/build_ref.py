@@ -16,14 +16,23 @@ oracle/compat_check.cpp and libsfh.so (the side-by-side check of the
 reference-API layer).  Outputs go to oracle/_ref/ only.
 Nothing here runs the reference's own build (submit_roar.slurm).
 
-usage: python oracle/build_ref.py [L T mass tol] ...   (default: the fixture set)
+usage: python oracle/build_ref.py --reference DIR [L T mass tol] ...
+       (DIR: a checkout of the reference; or set SFH_REFERENCE_DIR.  Without
+       L T mass tol the fixture and benchmark set is built.)
 """
 import os
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("SFH_REFERENCE_DIR", "/root/reference")
+# the reference checkout: --reference DIR on the command line, else the
+# SFH_REFERENCE_DIR environment variable; None = not available
+REF = os.environ.get("SFH_REFERENCE_DIR") or None
+
+
+def set_reference(path):
+    global REF
+    REF = path
 OUT = os.path.join(HERE, "_ref")
 SOURCES = ["Lattice.cpp", "Fermions.cpp", "SU3_Sampling.cpp", "rng.cpp"]
 HEADERS = ["Lattice.h", "Fermions.h", "SU3_Sampling.h", "rng.h"]
@@ -159,8 +168,14 @@ def exe_path(L, T, mass, tol):
 
 
 def main(argv):
-    if not os.path.isdir(REF):
-        print(f"reference sources not found at {REF}; nothing to build")
+    argv = list(argv)
+    if "--reference" in argv:
+        k = argv.index("--reference")
+        set_reference(argv[k + 1])
+        del argv[k:k + 2]
+    if not REF or not os.path.isdir(REF):
+        print(f"reference sources not found ({REF!r}; give --reference DIR or set SFH_REFERENCE_DIR); "
+              "nothing to build")
         return 0
     configs = DEFAULT_CONFIGS
     if len(argv) >= 4:

@@ -430,12 +430,14 @@ typedef void (*PersistentKernel)(CgArgs);
 // ===========================================================================
 // Allocation-free CG entry point.
 //
-// For callers that cannot call cudaMalloc: code that runs while a stream is
-// being captured into a CUDA graph, host runtimes that own all device memory
-// through their own pool and forbid outside allocations, and trajectory loops
-// that must not allocate after start-up.  The solver's work vectors and
-// control data live in the file-scope array below instead of device
-// allocations; the caller passes device inputs and outputs.
+// For callers that cannot call cudaMalloc: host runtimes that own all device
+// memory through their own pool and forbid outside allocations, and
+// trajectory loops that must not allocate after start-up.  FP64 CG only; the
+// call copies the lane's status back to the host and waits for the stream,
+// and reports no true residual (true_resid = -1: no array is spare for it).
+// The solver's work vectors and control data live in the file-scope array
+// below instead of device allocations; the caller passes device inputs and
+// outputs.
 // ===========================================================================
 namespace sfh {
 namespace {

@@ -6,7 +6,8 @@ from the reference sources) on seeded inputs and stores inputs and outputs as
 compressed .npz files.  Needs the reference sources, so it runs only where
 they are present; the committed fixtures are what the tests read.
 
-usage: python tests/golden/make_golden.py
+usage: python tests/golden/make_golden.py --reference DIR
+       (DIR: a checkout of the reference; or set SFH_REFERENCE_DIR)
 """
 import os
 import subprocess
@@ -96,11 +97,15 @@ def make_heatbath():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
-def main():
+def main(argv):
+    if "--reference" in argv:
+        build_ref.set_reference(argv[argv.index("--reference") + 1])
+    if not build_ref.REF or not os.path.isdir(build_ref.REF):
+        sys.exit("give --reference DIR (a checkout of the reference) or set SFH_REFERENCE_DIR")
     for fx in FIXTURES:
         make(*fx)
     make_heatbath()
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

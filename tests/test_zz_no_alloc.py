@@ -1,17 +1,19 @@
 """The allocation-free solve, sfh_cg_solve_noalloc, against the regular solve.
 
-Some callers of this library cannot call cudaMalloc: code that runs while a
-stream is captured into a CUDA graph, host runtimes that hand out all device
-memory from their own pool, and trajectory loops that must not allocate after
-start-up.  sfh_cg_solve_noalloc serves them by keeping the solver's work
-vectors in a fixed array inside the library; the caller brings its own device
-buffers for the links, the source and the solution.
+Some callers of this library cannot call cudaMalloc: host runtimes that hand
+out all device memory from their own pool and forbid allocations outside it,
+and trajectory loops that must not allocate after start-up.
+sfh_cg_solve_noalloc serves them by keeping the solver's work vectors in a
+fixed array inside the library; the caller brings its own device buffers for
+the links, the source and the solution.
 
 Here the test allocates those buffers itself (with torch), in the library's
 even-odd layout, calls the entry point twice in a row with different sources,
 and compares each solution with sfh_cg_solve (FP64) on the same inputs, to the
-1e-11 relative tolerance the FP64 solver tests use.  This file is named so
-that pytest collects it last.
+1e-11 relative tolerance the FP64 solver tests use, and with the oracle's
+D D^dag (true residual).  Around the second call it checks the entry point's
+defining property: the device's free memory does not go down.  This file is
+named so that pytest collects it last.
 """
 import ctypes
 
@@ -74,14 +76,22 @@ def test_noalloc_solve_matches_regular_solve_twice(orc):
         x_eo = torch.full_like(phi_eo, float("nan"))
         torch.cuda.synchronize()
         info = sfh.CgInfo()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         st = lib.sfh_cg_solve_noalloc(cdims, mass, U_eo.data_ptr(), phi_eo.data_ptr(), x_eo.data_ptr(),
                                       tol, 50000, stream, ctypes.byref(info))
+        torch.cuda.synchronize()
+        free_after = torch.cuda.mem_get_info(dev)[0]
         assert st == sfh.SFH_OK
+        if seed == 79:  # the second call: nothing left to set up, nothing allocated
+            assert free_after >= free_before, (free_before, free_after)
         X = spinor_from_eo(dims, x_eo.cpu().numpy())
         assert np.all(np.isfinite(X))
         assert rel(X, X_ref) < 1e-11
         assert info.iters == info_ref["iters"]
         assert info.status == sfh.SFH_OK
+        assert info.true_resid == -1.0  # documented: not computed by this entry point
+        r = phi - orc.ddag(dims, mass, U, X)
+        assert np.linalg.norm(r) / np.linalg.norm(phi) < 2e-10
     lat.close()
 
 
