@@ -211,52 +211,128 @@ def time_steps(torch, stream_ptr, fn, steps, warmup):
 
 
 # ---------------------------------------------------------------------------
-# CPU baselines
+# CPU baselines: the reference's own CG on a sample stratified over the
+# batch's (lattice, mass, eps) classes
+#
+# The batch's 296 solves fall into at most 24 classes (4 lattices x 3 masses x
+# 2 gauge roughnesses).  A sample times one reference solve of a class's first
+# system (its first right-hand side), classes taken in a fixed rotation that
+# continues from step to step.  The batch's CPU time is estimated as
+# sum_c n_c t_c (n_c the class's number of solves, t_c its mean timed solve),
+# and the CPU solves/s as total_solves / that time, so every class counts
+# with its share of the batch.  Inputs come from the oracle's restatement of
+# the library's seeded generators (identical fields to the GPU arm's, without
+# loading the library).
 # ---------------------------------------------------------------------------
-def cpu_sample(spec, fields, budget_s=12.0, use_ref=True):
-    """Time CPU solves of the batch's own systems (same inputs) in batch order
-    until the budget is spent.  Returns (solves, seconds, kind, description)."""
-    import oracle
-    ref_ok = False
-    if use_ref:
-        from oracle import build_ref
-        ref_ok = True
-    solved, secs, used = 0, 0.0, []
-    kind = "port"
+def batch_classes(spec):
+    """[(key, first system index, number of solves)] in batch order of first
+    appearance; key = (dims, mass, eps)."""
+    order, info = [], {}
     for k, s in enumerate(spec):
-        if secs >= budget_s:
-            break
-        U, rhs = fields(k)
-        exe = None
-        if ref_ok:
-            exe = build_ref.exe_path(s["dims"][0], s["dims"][3], s["mass"], TOL)
-            if not (s["dims"][0] == s["dims"][1] == s["dims"][2] and os.path.exists(exe)):
-                exe = None
-        for j, b in enumerate(rhs):
-            if secs >= budget_s:
-                break
-            if exe:
-                t = ref_time_solve(exe, U, b)
-                kind = "reference"
-            else:
-                t0 = time.perf_counter()
-                oracle.cg(s["dims"], s["mass"], U, b, TOL, MAXIT)
-                t = time.perf_counter() - t0
-            secs += t
-            solved += 1
-            used.append(f"{'x'.join(map(str, s['dims']))}/m{s['mass']}")
-    desc = f"first {solved} solves of the batch in order ({', '.join(sorted(set(used)))})"
-    return solved, secs, kind, desc
+        key = (tuple(s["dims"]), s["mass"], s["eps"])
+        if key not in info:
+            info[key] = [k, 0]
+            order.append(key)
+        info[key][1] += s["nrhs"]
+    return [(key, info[key][0], info[key][1]) for key in order]
 
 
-def ref_time_solve(exe, U, b):
-    import tempfile
-    with tempfile.TemporaryDirectory() as td:
-        U.astype("<f8").tofile(os.path.join(td, "U.bin"))
-        b.astype("<f8").tofile(os.path.join(td, "phi.bin"))
-        out = subprocess.run([exe, "time", td, "1"], check=True, capture_output=True, text=True,
-                             env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count())))
-    return float(json.loads(out.stdout.strip().splitlines()[-1])["solve_s"])
+def class_name(key):
+    dims, mass, eps = key
+    return f"{'x'.join(map(str, dims))}/m{mass}/eps{eps}"
+
+
+class CpuSampler:
+    """Times reference solves class by class, in rotation.  kind per sample:
+    'reference' (oracle/_ref, the reference's own sources) or 'port' (the C
+    restatement in-process, where no reference binary exists)."""
+
+    def __init__(self, spec, workdir):
+        import oracle
+        oracle.lib()
+        self.oracle = oracle
+        self.spec = spec
+        self.classes = batch_classes(spec)
+        self.cursor = 0
+        self.workdir = workdir
+        self.inputs = {}
+
+    def _exe(self, key):
+        from oracle import build_ref
+        dims, mass, _ = key
+        if not (dims[0] == dims[1] == dims[2]):
+            return None
+        exe = build_ref.exe_path(dims[0], dims[3], mass, TOL)
+        return exe if os.path.exists(exe) else None
+
+    def _input_dir(self, ci):
+        """U.bin / phi.bin of class ci's representative solve, written once."""
+        if ci not in self.inputs:
+            key, k, _ = self.classes[ci]
+            s = self.spec[k]
+            d = os.path.join(self.workdir, f"class{ci}")
+            os.makedirs(d, exist_ok=True)
+            U = self.oracle.philox_gauge(s["dims"], s["eps"], s["gauge_seed"])
+            b = self.oracle.philox_spinor(s["dims"], s["rhs_seed"])
+            U.astype("<f8").tofile(os.path.join(d, "U.bin"))
+            b.astype("<f8").tofile(os.path.join(d, "phi.bin"))
+            self.inputs[ci] = d
+        return self.inputs[ci]
+
+    def time_class(self, ci):
+        key, k, _ = self.classes[ci]
+        d = self._input_dir(ci)
+        exe = self._exe(key)
+        if exe:
+            out = subprocess.run([exe, "time", d, "1"], check=True, capture_output=True, text=True,
+                                 env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count())))
+            return float(json.loads(out.stdout.strip().splitlines()[-1])["solve_s"]), "reference"
+        dims, mass, _ = key
+        U = np.fromfile(os.path.join(d, "U.bin"))
+        b = np.fromfile(os.path.join(d, "phi.bin"))
+        t0 = time.perf_counter()
+        self.oracle.cg(dims, mass, U, b, TOL, MAXIT)
+        return time.perf_counter() - t0, "port"
+
+    def step(self, budget_s, max_classes=None):
+        """Time classes in rotation until budget_s of wall time is spent (at
+        least one); returns [(class index, solve seconds, kind)]."""
+        out, t0 = [], time.perf_counter()
+        while not out or (time.perf_counter() - t0 < budget_s
+                          and (max_classes is None or len(out) < max_classes)):
+            ci = self.cursor
+            self.cursor = (self.cursor + 1) % len(self.classes)
+            t, kind = self.time_class(ci)
+            out.append((ci, t, kind))
+        return out
+
+    def estimate(self, samples):
+        """Class-weighted CPU solves/s over the classes that have samples."""
+        per = {}
+        for ci, t, _ in samples:
+            per.setdefault(ci, []).append(t)
+        covered = sorted(per)
+        n = sum(self.classes[ci][2] for ci in covered)
+        secs = sum(self.classes[ci][2] * float(np.mean(per[ci])) for ci in covered)
+        kinds = sorted({kind for _, _, kind in samples})
+        kind = kinds[0] if len(kinds) == 1 else "mixed"
+        total = sum(c[2] for c in self.classes)
+        return {
+            "value": n / secs, "kind": kind,
+            "classes_timed": len(covered), "classes": len(self.classes),
+            "solves_timed": len(samples),
+            "reference_solves": sum(1 for x in samples if x[2] == "reference"),
+            "port_solves": sum(1 for x in samples if x[2] == "port"),
+            "batch_cpu_seconds_estimate": secs * total / n,
+            "per_class_seconds": {class_name(self.classes[ci][0]): float(np.mean(per[ci])) for ci in covered},
+        }
+
+
+def cpu_sample_desc(est):
+    return (f"{est['solves_timed']} reference CG solves (solve_CG_DDdagger) stratified over "
+            f"{est['classes_timed']} of the batch's {est['classes']} (lattice, mass, eps) classes, "
+            f"one solve of each class's first system, weighted by the class's share of the batch's "
+            f"solves; inputs from the oracle's Philox generators (the GPU arm's fields)")
 
 
 # ---------------------------------------------------------------------------
@@ -284,50 +360,79 @@ def dist_setup():
     return world, rank, local
 
 
+def workload_config(spec, world):
+    """The workload both arms report (the same dict in both lines)."""
+    return {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
+                        " x eps{0.3,1.0}, 1-8 RHS, seed 7",
+            "total_solves": sum(s["nrhs"] for s in spec), "tol": TOL,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"}
+
+
 def run_reference_arm(args, spec):
+    """The reference's own CG (oracle/_ref, all host threads) on the batch's
+    classes in rotation, each step a bounded sample (--ref-budget seconds of
+    solves).  The value is the class-weighted CPU solves/s over the timed
+    steps' samples; ms_per_step is the measured wall time of a step."""
+    import tempfile
     world, rank, local = dist_setup()
     if rank != 0:
         return
-    import oracle
-    oracle.lib()
-    total_rhs = sum(s["nrhs"] for s in spec)
-
-    # identical inputs, generated by the library's seeded generators on the GPU
-    # when available; the reference arm itself only times CPU work.
-    fields = make_host_fields(spec, local)
-    vals = []
-    desc = kind = None
-    for step in range(args.warmup + args.steps):
-        n, secs, kind, desc = cpu_sample(spec, fields, budget_s=args.ref_budget)
-        if step >= args.warmup:
-            vals.append(n / secs)
-    v = statistics.median(vals)
+    with tempfile.TemporaryDirectory() as td:
+        sampler = CpuSampler(spec, td)
+        warm, timed, step_ms = [], [], []
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            got = sampler.step(args.ref_budget)
+            ms = 1000.0 * (time.perf_counter() - t0)
+            if step < args.warmup:
+                warm += got
+            else:
+                timed += got
+                step_ms.append(ms)
+        # classes no timed step reached keep their warm-up samples
+        seen = {ci for ci, _, _ in timed}
+        est = sampler.estimate(timed + [x for x in warm if x[0] not in seen])
+    v = est["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * total_rhs / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "uneven batch: 64 systems, seed 7", "total_solves": total_rhs},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": kind,
-                             "sample": desc},
-            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "ms_per_step": statistics.mean(step_ms), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
+            "config": workload_config(spec, world),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": est["kind"],
+                             "sample": cpu_sample_desc(est)},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_sample": {k: est[k] for k in ("classes_timed", "classes", "solves_timed", "reference_solves",
+                                                     "port_solves", "batch_cpu_seconds_estimate")},
+            "per_class_seconds": est["per_class_seconds"]}
     print(json.dumps(line), flush=True)
 
 
-def make_host_fields(spec, device):
-    cache = {}
-
-    def fields(k):
-        if k not in cache:
-            import staggered_fermions_hmc_b200 as sfh
-            s = spec[k]
-            B = build_batch(sfh, [s], "f64", device)
-            U = B.gauge(0)
-            rhs = [B.rhs(0, j) for j in range(s["nrhs"])]
-            B.close()
-            cache.clear()
-            cache[k] = (U, rhs)
-        return cache[k]
-    return fields
+def c4_oracle_check(B, spec):
+    """The batch's solutions against the oracle on the host: for the first
+    system of every (lattice, mass, eps) class, the FP64 true residual of its
+    first solution by the oracle's D D^dag (apply_DDdagger,
+    Fermions.cpp:530-547); for the first system of each lattice also the
+    distance to the oracle's FP64 CG solution (Fermions.cpp:553-617) and the
+    oracle's iteration count beside the lane's."""
+    import oracle
+    oracle.lib()
+    out, worst = {}, 0.0
+    seen_dims = set()
+    for key, k, _ in batch_classes(spec):
+        s = spec[k]
+        dims = s["dims"]
+        U, b, X = B.gauge(k), B.rhs(k, 0), B.solution(k, 0)
+        r = float(np.linalg.norm(b - oracle.ddag(dims, s["mass"], U, X)) / np.linalg.norm(b))
+        worst = max(worst, r)
+        row = {"true_resid": r, "iters": B.info(k, 0)["iters_parity"]}
+        if dims not in seen_dims:
+            seen_dims.add(dims)
+            Xo, it, _, _ = oracle.cg(dims, s["mass"], U, b, TOL, MAXIT)
+            row["err_vs_oracle_fp64"] = float(np.linalg.norm(X - Xo) / np.linalg.norm(Xo))
+            row["oracle_iters_full_lattice"] = it
+        out[class_name(key)] = row
+    return {"worst_true_resid_oracle": worst, "per_class": out}
 
 
 # algorithmic bytes per output site of one hop: its 8 links (144 / 48 / 24 /
@@ -355,13 +460,21 @@ def run_extras(sfh, hbm, quick=False):
         ds[DSLASH_NAMES[st]] = {"ms_per_hop": ms, "GB/s": gbs, "frac": gbs / hbm,
                                 "bytes_per_site": DSLASH_BYTES[st]}
     ex["dslash_32x32x32x64"] = ds
-    # ill-conditioned single solve: 32^3x64, eps = 1.0, m = 0.01
+    # ill-conditioned single solve: 32^3x64, eps = 1.0, m = 0.01; each
+    # solution's true residual by the oracle's D D^dag on the host
     phi = lat.gaussian_spinor(11)
+    U = lat.download_gauge()
+
+    def oracle_resid(X):
+        return float(np.linalg.norm(phi - oracle.ddag(dims, 0.01, U, X)) / np.linalg.norm(phi))
+
     sol = {}
+    for prec in ("f64", "f16", "bf16", "f32"):  # the first solve of each builds its workspace
+        lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec)
     t0 = time.perf_counter()
     X64, i64 = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision="f64", info=True)
     t64 = time.perf_counter() - t0
-    sol["f64"] = {"iters": i64["iters"], "seconds": t64}
+    sol["f64"] = {"iters": i64["iters"], "seconds": t64, "true_resid_oracle": oracle_resid(X64)}
     for prec in ("f16", "bf16", "f32"):
         t0 = time.perf_counter()
         try:
@@ -371,9 +484,13 @@ def run_extras(sfh, hbm, quick=False):
             continue
         tm = time.perf_counter() - t0
         sol[prec] = {"iters": im["iters"], "reliable_updates": im["reliable_updates"], "seconds": tm,
-                     "err_vs_f64": float(np.linalg.norm(Xm - X64) / np.linalg.norm(X64)),
-                     "speedup_vs_f64": t64 / tm}
+                     "true_resid_oracle": oracle_resid(Xm),
+                     "dist_to_f64_solution": float(np.linalg.norm(Xm - X64) / np.linalg.norm(X64)),
+                     "speedup_vs_f64": t64 / tm, "arithmetic": ARITHMETIC[prec]}
+    sol["note"] = ("bf16 and f32 are the configuration's 'FP32 math' (f32 products); f16 multiplies in "
+                   "packed half2 and accumulates in f32")
     ex["c3_32x32x32x64_m0.01"] = sol
+    del U
     lat.close()
     if quick:
         return ex
@@ -382,14 +499,19 @@ def run_extras(sfh, hbm, quick=False):
     lat = sfh.Lattice((16, 16, 16, 16), 0.1, 4.2)
     for geps in (0.3, 1.0):
         lat.random_gauge(geps, 21)
+        U = lat.download_gauge()
         phi = lat.gaussian_spinor(22)
         for m in (0.1, 0.02):
             lat.set_mass(m)
-            row = {}
+            Xo, it_o, _, _ = oracle.cg(lat.dims, m, U, phi, TOL, 40000)
+            row = {"oracle_fp64_iters": it_o}
             for prec in ("f64", "f32_18", "f32", "f16", "bf16"):
                 t0 = time.perf_counter()
-                _, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
-                row[prec] = {"iters": inf["iters"], "ms": 1e3 * (time.perf_counter() - t0)}
+                X, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+                row[prec] = {"iters": inf["iters"], "ms": 1e3 * (time.perf_counter() - t0),
+                             "true_resid_oracle": float(np.linalg.norm(phi - oracle.ddag(lat.dims, m, U, X))
+                                                        / np.linalg.norm(phi)),
+                             "err_vs_oracle_fp64": float(np.linalg.norm(X - Xo) / np.linalg.norm(Xo))}
             grid[f"eps{geps}_m{m}"] = row
     ex["c2_16^4"] = grid
     lat.close()
@@ -474,7 +596,10 @@ def main():
                          "scale; packed-half products, f32 accumulation), bf16 (per-site scale; f32 products), "
                          "f32 (12-real links) or f32_18; reliable updates f64")
     ap.add_argument("--nsys", type=int, default=64)
-    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--ref-budget", type=float, default=6.0,
+                    help="seconds of reference CPU solves per step of the reference arm")
+    ap.add_argument("--cpu-budget", type=float, default=30.0,
+                    help="seconds of reference CPU solves for the cpu_baseline of the GPU arm")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
@@ -624,16 +749,21 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        import oracle
-        oracle.lib()
+        # one pass over the batch's classes (bounded by --cpu-budget seconds)
+        import tempfile
+        with tempfile.TemporaryDirectory() as td:
+            sampler = CpuSampler(spec, td)
+            est = sampler.estimate(sampler.step(args.cpu_budget, max_classes=len(sampler.classes)))
+        cpu = {"value": est["value"], "unit": "solves/s", "cores": os.cpu_count(), "kind": est["kind"],
+               "sample": cpu_sample_desc(est), "classes_timed": est["classes_timed"],
+               "batch_cpu_seconds_estimate": est["batch_cpu_seconds_estimate"]}
 
-        def fields(k):
-            s = spec[k]
-            return B.gauge(k), [B.rhs(k, j) for j in range(s["nrhs"])]
-
-        n, secs, kind, desc = cpu_sample(spec, fields, budget_s=args.ref_budget)
-        cpu = {"value": n / secs, "unit": "solves/s", "cores": os.cpu_count(), "kind": kind,
-               "sample": desc}
+    c4_check = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            c4_check = c4_oracle_check(B, spec)
+        except Exception as e:  # a secondary check never hides the headline
+            c4_check = {"error": f"{type(e).__name__}: {e}"}
 
     extras = None
     if rank == 0 and not args.no_extras:
@@ -651,29 +781,27 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": DTYPE[args.precision],
         "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
-        "config": {"workload": "uneven batch: 64 systems from {8^4,12^4,16^4,16^3x32} x m{0.05,0.1,0.2}"
-                               " x eps{0.3,1.0}, 1-8 RHS, seed 7",
-                   "total_solves": total_rhs, "tol": TOL, "precision": args.precision,
-                   "arithmetic": ARITHMETIC[args.precision],
-                   "parallelism": f"replicas x{world}", "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
-                                                                      "staged_links": schedule[2]},
-                   "l2": "inputs larger than L2 (gauge+vectors of the batch >> 126 MB)"},
+        "config": workload_config(spec, world),
         "roofline": {"bound": "hbm", "achieved": top_gbs, "peak": hbm, "unit": "GB/s",
                      "frac": top_gbs / hbm, "traffic": top_traffic, "peak_kind": peak_kind,
                      "kernel": top, "alg_bytes_per_launch": kbytes[top] / top_n,
                      "ms_per_launch": kernels[top]["ms_total"] / top_n},
+        "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "gpu_launches": args.steps * launches_per_solve,
+        "extras": extras,
         "kernels": kernels,
         "solve_roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                            "alg_bytes_per_step": alg_bytes,
                            "what": "all three iteration kernels, graph replay, per timed step"},
         "other_mixed_precisions": other,
-        "fp64_batched": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms64,
-                         "mixed_over_fp64": value / world / fp64_value},
+        "solver_config": {"precision": args.precision, "arithmetic": ARITHMETIC[args.precision],
+                          "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
+                                       "staged_links": schedule[2]}},
+        "c4_oracle_check": c4_check,
         "solver": {"iters_mean": float(np.mean(iters)), "iters_max": int(max(iters)),
                    "reliable_updates_mean": float(np.mean(nru)), "worst_true_resid": worst},
-        "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-        "gpu_launches": args.steps * launches_per_solve,
-        "extras": extras,
+        "fp64_batched": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms64,
+                         "mixed_over_fp64": value / world / fp64_value},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -77,6 +77,12 @@ def lib():
             "orc_heatbath": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, D]),
             "orc_exp_field": (ctypes.c_int, [ctypes.c_long, ctypes.c_double, D, D]),
+            "orc_philox4x32_10": (None, [ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint),
+                                         ctypes.POINTER(ctypes.c_uint)]),
+            "orc_gen_normals": (None, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_ulonglong, ctypes.c_int, D]),
+            "orc_gen_gauge": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_ulonglong, D]),
+            "orc_gen_spinor": (None, [dims, ctypes.c_double, ctypes.c_ulonglong, D]),
+            "orc_gen_momenta": (None, [dims, ctypes.c_ulonglong, D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -338,3 +344,42 @@ def cold_gauge(dims):
     U = np.zeros((4 * V, 3, 3), np.complex128)
     U[:, 0, 0] = U[:, 1, 1] = U[:, 2, 2] = 1
     return np.ascontiguousarray(U.view(np.float64).reshape(72 * V))
+
+
+# ---------------------------------------------------------------------------
+# the library's seeded generators restated on the CPU (Philox-4x32-10 keyed by
+# the seed, Box-Muller normals): the same fields sfh_random_gauge,
+# sfh_gaussian_spinor / sfh_batch_random_rhs and sfh_random_momenta produce
+# ---------------------------------------------------------------------------
+def philox4x32_10(ctr, key):
+    c = (ctypes.c_uint * 4)(*[int(x) & 0xFFFFFFFF for x in ctr])
+    k = (ctypes.c_uint * 2)(*[int(x) & 0xFFFFFFFF for x in key])
+    o = (ctypes.c_uint * 4)()
+    lib().orc_philox4x32_10(c, k, o)
+    return [int(x) for x in o]
+
+
+def philox_normals(seed, stream, obj_id, n):
+    z = np.zeros(n)
+    lib().orc_gen_normals(int(seed), int(stream), int(obj_id), int(n), _d(z))
+    return z
+
+
+def philox_gauge(dims, eps, seed):
+    U = np.zeros(72 * volume(dims))
+    st = lib().orc_gen_gauge(_dims(dims), float(eps), int(seed), _d(U))
+    if st != ORC_OK:
+        raise OracleError(st, "philox_gauge")
+    return U
+
+
+def philox_spinor(dims, seed, sigma=1.0):
+    out = np.zeros(6 * volume(dims))
+    lib().orc_gen_spinor(_dims(dims), float(sigma), int(seed), _d(out))
+    return out
+
+
+def philox_momenta(dims, seed):
+    P = np.zeros(72 * volume(dims))
+    lib().orc_gen_momenta(_dims(dims), int(seed), _d(P))
+    return P

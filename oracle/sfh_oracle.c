@@ -1374,3 +1374,110 @@ int orc_hex(const int dims[4], const double alphas[3], double* U)
     tab_free(&t);
     return bad ? ORC_ERR_DOMAIN : ORC_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* seeded generators (the library's, restated on the CPU)                   */
+/* ------------------------------------------------------------------------ */
+/*
+ * The reference draws its fields from an unseeded std::mt19937
+ * (rng.cpp:7-15): the Gaussian Hermitian generator of
+ * random_traceless_hermitian_SU3 (Lattice.cpp:1001-1033), complex Gaussian
+ * spinors (generateGaussianComplex, Fermions.cpp:207-212) and momenta
+ * P = sum_a 1/2 p_a lambda_a (generate_conjugate_field_configuration,
+ * Fermions.cpp:342-360).  The library keeps those distributions but draws
+ * from Philox-4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11; checked here
+ * against the published known-answer vectors) keyed by the seed, with one
+ * counter per object: (id_lo, id_hi, k, stream), id = site (spinors) or
+ * 4 site + mu (links), k = pair index, stream 1 gauge, 2 spinor, 3 momenta.
+ * Each block gives two N(0,1) by Box-Muller from two 53-bit uniforms in
+ * (0, 1).  These functions give the same fields on the CPU, so both sides
+ * of a comparison start from identical inputs (to the last few ulps: the
+ * log and sin/cos of the C library and of CUDA may differ in the last bit).
+ */
+void orc_philox4x32_10(const unsigned ctr[4], const unsigned key[2], unsigned out[4])
+{
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox_4x32_10(c, key[0], key[1]);
+    for (int i = 0; i < 4; ++i) out[i] = c[i];
+}
+
+static void gen_normals(unsigned long long seed, uint32_t stream, unsigned long long id, int n, double* z)
+{
+    const double inv53 = 1.0 / 9007199254740992.0;
+    for (int k = 0; k < (n + 1) / 2; ++k) {
+        uint32_t c[4] = {(uint32_t)id, (uint32_t)(id >> 32), (uint32_t)k, stream};
+        philox_4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        uint64_t a = (((uint64_t)c[0] << 21) ^ (uint64_t)(c[1] >> 11)) & ((1ull << 53) - 1);
+        uint64_t b = (((uint64_t)c[2] << 21) ^ (uint64_t)(c[3] >> 11)) & ((1ull << 53) - 1);
+        double u1 = ((double)a + 0.5) * inv53, u2 = ((double)b + 0.5) * inv53;
+        double rad = sqrt(-2.0 * log(u1));
+        double ang = 2.0 * 3.14159265358979323846 * u2;
+        z[2 * k] = rad * cos(ang);
+        if (2 * k + 1 < n) z[2 * k + 1] = rad * sin(ang);
+    }
+}
+
+void orc_gen_normals(unsigned long long seed, unsigned stream, unsigned long long id, int n, double* z)
+{
+    gen_normals(seed, stream, id, n, z);
+}
+
+int orc_gen_gauge(const int dims[4], double eps, unsigned long long seed, double* U)
+{
+    const long n = 4L * dims[0] * dims[1] * dims[2] * dims[3];
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long l = 0; l < n; ++l) {  /* l = 4 s + mu */
+        double z[9];
+        gen_normals(seed, 1u, (unsigned long long)l, 9, z);
+        const double tr3 = (z[0] + z[1] + z[2]) / 3.0;
+        cx H[9];
+        H[0] = z[0] - tr3;
+        H[4] = z[1] - tr3;
+        H[8] = z[2] - tr3;
+        H[1] = z[3] + I * z[4];
+        H[3] = z[3] - I * z[4];
+        H[2] = z[5] + I * z[6];
+        H[6] = z[5] - I * z[6];
+        H[5] = z[7] + I * z[8];
+        H[7] = z[7] - I * z[8];
+        for (int k = 0; k < 9; ++k) H[k] *= eps;
+        if (expiq_cx(H, (cx*)(U + l * 18)) != ORC_OK) bad = 1;
+    }
+    return bad ? ORC_ERR_DOMAIN : ORC_OK;
+}
+
+void orc_gen_spinor(const int dims[4], double sigma, unsigned long long seed, double* out)
+{
+    const long V = (long)dims[0] * dims[1] * dims[2] * dims[3];
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s) {
+        double z[6];
+        gen_normals(seed, 2u, (unsigned long long)s, 6, z);
+        for (int k = 0; k < 6; ++k) out[s * 6 + k] = sigma * z[k];
+    }
+}
+
+void orc_gen_momenta(const int dims[4], unsigned long long seed, double* P)
+{
+    const long n = 4L * dims[0] * dims[1] * dims[2] * dims[3];
+    const double a8 = 1.0 / sqrt(3.0);
+#pragma omp parallel for schedule(static)
+    for (long l = 0; l < n; ++l) {
+        double z[8];
+        gen_normals(seed, 3u, (unsigned long long)l, 8, z);
+        /* 1/2 sum_a p_a lambda_a, Gell-Mann basis of Fermions.cpp:321-340 */
+        cx M[9];
+        M[0] = z[2] + a8 * z[7];
+        M[4] = -z[2] + a8 * z[7];
+        M[8] = -2.0 * a8 * z[7];
+        M[1] = z[0] - I * z[1];
+        M[3] = z[0] + I * z[1];
+        M[2] = z[3] - I * z[4];
+        M[6] = z[3] + I * z[4];
+        M[5] = z[5] - I * z[6];
+        M[7] = z[5] + I * z[6];
+        cx* o = (cx*)(P + l * 18);
+        for (int k = 0; k < 9; ++k) o[k] = 0.5 * M[k];
+    }
+}

@@ -130,6 +130,17 @@ int orc_stout_force(const int dims[4], double rho, int n_levels, const double* U
 /* U[i] = exp(i eps H[i]) for n matrices (used to build seeded gauge fields). */
 int orc_exp_field(long n, double eps, const double* H, double* U);
 
+/* Seeded generators: the library's Philox-4x32-10 + Box-Muller fields on the
+ * CPU, keyed like the device generators (counter (id, id >> 32, pair, stream),
+ * key = seed).  Gauge: U = exp(i eps H) per link, H traceless Hermitian with
+ * N(0,1) entries (Lattice.cpp:1001-1033); spinor: N(0, sigma^2) per real;
+ * momenta: 1/2 sum_a p_a lambda_a (Fermions.cpp:342-360).  AoS layouts. */
+void orc_philox4x32_10(const unsigned ctr[4], const unsigned key[2], unsigned out[4]);
+void orc_gen_normals(unsigned long long seed, unsigned stream, unsigned long long id, int n, double* z);
+int orc_gen_gauge(const int dims[4], double eps, unsigned long long seed, double* U);
+void orc_gen_spinor(const int dims[4], double sigma, unsigned long long seed, double* out);
+void orc_gen_momenta(const int dims[4], unsigned long long seed, double* P);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,3 +70,58 @@ def test_batch_spec_is_the_seeded_workload():
     assert all(s["dims"] in bench.LATTICES and s["mass"] in bench.MASSES and s["eps"] in bench.EPSES
                and 1 <= s["nrhs"] <= 8 for s in a)
     assert sum(s["nrhs"] for s in a) == 296
+
+
+def test_batch_classes_cover_the_batch():
+    """The reference sample's strata: (lattice, mass, eps) classes, with every
+    solve of the batch in exactly one class."""
+    import bench
+    spec = bench.batch_spec()
+    classes = bench.batch_classes(spec)
+    assert len(classes) <= 24 and len({c[0] for c in classes}) == len(classes)
+    assert sum(c[2] for c in classes) == 296
+    for key, k, n in classes:
+        assert (tuple(spec[k]["dims"]), spec[k]["mass"], spec[k]["eps"]) == key
+        assert n == sum(s["nrhs"] for s in spec if (tuple(s["dims"]), s["mass"], s["eps"]) == key)
+
+
+def test_cpu_estimate_weights_classes_by_their_solves(tmp_path):
+    """solves/s = sum of the sampled classes' solves / sum n_c * mean t_c."""
+    import bench
+    spec = [{"dims": (4, 4, 4, 4), "mass": 0.1, "eps": 0.3, "nrhs": 3, "gauge_seed": 1, "rhs_seed": 2},
+            {"dims": (4, 4, 4, 8), "mass": 0.2, "eps": 1.0, "nrhs": 1, "gauge_seed": 3, "rhs_seed": 4},
+            {"dims": (4, 4, 4, 4), "mass": 0.1, "eps": 0.3, "nrhs": 2, "gauge_seed": 5, "rhs_seed": 6}]
+    s = bench.CpuSampler(spec, str(tmp_path))
+    assert [c[2] for c in s.classes] == [5, 1]
+    est = s.estimate([(0, 1.0, "reference"), (0, 3.0, "reference"), (1, 10.0, "port")])
+    assert est["value"] == pytest.approx(6 / (5 * 2.0 + 1 * 10.0))
+    assert est["kind"] == "mixed" and est["reference_solves"] == 2 and est["port_solves"] == 1
+    assert est["batch_cpu_seconds_estimate"] == pytest.approx(20.0)
+    partial = s.estimate([(1, 10.0, "port")])
+    assert partial["classes_timed"] == 1 and partial["value"] == pytest.approx(0.1)
+
+
+def test_reference_arm_is_cpu_only_and_reports_the_same_workload(monkeypatch, capsys):
+    """The reference arm builds its inputs with the oracle's generators and
+    times CPU solves only: the library is never imported, the config equals
+    the GPU arm's, and ms_per_step is the measured step time."""
+    import json
+    import sys
+
+    import bench
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    spec = [{"dims": (8, 8, 8, 8), "mass": m, "eps": 0.3, "nrhs": 2, "gauge_seed": 10 + i,
+             "rhs_seed": 100 + i} for i, m in enumerate((0.2, 0.1))]
+
+    class Args:
+        warmup, steps, gpus, ref_budget = 1, 2, 1, 0.01
+    loaded_before = "staggered_fermions_hmc_b200" in sys.modules
+    bench.run_reference_arm(Args(), spec)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    if not loaded_before:
+        assert "staggered_fermions_hmc_b200" not in sys.modules
+    assert line["impl"] == "reference" and line["config"] == bench.workload_config(spec, 1)
+    assert line["cpu_baseline"]["kind"] in ("reference", "port", "mixed")
+    assert line["reference_sample"]["solves_timed"] >= 2
+    assert line["value"] > 0 and 0 < line["ms_per_step"] < 60000

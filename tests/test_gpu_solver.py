@@ -241,20 +241,29 @@ def test_batch_timed_solve_matches_graph_solve(sfh, orc):
 
 
 @pytest.mark.parametrize("precision,bound", [("f16", 1.25), ("f32", 1.25), ("bf16", 1.35)])
-def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, precision, bound):
+def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, orc, precision, bound):
     """eps = 1 links at m = 0.02 on 16^4: the mixed-precision CG needs at most
     `bound` times FP64's iterations (the reliable update rebuilds the search
     direction on the true residual; without it FP16 took 4.9 times FP64's
-    count here), and reaches the FP64 true residual."""
+    count here), and reaches the FP64 true residual, recomputed by the
+    oracle's D D^dag (apply_DDdagger, Fermions.cpp:530-547) on the host; the
+    FP64 solve is the oracle's CG (Fermions.cpp:553-617) to 1e-10."""
     tol = 1e-10
-    lat = sfh.Lattice((16, 16, 16, 16), 0.02, 4.2)
+    dims, mass = (16, 16, 16, 16), 0.02
+    lat = sfh.Lattice(dims, mass, 4.2)
     try:
         lat.random_gauge(1.0, 21)
+        U = lat.download_gauge()
         phi = lat.gaussian_spinor(22)
         X64, i64 = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision="f64", info=True)
         X, inf = lat.solve_CG_DDdagger(phi, tol=tol, max_iter=40000, precision=precision, info=True)
         assert inf["status"] == 0
         assert inf["iters"] <= bound * i64["iters"], (inf, i64)
-        assert rel(X, X64) < 1e-6
+        assert true_resid(orc, dims, mass, U, phi, X) < 1.05 * tol
+        Xo, it_o, _, st = orc.cg(dims, mass, U, phi, tol, 40000)
+        assert st == 0 and abs(i64["iters"] - it_o) <= 1
+        assert np.linalg.norm(X64 - Xo) / np.linalg.norm(Xo) < 1e-10
+        # |x - x*| / |x*| <= cond(M) resid, cond(M) <= (m^2 + 16) / m^2 = 40001
+        assert np.linalg.norm(X - Xo) / np.linalg.norm(Xo) < 40001 * 2 * tol
     finally:
         lat.close()
