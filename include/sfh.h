@@ -249,6 +249,17 @@ int sfh_load_gauge(sfh_ctx* ctx, const char* path);
 /* nlevels stout levels U <- exp(rho proj(C U^dag)) U with plaquette staples
  * (the single-level analogue of the HEX steps of Smearing.cpp:132-155). */
 int sfh_smear_stout(sfh_ctx* ctx, double rho, int nlevels);
+/* The staple steps of HEX on their own, on host fields in the reference's
+ * flat tensor layouts (combo * V + s, 18 doubles per matrix):
+ *   level 1: apply_step_1 (Smearing.cpp:76-123): in = gauge links (link-field
+ *            layout), out = Gamma1 [64][V], combo (4 mu + nu) 4 + rho;
+ *   level 2: apply_step_3 (Smearing.cpp:157-211): in = V1 [64][V], out =
+ *            Gamma2 [16][V], combo 4 mu + nu;
+ *   level 3: apply_step_5 (Smearing.cpp:236-275): in = V2 [16][V], out =
+ *            Gamma3 [4][V] (summed from zero).
+ * The fused smearing below keeps only the decorated links the next level
+ * uses; this is its checking path against the reference's own steps. */
+int sfh_hex_staples(sfh_ctx* ctx, int level, const double* in, double* out);
 /* npasses HEX passes: Apply_HEX_smearing (Smearing.cpp:304-311); npasses = 4
  * is Apply_4HEX_smearing (Smearing.cpp:313-318).  Alphas as Smearing.h:7-9. */
 int sfh_smear_hex(sfh_ctx* ctx, double alpha1, double alpha2, double alpha3, int npasses);

@@ -77,6 +77,9 @@ def lib():
             "orc_heatbath": (ctypes.c_int, [dims, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int, D]),
             "orc_exp_field": (ctypes.c_int, [ctypes.c_long, ctypes.c_double, D, D]),
+            "orc_hex_gamma1": (None, [dims, D, D]),
+            "orc_hex_gamma2": (None, [dims, D, D]),
+            "orc_hex_gamma3": (None, [dims, D, D]),
             "orc_philox4x32_10": (None, [ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_uint),
                                          ctypes.POINTER(ctypes.c_uint)]),
             "orc_gen_normals": (None, [ctypes.c_ulonglong, ctypes.c_uint, ctypes.c_ulonglong, ctypes.c_int, D]),
@@ -383,3 +386,13 @@ def philox_momenta(dims, seed):
     P = np.zeros(72 * volume(dims))
     lib().orc_gen_momenta(_dims(dims), int(seed), _d(P))
     return P
+
+
+# HEX staple steps in the reference's flat tensor layouts (combo * V + site)
+def hex_gamma(level, dims, field):
+    V = volume(dims)
+    n = {1: 64, 2: 16, 3: 4}[level]
+    out = np.zeros(n * V * 18)
+    fn = {1: lib().orc_hex_gamma1, 2: lib().orc_hex_gamma2, 3: lib().orc_hex_gamma3}[level]
+    fn(_dims(dims), _d(np.ascontiguousarray(field, dtype=np.float64)), _d(out))
+    return out

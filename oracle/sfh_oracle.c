@@ -1269,7 +1269,118 @@ int orc_heatbath(const int dims[4], double beta, double c11, double c12, unsigne
 /* HEX, Smearing.cpp:76-311.  Decorated fields are stored as
  * [combo][site][9] with combo = (4 mu + nu) 4 + rho (level 1),
  * 4 mu + nu (level 2), mu (level 3), as in the reference's flat indices
- * (Smearing.cpp:14-73). */
+ * (Smearing.cpp:14-73).  The staple steps are exposed on their own
+ * (orc_hex_gamma1/2/3) so that they can be checked against the reference's
+ * apply_step_1/3/5, which run unmodified; the exp steps cannot (see
+ * orc_hex). */
+#define LNK(s, mu) (Uc + ((long)(s) * 4 + (mu)) * 9)
+#define F3(arr, a, b, c, s) ((arr) + ((((long)(a) * 4 + (b)) * 4 + (c)) * V + (s)) * 9)
+#define F2(arr, a, b, s) ((arr) + (((long)(a) * 4 + (b)) * V + (s)) * 9)
+
+/* step 1 (Smearing.cpp:76-123): G1[mu,nu,rho](x) = sum over sigma not in
+ * {mu, nu, rho} of the up and down staples of U from x to x+mu */
+static void hex_gamma1(const tab_t* t, const cx* Uc, cx* G1)
+{
+    const long V = t->V;
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = 0; nu < 4; ++nu)
+                for (int rh = 0; rh < 4; ++rh) {
+                    cx* g = F3(G1, mu, nu, rh, s);
+                    for (int i = 0; i < 9; ++i) g[i] = 0;
+                    for (int sg = 0; sg < 4; ++sg) {
+                        if (sg == mu || sg == nu || sg == rh) continue;
+                        long xs = t->up[s * 4 + sg], xm = t->up[s * 4 + mu];
+                        long xd = t->dn[s * 4 + sg], xdm = t->up[xd * 4 + mu];
+                        cx a[9], b[9];
+                        m_mul(LNK(s, sg), LNK(xs, mu), a);
+                        m_mul_adj(a, LNK(xm, sg), a);
+                        m_adj(LNK(xd, sg), b);
+                        m_mul(b, LNK(xd, mu), b);
+                        m_mul(b, LNK(xdm, sg), b);
+                        for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+                    }
+                }
+}
+
+/* step 3 (Smearing.cpp:157-209): G2[mu,nu](x) = sum over sigma not in
+ * {mu, nu} of staples with side links V1[sigma,mu,nu] and middle link
+ * V1[mu,nu,sigma] */
+static void hex_gamma2(const tab_t* t, const cx* V1, cx* G2)
+{
+    const long V = t->V;
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu)
+            for (int nu = 0; nu < 4; ++nu) {
+                cx* g = F2(G2, mu, nu, s);
+                for (int i = 0; i < 9; ++i) g[i] = 0;
+                for (int sg = 0; sg < 4; ++sg) {
+                    if (sg == mu || sg == nu) continue;
+                    long xs = t->up[s * 4 + sg], xm = t->up[s * 4 + mu];
+                    long xd = t->dn[s * 4 + sg], xdm = t->up[xd * 4 + mu];
+                    cx a[9], b[9];
+                    m_mul(F3(V1, sg, mu, nu, s), F3(V1, mu, nu, sg, xs), a);
+                    m_mul_adj(a, F3(V1, sg, mu, nu, xm), a);
+                    m_adj(F3(V1, sg, mu, nu, xd), b);
+                    m_mul(b, F3(V1, mu, nu, sg, xd), b);
+                    m_mul(b, F3(V1, sg, mu, nu, xdm), b);
+                    for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+                }
+            }
+}
+
+/* step 5 (Smearing.cpp:236-275), Gamma_3 starting at zero: G3[mu](x) =
+ * sum over nu != mu of staples with side links V2[nu,mu] and middle link
+ * V2[mu,nu]; G3 as [mu][site][9] */
+static void hex_gamma3(const tab_t* t, const cx* V2, cx* G3)
+{
+    const long V = t->V;
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu) {
+            cx* g = G3 + ((long)mu * V + s) * 9;
+            for (int i = 0; i < 9; ++i) g[i] = 0;
+            for (int nu = 0; nu < 4; ++nu) {
+                if (nu == mu) continue;
+                long xn = t->up[s * 4 + nu], xm = t->up[s * 4 + mu];
+                long xd = t->dn[s * 4 + nu], xdm = t->up[xd * 4 + mu];
+                cx a[9], b[9];
+                m_mul(F2(V2, nu, mu, s), F2(V2, mu, nu, xn), a);
+                m_mul_adj(a, F2(V2, nu, mu, xm), a);
+                m_adj(F2(V2, nu, mu, xd), b);
+                m_mul(b, F2(V2, mu, nu, xd), b);
+                m_mul(b, F2(V2, nu, mu, xdm), b);
+                for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
+            }
+        }
+}
+
+void orc_hex_gamma1(const int dims[4], const double* U, double* G1)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    hex_gamma1(&t, (const cx*)U, (cx*)G1);
+    tab_free(&t);
+}
+
+void orc_hex_gamma2(const int dims[4], const double* V1, double* G2)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    hex_gamma2(&t, (const cx*)V1, (cx*)G2);
+    tab_free(&t);
+}
+
+void orc_hex_gamma3(const int dims[4], const double* V2, double* G3)
+{
+    tab_t t;
+    tab_build(&t, dims);
+    hex_gamma3(&t, (const cx*)V2, (cx*)G3);
+    tab_free(&t);
+}
+
 int orc_hex(const int dims[4], const double alphas[3], double* U)
 {
     tab_t t;
@@ -1280,32 +1391,10 @@ int orc_hex(const int dims[4], const double alphas[3], double* U)
     cx* V1 = (cx*)malloc(sizeof(cx) * 9 * 64 * V);
     cx* G2 = (cx*)malloc(sizeof(cx) * 9 * 16 * V);
     cx* V2 = (cx*)malloc(sizeof(cx) * 9 * 16 * V);
+    cx* G3 = (cx*)malloc(sizeof(cx) * 9 * 4 * V);
     cx* Unew = (cx*)malloc(sizeof(cx) * 9 * 4 * V);
     int bad = 0;
-#define LNK(s, mu) (Uc + ((long)(s) * 4 + (mu)) * 9)
-#define F3(arr, a, b, c, s) ((arr) + ((((long)(a) * 4 + (b)) * 4 + (c)) * V + (s)) * 9)
-#define F2(arr, a, b, s) ((arr) + (((long)(a) * 4 + (b)) * V + (s)) * 9)
-    /* step 1 (Smearing.cpp:76-123) */
-#pragma omp parallel for schedule(static)
-    for (long s = 0; s < V; ++s)
-        for (int mu = 0; mu < 4; ++mu)
-            for (int nu = 0; nu < 4; ++nu)
-                for (int rh = 0; rh < 4; ++rh) {
-                    cx* g = F3(G1, mu, nu, rh, s);
-                    for (int i = 0; i < 9; ++i) g[i] = 0;
-                    for (int sg = 0; sg < 4; ++sg) {
-                        if (sg == mu || sg == nu || sg == rh) continue;
-                        long xs = t.up[s * 4 + sg], xm = t.up[s * 4 + mu];
-                        long xd = t.dn[s * 4 + sg], xdm = t.up[xd * 4 + mu];
-                        cx a[9], b[9];
-                        m_mul(LNK(s, sg), LNK(xs, mu), a);
-                        m_mul_adj(a, LNK(xm, sg), a);
-                        m_adj(LNK(xd, sg), b);
-                        m_mul(b, LNK(xd, mu), b);
-                        m_mul(b, LNK(xdm, sg), b);
-                        for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
-                    }
-                }
+    hex_gamma1(&t, Uc, G1);
     /* step 2 (Smearing.cpp:132-155) */
 #pragma omp parallel for schedule(static) reduction(| : bad)
     for (long s = 0; s < V; ++s)
@@ -1315,26 +1404,7 @@ int orc_hex(const int dims[4], const double alphas[3], double* U)
                            alphas[2] * 0.5, V1 + ((long)c * V + s) * 9) != ORC_OK)
                 bad = 1;
         }
-    /* step 3 (Smearing.cpp:157-209) */
-#pragma omp parallel for schedule(static)
-    for (long s = 0; s < V; ++s)
-        for (int mu = 0; mu < 4; ++mu)
-            for (int nu = 0; nu < 4; ++nu) {
-                cx* g = F2(G2, mu, nu, s);
-                for (int i = 0; i < 9; ++i) g[i] = 0;
-                for (int sg = 0; sg < 4; ++sg) {
-                    if (sg == mu || sg == nu) continue;
-                    long xs = t.up[s * 4 + sg], xm = t.up[s * 4 + mu];
-                    long xd = t.dn[s * 4 + sg], xdm = t.up[xd * 4 + mu];
-                    cx a[9], b[9];
-                    m_mul(F3(V1, sg, mu, nu, s), F3(V1, mu, nu, sg, xs), a);
-                    m_mul_adj(a, F3(V1, sg, mu, nu, xm), a);
-                    m_adj(F3(V1, sg, mu, nu, xd), b);
-                    m_mul(b, F3(V1, mu, nu, sg, xd), b);
-                    m_mul(b, F3(V1, sg, mu, nu, xdm), b);
-                    for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
-                }
-            }
+    hex_gamma2(&t, V1, G2);
     /* step 4 (Smearing.cpp:213-234) */
 #pragma omp parallel for schedule(static) reduction(| : bad)
     for (long s = 0; s < V; ++s)
@@ -1344,36 +1414,22 @@ int orc_hex(const int dims[4], const double alphas[3], double* U)
                            alphas[1] * 0.5, V2 + ((long)c * V + s) * 9) != ORC_OK)
                 bad = 1;
         }
-    /* steps 5 and 6 (Smearing.cpp:236-301); Gamma_3 starts at zero */
+    hex_gamma3(&t, V2, G3);
+    /* step 6 (Smearing.cpp:278-301) */
 #pragma omp parallel for schedule(static) reduction(| : bad)
     for (long s = 0; s < V; ++s)
-        for (int mu = 0; mu < 4; ++mu) {
-            cx g[9];
-            for (int i = 0; i < 9; ++i) g[i] = 0;
-            for (int nu = 0; nu < 4; ++nu) {
-                if (nu == mu) continue;
-                long xn = t.up[s * 4 + nu], xm = t.up[s * 4 + mu];
-                long xd = t.dn[s * 4 + nu], xdm = t.up[xd * 4 + mu];
-                cx a[9], b[9];
-                m_mul(F2(V2, nu, mu, s), F2(V2, mu, nu, xn), a);
-                m_mul_adj(a, F2(V2, nu, mu, xm), a);
-                m_adj(F2(V2, nu, mu, xd), b);
-                m_mul(b, F2(V2, mu, nu, xd), b);
-                m_mul(b, F2(V2, nu, mu, xdm), b);
-                for (int i = 0; i < 9; ++i) g[i] += a[i] + b[i];
-            }
-            if (smear_link(g, LNK(s, mu), alphas[0] * 0.5,
+        for (int mu = 0; mu < 4; ++mu)
+            if (smear_link(G3 + ((long)mu * V + s) * 9, LNK(s, mu), alphas[0] * 0.5,
                            Unew + ((long)s * 4 + mu) * 9) != ORC_OK)
                 bad = 1;
-        }
-#undef LNK
-#undef F3
-#undef F2
     if (!bad) memcpy(U, Unew, sizeof(cx) * 9 * 4 * V);
-    free(G1); free(V1); free(G2); free(V2); free(Unew);
+    free(G1); free(V1); free(G2); free(V2); free(G3); free(Unew);
     tab_free(&t);
     return bad ? ORC_ERR_DOMAIN : ORC_OK;
 }
+#undef LNK
+#undef F3
+#undef F2
 
 /* ------------------------------------------------------------------------ */
 /* seeded generators (the library's, restated on the CPU)                   */

@@ -116,6 +116,15 @@ int orc_stout(const int dims[4], double rho, int n_levels, double* U);
  * alphas = {alpha1, alpha2, alpha3} as in Smearing.h:7-9. */
 int orc_hex(const int dims[4], const double alphas[3], double* U);
 
+/* The staple steps of HEX on their own, in the reference's flat tensor
+ * layouts (combo * V + site, 18 doubles per matrix): G1 = apply_step_1(U)
+ * [64][V] (Smearing.cpp:76-123), G2 = apply_step_3(V1) [16][V] from V1
+ * [64][V] (Smearing.cpp:157-211), G3 = apply_step_5(V2) [4][V] from V2 [16][V]
+ * (Smearing.cpp:236-275, Gamma_3 starting at zero). */
+void orc_hex_gamma1(const int dims[4], const double* U, double* G1);
+void orc_hex_gamma2(const int dims[4], const double* V1, double* G2);
+void orc_hex_gamma3(const int dims[4], const double* V2, double* G3);
+
 /* nsweeps heatbath sweeps (single_link_heatbath, Lattice.cpp:722-757, in
  * colour order; seeded Philox uniforms), sweep indices sweep0.. */
 int orc_heatbath(const int dims[4], double beta, double c11, double c12, unsigned long long seed, int sweep0,

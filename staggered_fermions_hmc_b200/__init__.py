@@ -139,6 +139,7 @@ SIGNATURES = {
     "sfh_load_gauge": (ctypes.c_int, [_VP, ctypes.c_char_p]),
     "sfh_smear_stout": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_smear_hex": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "sfh_hex_staples": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -472,6 +473,14 @@ class Lattice:
     # --- smearing (Smearing.cpp) ---------------------------------------------
     def smear_stout(self, rho, n_levels=1):
         self._check(self.lib.sfh_smear_stout(self.h, rho, n_levels), "stout smearing")
+
+    def hex_staples(self, level, field):
+        """apply_step_1 / apply_step_3 / apply_step_5 (Smearing.cpp:76-275) for
+        level 1 / 2 / 3 on a host field in the reference's flat tensor layout."""
+        field = _f64(field).reshape(-1)
+        out = np.empty({1: 64, 2: 16, 3: 4}[level] * self.V * 18)
+        self._check(self.lib.sfh_hex_staples(self.h, level, _dptr(field), _dptr(out)), "hex_staples")
+        return out
 
     def Apply_HEX_smearing(self, alphas=(0.95, 0.76, 0.38), passes=1):
         self._check(self.lib.sfh_smear_hex(self.h, alphas[0], alphas[1], alphas[2], passes), "HEX smearing")

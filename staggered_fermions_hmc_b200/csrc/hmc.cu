@@ -614,6 +614,25 @@ extern "C" int sfh_smear_stout(sfh_ctx* c, double rho, int nlevels)
     return take_device_error(c, "stout smearing");
 }
 
+extern "C" int sfh_hex_staples(sfh_ctx* c, int level, const double* in, double* out)
+{
+    if (!c || !in || !out || level < 1 || level > 3) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    const size_t V = (size_t)c->g.V;
+    const size_t nin = (level == 1 ? 4 : (level == 2 ? 64 : 16)) * V * 18 * sizeof(double);
+    const size_t nout = (level == 1 ? 64 : (level == 2 ? 16 : 4)) * V * 18 * sizeof(double);
+    void *din = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&din, nin);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, nout);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(din, in, nin, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_hex_gamma(c->g, level, din, dout, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, nout, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (din) cudaFree(din);
+    if (dout) cudaFree(dout);
+    return cuda_check(c, e, "hex staples");
+}
+
 extern "C" int sfh_smear_hex(sfh_ctx* c, double alpha1, double alpha2, double alpha3, int npasses)
 {
     if (!c || npasses < 0) return SFH_ERR_INVALID;

@@ -110,6 +110,7 @@ cudaError_t launch_heatbath(const Geom& g, void* U, double beta, double c11, dou
                             int sweep0, int nsweeps, cudaStream_t s);
 cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double a2, double a3, int n, int* err,
                        cudaStream_t s);
+cudaError_t launch_hex_gamma(const Geom& g, int level, const void* in, void* out, cudaStream_t s);
 cudaError_t launch_reduce(const Geom& g, int kind, const void* A, const void* B, double beta, double c11,
                           double c12, double* partial, double* out, cudaStream_t s);
 

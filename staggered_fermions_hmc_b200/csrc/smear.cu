@@ -403,6 +403,95 @@ cudaError_t launch_stout(const Geom& g, void* U, void* tmp, double rho, int n, i
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// The staple steps of HEX on their own, in the reference's flat tensor
+// layouts (apply_step_1/3/5, Smearing.cpp:76-275): fields of 3x3 matrices
+// indexed combo * V + s, s the lexicographic site, combo (4 mu + nu) 4 + rho
+// (level 1 output, level 2 input), 4 mu + nu (level 2 output, level 3 input)
+// or mu (level 3 output); level 1 reads the gauge field in its host layout
+// [s][mu].  One thread per output matrix; a checking path for the fused
+// kernels above, which keep only the decorated links the next level uses.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ M3 ld_mat(const double2* f, long k)
+{
+    M3 m;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        const double2 v = f[k * 9 + e];
+        m.e[e] = {v.x, v.y};
+    }
+    return m;
+}
+
+__device__ __forceinline__ int lex_shift(const Geom& g, int s, int d, int dir)
+{
+    int c[4];
+    int r = s;
+    for (int k = 3; k >= 0; --k) {
+        c[k] = r % g.L[k];
+        r /= g.L[k];
+    }
+    c[d] = (c[d] + dir + g.L[d]) % g.L[d];
+    return ((c[0] * g.L[1] + c[1]) * g.L[2] + c[2]) * g.L[3] + c[3];
+}
+
+// index of matrix (combo, s) of the level's input field
+__device__ __forceinline__ long gamma_in(int level, const Geom& g, int a, int b, int c, int s)
+{
+    if (level == 1) return (long)s * 4 + a;                          // U_a(s)
+    if (level == 2) return (long)((a * 4 + b) * 4 + c) * g.V + s;     // V1[a, b, c](s)
+    return (long)(a * 4 + b) * g.V + s;                               // V2[a, b](s)
+}
+
+__global__ void __launch_bounds__(kThreads) hex_gamma_kernel(Geom g, int level, const double2* in, double2* out)
+{
+    const int ncombo = level == 1 ? 64 : (level == 2 ? 16 : 4);
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long)ncombo * g.V) return;
+    const int combo = (int)(idx / g.V), s = (int)(idx % g.V);
+    int mu, nu = 0, rho = 0;
+    if (level == 1) { mu = combo / 16; nu = (combo / 4) & 3; rho = combo & 3; }
+    else if (level == 2) { mu = combo / 4; nu = combo & 3; }
+    else { mu = combo; }
+    M3 G = m3_zero();
+    for (int sg = 0; sg < 4; ++sg) {
+        if (sg == mu || (level < 3 && sg == nu) || (level == 1 && sg == rho)) continue;
+        // side links S (direction sg) and middle link M (direction mu) of
+        // the staple through sg: level 1 U_sg, U_mu; level 2 V1[sg, mu, nu],
+        // V1[mu, nu, sg]; level 3 V2[sg, mu], V2[mu, sg]
+        const int xs = lex_shift(g, s, sg, +1), xm = lex_shift(g, s, mu, +1);
+        const int xd = lex_shift(g, s, sg, -1), xdm = lex_shift(g, xd, mu, +1);
+        long sx, sxm, sxd, sxdm, mxs, mxd;
+        if (level == 1) {
+            sx = gamma_in(1, g, sg, 0, 0, s); sxm = gamma_in(1, g, sg, 0, 0, xm);
+            sxd = gamma_in(1, g, sg, 0, 0, xd); sxdm = gamma_in(1, g, sg, 0, 0, xdm);
+            mxs = gamma_in(1, g, mu, 0, 0, xs); mxd = gamma_in(1, g, mu, 0, 0, xd);
+        } else if (level == 2) {
+            sx = gamma_in(2, g, sg, mu, nu, s); sxm = gamma_in(2, g, sg, mu, nu, xm);
+            sxd = gamma_in(2, g, sg, mu, nu, xd); sxdm = gamma_in(2, g, sg, mu, nu, xdm);
+            mxs = gamma_in(2, g, mu, nu, sg, xs); mxd = gamma_in(2, g, mu, nu, sg, xd);
+        } else {
+            sx = gamma_in(3, g, sg, mu, 0, s); sxm = gamma_in(3, g, sg, mu, 0, xm);
+            sxd = gamma_in(3, g, sg, mu, 0, xd); sxdm = gamma_in(3, g, sg, mu, 0, xdm);
+            mxs = gamma_in(3, g, mu, sg, 0, xs); mxd = gamma_in(3, g, mu, sg, 0, xd);
+        }
+        M3 up = m3_mul_adj(m3_mul(ld_mat(in, sx), ld_mat(in, mxs)), ld_mat(in, sxm));
+        M3 dn = m3_mul(m3_adj_mul(ld_mat(in, sxd), ld_mat(in, mxd)), ld_mat(in, sxdm));
+        m3_acc(G, up);
+        m3_acc(G, dn);
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) out[idx * 9 + e] = make_double2(G.e[e].re, G.e[e].im);
+}
+
+cudaError_t launch_hex_gamma(const Geom& g, int level, const void* in, void* out, cudaStream_t s)
+{
+    const long n = (long)(level == 1 ? 64 : (level == 2 ? 16 : 4)) * g.V;
+    hex_gamma_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(g, level, (const double2*)in,
+                                                                                    (double2*)out);
+    return cudaGetLastError();
+}
+
 // n HEX passes; scratch holds six link fields (V1: 3, V2: 3)
 cudaError_t launch_hex(const Geom& g, void* U, void* scratch, double a1, double a2, double a3, int n, int* err,
                        cudaStream_t s)

@@ -6,7 +6,7 @@ from the reference sources) on seeded inputs and stores inputs and outputs as
 compressed .npz files.  Needs the reference sources, so it runs only where
 they are present; the committed fixtures are what the tests read.
 
-usage: python tests/golden/make_golden.py --reference DIR
+usage: python tests/golden/make_golden.py --reference DIR [--hex-only]
        (DIR: a checkout of the reference; or set SFH_REFERENCE_DIR)
 """
 import os
@@ -97,14 +97,71 @@ def make_heatbath():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# HEX staple steps: the reference's apply_step_1 / 3 / 5 (Smearing.cpp:76-275)
+# on 4^4 with seeded SU(3) inputs (gauge links; decorated V1 [64][V] and
+# V2 [16][V] fields drawn as plain SU(3) matrices by the oracle's Philox
+# generator: the steps are defined for any inputs).  Stored: the seeds, the
+# outputs at a fixed subset of sites and, over every matrix, a checksum with
+# seeded N(0,1) weights, sum_k w_k G_k.
+HEX = {"dims": (4, 4, 4, 4), "eps": 0.5, "seeds": (31, 32, 33), "weight_seed": 34,
+       "sites": {1: 8, 2: 16, 3: 64}}
+
+
+def hex_inputs(dims, eps, seeds):
+    L, T = dims[0], dims[3]
+    U = oracle.philox_gauge(dims, eps, seeds[0])
+    V1 = oracle.philox_gauge((L, L, L, 16 * T), eps, seeds[1])  # 64 V matrices
+    V2 = oracle.philox_gauge((L, L, L, 4 * T), eps, seeds[2])   # 16 V matrices
+    return U, V1, V2
+
+
+def hex_checksum(G, weight_seed, level):
+    w = np.random.default_rng(weight_seed + level).standard_normal(G.size // 18)
+    return np.einsum("k,kx->x", w, G.reshape(-1, 18))
+
+
+def hex_site_subset(V, n):
+    return np.linspace(0, V - 1, n).astype(np.int64)
+
+
+def make_hex():
+    dims, eps, seeds = HEX["dims"], HEX["eps"], HEX["seeds"]
+    exe = build_ref.build_hex()
+    U, V1, V2 = hex_inputs(dims, eps, seeds)
+    V = oracle.volume(dims)
+    res = {}
+    with tempfile.TemporaryDirectory() as td:
+        ind, outd = os.path.join(td, "in"), os.path.join(td, "out")
+        os.makedirs(ind)
+        os.makedirs(outd)
+        for name, arr in (("U", U), ("V1", V1), ("V2", V2)):
+            arr.astype("<f8").tofile(os.path.join(ind, name + ".bin"))
+        subprocess.run([exe, ind, outd], check=True)
+        for level in (1, 2, 3):
+            G = np.fromfile(os.path.join(outd, f"G{level}.bin"), dtype="<f8")
+            n = G.size // (18 * V)
+            sites = hex_site_subset(V, HEX["sites"][level])
+            res[f"G{level}_sites"] = sites
+            res[f"G{level}_at_sites"] = G.reshape(n, V, 18)[:, sites, :]
+            res[f"G{level}_checksum"] = hex_checksum(G, HEX["weight_seed"], level)
+    meta = np.array(list(dims) + [eps] + list(seeds) + [HEX["weight_seed"]], dtype=np.float64)
+    path = os.path.join(HERE, "hex_ref_L4T4.npz")
+    np.savez_compressed(path, meta=meta, **res)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def main(argv):
     if "--reference" in argv:
         build_ref.set_reference(argv[argv.index("--reference") + 1])
     if not build_ref.REF or not os.path.isdir(build_ref.REF):
         sys.exit("give --reference DIR (a checkout of the reference) or set SFH_REFERENCE_DIR")
+    if "--hex-only" in argv:
+        make_hex()
+        return
     for fx in FIXTURES:
         make(*fx)
     make_heatbath()
+    make_hex()
 
 
 if __name__ == "__main__":

@@ -7,8 +7,10 @@ Tolerances: per-link quantities (staples, forces, exp) 1e-12 relative
 relative against the reference's own trajectory (it contains 11 CG solves at
 the reference's 1e-12 tolerance); reversibility 1e-10 absolute on the links
 (Fermions.cpp:947); dH(eps)/dH(eps/2) in [3.5, 4.5] (Fermions.cpp:1098).
-Smearing compares with the oracle restatement (parity with the reference
-itself is not possible: its HEX code cannot run, see the oracle's header).
+Smearing compares with the oracle restatement: the reference's HEX cannot run
+as shipped (its exp steps reject their input), but its exp-free staple steps
+apply_step_1/3/5 do, and the device's staple steps are checked against their
+outputs (tests/golden/hex_ref_L4T4.npz) to 1e-12.
 """
 import glob
 import os
@@ -271,6 +273,20 @@ def test_hex_vs_oracle(sfh, orc, dims):
     for _ in range(4):
         ref = orc.hex_smear(dims, ref)
     assert rel(lat.download_gauge(), ref) < 1e-11
+
+
+@pytest.mark.parametrize("level", [1, 2, 3])
+def test_hex_staple_steps_vs_reference(sfh, orc, level):
+    """apply_step_1 / 3 / 5 (Smearing.cpp:76-275) on the device against the
+    reference's own outputs on the same seeded inputs."""
+    from test_oracle_golden import check_hex_level, hex_fixture
+    g, dims, (U, V1, V2), wseed, checksum = hex_fixture()
+    lat = sfh.Lattice(dims, 0.1)
+    try:
+        G = lat.hex_staples(level, {1: U, 2: V1, 3: V2}[level])
+    finally:
+        lat.close()
+    check_hex_level(g, level, G, orc.volume(dims), wseed, checksum)
 
 
 def test_smeared_links_stay_special_unitary(sfh, orc):

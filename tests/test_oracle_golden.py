@@ -259,3 +259,40 @@ def test_heatbath_oracle_vs_reference_statistics(orc):
         assert abs(mean - ref_mean) < tol, (beta, mean, ref_mean, tol)
     V = U.view(np.complex128).reshape(-1, 3, 3)
     assert np.abs(np.einsum("lij,lkj->lik", V, V.conj()) - np.eye(3)).max() < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# HEX staple steps against the reference's own apply_step_1 / 3 / 5
+# (Smearing.cpp:76-275, run unmodified by oracle/hex_harness.cpp; fixture
+# tests/golden/hex_ref_L4T4.npz).  Their exp steps cannot run as shipped, so
+# the staple steps carry the index conventions of the smearing restatement:
+# which links form the decorated staples, and in which tensor slots.
+# ---------------------------------------------------------------------------
+HEX_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "hex_ref_L4T4.npz")
+
+
+def hex_fixture():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    g = np.load(HEX_GOLDEN)
+    m = g["meta"]
+    dims = tuple(int(x) for x in m[:4])
+    eps, seeds, wseed = float(m[4]), tuple(int(x) for x in m[5:8]), int(m[8])
+    return g, dims, make_golden.hex_inputs(dims, eps, seeds), wseed, make_golden.hex_checksum
+
+
+def check_hex_level(g, level, G, V, wseed, checksum):
+    n = G.size // (18 * V)
+    sites = g[f"G{level}_sites"]
+    ref = g[f"G{level}_at_sites"]
+    assert rel(G.reshape(n, V, 18)[:, sites, :], ref) < 1e-12
+    cs = checksum(G, wseed, level)
+    assert np.abs(cs - g[f"G{level}_checksum"]).max() < 1e-12 * np.abs(g[f"G{level}_checksum"]).max()
+
+
+@pytest.mark.parametrize("level", [1, 2, 3])
+def test_hex_staple_steps_vs_reference(orc, level):
+    g, dims, (U, V1, V2), wseed, checksum = hex_fixture()
+    G = orc.hex_gamma(level, dims, {1: U, 2: V1, 3: V2}[level])
+    check_hex_level(g, level, G, orc.volume(dims), wseed, checksum)
