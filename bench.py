@@ -139,13 +139,15 @@ LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72, "bf16": 24}
 KERNELS = ("cg_hop1", "cg_hop2", "cg_update")
 
 
-def kernel_bytes(spec, infos, precision):
+def kernel_bytes(spec, infos, precision, ru_separate=False):
     """{kernel: algorithmic bytes over one solve} from the lanes' iteration
-    and reliable-update counts."""
+    and reliable-update counts.  ru_separate: the reliable-update hops run in
+    kernels of their own (cg_ru1, cg_ru2; the system-blocked schedule)."""
     s = SPINOR_BYTES[precision]
     sx = 48 if precision == "f64" else 24
     lb = LINK_BYTES[precision]
-    out = dict.fromkeys(KERNELS, 0.0)
+    out = dict.fromkeys(KERNELS + (("cg_ru1", "cg_ru2") if ru_separate else ()), 0.0)
+    ru1, ru2 = ("cg_ru1", "cg_ru2") if ru_separate else ("cg_hop1", "cg_hop2")
     for k, sys_ in enumerate(spec):
         Vh = int(np.prod(sys_["dims"])) // 2
         group_iters = [0, 0]
@@ -159,9 +161,10 @@ def kernel_bytes(spec, infos, precision):
                 out["cg_update"] += it * Vh * (5 * s + 2 * sx)
                 if precision != "f64":
                     # FP64 hop of x (links, x_hi + x_lo in, t_hi out); FP64
-                    # hop of t_hi, x_hi, x_lo, b in, x_hi, x_lo, r out
-                    out["cg_hop1"] += nru * Vh * (8 * 144 + 48 + 24 + 48)
-                    out["cg_hop2"] += nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s)
+                    # hop of t_hi, x_hi, x_lo, b in, x_hi, x_lo, r out, and
+                    # the search direction rebuilt (r, p in, p out)
+                    out[ru1] += nru * Vh * (8 * 144 + 48 + 24 + 48)
+                    out[ru2] += nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s + 3 * s)
                 group_iters[par] = max(group_iters[par], it)
         for par in (0, 1):
             out["cg_hop1"] += group_iters[par] * 8 * lb * Vh
@@ -170,7 +173,7 @@ def kernel_bytes(spec, infos, precision):
 
 
 def solve_bytes(spec, infos, precision):
-    return sum(kernel_bytes(spec, infos, precision).values())
+    return sum(kernel_bytes(spec, infos, precision).values())  # the same whichever kernels do the hops
 
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
@@ -669,7 +672,7 @@ def main():
     # per-kernel device time: one more solve with the kernels launched one by
     # one between CUDA events on the batch's stream (same kernels and results)
     per_kernel = B.solve_timed(tol=TOL, max_iter=MAXIT)
-    kbytes = kernel_bytes(spec, infos, args.precision)
+    kbytes = kernel_bytes(spec, infos, args.precision, ru_separate="cg_ru1" in per_kernel)
     ktot = sum(v[0] for v in per_kernel.values())
     kernels = {}
     for name, (kms, kn) in per_kernel.items():

@@ -540,14 +540,20 @@ class Batch:
         return w.value
 
     def solve_timed(self, tol=1e-10, max_iter=20000):
-        """Solve with per-kernel CUDA-event timing; returns {kernel: (ms, launches)}."""
-        ms = np.zeros(3)
-        n = (ctypes.c_long * 3)()
+        """Solve with per-kernel CUDA-event timing; returns {kernel: (ms, launches)}
+        for the kernels the schedule launched (the reliable-update kernels
+        cg_ru1 / cg_ru2 with the system-blocked schedule only)."""
+        ms = np.zeros(5)
+        n = (ctypes.c_long * 5)()
         self._check(self.lib.sfh_batch_solve_timed(self.h, tol, max_iter, _dptr(ms), n), "solve_timed")
-        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(("cg_hop1", "cg_hop2", "cg_update"))}
+        names = ("cg_hop1", "cg_hop2", "cg_update", "cg_ru1", "cg_ru2")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names) if i < 3 or n[i] > 0}
 
-    def set_schedule(self, width, tiles_per_block, stage_links=False):
-        self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, 1 if stage_links else 0),
+    def set_schedule(self, width, tiles_per_block, stage_links=0):
+        """stage_links: 0 (or False) links read directly, 1 (or True) staged per
+        work item, 2 system-blocked (one tile per block serving every RHS of
+        the system, links read once per tile)."""
+        self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
 
     def set_reliable_delta(self, delta):
@@ -556,11 +562,12 @@ class Batch:
         self._check(self.lib.sfh_batch_set_reliable_delta(self.h, delta), "set_reliable_delta")
 
     def schedule(self):
-        """(RHS-block width, tiles per block, links staged) the next solve uses."""
+        """(RHS-block width, tiles per block, link staging 0 / 1 / 2) the next
+        solve uses."""
         w, t, g = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
         self._check(self.lib.sfh_batch_get_schedule(self.h, ctypes.byref(w), ctypes.byref(t), ctypes.byref(g)),
                     "schedule")
-        return w.value, t.value, bool(g.value)
+        return w.value, t.value, g.value
 
     def set_gauge(self, k, U):
         U = _f64(U).reshape(-1)

@@ -800,6 +800,326 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// System-blocked hop kernels: one block per 256-site tile of one parity of
+// one system, serving every right-hand side of the system.  The tile's links
+// are read from HBM once and kept in shared memory for all RHS groups: FP16
+// links unpacked (row 2 rebuilt) to nine half2 each, so the groups only read
+// them; the other reduced precisions staged as stored and unpacked per
+// group.  Within the block the RHS are taken NB at a time (register-blocked
+// accumulators), the neighbour indices and hop signs computed once per site.
+// The CG sums of cg_hop2_sys are reduced per group through shared memory in
+// a fixed order (each site's dot products in FP32, summed in FP64).  The
+// FP64 reliable-update hops run in kernels of their own (cg_ru1_sys,
+// cg_ru2_sys), so that their registers do not weigh on the hop kernels.
+// ---------------------------------------------------------------------------
+// unpacked FP16 links of a tile: [direction slot 8][half2 word 9][kTile]
+constexpr size_t kHStageBytes = (size_t)8 * 9 * kTile * sizeof(uint32_t);
+
+template <int GP, int SP> struct SysStage {
+    static constexpr bool unpacked = (GP == GP_F16_12 && SP == SP_F16);
+    static constexpr size_t bytes = unpacked ? kHStageBytes : StageBytes<GP>::v;
+};
+
+// resident blocks per SM of the system-blocked kernels: hop1 three (FP16
+// unpacked links 72 KB, BF16 staged 48 KB), two for FP32-12 (96 KB staged);
+// hop2 two (its per-group reduction rows on top of the links)
+template <int GP, bool HOP2> struct SysOcc {
+    static constexpr int v = (HOP2 || GP == GP_F32_12) ? 2 : 3;
+};
+
+// FP16 links of this thread's site (4 forward at the site, 4 backward at its
+// neighbours), unpacked into its own column of the staging area
+__device__ __forceinline__ void stage_hlinks(uint32_t* s, const void* Ulo, const Nbr& n, int q, int i, int Vh)
+{
+    const int nq = 1 - q, t = threadIdx.x;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        const uint2* f = (const uint2*)Ulo + ((size_t)(q * 4 + mu) * 3) * Vh + i;
+        const uint2* b = (const uint2*)Ulo + ((size_t)(nq * 4 + mu) * 3) * Vh + n.dn[mu];
+        uint2 w[2][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            w[0][k] = __ldg(f + (size_t)k * Vh);
+            w[1][k] = __ldg(b + (size_t)k * Vh);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            __half2 e[9];
+            hlink_unpack(w[h], e);
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                s[((2 * mu + h) * 9 + k) * kTile + t] = *reinterpret_cast<const uint32_t*>(&e[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ void hlink_smem(const uint32_t* s, int d, __half2 (&e)[9])
+{
+#pragma unroll
+    for (int k = 0; k < 9; ++k) e[k] = h2_bits(s[(d * 9 + k) * kTile + threadIdx.x]);
+}
+
+// acc[l] += K in_l at the site for the lanes with on[l], links from the
+// tile's staging area (unpacked FP16, or as stored for the other formats)
+template <int GP, int SP, int NB>
+__device__ __forceinline__ void hop_lanes_sys(const void* Ulo, const void* stage, const Nbr& n, int q, int i,
+                                              int Vh, const void* const (&in)[NB], const bool (&on)[NB],
+                                              Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
+{
+    if constexpr (SysStage<GP, SP>::unpacked) {
+        const uint32_t* sl = (const uint32_t*)stage;
+        const int nq = 1 - q;
+#pragma unroll
+        for (int mu = 0; mu < 4; ++mu) {
+            const float s = ((n.eta >> mu) & 1u) ? -0.5f : 0.5f;
+            __half2 U[9];
+            hlink_smem(sl, 2 * mu, U);
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (on[l]) hop_half<false>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
+            hlink_smem(sl, 2 * mu + 1, U);
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (on[l]) hop_half<true>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
+        }
+    } else {
+        hop_lanes<GP, SP, NB, true>(Ulo, (const typename GaugeFmt<GP>::E*)stage, n, q, i, Vh, in, on, acc);
+    }
+}
+
+template <int GP, int SP>
+__device__ __forceinline__ void stage_tile_links(void* stage, const void* Ulo, const Nbr& n, int q, int i, int Vh)
+{
+    if constexpr (SysStage<GP, SP>::unpacked) {
+        stage_hlinks((uint32_t*)stage, Ulo, n, q, i, Vh);
+    } else {
+        stage_links<GP>((typename GaugeFmt<GP>::E*)stage, Ulo, n, q, i, Vh);
+        cp_async_wait_all();
+    }
+}
+
+// which of the system's lanes take part in this phase (uniform in the block)
+__device__ __forceinline__ void scan_lanes(const CgArgs& a, const CgSys& S, int q, bool hop1, int cur, bool* anyA,
+                                           bool* anyR)
+{
+    bool A = false, R = false;
+    for (int r = 0; r < S.nrhs; ++r) {
+        const int m = ld_int(&a.lanes[lane_of(S, r, q, hop1)].mode[cur]);
+        A |= m == LM_ACTIVE || m == LM_RESTART;
+        R |= m == LM_RU;
+    }
+    *anyA = A;
+    *anyR = R;
+}
+
+// hop1, system-blocked: t = K p for every active lane of the system on one
+// tile (the lanes in a reliable update are cg_ru1_sys's)
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, (SysOcc<GP, false>::v)) cg_hop1_sys(CgArgs a, const int2* __restrict__ items,
+                                                                              int cur)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    typedef typename GaugeFmt<GP>::R R;
+    typedef typename SpinorFmt<SP>::R RS;
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, it.x);
+    const int q = ti.q, Vh = S.g.Vh;
+    bool anyA, anyR;
+    scan_lanes(a, S, q, true, cur, &anyA, &anyR);
+    if (!anyA || !ti.valid) return;  // no barrier below
+    const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+    stage_tile_links<GP, SP>(s_dyn, S.Ulo, n, q, ti.i, Vh);
+    for (int base = 0; base < S.nrhs; base += NB) {
+        LanePass<NB> P;
+        gather_pass<NB>(a, S, base, q, true, cur, false, P);
+        if (!P.anyA) continue;
+        const void* pin[NB];
+        bool on[NB];
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+            pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
+        }
+        Vec3<R> acc[NB];
+#pragma unroll
+        for (int l = 0; l < NB; ++l) vzero(acc[l]);
+        hop_lanes_sys<GP, SP, NB>(S.Ulo, s_dyn, n, q, ti.i, Vh, pin, on, acc);
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+            if (on[l]) SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(acc[l]));
+    }
+}
+
+// Fixed-order block sum of F float rows (one value per thread each) in FP64:
+// lane j of warp w adds the row's elements j, j + 32, ... in order, then the
+// warp's lanes by the xor tree; results in tot[F] (all threads).
+template <int F>
+__device__ __forceinline__ void rows_sum(const float (&v)[F], float (*red)[kTile], double* tot)
+{
+#pragma unroll
+    for (int f = 0; f < F; ++f) red[f][threadIdx.x] = v[f];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int f = warp; f < F; f += kTile / 32) {
+        double x = 0.0;
+#pragma unroll
+        for (int k = 0; k < kTile / 32; ++k) x += (double)red[f][lane + 32 * k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) tot[f] = x;
+    }
+    __syncthreads();
+}
+
+// hop2, system-blocked: v = m^2 p - K t and the four CG sums for every active
+// lane of the system on one tile (the lanes in a reliable update are
+// cg_ru2_sys's)
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgArgs a, const int2* __restrict__ items,
+                                                                             int cur)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    typedef typename GaugeFmt<GP>::R R;
+    typedef typename SpinorFmt<SP>::R RS;
+    static_assert(sizeof(RS) == 4, "system-blocked kernels serve the reduced precisions");
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    __shared__ float s_red[NB * kSums][kTile];
+    __shared__ double s_tot[NB * kSums];
+    __shared__ unsigned s_mask;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, it.x);
+    const int q = ti.q, Vh = S.g.Vh;
+    const ItemRange ir = item_range(a, S, it.x);
+    const unsigned nsq = (unsigned)item_groups(a, S);
+    bool anyA, anyR;
+    scan_lanes(a, S, q, false, cur, &anyA, &anyR);
+    if (!anyA) return;  // uniform in the block
+    Nbr n;
+    if (ti.valid) {
+        n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+        stage_tile_links<GP, SP>(s_dyn, S.Ulo, n, q, ti.i, Vh);
+    }
+    const R m2 = (R)S.m2;
+    for (int base = 0; base < S.nrhs; base += NB) {
+        LanePass<NB> P;
+        gather_pass<NB>(a, S, base, q, false, cur, false, P);
+        if (!P.anyA) continue;  // uniform in the block
+        bool on[NB];
+        const void* tin[NB];
+        float v[NB * kSums];
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
+            tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
+#pragma unroll
+            for (int f = 0; f < kSums; ++f) v[l * kSums + f] = 0.f;
+        }
+        if (ti.valid) {
+            Vec3<R> acc[NB];
+#pragma unroll
+            for (int l = 0; l < NB; ++l) vzero(acc[l]);
+            hop_lanes_sys<GP, SP, NB>(S.Ulo, s_dyn, n, q, ti.i, Vh, tin, on, acc);
+#pragma unroll
+            for (int l = 0; l < NB; ++l) {
+                if (!on[l]) continue;
+                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+                Vec3<RS> p = r;
+                if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
+                    SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
+                else
+                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+                Vec3<R> pr = vcvt<R>(p), w;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
+                    w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
+                }
+                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+                v[l * kSums + 0] = (float)site_dot(p, vn);
+                v[l * kSums + 1] = (float)site_dot(r, vn);
+                v[l * kSums + 2] = (float)site_dot(vn, vn);
+                v[l * kSums + 3] = (float)site_dot(r, r);
+            }
+        }
+        rows_sum<NB * kSums>(v, s_red, s_tot);
+        double sums[NB * kSums];
+#pragma unroll
+        for (int f = 0; f < NB * kSums; ++f) sums[f] = s_tot[f];
+        const unsigned mask = arrive_sums<NB>(a, S, P, on, sums, ir.slot, nsq, &s_mask);
+        if (mask && threadIdx.x < 32) {
+#pragma unroll
+            for (int l = 0; l < NB; ++l)
+                if (mask & (1u << l)) finish_lane(a, S, P.lane[l], P.mode[l], cur);
+        }
+        __syncthreads();
+    }
+}
+
+// The FP64 reliable-update hops of the system-blocked schedule, one block
+// per tile; blocks without a lane in a reliable update return at once.
+// ru1: thi = K (x_hi + x_lo) at output parity q for the lanes of parity
+// 1 - q; ru2: x_hi += x_lo, r = b - M x_hi and |r|^2 for the lanes of parity
+// q, whose partial sums complete the lanes' tickets.
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru1_sys(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, it.x);
+    bool anyA, anyR;
+    scan_lanes(a, S, ti.q, true, cur, &anyA, &anyR);
+    if (!anyR || !ti.valid) return;
+    const Coord c = eo_coords(S.g, ti.q, ti.i);
+#pragma unroll 1
+    for (int r = 0; r < S.nrhs; ++r) {
+        const CgLane* L = a.lanes + lane_of(S, r, ti.q, true);
+        if (ld_int(&L->mode[cur]) == LM_RU) ru_hop1<XP>(a, S, c, ti.q, ti.i, __ldg(&L->rhs));
+    }
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru2_sys(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    constexpr int XP = XFmt<SP>::v;
+    const int2 it = items[blockIdx.x];
+    __shared__ CgSys s_sys;
+    __shared__ double smem[32];
+    __shared__ unsigned s_mask;
+    stage_sys(a, it.x, &s_sys);
+    const CgSys& S = s_sys;
+    const TileInfo ti = decode_tile(S, it.x);
+    const int q = ti.q;
+    bool anyA, anyR;
+    scan_lanes(a, S, q, false, cur, &anyA, &anyR);
+    if (!anyR) return;  // uniform in the block
+    const ItemRange ir = item_range(a, S, it.x);
+    const unsigned nsq = (unsigned)item_groups(a, S);
+    const Coord c = eo_coords(S.g, q, ti.valid ? ti.i : 0);
+#pragma unroll 1
+    for (int r = 0; r < S.nrhs; ++r) {
+        LanePass<1> P;
+        gather_pass<1>(a, S, r, q, false, cur, false, P);
+        if (P.mode[0] != LM_RU) continue;
+        double sums[kSums] = {0.0, 0.0, 0.0, 0.0};
+        if (ti.valid) sums[3] = ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[0]);
+        block_sum<kSums>(sums, smem);
+        const bool part[1] = {true};
+        const unsigned mask = arrive_sums<1>(a, S, P, part, sums, ir.slot, nsq, &s_mask);
+        if (mask && threadIdx.x < 32) finish_lane(a, S, P.lane[0], P.mode[0], cur);
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -809,12 +1129,63 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restr
 typedef void (*InitKernel)(CgArgs);
 typedef void (*HopKernel)(CgArgs, const int2*, int);
 
+// the kernels of one CG iteration, in launch order, with their work items
+// and timing slots
+enum { PH_HOP1 = 0, PH_HOP2 = 1, PH_UPDATE = 2, PH_RU1 = 3, PH_RU2 = 4, kTimedPhases = 5 };
+constexpr int kMaxPhases = 5;
+
 struct CgKernels {
     InitKernel init;
     HopKernel hop1, hop2, update;
-    int nb1, nb2;   // RHS-group widths the hop kernels are compiled for
+    HopKernel ru1, ru2;  // separate reliable-update kernels (system-blocked schedule only)
+    int nb1, nb2;   // RHS widths of the hop kernels' work items
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
+    bool sys;       // system-blocked hop kernels (one tile per block, every RHS)
 };
+
+struct Phase {
+    HopKernel fn;
+    int width;      // RHS width of the work items
+    size_t smem;
+    int slot;       // timing slot
+};
+
+static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
+{
+    int n = 0;
+    ph[n++] = {k.hop1, k.nb1, k.smem, PH_HOP1};
+    if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1};
+    ph[n++] = {k.hop2, k.nb2, k.smem, PH_HOP2};
+    if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2};
+    ph[n++] = {k.update, 1, 0, PH_UPDATE};
+    return n;
+}
+
+// work-item width of the system-blocked kernels: one item per tile, covering
+// every RHS of the system
+constexpr int kSysItems = 1 << 20;
+
+template <int GP, int SP>
+static CgKernels pick_sys(int nb)
+{
+    CgKernels k;
+    // FP32 arithmetic on FP32 links keeps at most four accumulators in
+    // registers; the packed-half FP16 products take eight
+    if (nb >= 4) { k.hop1 = cg_hop1_sys<GP, SP, 4>; k.hop2 = cg_hop2_sys<GP, SP, 4>; }
+    else if (nb >= 2) { k.hop1 = cg_hop1_sys<GP, SP, 2>; k.hop2 = cg_hop2_sys<GP, SP, 2>; }
+    else { k.hop1 = cg_hop1_sys<GP, SP, 1>; k.hop2 = cg_hop2_sys<GP, SP, 1>; }
+    if constexpr (SysStage<GP, SP>::unpacked) {
+        if (nb >= 8) { k.hop1 = cg_hop1_sys<GP, SP, 8>; k.hop2 = cg_hop2_sys<GP, SP, 8>; }
+    }
+    k.init = cg_init<SP, 2>;
+    k.update = cg_update<SP>;
+    k.ru1 = cg_ru1_sys<SP>;
+    k.ru2 = cg_ru2_sys<SP>;
+    k.nb1 = k.nb2 = kSysItems;
+    k.smem = SysStage<GP, SP>::bytes;
+    k.sys = true;
+    return k;
+}
 
 template <int GP, int SP, bool STG>
 static HopKernel pick_hop1(int nb, int* nb_eff)
@@ -847,7 +1218,9 @@ static CgKernels pick_typed(int nb1, int nb2)
     k.hop1 = pick_hop1<GP, SP, STG>(nb1, &k.nb1);
     pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
+    k.ru1 = k.ru2 = nullptr;  // the reliable-update hops run inside hop1 / hop2
     k.smem = STG ? StageBytes<GP>::v : 0;
+    k.sys = false;
     return k;
 }
 
@@ -861,14 +1234,19 @@ static CgKernels pick_staged(int nb1, int nb2, bool stage)
     }
 }
 
-static CgKernels pick_kernels(int prec, int nb1, int nb2, bool stage)
+// stage: 0 links read directly, 1 staged per work item, 2 system-blocked
+// kernels (FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
+static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
 {
     CgKernels k;
     if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false);
-    else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage);
-    else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage);
-    else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stage);
-    else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stage);
+    else if (stage == 2 && prec == SFH_PREC_F16) k = pick_sys<GP_F16_12, SP_F16>(nb1);
+    else if (stage == 2 && prec == SFH_PREC_BF16) k = pick_sys<GP_BF16_12, SP_BF16>(nb1);
+    else if (stage == 2 && prec == SFH_PREC_F32) k = pick_sys<GP_F32_12, SP_F32>(nb1);
+    else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage != 0);
+    else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage != 0);
+    else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stage != 0);
+    else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stage != 0);
     if (k.smem) {  // opt in to the staged kernels' shared memory (idempotent)
         cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
         cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
@@ -1045,9 +1423,6 @@ static int default_nb(int max_nrhs, int cap)
 }
 
 constexpr int kChunk = 16;  // CG iterations per graph launch (even)
-// kernels per CG iteration: hop1, hop2, update (the hop kernels also do the
-// FP64 hops of lanes in a reliable update)
-constexpr int kPhases = 3;
 
 // Work items (first tile, first RHS): tpi tiles of one parity of a system and
 // one RHS group of width nb; one block each.  The groups of a tile range are
@@ -1099,37 +1474,41 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     return a;
 }
 
-// (Re)build the graph of kChunk iterations: hop1, hop2, update, hop1, ...
+// (Re)build the graph of kChunk iterations: the iteration's kernels in order
+// (hop1, hop2, update; with the system-blocked schedule hop1, ru1, hop2, ru2,
+// update), repeated
+static bool same_kernels(const CgKernels& a, const CgKernels& b)
+{
+    return a.hop1 == b.hop1 && a.hop2 == b.hop2 && a.update == b.update && a.ru1 == b.ru1 && a.ru2 == b.ru2;
+}
+
 static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, double tol, int maxit,
                                 double delta)
 {
-    if (w.exec && w.gk.hop1 == k.hop1 && w.gk.hop2 == k.hop2 && w.gk.update == k.update && w.g_tol == tol &&
-        w.g_tpi == a.tpi &&
-        w.g_maxit == maxit &&
+    if (w.exec && same_kernels(w.gk, k) && w.g_tol == tol && w.g_tpi == a.tpi && w.g_maxit == maxit &&
         w.g_delta == delta)
         return cudaSuccess;
     w.release_graph();
-    const int2* items[kPhases];
-    int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb2, 1};
-    const HopKernel fn[kPhases] = {k.hop1, k.hop2, k.update};
+    Phase ph[kMaxPhases];
+    const int nph = phases_of(k, ph);
+    const int2* items[kMaxPhases];
+    int nitems[kMaxPhases];
     cudaError_t e;
-    for (int ph = 0; ph < kPhases; ++ph)
-        if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
+    for (int j = 0; j < nph; ++j)
+        if ((e = items_for(w, ph[j].width, a.tpi, &items[j], &nitems[j])) != cudaSuccess) return e;
     e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
     cudaGraphNode_t prev = nullptr;
     for (int it = 0; it < kChunk; ++it) {
         int cur = it & 1;
-        for (int ph = 0; ph < kPhases; ++ph) {
-            if (!fn[ph]) continue;
+        for (int j = 0; j < nph; ++j) {
             cudaKernelNodeParams p;
             std::memset(&p, 0, sizeof(p));
-            p.func = (void*)fn[ph];
-            p.gridDim = dim3(nitems[ph]);
+            p.func = (void*)ph[j].fn;
+            p.gridDim = dim3(nitems[j]);
             p.blockDim = dim3(kTile);
-            p.sharedMemBytes = ph < 2 ? (unsigned)k.smem : 0u;  // the hop kernels
-            void* args[] = {&a, (void*)&items[ph], &cur};
+            p.sharedMemBytes = (unsigned)ph[j].smem;
+            void* args[] = {&a, (void*)&items[j], &cur};
             p.kernelParams = args;
             cudaGraphNode_t node;
             e = cudaGraphAddKernelNode(&node, w.graph, prev ? &prev : nullptr, prev ? 1 : 0, &p);
@@ -1148,10 +1527,11 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
 }
 
 // Device time of each iteration kernel over one solve (timed solves launch
-// the kernels one by one between CUDA events instead of replaying the graph).
+// the kernels one by one between CUDA events instead of replaying the graph),
+// by timing slot: hop1, hop2, update, ru1, ru2.
 struct PhaseTimes {
-    double ms[3];  // hop1, hop2, update
-    long n[3];
+    double ms[kTimedPhases];
+    long n[kTimedPhases];
 };
 
 // Reliable-update threshold (|r| drop between FP64 updates) of the mixed
@@ -1168,7 +1548,7 @@ static double default_reliable_delta(int prec)
 // the iteration kernels (0 = 2); stage: hop kernels stage their links in
 // shared memory (reduced precisions only).  Returns a cudaError.
 static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double delta, int nb1, int nb2,
-                                   int tpi, bool stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
+                                   int tpi, int stage, cudaStream_t stream, PhaseTimes* timing = nullptr)
 {
     int max_nrhs = 1;
     for (const CgSys& S : w.sys) max_nrhs = std::max(max_nrhs, S.nrhs);
@@ -1190,26 +1570,29 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     w.h_active[0] = w.h_active[1] = w.nlanes;
     if ((e = cudaMemcpyAsync(w.d_active, &w.h_active[0], sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
-    CgArgs a = make_args(w, tol, maxit, delta, tpi > 0 ? tpi : 2);
     CgKernels k = pick_kernels(w.prec, nb1, nb2, stage);
+    // the system-blocked kernels serve one tile per block: one partial-sum
+    // slot per tile, so every kernel of the iteration takes single tiles
+    CgArgs a = make_args(w, tol, maxit, delta, k.sys ? 1 : (tpi > 0 ? tpi : 2));
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (!timing && (e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
     // timed solves: the same kernels and work items, launched one by one
-    const int2* items[kPhases];
-    int nitems[kPhases];
-    const int widths[kPhases] = {k.nb1, k.nb2, 1};
-    HopKernel fn[kPhases] = {k.hop1, k.hop2, k.update};
+    Phase ph[kMaxPhases];
+    const int nph = phases_of(k, ph);
+    const int2* items[kMaxPhases];
+    int nitems[kMaxPhases];
     std::vector<cudaEvent_t> tev;
+    const int per_chunk = nph * kChunk;
     if (timing) {
-        for (int ph = 0; ph < kPhases; ++ph)
-            if ((e = items_for(w, widths[ph], a.tpi, &items[ph], &nitems[ph])) != cudaSuccess) return e;
-        for (int r = 0; r < 3; ++r) {
+        for (int j = 0; j < nph; ++j)
+            if ((e = items_for(w, ph[j].width, a.tpi, &items[j], &nitems[j])) != cudaSuccess) return e;
+        for (int r = 0; r < kTimedPhases; ++r) {
             timing->ms[r] = 0.0;
             timing->n[r] = 0;
         }
-        tev.resize(2 * (kPhases * kChunk + 1));
+        tev.resize(2 * (per_chunk + 1));
         for (cudaEvent_t& ev : tev)
             if ((e = cudaEventCreate(&ev)) != cudaSuccess) return e;
     }
@@ -1219,11 +1602,11 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         tev.clear();
     };
     auto accumulate = [&](int pool) {  // a finished chunk's per-kernel times
-        cudaEvent_t* ev = tev.data() + pool * (kPhases * kChunk + 1);
-        for (int j = 0; j < kPhases * kChunk; ++j) {
+        cudaEvent_t* ev = tev.data() + pool * (per_chunk + 1);
+        for (int j = 0; j < per_chunk; ++j) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev[j], ev[j + 1]);
-            const int r = j % kPhases;
+            const int r = ph[j % nph].slot;
             timing->ms[r] += ms;
             timing->n[r] += 1;
         }
@@ -1232,14 +1615,12 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     // keep one chunk queued ahead of the convergence check
     for (int c = 0; c < max_chunks; ++c) {
         if (timing) {
-            cudaEvent_t* ev = tev.data() + (c & 1) * (kPhases * kChunk + 1);
+            cudaEvent_t* ev = tev.data() + (c & 1) * (per_chunk + 1);
             if ((e = cudaEventRecord(ev[0], stream)) != cudaSuccess) { destroy_events(); return e; }
             for (int it = 0; it < kChunk; ++it)
-                for (int ph = 0; ph < kPhases; ++ph) {
-                    if (fn[ph])
-                        fn[ph]<<<nitems[ph], kTile, ph < 2 ? k.smem : 0, stream>>>(a, items[ph],
-                                                                                               it & 1);
-                    if ((e = cudaEventRecord(ev[kPhases * it + ph + 1], stream)) != cudaSuccess) {
+                for (int j = 0; j < nph; ++j) {
+                    ph[j].fn<<<nitems[j], kTile, ph[j].smem, stream>>>(a, items[j], it & 1);
+                    if ((e = cudaEventRecord(ev[nph * it + j + 1], stream)) != cudaSuccess) {
                         destroy_events();
                         return e;
                     }
@@ -1247,7 +1628,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         } else if ((e = cudaGraphLaunch(w.exec, stream)) != cudaSuccess) {
             return e;
         }
-        w.launches += kPhases * kChunk;
+        w.launches += per_chunk;
         if ((e = cudaMemcpyAsync(&w.h_active[c & 1], w.d_active, sizeof(int), cudaMemcpyDeviceToHost, stream)) !=
             cudaSuccess)
             return e;
@@ -1478,7 +1859,7 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
 {
     if (!b || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links != 0, b->stream),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links, b->stream),
                         "batched CG");
     if (st) return st;
     for (const sfh::CgLane& L : b->ws.lanes_h)
@@ -1707,17 +2088,17 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
 }
 
-extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double* ms3, long* n3)
+extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double* ms5, long* n5)
 {
-    if (!b || !ms3 || !n3 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    if (!b || !ms5 || !n5 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
     sfh::PhaseTimes t;
-    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links != 0, b->stream, &t),
+    int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links, b->stream, &t),
                         "timed batched CG");
     if (st) return st;
-    for (int k = 0; k < 3; ++k) {
-        ms3[k] = t.ms[k];
-        n3[k] = t.n[k];
+    for (int k = 0; k < sfh::kTimedPhases; ++k) {
+        ms5[k] = t.ms[k];
+        n5[k] = t.n[k];
     }
     for (const sfh::CgLane& L : b->ws.lanes_h)
         if (L.status != SFH_OK) return L.status;
@@ -1732,8 +2113,9 @@ extern "C" int sfh_batch_kernel_launches(sfh_batch* b, long* n)
 }
 
 // Autotuner: times a capped solve (probe_iters iterations, no lane converges)
-// for every RHS-block width and tiles-per-block count and keeps the fastest.
-// Results do not depend on either; only the schedule does.
+// for every RHS-block width, tiles-per-block count and link staging mode
+// (read directly, staged per work item, system-blocked) and keeps the
+// fastest.
 extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width)
 {
     if (!b || probe_iters < 1) return SFH_ERR_INVALID;
@@ -1746,14 +2128,16 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
     int bw = 1, bt = 2, bs = 0;
-    for (int stage = 0; stage < (f64 ? 1 : 2); ++stage)
+    const int nstage = f64 ? 1 : (b->prec == SFH_PREC_F32_18 ? 2 : 3);
+    for (int stage = 0; stage < nstage; ++stage)
         for (int c = 0; c < ncand; ++c)
             for (int tp : tiles) {
+                if (stage == 2 && tp != 1) continue;  // system-blocked: one tile per block
                 double t = 0.0;
                 for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
                     auto t0 = std::chrono::steady_clock::now();
                     cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], tp,
-                                                         stage != 0, b->stream);
+                                                         stage, b->stream);
                     if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
                     t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
                 }
@@ -1776,7 +2160,8 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
-    b->stage_links = stage_links ? 1 : 0;
+    if (stage_links < 0 || stage_links > 2) return SFH_ERR_INVALID;
+    b->stage_links = stage_links;
     return SFH_OK;
 }
 

@@ -34,7 +34,9 @@ def test_kernel_bytes_fp64_one_rhs():
 def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
     """FP16, two RHS of one system: links are counted once per (system,
     parity, iteration) with the longer lane's count, spinors per RHS; each
-    reliable update adds an FP64 hop to both hop kernels."""
+    reliable update adds an FP64 hop to both hop kernels (or to the two
+    reliable-update kernels of the system-blocked schedule), the second with
+    the search direction rebuilt."""
     import bench
     dims = (4, 4, 4, 8)
     Vh = 256
@@ -44,13 +46,19 @@ def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
     s, sx, lb = 16, 24, 24
     its = 12 + 20
     nru = (2 + 4) / 2.0  # per parity
-    hop1 = its * Vh * 2 * s + nru * Vh * (8 * 144 + 48 + 24 + 48) + 20 * 8 * lb * Vh
-    hop2 = its * Vh * 4 * s + nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s) + 20 * 8 * lb * Vh
+    ru1 = nru * Vh * (8 * 144 + 48 + 24 + 48)
+    ru2 = nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s + 3 * s)
+    hop1 = its * Vh * 2 * s + 20 * 8 * lb * Vh
+    hop2 = its * Vh * 4 * s + 20 * 8 * lb * Vh
     upd = its * Vh * (5 * s + 2 * sx)
-    assert out["cg_hop1"] == pytest.approx(2 * hop1)
-    assert out["cg_hop2"] == pytest.approx(2 * hop2)
+    assert out["cg_hop1"] == pytest.approx(2 * (hop1 + ru1))
+    assert out["cg_hop2"] == pytest.approx(2 * (hop2 + ru2))
     assert out["cg_update"] == pytest.approx(2 * upd)
-    assert bench.solve_bytes(spec, infos, "f16") == pytest.approx(2 * (hop1 + hop2 + upd))
+    assert bench.solve_bytes(spec, infos, "f16") == pytest.approx(2 * (hop1 + hop2 + upd + ru1 + ru2))
+    sep = bench.kernel_bytes(spec, infos, "f16", ru_separate=True)
+    assert sep["cg_hop1"] == pytest.approx(2 * hop1) and sep["cg_ru1"] == pytest.approx(2 * ru1)
+    assert sep["cg_hop2"] == pytest.approx(2 * hop2) and sep["cg_ru2"] == pytest.approx(2 * ru2)
+    assert sum(sep.values()) == pytest.approx(sum(out.values()))
 
 
 def test_dslash_bytes_table():

@@ -267,3 +267,57 @@ def test_mixed_cg_rough_light_mass_keeps_krylov_progress(sfh, orc, precision, bo
         assert np.linalg.norm(X - Xo) / np.linalg.norm(Xo) < 40001 * 2 * tol
     finally:
         lat.close()
+
+
+SYS_SYSTEMS = [((8, 8, 8, 8), 0.1, 5), ((6, 6, 6, 8), 0.05, 3), ((4, 4, 4, 4), 0.2, 9)]
+
+
+def _sys_batch(sfh, orc, precision, schedule):
+    B = sfh.Batch(SYS_SYSTEMS, precision=precision)
+    B.set_schedule(*schedule)
+    data = []
+    for k, (dims, mass, nrhs) in enumerate(SYS_SYSTEMS):
+        U = orc.random_gauge(dims, 1.0 if k % 2 == 0 else 0.3, 800 + k)
+        B.set_gauge(k, U)
+        bs = [orc.random_spinor(dims, 900 + 10 * k + j) for j in range(nrhs)]
+        for j, b in enumerate(bs):
+            B.set_rhs(k, j, b)
+        data.append((U, bs))
+    return B, data
+
+
+@pytest.mark.parametrize("precision", ["f16", "bf16", "f32"])
+def test_batch_system_blocked_schedule(sfh, orc, precision):
+    """The system-blocked schedule (one block per tile serving every RHS of
+    its system, links staged once per tile, reliable updates in kernels of
+    their own) on systems with several tiles, a partial last tile and more
+    RHS than one group: every RHS-group width gives bit-identical solutions
+    (the per-group sums have a fixed order), each reaches the FP64 true
+    residual by the oracle's D D^dag, and the timed solve runs the same
+    kernels to the same solutions."""
+    tol = 1e-10
+    outs = []
+    for w in (1, 2, 4, 8):
+        B, data = _sys_batch(sfh, orc, precision, (w, 1, 2))
+        assert B.schedule() == (w, 1, 2)
+        B.solve(tol=tol, max_iter=20000)
+        sol = []
+        for k, (dims, mass, nrhs) in enumerate(SYS_SYSTEMS):
+            U, bs = data[k]
+            for j in range(nrhs):
+                X = B.solution(k, j)
+                info = B.info(k, j)
+                assert info["status"] == 0 and info["reliable_updates"] >= 1
+                assert true_resid(orc, dims, mass, U, bs[j], X) < 1.05 * tol, (w, k, j)
+                sol.append(X)
+        outs.append(np.concatenate(sol))
+        B.close()
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    B, _ = _sys_batch(sfh, orc, precision, (4, 1, 2))
+    times = B.solve_timed(tol=tol)
+    timed = np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(SYS_SYSTEMS) for j in range(n)])
+    B.close()
+    assert np.array_equal(timed, outs[0])
+    assert set(times) == {"cg_hop1", "cg_hop2", "cg_update", "cg_ru1", "cg_ru2"}
+    assert len({times[k][1] for k in times}) == 1  # every iteration launches all five
