@@ -116,8 +116,10 @@ extern "C" int sfh_destroy(sfh_ctx* c)
     if (!c) return SFH_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (int k = 0; k < kNumPrecisions; ++k)
+    for (int k = 0; k < kNumPrecisions; ++k) {
         if (c->ws[k]) workspace_free(c->ws[k]);
+        if (c->ws_pair[k]) workspace_free(c->ws_pair[k]);
+    }
     void* ptrs[] = {c->U64, c->U32, c->U16, c->Ubf16, c->U32_18, c->U64_12, c->Pmom, c->Fbuf, c->stage, c->red, c->derr, c->Utrial,
                     c->smear, c->hphi, c->hX};
     for (void* p : ptrs)

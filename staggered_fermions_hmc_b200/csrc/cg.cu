@@ -2011,6 +2011,85 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     return SFH_OK;
 }
 
+// Two solves on the context's links at two masses (a Hasenbusch pair) as one
+// batch of two systems sharing the links: their lanes iterate together and
+// the heavy system's retire first, instead of two solves one after the
+// other.  FP64 runs full-lattice lanes (the reference's CG), as
+// ctx_solve_device does.
+int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_eo[2], const double mass[2],
+                          double tol, int maxit, int prec, sfh_cg_info info[2])
+{
+    if (!valid_precision(prec)) return set_error(c, SFH_ERR_INVALID, "precision");
+    if (prec != SFH_PREC_F64 && !c->lowp_valid) {
+        launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18, c->Ubf16);
+        c->lowp_valid = true;
+    }
+    cudaError_t e = cudaSuccess;
+    CgWorkspace* w = c->ws_pair[prec];
+    if (!w) {
+        w = new CgWorkspace();
+        const void* const lo[5] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16};
+        std::vector<SolverSystemHost> hs(2);
+        for (int k = 0; k < 2; ++k) {
+            hs[k].g = c->g;
+            hs[k].mass = mass[k];
+            hs[k].nrhs = 1;
+            hs[k].U64 = c->U64;
+            hs[k].Ulo = lo[prec];
+        }
+        e = workspace_build(*w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
+        if (e != cudaSuccess) {
+            delete w;
+            return cuda_check(c, e, "cg pair workspace");
+        }
+        c->ws_pair[prec] = w;
+        c->ws_pair_mass[prec][0] = mass[0];
+        c->ws_pair_mass[prec][1] = mass[1];
+    }
+    if (c->ws_pair_mass[prec][0] != mass[0] || c->ws_pair_mass[prec][1] != mass[1]) {
+        for (int k = 0; k < 2; ++k) {
+            w->sys[k].m2 = mass[k] * mass[k];
+            c->ws_pair_mass[prec][k] = mass[k];
+        }
+        e = cudaMemcpyAsync(w->d_sys, w->sys.data(), 2 * sizeof(CgSys), cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cg pair masses");
+    }
+    const size_t fs = (size_t)c->g.V * 6 * sizeof(double);
+    for (int k = 0; k < 2; ++k) {
+        e = cudaMemcpyAsync(w->rhs[w->rhs0[k]].b, b_eo[k], fs, cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cg pair rhs");
+    }
+    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), 0, 0, 0, 0, c->stream);
+    if (e != cudaSuccess) return cuda_check(c, e, "cg pair solve");
+    for (int k = 0; k < 2; ++k) {
+        e = cudaMemcpyAsync(x_eo[k], w->rhs[w->rhs0[k]].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cg pair solution");
+    }
+    int status = SFH_OK;
+    for (int k = 0; k < 2; ++k) {
+        sfh_cg_info inf;
+        std::memset(&inf, 0, sizeof(inf));
+        double rr = 0, bb = 0;
+        for (const CgLane& L : w->lanes_h) {
+            if (L.sys != k) continue;
+            if (L.status != SFH_OK && inf.status == SFH_OK) inf.status = L.status;
+            inf.iters = std::max(inf.iters, L.iters);
+            if (L.parity < 2) inf.iters_parity[L.parity] = L.iters;
+            else inf.iters_parity[0] = inf.iters_parity[1] = L.iters;
+            inf.reliable_updates += L.nru;
+            rr += L.rr_next;
+            bb += L.bb;
+        }
+        inf.rsq_rel = bb > 0 ? rr / bb : 0.0;
+        inf.true_resid = -1.0;
+        if (inf.status != SFH_OK && status == SFH_OK) status = inf.status;
+        if (info) info[k] = inf;
+    }
+    if (status != SFH_OK)
+        return set_error(c, status, status == SFH_ERR_NOCONV ? "CG Solver failed to converge" : "CG breakdown");
+    return SFH_OK;
+}
+
 }  // namespace sfh
 
 // ===========================================================================

@@ -156,6 +156,32 @@ int pf_terms(sfh_ctx* c, const void* phi, void* X, PfTerm (&t)[2])
     return 1;
 }
 
+// X_k = M(m_k)^-1 phi_k for the pseudofermion terms: a Hasenbusch pair as
+// one batch of two systems on the same links, a single term alone
+int solve_terms(sfh_ctx* c, const PfTerm* t, int n, double tol, int maxit, int prec, long* iters, int* solves)
+{
+    if (n == 2) {
+        const void* b[2] = {t[0].phi, t[1].phi};
+        void* x[2] = {t[0].X, t[1].X};
+        const double ms[2] = {t[0].mass, t[1].mass};
+        sfh_cg_info inf[2];
+        std::memset(inf, 0, sizeof(inf));
+        int st = ctx_solve_pair_device(c, b, x, ms, tol, maxit, prec, inf);
+        if (iters) *iters += inf[0].iters + inf[1].iters;
+        if (solves) *solves += 2;
+        return st;
+    }
+    const double m = c->mass;
+    c->mass = t[0].mass;
+    sfh_cg_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    int st = ctx_solve_device(c, t[0].phi, t[0].X, tol, maxit, prec, &inf);
+    c->mass = m;
+    if (iters) *iters += inf.iters;
+    if (solves) *solves += 1;
+    return st;
+}
+
 // Fbuf = sum_k w_k F_f(X_k, Y_k) on the links in U64
 int fermion_force_terms(sfh_ctx* c, const void* phi, void* X, void* Y, double tol, int maxit, int prec,
                         long* iters, int* solves)
@@ -164,14 +190,9 @@ int fermion_force_terms(sfh_ctx* c, const void* phi, void* X, void* Y, double to
     const int n = pf_terms(c, phi, X, t);
     const double m = c->mass;
     int st = cuda_check(c, cudaMemsetAsync(c->Fbuf, 0, link_bytes(c), c->stream), "fermion force");
+    if (!st) st = solve_terms(c, t, n, tol, maxit, prec, iters, solves);
     for (int k = 0; k < n && !st; ++k) {
         c->mass = t[k].mass;
-        sfh_cg_info inf;
-        std::memset(&inf, 0, sizeof(inf));
-        st = ctx_solve_device(c, t[k].phi, t[k].X, tol, maxit, prec, &inf);
-        if (iters) *iters += inf.iters;
-        if (solves) *solves += 1;
-        if (st) break;
         launch_hop(c->g, GP_F64_18, c->U64, SP_F64, t[k].X, SP_F64, Y, t[k].X, t[k].mass, -1.0, 0, 2, c->stream);
         // Fbuf -= (-w) F: the kick form of force_kernel accumulates w F
         st = cuda_check(c, launch_force(c->g, c->U64, t[k].X, Y, c->beta, c->c11, c->c12, 2, nullptr, c->Fbuf,
@@ -218,15 +239,10 @@ int fermion_action(sfh_ctx* c, const void* phi, void* X, double tol, int maxit, 
     const double m = c->mass;
     int st = c->fsmear_n > 0 ? smear_in(c) : SFH_OK;
     double sum = 0.0;
+    if (!st) st = solve_terms(c, t, n, tol, maxit, prec, iters, solves);
     for (int k = 0; k < n && !st; ++k) {
-        c->mass = t[k].mass;
-        sfh_cg_info inf;
-        std::memset(&inf, 0, sizeof(inf));
-        st = ctx_solve_device(c, t[k].phi, t[k].X, tol, maxit, prec, &inf);
-        if (iters) *iters += inf.iters;
-        if (solves) *solves += 1;
         double d = 0.0;
-        if (!st) st = reduce(c, RED_DOT, t[k].phi, t[k].X, &d);
+        st = reduce(c, RED_DOT, t[k].phi, t[k].X, &d);
         sum += t[k].weight * d;
     }
     c->mass = m;

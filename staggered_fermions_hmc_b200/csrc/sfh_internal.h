@@ -42,6 +42,8 @@ struct sfh_ctx {
 
     sfh::CgWorkspace* ws[sfh::kNumPrecisions] = {};  // cached solver workspaces per precision
     double ws_mass[sfh::kNumPrecisions] = {};
+    sfh::CgWorkspace* ws_pair[sfh::kNumPrecisions] = {};  // two systems on the links (Hasenbusch pair)
+    double ws_pair_mass[sfh::kNumPrecisions][2] = {};
     void* Utrial = nullptr;        // gauge backup for the Metropolis step
     void* smear = nullptr;         // scratch link fields (smearing, staples)
     size_t smear_bytes = 0;
@@ -90,6 +92,9 @@ int ctx_cg_solve(sfh_ctx* c, const double* phi, double* X, double tol, int maxit
                  sfh_cg_info* info);
 int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int maxit, int prec,
                      sfh_cg_info* info);
+// two solves on the context's links at two masses, as one batch of two systems
+int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_eo[2], const double mass[2],
+                          double tol, int maxit, int prec, sfh_cg_info info[2]);
 void workspace_free(CgWorkspace* w);
 int ensure_scratch(sfh_ctx* c, int nfields);
 
