@@ -192,6 +192,25 @@ int sfh_smeared_fermion_force(sfh_ctx* ctx, const double* phi, double tol, int m
  * check = 1, which rejects a non-Hermitian P as the reference does;
  * Fermions.cpp:984-994 with check = 0). */
 int sfh_link_update(sfh_ctx* ctx, double eps, int check);
+/* Device time (ms per launch, CUDA events on the context's stream) of one HMC
+ * kernel on the context's current fields, a measurement aid with no
+ * counterpart in the reference: the gauge force with the momentum kick
+ * (compute_gauge_force_at_link, Fermions.cpp:372-384), the fermion force
+ * (Fermions.cpp:443-515) of the context's spinor work fields, the plaquette
+ * and rectangle staple sums (Lattice.cpp:249-499), the link update
+ * U <- exp(i eps P) U (Fermions.cpp:699-723) on a scratch copy, one stout level
+ * (rho 0.125), one level of the stout chain-rule force, the Symanzik action
+ * (Lattice.cpp:759-781) and the plaquette (Lattice.cpp:784-804).  Kicks use a
+ * zero step: the context's links and momenta are left as they were. */
+#define SFH_KERNEL_GAUGE_FORCE 0
+#define SFH_KERNEL_FERMION_FORCE 1
+#define SFH_KERNEL_STAPLES 2
+#define SFH_KERNEL_LINK_UPDATE 3
+#define SFH_KERNEL_STOUT_LEVEL 4
+#define SFH_KERNEL_STOUT_FORCE 5
+#define SFH_KERNEL_ACTION 6
+#define SFH_KERNEL_PLAQUETTE 7
+int sfh_kernel_timing(sfh_ctx* ctx, int kernel, int nrep, double* ms);
 /* sum over links of Re Tr P^2: compute_Tr_P2 (Fermions.cpp:662-678) */
 int sfh_trp2(sfh_ctx* ctx, double* out);
 /* Symanzik gauge action: compute_action (Lattice.cpp:759-781) */

@@ -34,6 +34,9 @@ SFH_ERR_INVALID = 7
 SFH_ERR_NOMEM = 8
 SFH_ERR_IO = 9
 FORCE_GAUGE = 1
+# sfh_kernel_timing's kernels (Lattice.HMC_KERNELS in the same order)
+(KERNEL_GAUGE_FORCE, KERNEL_FERMION_FORCE, KERNEL_STAPLES, KERNEL_LINK_UPDATE, KERNEL_STOUT_LEVEL,
+ KERNEL_STOUT_FORCE, KERNEL_ACTION, KERNEL_PLAQUETTE) = range(8)
 FORCE_FERMION = 2
 
 PREC_F64, PREC_F32, PREC_F16, PREC_F32_18, PREC_BF16 = 0, 1, 2, 3, 4
@@ -140,6 +143,7 @@ SIGNATURES = {
     "sfh_smear_stout": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int]),
     "sfh_smear_hex": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "sfh_hex_staples": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
+    "sfh_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -473,6 +477,17 @@ class Lattice:
     # --- smearing (Smearing.cpp) ---------------------------------------------
     def smear_stout(self, rho, n_levels=1):
         self._check(self.lib.sfh_smear_stout(self.h, rho, n_levels), "stout smearing")
+
+    HMC_KERNELS = ("gauge_force", "fermion_force", "staples", "link_update", "stout_level", "stout_force",
+                   "action", "plaquette")
+
+    def kernel_timing(self, kernel, nrep=10):
+        """ms per launch of one HMC kernel (a name of HMC_KERNELS) on the
+        context's fields, CUDA events on its stream."""
+        ms = ctypes.c_double(0.0)
+        self._check(self.lib.sfh_kernel_timing(self.h, self.HMC_KERNELS.index(kernel), nrep, ctypes.byref(ms)),
+                    "kernel_timing")
+        return ms.value
 
     def hex_staples(self, level, field):
         """apply_step_1 / apply_step_3 / apply_step_5 (Smearing.cpp:76-275) for

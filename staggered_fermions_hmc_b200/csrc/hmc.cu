@@ -630,6 +630,70 @@ extern "C" int sfh_smear_stout(sfh_ctx* c, double rho, int nlevels)
     return take_device_error(c, "stout smearing");
 }
 
+// Device time of one launch of an HMC kernel on the context's fields (CUDA
+// events on the context's stream, nrep timed launches after two untimed
+// ones).  Inputs are whatever the context holds; the kick forms use a zero
+// step, the link update runs on a scratch copy of the links, so the
+// context's gauge field and momenta are unchanged.
+extern "C" int sfh_kernel_timing(sfh_ctx* c, int kernel, int nrep, double* ms)
+{
+    if (!c || !ms || nrep < 1 || kernel < 0 || kernel > SFH_KERNEL_PLAQUETTE) return SFH_ERR_INVALID;
+    cudaSetDevice(c->device);
+    int st = ensure_scratch(c, 5);
+    if (st) return st;
+    void* s0 = scratch_field(c, 0);
+    void* s1 = scratch_field(c, 1);
+    void* lev[2] = {s0, s1};
+    void* lev_u[2] = {c->U64, s1};  // one stout level of the context's links into scratch
+    if (kernel == SFH_KERNEL_LINK_UPDATE || kernel == SFH_KERNEL_STOUT_FORCE)
+        st = cuda_check(c, cudaMemcpyAsync(s0, c->U64, link_bytes(c), cudaMemcpyDeviceToDevice, c->stream), "timing");
+    if (!st && kernel == SFH_KERNEL_STOUT_FORCE)
+        st = cuda_check(c, launch_stout_levels(c->g, lev, 0.125, 1, c->derr, c->stream), "timing");
+    if (st) return st;
+    auto launch = [&]() -> cudaError_t {
+        switch (kernel) {
+        case SFH_KERNEL_GAUGE_FORCE:
+            return launch_force(c->g, c->U64, nullptr, nullptr, c->beta, c->c11, c->c12, 1, nullptr, c->Pmom, 0.0,
+                                c->stream);
+        case SFH_KERNEL_FERMION_FORCE:
+            return launch_force(c->g, c->U64, c->spin[0], c->spin[1], c->beta, c->c11, c->c12, 2, nullptr, c->Pmom,
+                                0.0, c->stream);
+        case SFH_KERNEL_STAPLES:
+            return launch_staples(c->g, c->U64, c->Fbuf, s1, c->stream);
+        case SFH_KERNEL_LINK_UPDATE:
+            return launch_link_update(c->g, s0, c->Pmom, 1e-3, 0, c->derr, c->stream);
+        case SFH_KERNEL_STOUT_LEVEL:
+            return launch_stout_levels(c->g, lev_u, 0.125, 1, c->derr, c->stream);
+        case SFH_KERNEL_STOUT_FORCE:
+            return launch_stout_force(c->g, lev, 1, 0.125, c->Fbuf, scratch_field(c, 2), scratch_field(c, 3),
+                                      scratch_field(c, 4), c->derr, c->stream);
+        case SFH_KERNEL_ACTION:
+            return launch_reduce(c->g, RED_ACTION, c->U64, nullptr, c->beta, c->c11, c->c12, c->red, c->red + 2048,
+                                 c->stream);
+        default:
+            return launch_reduce(c->g, RED_PLAQ, c->U64, nullptr, c->beta, c->c11, c->c12, c->red, c->red + 2048,
+                                 c->stream);
+        }
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+    for (int k = 0; k < nrep && e == cudaSuccess; ++k) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st = cuda_check(c, e, "kernel timing");
+    if (st) return st;
+    *ms = (double)t / nrep;
+    return take_device_error(c, "kernel timing");
+}
+
 extern "C" int sfh_hex_staples(sfh_ctx* c, int level, const double* in, double* out)
 {
     if (!c || !in || !out || level < 1 || level > 3) return SFH_ERR_INVALID;

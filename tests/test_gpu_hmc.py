@@ -477,3 +477,22 @@ def test_hasenbusch_trajectory_second_order(sfh, orc, smear):
 
     d1, d2 = dH(0.04, 5), dH(0.02, 10)
     assert 3.5 < abs(d1) / abs(d2) < 4.5, (d1, d2)
+
+
+def test_kernel_timing_leaves_fields_unchanged(sfh, orc):
+    """sfh_kernel_timing times every HMC kernel on the context's fields and
+    leaves its links and momenta as they were (zero kicks, scratch copies)."""
+    dims = (8, 8, 8, 8)
+    lat = sfh.Lattice(dims, 0.1)
+    try:
+        U = orc.random_gauge(dims, 0.5, 151)
+        P = orc.random_momenta(dims, 152)
+        lat.upload_gauge(U)
+        lat.upload_momenta(P)
+        for name in lat.HMC_KERNELS:
+            ms = lat.kernel_timing(name, nrep=3)
+            assert 0.0 < ms < 1e3, name
+        assert np.array_equal(lat.download_gauge(), U)
+        assert np.array_equal(lat.download_momenta(), P)
+    finally:
+        lat.close()
