@@ -448,7 +448,8 @@ DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18", 4: "bf16_12"
 def run_extras(sfh, hbm, quick=False):
     """Secondary measurements on the other configurations of the workload
     family: Dslash GB/s at 32^3x64, the ill-conditioned 32^3x64 solve, the
-    16^4 precision grid, the 4^4 trajectory and a 24^4 trajectory."""
+    16^4 precision grid and the 4^4 trajectory (the 24^4 HMC configuration
+    is its own run: --workload c5)."""
     import oracle
     ex = {}
     # Dslash at 32^3x64 (eps = 1.0 links), one parity per hop, inputs >> L2
@@ -539,40 +540,125 @@ def run_extras(sfh, hbm, quick=False):
     ex["c1_4^4_trajectory"]["hmc"] = {"dH": info["dH"], "accepted": info["accepted"],
                                       "plaquette": info["plaquette"], "seconds": info["seconds"]}
     lat.close()
-    # 24^4 trajectories: beta 4.2, Hasenbusch pair m 0.02 / 0.2, fermion links
-    # with 4 stout levels (rho 0.125), tau = 1 with N = 20, after 20 heatbath
-    # sweeps from an eps = 0.3 start (the run keeps 2 of the 50 trajectories)
-    lat = sfh.Lattice((24, 24, 24, 24), 0.02, 4.2)
-    lat.random_gauge(0.3, 5)
-    t0 = time.perf_counter()
-    hb_plaq, _ = lat.heatbath_update(20, seed=5)
-    hb_s = time.perf_counter() - t0
-    lat.set_fermion_smearing(0.125, 4)
-    lat.set_hasenbusch(0.2)
-    trajs = []
-    for k in range(2):
-        # the mixed-precision trajectory, then the FP64 path from the same
-        # start with the same draws; the chain continues from the mixed one
-        U0 = lat.download_gauge()
-        info = lat.hmc_trajectory(1.0 / 20, 20, seed=100 + 10 * k, tol=TOL, precision="f32")
-        U1 = lat.download_gauge()
-        lat.upload_gauge(U0)
-        i64 = lat.hmc_trajectory(1.0 / 20, 20, seed=100 + 10 * k, tol=TOL, precision="f64")
-        lat.upload_gauge(U1)
-        trajs.append({"dH": info["dH"], "accepted": info["accepted"], "plaquette": info["plaquette"],
-                      "seconds": info["seconds"], "cg_iters": info["cg_iters"], "solves": info["solves"],
-                      "fp64_path": {"dH": i64["dH"], "accepted": i64["accepted"], "plaquette": i64["plaquette"],
-                                    "seconds": i64["seconds"], "cg_iters": i64["cg_iters"]},
-                      "dH_minus_fp64": info["dH"] - i64["dH"]})
-    poly = lat.precompute_polyakov_grid()
-    ex["c5_24^4_trajectory"] = {"heatbath_20_sweeps": {"seconds": hb_s, "plaquette": hb_plaq},
-                                "trajectories": trajs, "polyakov_mean": [float(poly.mean().real),
-                                                                          float(poly.mean().imag)],
-                                "trajectories_per_hour": 3600.0 / np.mean([t["seconds"] for t in trajs]),
-                                "action": "Symanzik gauge + Hasenbusch pair m 0.02/0.2 on 4-level stout "
-                                          "(rho 0.125) fermion links, mixed-precision f32 solves"}
-    lat.close()
     return ex
+
+
+# ---------------------------------------------------------------------------
+# C5: full HMC on 24^4 (bench.py --workload c5)
+# ---------------------------------------------------------------------------
+# algorithmic bytes and flops per link of the HMC kernels (FP64 links 144 B,
+# momenta 144 B, spinors 48 B per site = 24 B per link of the site):
+#   gauge force + kick   U in, P in and out; 84 staple matmuls + U V, 198 flop each
+#   fermion force + kick U, X, Y in, P in and out; two outer products and matmuls
+#   staples              U in, A1 and A2 out; 84 matmuls
+#   link update          U in and out, P in; exp(iQ) and one matmul
+#   stout level          U in, U' out; 12 plaquette-staple matmuls, exp, one matmul
+#   action, plaquette    U in; 84 / 12 staple matmuls and the traces
+HMC_KERNEL_COST = {  # (bytes, flops) per link
+    "gauge_force": (3 * 144, 85 * 198),
+    "fermion_force": (3 * 144 + 2 * 24, 4 * 198),
+    "staples": (3 * 144, 84 * 198),
+    "link_update": (3 * 144, 3 * 198 + 200),
+    "stout_level": (2 * 144, 14 * 198 + 200),
+    "action": (144, 85 * 198),
+    "plaquette": (144, 13 * 198),
+}
+FP64_TFLOPS_NOMINAL = 40.0  # B200 datasheet FP64 (no measured FP64 peak on this pool)
+
+
+def hmc_kernel_table(lat, hbm):
+    """ms per launch and roofline fractions of the HMC kernels on the
+    lattice's current fields."""
+    nlinks = 4 * lat.V
+    out = {}
+    for name in lat.HMC_KERNELS:
+        ms = lat.kernel_timing(name, nrep=10)
+        row = {"ms": ms}
+        if name in HMC_KERNEL_COST:
+            b, f = HMC_KERNEL_COST[name]
+            gbs = b * nlinks / (ms * 1e-3) / 1e9
+            tfs = f * nlinks / (ms * 1e-3) / 1e12
+            row.update({"GB/s": gbs, "frac_hbm": gbs / hbm, "TFLOP/s_fp64": tfs,
+                        "frac_fp64_nominal": tfs / FP64_TFLOPS_NOMINAL,
+                        "bound": "fp64" if f / b > FP64_TFLOPS_NOMINAL * 1e3 / hbm else "hbm"})
+        out[name] = row
+    return out
+
+
+def run_c5(args):
+    """24^4, beta 4.2, Hasenbusch pair m 0.02 / 0.2 on fermion links with 4
+    stout levels (rho 0.125), leapfrog tau = 1 with N = 20 steps, --c5-traj
+    trajectories from an eps = 0.3 start; the same chain with FP64 solves from
+    the same start and seeds beside it; a step-size scan of dH; the HMC
+    kernels' device times."""
+    import staggered_fermions_hmc_b200 as sfh
+    sfh.load_library()
+    hbm, peak_kind = peaks()
+    dims, N, ntraj = (24, 24, 24, 24), args.c5_steps, args.c5_traj
+
+    def new_lattice():
+        lat = sfh.Lattice(dims, 0.02, 4.2)
+        lat.random_gauge(0.3, 5)
+        lat.set_fermion_smearing(0.125, 4)
+        lat.set_hasenbusch(0.2)
+        return lat
+
+    def chain(precision):
+        lat = new_lattice()
+        rows, poly = [], []
+        for k in range(ntraj):
+            inf = lat.hmc_trajectory(1.0 / N, N, seed=1000 + k, tol=TOL, precision=precision)
+            g = lat.precompute_polyakov_grid()
+            parts = [f - i for f, i in zip(inf["H_final"], inf["H_initial"])]
+            rows.append({"dH": inf["dH"], "dH_kinetic": parts[0], "dH_gauge": parts[1], "dH_fermion": parts[2],
+                         "accepted": inf["accepted"], "plaquette": inf["plaquette"], "seconds": inf["seconds"],
+                         "cg_iters": inf["cg_iters"], "solves": inf["solves"]})
+            poly.append(complex(g.mean()))
+        return lat, rows, poly
+
+    def summary(rows, poly):
+        acc = [r["accepted"] for r in rows]
+        return {"trajectories": len(rows), "acceptance": float(np.mean(acc)),
+                "plaquette_mean": float(np.mean([r["plaquette"] for r in rows])),
+                "plaquette_conventional_mean": float(np.mean([r["plaquette"] for r in rows])) / 6.0,
+                "polyakov_mean": [float(np.mean([p.real for p in poly])), float(np.mean([p.imag for p in poly]))],
+                "dH_mean": float(np.mean([r["dH"] for r in rows])),
+                "dH_parts_mean": {k: float(np.mean([r[k] for r in rows]))
+                                  for k in ("dH_kinetic", "dH_gauge", "dH_fermion")},
+                "seconds_per_trajectory": float(np.mean([r["seconds"] for r in rows])),
+                "trajectories_per_hour": 3600.0 / float(np.mean([r["seconds"] for r in rows])),
+                "cg_iters_per_trajectory": float(np.mean([r["cg_iters"] for r in rows]))}
+
+    lat, mixed, pmix = chain(args.c5_precision)
+    kernels = hmc_kernel_table(lat, hbm)
+    lat.close()
+    lat, f64, p64 = chain("f64")
+    lat.close()
+    same = [a["accepted"] == b["accepted"] for a, b in zip(mixed, f64)]
+    # step-size scan from the start configuration, same momenta and
+    # pseudofermions: dH ~ eps^2 for a second-order integrator
+    scan = {}
+    for n in (N, 2 * N, 4 * N):
+        lat = new_lattice()
+        inf = lat.hmc_trajectory(1.0 / n, n, seed=1000, tol=TOL, precision=args.c5_precision)
+        scan[str(n)] = {"eps": 1.0 / n, "dH": inf["dH"]}
+        lat.close()
+    ns = sorted(int(n) for n in scan)
+    ratios = [scan[str(a)]["dH"] / scan[str(b)]["dH"] for a, b in zip(ns, ns[1:])]
+    line = {
+        "metric": "C5 full HMC on 24^4: trajectories/hour, acceptance, plaquette, Polyakov loop vs the FP64 path",
+        "workload": "24^4, Symanzik beta 4.2, Hasenbusch pair m 0.02 / 0.2 on 4-level stout (rho 0.125) fermion "
+                    f"links, leapfrog tau = 1 with {N} steps, {ntraj} trajectories from an eps = 0.3 start "
+                    "(seed 5), no heatbath",
+        "precision": {"mixed": args.c5_precision, "arithmetic": ARITHMETIC[args.c5_precision]},
+        "mixed": summary(mixed, pmix), "fp64": summary(f64, p64),
+        "accept_decisions_equal": float(np.mean(same)),
+        "dH_mixed_minus_fp64_max": float(max(abs(a["dH"] - b["dH"]) for a, b in zip(mixed, f64))),
+        "step_size_scan": {"dH": scan, "ratios_per_halving": ratios},
+        "hmc_kernels_24^4": kernels, "peak_hbm": hbm, "peak_kind": peak_kind,
+        "per_trajectory_mixed": mixed,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_profile_case(args, spec):
@@ -614,8 +700,16 @@ def main():
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
     ap.add_argument("--maxit", type=int, default=MAXIT)
+    ap.add_argument("--workload", default="batch", choices=["batch", "c5"],
+                    help="batch: the headline uneven-batch CG (default); c5: full HMC on 24^4, its own JSON line")
+    ap.add_argument("--c5-traj", type=int, default=50)
+    ap.add_argument("--c5-steps", type=int, default=20)
+    ap.add_argument("--c5-precision", default="f32", choices=["f32", "f16", "bf16", "f32_18"])
     args = ap.parse_args()
     spec = batch_spec(nsys=args.nsys)
+    if args.workload == "c5":
+        run_c5(args)
+        return
     if args.profile_case:
         run_profile_case(args, spec)
         return
