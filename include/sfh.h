@@ -308,7 +308,7 @@ void* sfh_batch_get_stream(sfh_batch* batch);
 int sfh_batch_set_rhs_block(sfh_batch* batch, int width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
  * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
- * (0, 1, 2 as below; FP64: 0) on the batch's current inputs and keep the
+ * (0 to 3 as below; FP64: 0) on the batch's current inputs and keep the
  * fastest.
  * The schedule never changes the results.  No counterpart in the reference
  * (its solver has no schedule). */
@@ -319,9 +319,13 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * item with asynchronous copies; 2 system-blocked: one block per tile serves
  * every RHS of its system in groups of the RHS-block width, the tile's links
  * read once into shared memory (FP16 unpacked), the tiles per block fixed at
- * 1, and the FP64 reliable-update hops in two kernels of their own (FP16,
- * BF16 and FP32 12-real storage; FP32 18-real takes 1).  Staging applies to
- * the reduced precisions only.  And its current values. */
+ * 1, and the FP64 reliable-update hops in two kernels of their own; 3
+ * persistent: the same per-tile work in one cooperative launch for the whole
+ * solve, its phases separated by a grid barrier whose waits are bounded (a
+ * wait that gives up fails the solve with SFH_ERR_TIMEOUT); the solutions
+ * equal those of 2 bit for bit.  2 and 3 serve FP16, BF16 and FP32 12-real
+ * storage (FP32 18-real takes 1).  Staging applies to the reduced precisions
+ * only.  And its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Reliable-update threshold of the mixed precisions (default 0.1 for
  * the 16-bit storages, 0.01 for the FP32 ones): an FP64
@@ -343,13 +347,15 @@ int sfh_batch_get_rhs(sfh_batch* batch, int sys, int rhs, double* phi);
 /* number of kernels the last sfh_batch_solve launched (init + graph chunks) */
 int sfh_batch_kernel_launches(sfh_batch* batch, long* n);
 /* sfh_batch_solve with the iteration kernels launched one by one between CUDA
- * events on the batch's stream (no graph replay): ms5 / n5 (five entries)
- * receive the summed device time and launch count of each kernel: t = K p;
- * v = m^2 p - K t with the CG sums; the x, r, p update; and, with the
- * system-blocked schedule, the two FP64 reliable-update kernels (zero
- * otherwise: the hop kernels do those hops).  Same kernels, same results; a
- * measurement aid with no counterpart in the reference. */
-int sfh_batch_solve_timed(sfh_batch* batch, double tol, int maxit, double* ms5, long* n5);
+ * events on the batch's stream (no graph replay): ms / n (SFH_TIMED_KERNELS
+ * entries) receive the summed device time and launch count of each kernel:
+ * t = K p; v = m^2 p - K t with the CG sums; the x, r, p update; with the
+ * system-blocked schedule the two FP64 reliable-update kernels (zero
+ * otherwise: the hop kernels do those hops); and with the persistent schedule
+ * the one cooperative launch (the others zero).  Same kernels, same results;
+ * a measurement aid with no counterpart in the reference. */
+#define SFH_TIMED_KERNELS 6
+int sfh_batch_solve_timed(sfh_batch* batch, double tol, int maxit, double* ms, long* n);
 /* FP64 |b - D D^dag x| / |b| for one solution (diagnostic) */
 int sfh_batch_true_residual(sfh_batch* batch, int sys, int rhs, double* rel);
 

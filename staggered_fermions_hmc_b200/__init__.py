@@ -175,6 +175,7 @@ SIGNATURES = {
 }
 
 NOALLOC_MAX_SITES = 65536
+TIMED_KERNELS = 6
 
 _lib = None
 
@@ -557,17 +558,19 @@ class Batch:
     def solve_timed(self, tol=1e-10, max_iter=20000):
         """Solve with per-kernel CUDA-event timing; returns {kernel: (ms, launches)}
         for the kernels the schedule launched (the reliable-update kernels
-        cg_ru1 / cg_ru2 with the system-blocked schedule only)."""
-        ms = np.zeros(5)
-        n = (ctypes.c_long * 5)()
+        cg_ru1 / cg_ru2 with the system-blocked schedule only; cg_persistent
+        alone with the persistent schedule)."""
+        ms = np.zeros(TIMED_KERNELS)
+        n = (ctypes.c_long * TIMED_KERNELS)()
         self._check(self.lib.sfh_batch_solve_timed(self.h, tol, max_iter, _dptr(ms), n), "solve_timed")
-        names = ("cg_hop1", "cg_hop2", "cg_update", "cg_ru1", "cg_ru2")
-        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names) if i < 3 or n[i] > 0}
+        names = ("cg_hop1", "cg_hop2", "cg_update", "cg_ru1", "cg_ru2", "cg_persistent")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(names) if n[i] > 0}
 
     def set_schedule(self, width, tiles_per_block, stage_links=0):
         """stage_links: 0 (or False) links read directly, 1 (or True) staged per
         work item, 2 system-blocked (one tile per block serving every RHS of
-        the system, links read once per tile)."""
+        the system, links read once per tile), 3 the system-blocked work in
+        one persistent cooperative launch."""
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
 

@@ -204,7 +204,7 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
-template <int GP, int SP, int NB, bool STG>
+template <int GP, int SP, int NB, bool STG, bool COH = false>
 __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeFmt<GP>::E* sl, const Nbr& n, int q,
                                           int i, int Vh, const void* const (&in)[NB], const bool (&on)[NB],
                                           Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
@@ -226,11 +226,11 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
             hlink_load<STG>(sl, kTile, Ulo, 2 * mu, q, mu, i, Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<false>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
+                if (on[l]) hop_half<false, COH>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
             hlink_load<STG>(sl, kTile, Ulo, 2 * mu + 1, nq, mu, n.dn[mu], Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<true>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
+                if (on[l]) hop_half<true, COH>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
         }
         return;
     }
@@ -244,9 +244,9 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
                     if constexpr (direct) {
-                        mv_add<false>(acc[l], U, hop_input<SP>(in[l], nq, n.up[mu], Vh, n.wu && mu == 3, s));
+                        mv_add<false>(acc[l], U, hop_input<SP, R, COH>(in[l], nq, n.up[mu], Vh, n.wu && mu == 3, s));
                     } else {
-                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.up[mu], Vh));
+                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::template load<COH>(in[l], nq, n.up[mu], Vh));
                         if (mu == 3) v = vneg_if(v, n.wu);
                         mv_add<true>(w[l], U, v);
                     }
@@ -258,9 +258,9 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
             for (int l = 0; l < NB; ++l)
                 if (on[l]) {
                     if constexpr (direct) {
-                        mdv_sub(acc[l], U, hop_input<SP>(in[l], nq, n.dn[mu], Vh, n.wd && mu == 3, s));
+                        mdv_sub(acc[l], U, hop_input<SP, R, COH>(in[l], nq, n.dn[mu], Vh, n.wd && mu == 3, s));
                     } else {
-                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::load(in[l], nq, n.dn[mu], Vh));
+                        Vec3<R> v = vcvt<R>(SpinorFmt<SP>::template load<COH>(in[l], nq, n.dn[mu], Vh));
                         if (mu == 3) v = vneg_if(v, n.wd);
                         mdv_sub(w[l], U, v);
                     }
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
 }
 
 // FP64 hop of x_hi + x_lo for a lane in a reliable update: thi = K x
-template <int XP>
+template <int XP, bool COH = false>
 __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     const int nq = 1 - q, Vh = S.g.Vh;
@@ -497,14 +497,14 @@ __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const C
         const bool wd = (mu == 3) && (c.x[3] == 0);
         {
             Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, lu, Vh), 1.0,
-                                   vcvt<double>(SpinorFmt<XP>::load(xlo, nq, lu, Vh)));
+            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::template load<COH>(xhi, nq, lu, Vh), 1.0,
+                                   vcvt<double>(SpinorFmt<XP>::template load<COH>(xlo, nq, lu, Vh)));
             vacc(acc, mul_mv(U, x), eta_neg != wu);
         }
         {
             Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::load(xhi, nq, ld, Vh), 1.0,
-                                   vcvt<double>(SpinorFmt<XP>::load(xlo, nq, ld, Vh)));
+            Vec3<double> x = vaxpy(SpinorFmt<SP_F64>::template load<COH>(xhi, nq, ld, Vh), 1.0,
+                                   vcvt<double>(SpinorFmt<XP>::template load<COH>(xlo, nq, ld, Vh)));
             vacc(acc, mul_adj_mv(U, x), !(eta_neg != wd));
         }
     }
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
 
 // reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
 // r = b - M x_hi; returns the |r|^2 contribution (FP64)
-template <int SP, int XP>
+template <int SP, int XP, bool COH = false>
 __device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const Coord& c, int q, int i, int rid)
 {
     typedef typename SpinorFmt<SP>::R RS;
@@ -597,9 +597,9 @@ __device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const 
         const bool wu = (mu == 3) && (c.x[3] == S.g.L[3] - 1);
         const bool wd = (mu == 3) && (c.x[3] == 0);
         Mat3<double> U = GaugeFmt<GP_F64_18>::load(S.U64, q, mu, i, Vh);
-        vacc(acc, mul_mv(U, SpinorFmt<SP_F64>::load(thi, nq, lu, Vh)), eta_neg != wu);
+        vacc(acc, mul_mv(U, SpinorFmt<SP_F64>::template load<COH>(thi, nq, lu, Vh)), eta_neg != wu);
         Mat3<double> Ud = GaugeFmt<GP_F64_18>::load(S.U64, nq, mu, ld, Vh);
-        vacc(acc, mul_adj_mv(Ud, SpinorFmt<SP_F64>::load(thi, nq, ld, Vh)), !(eta_neg != wd));
+        vacc(acc, mul_adj_mv(Ud, SpinorFmt<SP_F64>::template load<COH>(thi, nq, ld, Vh)), !(eta_neg != wd));
     }
     void* xhi = rhs_ptr(a, rid, F_XHI);
     void* xlo = rhs_ptr(a, rid, F_XLO);
@@ -757,16 +757,14 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
 
 // own sites of one lane (work item: tpi tiles, one RHS) if ACTIVE:
 // x += alpha p, r -= alpha v, p = r + beta p
-template <int SP>
-__global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restrict__ items, int cur)
+template <int SP, bool COH>
+__device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, CgSys* s_sys)
 {
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
     typedef typename SpinorFmt<XP>::R RX;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
+    stage_sys(a, it.x, s_sys);
+    const CgSys& S = *s_sys;
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
     CgLane* L = a.lanes + lane_of(S, it.y, q, false);
@@ -789,15 +787,22 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restr
     for (int t = ir.first; t < ir.end; ++t) {
         const TileInfo ti = decode_tile(S, t);
         if (!ti.valid) break;
-        Vec3<RS> p = SpinorFmt<SP>::load(pp, q, ti.i, Vh);
-        Vec3<RS> r = SpinorFmt<SP>::load(rp, q, ti.i, Vh);
-        Vec3<RS> v = SpinorFmt<SP>::load(vp, q, ti.i, Vh);
-        Vec3<RX> x = SpinorFmt<XP>::load(xp, q, ti.i, Vh);
+        Vec3<RS> p = SpinorFmt<SP>::template load<COH>(pp, q, ti.i, Vh);
+        Vec3<RS> r = SpinorFmt<SP>::template load<COH>(rp, q, ti.i, Vh);
+        Vec3<RS> v = SpinorFmt<SP>::template load<COH>(vp, q, ti.i, Vh);
+        Vec3<RX> x = SpinorFmt<XP>::template load<COH>(xp, q, ti.i, Vh);
         SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
         Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
         SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
         SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
     }
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    __shared__ CgSys s_sys;
+    update_body<SP, false>(a, items[blockIdx.x], cur, &s_sys);
 }
 
 // ---------------------------------------------------------------------------
@@ -862,7 +867,7 @@ __device__ __forceinline__ void hlink_smem(const uint32_t* s, int d, __half2 (&e
 
 // acc[l] += K in_l at the site for the lanes with on[l], links from the
 // tile's staging area (unpacked FP16, or as stored for the other formats)
-template <int GP, int SP, int NB>
+template <int GP, int SP, int NB, bool COH>
 __device__ __forceinline__ void hop_lanes_sys(const void* Ulo, const void* stage, const Nbr& n, int q, int i,
                                               int Vh, const void* const (&in)[NB], const bool (&on)[NB],
                                               Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
@@ -877,14 +882,14 @@ __device__ __forceinline__ void hop_lanes_sys(const void* Ulo, const void* stage
             hlink_smem(sl, 2 * mu, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<false>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
+                if (on[l]) hop_half<false, COH>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
             hlink_smem(sl, 2 * mu + 1, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<true>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
+                if (on[l]) hop_half<true, COH>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
         }
     } else {
-        hop_lanes<GP, SP, NB, true>(Ulo, (const typename GaugeFmt<GP>::E*)stage, n, q, i, Vh, in, on, acc);
+        hop_lanes<GP, SP, NB, true, COH>(Ulo, (const typename GaugeFmt<GP>::E*)stage, n, q, i, Vh, in, on, acc);
     }
 }
 
@@ -914,25 +919,21 @@ __device__ __forceinline__ void scan_lanes(const CgArgs& a, const CgSys& S, int 
 }
 
 // hop1, system-blocked: t = K p for every active lane of the system on one
-// tile (the lanes in a reliable update are cg_ru1_sys's)
-template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (SysOcc<GP, false>::v)) cg_hop1_sys(CgArgs a, const int2* __restrict__ items,
-                                                                              int cur)
+// tile (the lanes in a reliable update are ru1's)
+template <int GP, int SP, int NB, bool COH>
+__device__ __forceinline__ void hop1_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys, void* stage)
 {
-    extern __shared__ __align__(16) unsigned char s_dyn[];
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
+    stage_sys(a, tile, s_sys);
+    const CgSys& S = *s_sys;
+    const TileInfo ti = decode_tile(S, tile);
     const int q = ti.q, Vh = S.g.Vh;
     bool anyA, anyR;
     scan_lanes(a, S, q, true, cur, &anyA, &anyR);
     if (!anyA || !ti.valid) return;  // no barrier below
     const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
-    stage_tile_links<GP, SP>(s_dyn, S.Ulo, n, q, ti.i, Vh);
+    stage_tile_links<GP, SP>(stage, S.Ulo, n, q, ti.i, Vh);
     for (int base = 0; base < S.nrhs; base += NB) {
         LanePass<NB> P;
         gather_pass<NB>(a, S, base, q, true, cur, false, P);
@@ -947,7 +948,7 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, false>::v)) cg_hop1_sys(CgA
         Vec3<R> acc[NB];
 #pragma unroll
         for (int l = 0; l < NB; ++l) vzero(acc[l]);
-        hop_lanes_sys<GP, SP, NB>(S.Ulo, s_dyn, n, q, ti.i, Vh, pin, on, acc);
+        hop_lanes_sys<GP, SP, NB, COH>(S.Ulo, stage, n, q, ti.i, Vh, pin, on, acc);
 #pragma unroll
         for (int l = 0; l < NB; ++l)
             if (on[l]) SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_T), q, ti.i, Vh, vcvt<RS>(acc[l]));
@@ -976,26 +977,19 @@ __device__ __forceinline__ void rows_sum(const float (&v)[F], float (*red)[kTile
 }
 
 // hop2, system-blocked: v = m^2 p - K t and the four CG sums for every active
-// lane of the system on one tile (the lanes in a reliable update are
-// cg_ru2_sys's)
-template <int GP, int SP, int NB>
-__global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgArgs a, const int2* __restrict__ items,
-                                                                             int cur)
+// lane of the system on one tile (the lanes in a reliable update are ru2's)
+template <int GP, int SP, int NB, bool COH>
+__device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys, void* stage,
+                                              float (*s_red)[kTile], double* s_tot, unsigned* s_mask)
 {
-    extern __shared__ __align__(16) unsigned char s_dyn[];
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     static_assert(sizeof(RS) == 4, "system-blocked kernels serve the reduced precisions");
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    __shared__ float s_red[NB * kSums][kTile];
-    __shared__ double s_tot[NB * kSums];
-    __shared__ unsigned s_mask;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
+    stage_sys(a, tile, s_sys);
+    const CgSys& S = *s_sys;
+    const TileInfo ti = decode_tile(S, tile);
     const int q = ti.q, Vh = S.g.Vh;
-    const ItemRange ir = item_range(a, S, it.x);
+    const ItemRange ir = item_range(a, S, tile);
     const unsigned nsq = (unsigned)item_groups(a, S);
     bool anyA, anyR;
     scan_lanes(a, S, q, false, cur, &anyA, &anyR);
@@ -1003,7 +997,7 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgAr
     Nbr n;
     if (ti.valid) {
         n = neighbours(S.g, eo_coords(S.g, q, ti.i));
-        stage_tile_links<GP, SP>(s_dyn, S.Ulo, n, q, ti.i, Vh);
+        stage_tile_links<GP, SP>(stage, S.Ulo, n, q, ti.i, Vh);
     }
     const R m2 = (R)S.m2;
     for (int base = 0; base < S.nrhs; base += NB) {
@@ -1024,16 +1018,16 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgAr
             Vec3<R> acc[NB];
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
-            hop_lanes_sys<GP, SP, NB>(S.Ulo, s_dyn, n, q, ti.i, Vh, tin, on, acc);
+            hop_lanes_sys<GP, SP, NB, COH>(S.Ulo, stage, n, q, ti.i, Vh, tin, on, acc);
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
                 if (!on[l]) continue;
-                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+                Vec3<RS> r = SpinorFmt<SP>::template load<COH>(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
                 Vec3<RS> p = r;
                 if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
                     SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
                 else
-                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+                    p = SpinorFmt<SP>::template load<COH>(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
                 Vec3<R> pr = vcvt<R>(p), w;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -1052,7 +1046,7 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgAr
         double sums[NB * kSums];
 #pragma unroll
         for (int f = 0; f < NB * kSums; ++f) sums[f] = s_tot[f];
-        const unsigned mask = arrive_sums<NB>(a, S, P, on, sums, ir.slot, nsq, &s_mask);
+        const unsigned mask = arrive_sums<NB>(a, S, P, on, sums, ir.slot, nsq, s_mask);
         if (mask && threadIdx.x < 32) {
 #pragma unroll
             for (int l = 0; l < NB; ++l)
@@ -1067,15 +1061,13 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgAr
 // ru1: thi = K (x_hi + x_lo) at output parity q for the lanes of parity
 // 1 - q; ru2: x_hi += x_lo, r = b - M x_hi and |r|^2 for the lanes of parity
 // q, whose partial sums complete the lanes' tickets.
-template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru1_sys(CgArgs a, const int2* __restrict__ items, int cur)
+template <int SP, bool COH>
+__device__ __forceinline__ void ru1_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys)
 {
     constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
+    stage_sys(a, tile, s_sys);
+    const CgSys& S = *s_sys;
+    const TileInfo ti = decode_tile(S, tile);
     bool anyA, anyR;
     scan_lanes(a, S, ti.q, true, cur, &anyA, &anyR);
     if (!anyR || !ti.valid) return;
@@ -1083,26 +1075,23 @@ __global__ void __launch_bounds__(kTile) cg_ru1_sys(CgArgs a, const int2* __rest
 #pragma unroll 1
     for (int r = 0; r < S.nrhs; ++r) {
         const CgLane* L = a.lanes + lane_of(S, r, ti.q, true);
-        if (ld_int(&L->mode[cur]) == LM_RU) ru_hop1<XP>(a, S, c, ti.q, ti.i, __ldg(&L->rhs));
+        if (ld_int(&L->mode[cur]) == LM_RU) ru_hop1<XP, COH>(a, S, c, ti.q, ti.i, __ldg(&L->rhs));
     }
 }
 
-template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru2_sys(CgArgs a, const int2* __restrict__ items, int cur)
+template <int SP, bool COH>
+__device__ __forceinline__ void ru2_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys, double* s_bs,
+                                             unsigned* s_mask)
 {
     constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
-    __shared__ CgSys s_sys;
-    __shared__ double smem[32];
-    __shared__ unsigned s_mask;
-    stage_sys(a, it.x, &s_sys);
-    const CgSys& S = s_sys;
-    const TileInfo ti = decode_tile(S, it.x);
+    stage_sys(a, tile, s_sys);
+    const CgSys& S = *s_sys;
+    const TileInfo ti = decode_tile(S, tile);
     const int q = ti.q;
     bool anyA, anyR;
     scan_lanes(a, S, q, false, cur, &anyA, &anyR);
     if (!anyR) return;  // uniform in the block
-    const ItemRange ir = item_range(a, S, it.x);
+    const ItemRange ir = item_range(a, S, tile);
     const unsigned nsq = (unsigned)item_groups(a, S);
     const Coord c = eo_coords(S.g, q, ti.valid ? ti.i : 0);
 #pragma unroll 1
@@ -1111,12 +1100,140 @@ __global__ void __launch_bounds__(kTile) cg_ru2_sys(CgArgs a, const int2* __rest
         gather_pass<1>(a, S, r, q, false, cur, false, P);
         if (P.mode[0] != LM_RU) continue;
         double sums[kSums] = {0.0, 0.0, 0.0, 0.0};
-        if (ti.valid) sums[3] = ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[0]);
-        block_sum<kSums>(sums, smem);
+        if (ti.valid) sums[3] = ru_hop2<SP, XP, COH>(a.rhs, S, c, q, ti.i, P.rid[0]);
+        block_sum<kSums>(sums, s_bs);
         const bool part[1] = {true};
-        const unsigned mask = arrive_sums<1>(a, S, P, part, sums, ir.slot, nsq, &s_mask);
+        const unsigned mask = arrive_sums<1>(a, S, P, part, sums, ir.slot, nsq, s_mask);
         if (mask && threadIdx.x < 32) finish_lane(a, S, P.lane[0], P.mode[0], cur);
         __syncthreads();
+    }
+}
+
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, (SysOcc<GP, false>::v)) cg_hop1_sys(CgArgs a, const int2* __restrict__ items,
+                                                                              int cur)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ CgSys s_sys;
+    hop1_sys_body<GP, SP, NB, false>(a, items[blockIdx.x].x, cur, &s_sys, s_dyn);
+}
+
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgArgs a, const int2* __restrict__ items,
+                                                                             int cur)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ CgSys s_sys;
+    __shared__ float s_red[NB * kSums][kTile];
+    __shared__ double s_tot[NB * kSums];
+    __shared__ unsigned s_mask;
+    hop2_sys_body<GP, SP, NB, false>(a, items[blockIdx.x].x, cur, &s_sys, s_dyn, s_red, s_tot, &s_mask);
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru1_sys(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    __shared__ CgSys s_sys;
+    ru1_sys_body<SP, false>(a, items[blockIdx.x].x, cur, &s_sys);
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru2_sys(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    __shared__ CgSys s_sys;
+    __shared__ double s_bs[32];
+    __shared__ unsigned s_mask;
+    ru2_sys_body<SP, false>(a, items[blockIdx.x].x, cur, &s_sys, s_bs, &s_mask);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent batched CG: the whole solve in one cooperative launch.  Every
+// block walks the work items of each phase (grid-stride), the phases of an
+// iteration separated by a grid barrier: {hop1, ru1}, {hop2, ru2}, update
+// (hop1 and ru1 touch different lanes, as do hop2 and ru2, so each pair
+// shares a phase).  The per-tile bodies are those of the system-blocked
+// kernels, with every load of data written during the solve taken through
+// L2 (coherent across the blocks), so the solutions equal the graph path's
+// bit for bit.  The grid barrier waits a bounded number of polls; a block
+// that gives up sets the error word and returns, and the others follow at
+// their next wait.
+// ---------------------------------------------------------------------------
+struct GridBar {
+    unsigned count, gen;
+    int err;  // set when a wait gave up
+    unsigned pad;
+};
+
+constexpr long long kBarrierPolls = 1ll << 25;  // about 4 s at the 128 ns back-off
+
+__device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblocks, int* s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &b->gen;
+        volatile int* verr = &b->err;
+        int ok = *verr == 0;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (ok) {
+            if (atomicAdd(&b->count, 1u) == nblocks - 1) {
+                atomicExch(&b->count, 0u);
+                __threadfence();
+                atomicAdd(&b->gen, 1u);
+            } else {
+                long long polls = 0;
+                while (*vgen == g) {
+                    if (*verr != 0 || ++polls > kBarrierPolls) {
+                        atomicOr(&b->err, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(128);
+                }
+            }
+        }
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+template <int GP, int SP, int NB>
+__global__ void __launch_bounds__(kTile, 2) cg_persistent_sys(CgArgs a, const int2* __restrict__ hop_items, int nhop,
+                                                              const int2* __restrict__ upd_items, int nupd,
+                                                              GridBar* bar)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ CgSys s_sys;
+    __shared__ float s_red[NB * kSums][kTile];
+    __shared__ double s_tot[NB * kSums];
+    __shared__ double s_bs[32];
+    __shared__ unsigned s_mask;
+    __shared__ int s_ok;
+    const unsigned nblk = gridDim.x;
+    for (int it = 0; it < a.maxloop; ++it) {
+        if (ld_int(a.n_active) <= 0) break;  // read after the last barrier: the same in every block
+        const int cur = it & 1;
+        for (int k = blockIdx.x; k < nhop; k += gridDim.x) {
+            __syncthreads();
+            hop1_sys_body<GP, SP, NB, true>(a, hop_items[k].x, cur, &s_sys, s_dyn);
+            __syncthreads();
+            ru1_sys_body<SP, true>(a, hop_items[k].x, cur, &s_sys);
+        }
+        if (!grid_barrier(bar, nblk, &s_ok)) return;
+        for (int k = blockIdx.x; k < nhop; k += gridDim.x) {
+            __syncthreads();
+            hop2_sys_body<GP, SP, NB, true>(a, hop_items[k].x, cur, &s_sys, s_dyn, s_red, s_tot, &s_mask);
+            __syncthreads();
+            ru2_sys_body<SP, true>(a, hop_items[k].x, cur, &s_sys, s_bs, &s_mask);
+        }
+        if (!grid_barrier(bar, nblk, &s_ok)) return;
+        for (int k = blockIdx.x; k < nupd; k += gridDim.x) {
+            __syncthreads();
+            update_body<SP, true>(a, upd_items[k], cur, &s_sys);
+        }
+        if (!grid_barrier(bar, nblk, &s_ok)) return;
     }
 }
 
@@ -1131,7 +1248,8 @@ typedef void (*HopKernel)(CgArgs, const int2*, int);
 
 // the kernels of one CG iteration, in launch order, with their work items
 // and timing slots
-enum { PH_HOP1 = 0, PH_HOP2 = 1, PH_UPDATE = 2, PH_RU1 = 3, PH_RU2 = 4, kTimedPhases = 5 };
+enum { PH_HOP1 = 0, PH_HOP2 = 1, PH_UPDATE = 2, PH_RU1 = 3, PH_RU2 = 4, PH_PERSISTENT = 5, kTimedPhases = 6 };
+typedef void (*PersKernel)(CgArgs, const int2*, int, const int2*, int, GridBar*);
 constexpr int kMaxPhases = 5;
 
 struct CgKernels {
@@ -1141,6 +1259,7 @@ struct CgKernels {
     int nb1, nb2;   // RHS widths of the hop kernels' work items
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
     bool sys;       // system-blocked hop kernels (one tile per block, every RHS)
+    PersKernel pers;  // the whole solve in one cooperative launch (or null)
 };
 
 struct Phase {
@@ -1166,7 +1285,7 @@ static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
 constexpr int kSysItems = 1 << 20;
 
 template <int GP, int SP>
-static CgKernels pick_sys(int nb)
+static CgKernels pick_sys(int nb, bool persistent)
 {
     CgKernels k;
     // FP32 arithmetic on FP32 links keeps at most four accumulators in
@@ -1174,8 +1293,18 @@ static CgKernels pick_sys(int nb)
     if (nb >= 4) { k.hop1 = cg_hop1_sys<GP, SP, 4>; k.hop2 = cg_hop2_sys<GP, SP, 4>; }
     else if (nb >= 2) { k.hop1 = cg_hop1_sys<GP, SP, 2>; k.hop2 = cg_hop2_sys<GP, SP, 2>; }
     else { k.hop1 = cg_hop1_sys<GP, SP, 1>; k.hop2 = cg_hop2_sys<GP, SP, 1>; }
+    k.pers = nullptr;
+    if (persistent) {
+        if (nb >= 4) k.pers = cg_persistent_sys<GP, SP, 4>;
+        else if (nb >= 2) k.pers = cg_persistent_sys<GP, SP, 2>;
+        else k.pers = cg_persistent_sys<GP, SP, 1>;
+    }
     if constexpr (SysStage<GP, SP>::unpacked) {
-        if (nb >= 8) { k.hop1 = cg_hop1_sys<GP, SP, 8>; k.hop2 = cg_hop2_sys<GP, SP, 8>; }
+        if (nb >= 8) {
+            k.hop1 = cg_hop1_sys<GP, SP, 8>;
+            k.hop2 = cg_hop2_sys<GP, SP, 8>;
+            if (persistent) k.pers = cg_persistent_sys<GP, SP, 8>;
+        }
     }
     k.init = cg_init<SP, 2>;
     k.update = cg_update<SP>;
@@ -1221,6 +1350,7 @@ static CgKernels pick_typed(int nb1, int nb2)
     k.ru1 = k.ru2 = nullptr;  // the reliable-update hops run inside hop1 / hop2
     k.smem = STG ? StageBytes<GP>::v : 0;
     k.sys = false;
+    k.pers = nullptr;
     return k;
 }
 
@@ -1235,14 +1365,16 @@ static CgKernels pick_staged(int nb1, int nb2, bool stage)
 }
 
 // stage: 0 links read directly, 1 staged per work item, 2 system-blocked
-// kernels (FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
+// kernels, 3 the system-blocked bodies in one persistent cooperative launch
+// (2 and 3: FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
 static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
 {
     CgKernels k;
+    const bool sys = stage >= 2, pers = stage == 3;
     if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false);
-    else if (stage == 2 && prec == SFH_PREC_F16) k = pick_sys<GP_F16_12, SP_F16>(nb1);
-    else if (stage == 2 && prec == SFH_PREC_BF16) k = pick_sys<GP_BF16_12, SP_BF16>(nb1);
-    else if (stage == 2 && prec == SFH_PREC_F32) k = pick_sys<GP_F32_12, SP_F32>(nb1);
+    else if (sys && prec == SFH_PREC_F16) k = pick_sys<GP_F16_12, SP_F16>(nb1, pers);
+    else if (sys && prec == SFH_PREC_BF16) k = pick_sys<GP_BF16_12, SP_BF16>(nb1, pers);
+    else if (sys && prec == SFH_PREC_F32) k = pick_sys<GP_F32_12, SP_F32>(nb1, pers);
     else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage != 0);
     else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage != 0);
     else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stage != 0);
@@ -1250,6 +1382,8 @@ static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
     if (k.smem) {  // opt in to the staged kernels' shared memory (idempotent)
         cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
         cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
+        if (k.pers)
+            cudaFuncSetAttribute((const void*)k.pers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
     }
     return k;
 }
@@ -1282,6 +1416,9 @@ struct CgWorkspace {
     int* d_tile_sys = nullptr;
     double* d_partial = nullptr;
     int* d_active = nullptr;
+    GridBar* d_bar = nullptr;  // grid barrier of the persistent solve
+    bool timed_out = false;    // the last persistent solve gave up at a barrier
+    int num_sms = 0;
     std::vector<void*> allocs;
     size_t bytes = 0;
     // iteration chunks replayed as one graph launch each
@@ -1321,7 +1458,7 @@ struct CgWorkspace {
         allocs.clear();
         item_cache.clear();
         d_sys = nullptr; d_rhs = nullptr; d_lanes = nullptr;
-        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr;
+        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr; d_bar = nullptr;
     }
     cudaError_t alloc(void** p, size_t n)
     {
@@ -1534,6 +1671,64 @@ struct PhaseTimes {
     long n[kTimedPhases];
 };
 
+static cudaError_t finish_solve(CgWorkspace& w, cudaStream_t stream);
+
+// The persistent schedule: the whole solve (after cg_init) in one cooperative
+// launch of as many blocks as fit on the GPU at once, each walking the work
+// items of every phase.  Same per-tile bodies and reductions as the
+// system-blocked graph path, so the same solutions.
+static cudaError_t persistent_solve(CgWorkspace& w, const CgKernels& k, CgArgs a, cudaStream_t stream,
+                                    PhaseTimes* timing)
+{
+    cudaError_t e;
+    if (!w.d_bar && (e = w.alloc((void**)&w.d_bar, sizeof(GridBar))) != cudaSuccess) return e;
+    if (!w.num_sms) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&w.num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    }
+    const int2* hop_items;
+    const int2* upd_items;
+    int nhop = 0, nupd = 0;
+    if ((e = items_for(w, kSysItems, 1, &hop_items, &nhop)) != cudaSuccess) return e;
+    if ((e = items_for(w, 1, 1, &upd_items, &nupd)) != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.pers, kTile, k.smem)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int grid = std::max(1, std::min(per_sm * w.num_sms, std::max(nhop, nupd)));
+    if ((e = cudaMemsetAsync(w.d_bar, 0, sizeof(GridBar), stream)) != cudaSuccess) return e;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    if (timing) {
+        for (int r = 0; r < kTimedPhases; ++r) {
+            timing->ms[r] = 0.0;
+            timing->n[r] = 0;
+        }
+        for (cudaEvent_t& x : ev)
+            if ((e = cudaEventCreate(&x)) != cudaSuccess) return e;
+        cudaEventRecord(ev[0], stream);
+    }
+    void* args[] = {&a, (void*)&hop_items, &nhop, (void*)&upd_items, &nupd, (void*)&w.d_bar};
+    e = cudaLaunchCooperativeKernel((const void*)k.pers, dim3(grid), dim3(kTile), args, k.smem, stream);
+    w.launches += 1;
+    if (timing) {
+        if (e == cudaSuccess) e = cudaEventRecord(ev[1], stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        timing->ms[PH_PERSISTENT] = ms;
+        timing->n[PH_PERSISTENT] = 1;
+        for (cudaEvent_t x : ev)
+            if (x) cudaEventDestroy(x);
+    }
+    if (e != cudaSuccess) return e;
+    int err = 0;
+    if ((e = cudaMemcpyAsync(&err, &w.d_bar->err, sizeof(int), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        return e;
+    if ((e = finish_solve(w, stream)) != cudaSuccess) return e;
+    w.timed_out = err != 0;
+    return cudaSuccess;
+}
+
 // Reliable-update threshold (|r| drop between FP64 updates) of the mixed
 // precisions: FP16 storage needs the tighter 0.1 (at 0.02 its recurrence
 // drifts too far to converge); FP32 keeps its recurrence to 0.01, half the
@@ -1576,7 +1771,9 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     CgArgs a = make_args(w, tol, maxit, delta, k.sys ? 1 : (tpi > 0 ? tpi : 2));
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
+    w.timed_out = false;
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (k.pers) return persistent_solve(w, k, a, stream, timing);
     if (!timing && (e = ensure_graph(w, k, a, tol, maxit, delta)) != cudaSuccess) return e;
     // timed solves: the same kernels and work items, launched one by one
     Phase ph[kMaxPhases];
@@ -1646,7 +1843,15 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         }
     }
     destroy_events();
-    e = cudaMemcpyAsync(w.lanes_h.data(), w.d_lanes, sizeof(CgLane) * w.nlanes, cudaMemcpyDeviceToHost, stream);
+    return finish_solve(w, stream);
+}
+
+// the lanes' final state to the host; a lane that never stopped did not
+// converge
+static cudaError_t finish_solve(CgWorkspace& w, cudaStream_t stream)
+{
+    cudaError_t e = cudaMemcpyAsync(w.lanes_h.data(), w.d_lanes, sizeof(CgLane) * w.nlanes, cudaMemcpyDeviceToHost,
+                                    stream);
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
@@ -1862,6 +2067,8 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
     int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links, b->stream),
                         "batched CG");
     if (st) return st;
+    if (b->ws.timed_out)
+        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a grid-barrier wait of the persistent solve gave up");
     for (const sfh::CgLane& L : b->ws.lanes_h)
         if (L.status != SFH_OK) return L.status;
     return SFH_OK;
@@ -2167,17 +2374,20 @@ extern "C" int sfh_batch_get_rhs(sfh_batch* b, int k, int j, double* phi)
     return batch_cuda(b, cudaStreamSynchronize(b->stream), "rhs download");
 }
 
-extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double* ms5, long* n5)
+extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double* ms, long* n)
 {
-    if (!b || !ms5 || !n5 || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
+    if (!b || !ms || !n || !(tol > 0.0) || maxit <= 0) return SFH_ERR_INVALID;
     cudaSetDevice(b->device);
     sfh::PhaseTimes t;
     int st = batch_cuda(b, sfh::workspace_solve(b->ws, tol, maxit, b->delta, b->nb, b->nb2, b->tpi, b->stage_links, b->stream, &t),
                         "timed batched CG");
     if (st) return st;
+    if (b->ws.timed_out)
+        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a grid-barrier wait of the persistent solve gave up");
+    static_assert(sfh::kTimedPhases == SFH_TIMED_KERNELS, "timing slots of include/sfh.h");
     for (int k = 0; k < sfh::kTimedPhases; ++k) {
-        ms5[k] = t.ms[k];
-        n5[k] = t.n[k];
+        ms[k] = t.ms[k];
+        n[k] = t.n[k];
     }
     for (const sfh::CgLane& L : b->ws.lanes_h)
         if (L.status != SFH_OK) return L.status;
@@ -2207,11 +2417,11 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
     int bw = 1, bt = 2, bs = 0;
-    const int nstage = f64 ? 1 : (b->prec == SFH_PREC_F32_18 ? 2 : 3);
+    const int nstage = f64 ? 1 : (b->prec == SFH_PREC_F32_18 ? 2 : 4);
     for (int stage = 0; stage < nstage; ++stage)
         for (int c = 0; c < ncand; ++c)
             for (int tp : tiles) {
-                if (stage == 2 && tp != 1) continue;  // system-blocked: one tile per block
+                if (stage >= 2 && tp != 1) continue;  // system-blocked: one tile per block
                 double t = 0.0;
                 for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
                     auto t0 = std::chrono::steady_clock::now();
@@ -2239,7 +2449,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
-    if (stage_links < 0 || stage_links > 2) return SFH_ERR_INVALID;
+    if (stage_links < 0 || stage_links > 3) return SFH_ERR_INVALID;
     b->stage_links = stage_links;
     return SFH_OK;
 }

@@ -82,15 +82,15 @@ __device__ __forceinline__ Vec3<R> vneg_if(const Vec3<R>& v, bool neg, R scale =
 
 // a neighbour spinor with the hop's scalar factor applied: the eta / 2 and
 // time-wrap sign, and for the 16-bit storages the per-site scale (one multiply)
-template <int SP, typename R>
+template <int SP, typename R, bool COH = false>
 __device__ __forceinline__ Vec3<R> hop_input(const void* in, int nq, int j, int Vh, bool neg, R s)
 {
     if constexpr (SpinorFmt<SP>::scaled) {
         float sc;
-        Vec3<R> v = SpinorFmt<SP>::load_unscaled(in, nq, j, Vh, &sc);
+        Vec3<R> v = SpinorFmt<SP>::template load_unscaled<COH>(in, nq, j, Vh, &sc);
         return vneg_if(v, neg, s * sc);
     } else {
-        return vneg_if(vcvt<R>(SpinorFmt<SP>::load(in, nq, j, Vh)), neg, s);
+        return vneg_if(vcvt<R>(SpinorFmt<SP>::template load<COH>(in, nq, j, Vh)), neg, s);
     }
 }
 
@@ -159,11 +159,11 @@ __device__ __forceinline__ void hlink_load(const uint2* s, int tile, const void*
 
 // acc += f (U v) (ADJ false) or acc += f (U^dag v) (ADJ true) for a stored
 // FP16 vector v with site scale sc: f = s sc, products in half2
-template <bool ADJ>
+template <bool ADJ, bool COH = false>
 __device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9], const void* in, int nq, int j,
                                          int Vh, float f)
 {
-    const uint4 w = __ldg((const uint4*)in + (size_t)nq * Vh + j);
+    const uint4 w = ld_vec<COH>((const uint4*)in + (size_t)nq * Vh + j);
     const __half2 v[3] = {h2_bits(w.x), h2_bits(w.y), h2_bits(w.z)};
     f *= __uint_as_float(w.w);
     __half2 vp[3];

@@ -210,17 +210,28 @@ enum GaugePrec { GP_F64_18 = 0, GP_F32_12 = 1, GP_F16_12 = 2, GP_F32_18 = 3, GP_
 
 template <int SP> struct SpinorFmt;
 
+// load of a vector word: through the read-only data cache (COH false; data
+// not written while the kernel runs) or through L2 only (COH true: data other
+// blocks of the same persistent kernel write between its phases)
+template <bool COH, typename T>
+__device__ __forceinline__ T ld_vec(const T* p)
+{
+    if constexpr (COH) return __ldcg(p);
+    else return __ldg(p);
+}
+
 template <> struct SpinorFmt<SP_F64> {
     typedef double R;
     static constexpr size_t site_bytes = 48;
     static constexpr bool scaled = false;
+    template <bool COH = false>
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const double2* b = (const double2*)base + (size_t)p * 3 * Vh;
         Vec3<R> v;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            double2 w = __ldg(b + (size_t)c * Vh + i);
+            double2 w = ld_vec<COH>(b + (size_t)c * Vh + i);
             v.c[c] = {w.x, w.y};
         }
         return v;
@@ -249,13 +260,14 @@ template <> struct SpinorFmt<SP_F32> {
     typedef float R;
     static constexpr size_t site_bytes = 24;
     static constexpr bool scaled = false;
+    template <bool COH = false>
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const float2* b = (const float2*)base + (size_t)p * 3 * Vh;
         Vec3<R> v;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float2 w = __ldg(b + (size_t)c * Vh + i);
+            float2 w = ld_vec<COH>(b + (size_t)c * Vh + i);
             v.c[c] = {w.x, w.y};
         }
         return v;
@@ -344,10 +356,11 @@ template <int SP> struct ScaledSpinorFmt {
     }
     __device__ static __forceinline__ Vec3<R> quantize(const Vec3<R>& v) { return unpack(pack(v)); }
     // the pairs converted, without the scale (returned in *scale)
+    template <bool COH = false>
     __device__ static __forceinline__ Vec3<R> load_unscaled(const void* base, int p, int i, int Vh, float* scale)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
-        uint4 w = __ldg(b + i);
+        uint4 w = ld_vec<COH>(b + i);
         *scale = __uint_as_float(w.w);
         Vec3<R> v;
         uint32_t words[3] = {w.x, w.y, w.z};
@@ -358,10 +371,11 @@ template <int SP> struct ScaledSpinorFmt {
         }
         return v;
     }
+    template <bool COH = false>
     __device__ static __forceinline__ Vec3<R> load(const void* base, int p, int i, int Vh)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
-        return unpack(__ldg(b + i));
+        return unpack(ld_vec<COH>(b + i));
     }
     __device__ static __forceinline__ void store(void* base, int p, int i, int Vh, const Vec3<R>& v)
     {

@@ -293,8 +293,9 @@ def test_batch_system_blocked_schedule(sfh, orc, precision):
     their own) on systems with several tiles, a partial last tile and more
     RHS than one group: every RHS-group width gives bit-identical solutions
     (the per-group sums have a fixed order), each reaches the FP64 true
-    residual by the oracle's D D^dag, and the timed solve runs the same
-    kernels to the same solutions."""
+    residual by the oracle's D D^dag, the timed solve runs the same kernels
+    to the same solutions, and so does the persistent schedule (one
+    cooperative launch)."""
     tol = 1e-10
     outs = []
     for w in (1, 2, 4, 8):
@@ -321,3 +322,16 @@ def test_batch_system_blocked_schedule(sfh, orc, precision):
     assert np.array_equal(timed, outs[0])
     assert set(times) == {"cg_hop1", "cg_hop2", "cg_update", "cg_ru1", "cg_ru2"}
     assert len({times[k][1] for k in times}) == 1  # every iteration launches all five
+    # the persistent schedule: the same per-tile work in one cooperative
+    # launch gives the same solutions bit for bit, in one launch per solve
+    for w, timed_solve in ((2, False), (8, True)):
+        B, _ = _sys_batch(sfh, orc, precision, (w, 1, 3))
+        if timed_solve:
+            times = B.solve_timed(tol=tol)
+            assert set(times) == {"cg_persistent"} and times["cg_persistent"][1] == 1
+        else:
+            B.solve(tol=tol, max_iter=20000)
+            assert B.kernel_launches() == 2  # cg_init and the persistent kernel
+        pers = np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(SYS_SYSTEMS) for j in range(n)])
+        B.close()
+        assert np.array_equal(pers, outs[0])
