@@ -509,13 +509,17 @@ def run_extras(sfh, hbm, quick=False):
             lat.set_mass(m)
             Xo, it_o, _, _ = oracle.cg(lat.dims, m, U, phi, TOL, 40000)
             row = {"oracle_fp64_iters": it_o}
-            for prec in ("f64", "f32_18", "f32", "f16", "bf16"):
+            for prec in ("f64", "f32_18", "f32", "f16", "bf16", "f16_persistent", "f32_persistent"):
+                sched = (1, 1, 3) if prec.endswith("_persistent") else (0, 0, 0)
+                lat.set_schedule(*sched)
                 t0 = time.perf_counter()
-                X, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec, info=True)
+                X, inf = lat.solve_CG_DDdagger(phi, tol=TOL, max_iter=40000, precision=prec.split("_p")[0],
+                                               info=True)
                 row[prec] = {"iters": inf["iters"], "ms": 1e3 * (time.perf_counter() - t0),
                              "true_resid_oracle": float(np.linalg.norm(phi - oracle.ddag(lat.dims, m, U, X))
                                                         / np.linalg.norm(phi)),
                              "err_vs_oracle_fp64": float(np.linalg.norm(X - Xo) / np.linalg.norm(Xo))}
+            lat.set_schedule(0, 0, 0)
             grid[f"eps{geps}_m{m}"] = row
     ex["c2_16^4"] = grid
     lat.close()

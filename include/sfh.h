@@ -128,6 +128,13 @@ int sfh_dslash_storage(sfh_ctx* ctx, int storage, const double* in, double* out)
 int sfh_cg_solve(sfh_ctx* ctx, const double* phi, double* X, double tol, int maxit,
                  int precision, sfh_cg_info* info);
 
+/* The schedule of the context's mixed-precision solves (sfh_cg_solve, the
+ * trajectory's solves), as sfh_batch_set_schedule: RHS-block width, tiles per
+ * block, link staging 0..3 (3: the whole solve in one persistent launch).
+ * Default 0, 0, 0; the FP64 CG keeps its own.  No counterpart in the
+ * reference. */
+int sfh_set_schedule(sfh_ctx* ctx, int width, int tiles_per_block, int stage_links);
+
 /* ---- forces, link update, observables (context's device fields) --------- */
 /* Per-link staple sums A1 (plaquette) and A2 (rectangle):
  * compute_staple_sum_at_link / compute_rectangle_staple_sum_at_link

@@ -144,6 +144,7 @@ SIGNATURES = {
     "sfh_smear_hex": (ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]),
     "sfh_hex_staples": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
+    "sfh_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -478,6 +479,11 @@ class Lattice:
     # --- smearing (Smearing.cpp) ---------------------------------------------
     def smear_stout(self, rho, n_levels=1):
         self._check(self.lib.sfh_smear_stout(self.h, rho, n_levels), "stout smearing")
+
+    def set_schedule(self, width=0, tiles_per_block=0, stage_links=0):
+        """Schedule of this lattice's mixed-precision solves (as
+        Batch.set_schedule; stage_links 3: one persistent launch per solve)."""
+        self._check(self.lib.sfh_set_schedule(self.h, width, tiles_per_block, int(stage_links)), "set_schedule")
 
     HMC_KERNELS = ("gauge_force", "fermion_force", "staples", "link_update", "stout_level", "stout_force",
                    "action", "plaquette")

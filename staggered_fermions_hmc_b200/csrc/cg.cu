@@ -2192,8 +2192,11 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     e = cudaMemcpyAsync(w->rhs[0].b, b_eo, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg rhs");
-    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), 0, 0, 0, false, c->stream);
+    const bool lowp = prec != SFH_PREC_F64;  // the FP64 CG keeps the reference's schedule
+    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), lowp ? c->sched_nb : 0, lowp ? c->sched_nb : 0,
+                        lowp ? c->sched_tpi : 0, lowp ? c->sched_stage : 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
+    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
     e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solution");
     int status = SFH_OK;
@@ -2266,8 +2269,11 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
         e = cudaMemcpyAsync(w->rhs[w->rhs0[k]].b, b_eo[k], fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair rhs");
     }
-    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), 0, 0, 0, 0, c->stream);
+    const bool lowp = prec != SFH_PREC_F64;
+    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), lowp ? c->sched_nb : 0, lowp ? c->sched_nb : 0,
+                        lowp ? c->sched_tpi : 0, lowp ? c->sched_stage : 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg pair solve");
+    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
     for (int k = 0; k < 2; ++k) {
         e = cudaMemcpyAsync(x_eo[k], w->rhs[w->rhs0[k]].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair solution");
@@ -2451,6 +2457,17 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     b->tpi = tiles_per_block;
     if (stage_links < 0 || stage_links > 3) return SFH_ERR_INVALID;
     b->stage_links = stage_links;
+    return SFH_OK;
+}
+
+extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int stage_links)
+{
+    if (!c || width < 0 || width > 8 || tiles_per_block < 0 || tiles_per_block > 64 || stage_links < 0 ||
+        stage_links > 3)
+        return SFH_ERR_INVALID;
+    c->sched_nb = width;
+    c->sched_tpi = tiles_per_block;
+    c->sched_stage = stage_links;
     return SFH_OK;
 }
 

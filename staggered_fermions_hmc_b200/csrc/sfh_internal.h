@@ -42,6 +42,7 @@ struct sfh_ctx {
 
     sfh::CgWorkspace* ws[sfh::kNumPrecisions] = {};  // cached solver workspaces per precision
     double ws_mass[sfh::kNumPrecisions] = {};
+    int sched_nb = 0, sched_tpi = 0, sched_stage = 0;  // schedule of the context's mixed-precision solves
     sfh::CgWorkspace* ws_pair[sfh::kNumPrecisions] = {};  // two systems on the links (Hasenbusch pair)
     double ws_pair_mass[sfh::kNumPrecisions][2] = {};
     void* Utrial = nullptr;        // gauge backup for the Metropolis step

@@ -335,3 +335,26 @@ def test_batch_system_blocked_schedule(sfh, orc, precision):
         pers = np.concatenate([B.solution(k, j) for k, (d, m, n) in enumerate(SYS_SYSTEMS) for j in range(n)])
         B.close()
         assert np.array_equal(pers, outs[0])
+
+
+@pytest.mark.parametrize("precision", ["f16", "f32"])
+def test_lattice_solve_persistent_schedule(sfh, orc, precision):
+    """A single solve with the context's schedule set to the persistent launch
+    (3) equals the system-blocked graph schedule (2) bit for bit and reaches
+    the FP64 true residual by the oracle's D D^dag."""
+    dims, mass, tol = (8, 8, 8, 12), 0.05, 1e-10
+    U = orc.random_gauge(dims, 1.0, 171)
+    b = orc.random_spinor(dims, 172)
+    lat = sfh.Lattice(dims, mass)
+    try:
+        lat.upload_gauge(U)
+        out = []
+        for stage in (2, 3):
+            lat.set_schedule(1, 1, stage)
+            X, info = lat.solve_CG_DDdagger(b, tol=tol, precision=precision, info=True)
+            assert info["status"] == 0
+            assert true_resid(orc, dims, mass, U, b, X) < 1.05 * tol
+            out.append(X)
+        assert np.array_equal(out[0], out[1])
+    finally:
+        lat.close()
