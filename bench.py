@@ -771,6 +771,8 @@ def main():
     # one between CUDA events on the batch's stream (same kernels and results)
     per_kernel = B.solve_timed(tol=TOL, max_iter=MAXIT)
     kbytes = kernel_bytes(spec, infos, args.precision, ru_separate="cg_ru1" in per_kernel)
+    if "cg_persistent" in per_kernel:  # the whole solve in one launch
+        kbytes = {"cg_persistent": sum(kbytes.values())}
     ktot = sum(v[0] for v in per_kernel.values())
     kernels = {}
     for name, (kms, kn) in per_kernel.items():

@@ -369,6 +369,10 @@ __device__ __forceinline__ void finish_lane(const CgArgs& a, const CgSys& S, int
             if (rr_next < L->target || r < a.delta * L->rmax || L->iters >= a.maxit ||
                 rr_next > 4.0 * L->rr_old) {
                 L->mode[nxt] = LM_RU;
+                if (a.ru_list) {  // the next iteration's reliable-update kernels walk this list
+                    int* lst = a.ru_list + nxt * (a.nlanes + 1);
+                    lst[1 + atomicAdd(lst, 1)] = lane;
+                }
             } else {
                 L->rmax = fmax(L->rmax, r);
                 L->mode[nxt] = LM_ACTIVE;
@@ -763,6 +767,9 @@ __device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, C
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
     typedef typename SpinorFmt<XP>::R RX;
+    // this iteration's reliable-update list was read by the kernels before
+    // this one: empty it for the iteration after next
+    if (a.ru_list && blockIdx.x == 0 && threadIdx.x == 0) a.ru_list[cur * (a.nlanes + 1)] = 0;
     stage_sys(a, it.x, s_sys);
     const CgSys& S = *s_sys;
     const ItemRange ir = item_range(a, S, it.x);
@@ -815,8 +822,9 @@ __global__ void __launch_bounds__(kTile) cg_update(CgArgs a, const int2* __restr
 // accumulators), the neighbour indices and hop signs computed once per site.
 // The CG sums of cg_hop2_sys are reduced per group through shared memory in
 // a fixed order (each site's dot products in FP32, summed in FP64).  The
-// FP64 reliable-update hops run in kernels of their own (cg_ru1_sys,
-// cg_ru2_sys), so that their registers do not weigh on the hop kernels.
+// FP64 reliable-update hops run in kernels of their own (cg_ru1_list,
+// cg_ru2_list, over the lanes due for one), so that their registers do not
+// weigh on the hop kernels.
 // ---------------------------------------------------------------------------
 // unpacked FP16 links of a tile: [direction slot 8][half2 word 9][kTile]
 constexpr size_t kHStageBytes = (size_t)8 * 9 * kTile * sizeof(uint32_t);
@@ -1056,57 +1064,87 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
     }
 }
 
-// The FP64 reliable-update hops of the system-blocked schedule, one block
-// per tile; blocks without a lane in a reliable update return at once.
-// ru1: thi = K (x_hi + x_lo) at output parity q for the lanes of parity
-// 1 - q; ru2: x_hi += x_lo, r = b - M x_hi and |r|^2 for the lanes of parity
-// q, whose partial sums complete the lanes' tickets.
+// The FP64 reliable updates of the lanes on this iteration's list (the
+// lanes whose recurrence asked for one in the last iteration), walked by a
+// small fixed grid: blk / nblk split each lane's work items among the blocks.
+// ru1: thi = K (x_hi + x_lo) on the tiles of the other parity; ru2: x_hi +=
+// x_lo, r = b - M x_hi and |r|^2 on the lane's own tiles, in work items of
+// tpi tiles whose sums complete the lane's partial-sum slots and ticket (the
+// same order of additions as the hop kernels' own reliable-update loops).
 template <int SP, bool COH>
-__device__ __forceinline__ void ru1_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys)
+__device__ __forceinline__ void ru1_list_body(const CgArgs& a, int cur, int blk, int nblk, CgSys* s_sys)
 {
     constexpr int XP = XFmt<SP>::v;
-    stage_sys(a, tile, s_sys);
-    const CgSys& S = *s_sys;
-    const TileInfo ti = decode_tile(S, tile);
-    bool anyA, anyR;
-    scan_lanes(a, S, ti.q, true, cur, &anyA, &anyR);
-    if (!anyR || !ti.valid) return;
-    const Coord c = eo_coords(S.g, ti.q, ti.i);
-#pragma unroll 1
-    for (int r = 0; r < S.nrhs; ++r) {
-        const CgLane* L = a.lanes + lane_of(S, r, ti.q, true);
-        if (ld_int(&L->mode[cur]) == LM_RU) ru_hop1<XP, COH>(a, S, c, ti.q, ti.i, __ldg(&L->rhs));
+    const int* lst = a.ru_list + cur * (a.nlanes + 1);
+    const int n = ld_int(lst);
+    for (int u = 0; u < n; ++u) {
+        const int lane = ld_int(lst + 1 + u);
+        const CgLane* L = a.lanes + lane;  // sys, rhs and parity are fixed for the solve
+        __syncthreads();
+        if (threadIdx.x == 0) *s_sys = a.sys[L->sys];
+        __syncthreads();
+        const CgSys& S = *s_sys;
+        const int q = 1 - L->parity, rid = L->rhs;
+        for (int j = blk; j < S.ntq; j += nblk) {
+            const int i = j * kTile + (int)threadIdx.x;
+            if (i < S.g.Vh) ru_hop1<XP, COH>(a, S, eo_coords(S.g, q, i), q, i, rid);
+        }
     }
 }
 
 template <int SP, bool COH>
-__device__ __forceinline__ void ru2_sys_body(const CgArgs& a, int tile, int cur, CgSys* s_sys, double* s_bs,
-                                             unsigned* s_mask)
+__device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk, int nblk, CgSys* s_sys,
+                                              double* s_bs, unsigned* s_mask)
 {
     constexpr int XP = XFmt<SP>::v;
-    stage_sys(a, tile, s_sys);
-    const CgSys& S = *s_sys;
-    const TileInfo ti = decode_tile(S, tile);
-    const int q = ti.q;
-    bool anyA, anyR;
-    scan_lanes(a, S, q, false, cur, &anyA, &anyR);
-    if (!anyR) return;  // uniform in the block
-    const ItemRange ir = item_range(a, S, tile);
-    const unsigned nsq = (unsigned)item_groups(a, S);
-    const Coord c = eo_coords(S.g, q, ti.valid ? ti.i : 0);
-#pragma unroll 1
-    for (int r = 0; r < S.nrhs; ++r) {
-        LanePass<1> P;
-        gather_pass<1>(a, S, r, q, false, cur, false, P);
-        if (P.mode[0] != LM_RU) continue;
-        double sums[kSums] = {0.0, 0.0, 0.0, 0.0};
-        if (ti.valid) sums[3] = ru_hop2<SP, XP, COH>(a.rhs, S, c, q, ti.i, P.rid[0]);
-        block_sum<kSums>(sums, s_bs);
-        const bool part[1] = {true};
-        const unsigned mask = arrive_sums<1>(a, S, P, part, sums, ir.slot, nsq, s_mask);
-        if (mask && threadIdx.x < 32) finish_lane(a, S, P.lane[0], P.mode[0], cur);
+    const int* lst = a.ru_list + cur * (a.nlanes + 1);
+    const int n = ld_int(lst);
+    for (int u = 0; u < n; ++u) {
+        const int lane = ld_int(lst + 1 + u);
+        const CgLane* L = a.lanes + lane;
         __syncthreads();
+        if (threadIdx.x == 0) *s_sys = a.sys[L->sys];
+        __syncthreads();
+        const CgSys& S = *s_sys;
+        const int p = L->parity, rid = L->rhs;
+        const int nsq = item_groups(a, S);
+        LanePass<1> P;
+        P.lane[0] = lane;
+        P.mode[0] = LM_RU;
+        P.rid[0] = rid;
+        P.alpha[0] = P.beta[0] = 0.0;
+        P.anyA = false;
+        P.anyR = true;
+        for (int g = blk; g < nsq; g += nblk) {
+            double sums[kSums] = {0.0, 0.0, 0.0, 0.0};
+            const int j1 = min((g + 1) * a.tpi, S.ntq);
+            for (int j = g * a.tpi; j < j1; ++j) {
+                const int i = j * kTile + (int)threadIdx.x;
+                if (i < S.g.Vh) sums[3] += ru_hop2<SP, XP, COH>(a.rhs, S, eo_coords(S.g, p, i), p, i, rid);
+            }
+            block_sum<kSums>(sums, s_bs);
+            const bool part[1] = {true};
+            const unsigned mask = arrive_sums<1>(a, S, P, part, sums, p * nsq + g, (unsigned)nsq, s_mask);
+            if (mask && threadIdx.x < 32) finish_lane(a, S, lane, LM_RU, cur);
+            __syncthreads();
+        }
     }
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru1_list(CgArgs a, const int2* __restrict__, int cur)
+{
+    __shared__ CgSys s_sys;
+    ru1_list_body<SP, false>(a, cur, blockIdx.x, gridDim.x, &s_sys);
+}
+
+template <int SP>
+__global__ void __launch_bounds__(kTile) cg_ru2_list(CgArgs a, const int2* __restrict__, int cur)
+{
+    __shared__ CgSys s_sys;
+    __shared__ double s_bs[32];
+    __shared__ unsigned s_mask;
+    ru2_list_body<SP, false>(a, cur, blockIdx.x, gridDim.x, &s_sys, s_bs, &s_mask);
 }
 
 template <int GP, int SP, int NB>
@@ -1130,28 +1168,12 @@ __global__ void __launch_bounds__(kTile, (SysOcc<GP, true>::v)) cg_hop2_sys(CgAr
     hop2_sys_body<GP, SP, NB, false>(a, items[blockIdx.x].x, cur, &s_sys, s_dyn, s_red, s_tot, &s_mask);
 }
 
-template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru1_sys(CgArgs a, const int2* __restrict__ items, int cur)
-{
-    __shared__ CgSys s_sys;
-    ru1_sys_body<SP, false>(a, items[blockIdx.x].x, cur, &s_sys);
-}
-
-template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru2_sys(CgArgs a, const int2* __restrict__ items, int cur)
-{
-    __shared__ CgSys s_sys;
-    __shared__ double s_bs[32];
-    __shared__ unsigned s_mask;
-    ru2_sys_body<SP, false>(a, items[blockIdx.x].x, cur, &s_sys, s_bs, &s_mask);
-}
-
 // ---------------------------------------------------------------------------
 // Persistent batched CG: the whole solve in one cooperative launch.  Every
 // block walks the work items of each phase (grid-stride), the phases of an
 // iteration separated by a grid barrier: {hop1, ru1}, {hop2, ru2}, update
 // (hop1 and ru1 touch different lanes, as do hop2 and ru2, so each pair
-// shares a phase).  The per-tile bodies are those of the system-blocked
+// shares a phase; the reliable updates walk the lane list).  The per-tile bodies are those of the system-blocked
 // kernels, with every load of data written during the solve taken through
 // L2 (coherent across the blocks), so the solutions equal the graph path's
 // bit for bit.  The grid barrier waits a bounded number of polls; a block
@@ -1218,16 +1240,14 @@ __global__ void __launch_bounds__(kTile, 2) cg_persistent_sys(CgArgs a, const in
         for (int k = blockIdx.x; k < nhop; k += gridDim.x) {
             __syncthreads();
             hop1_sys_body<GP, SP, NB, true>(a, hop_items[k].x, cur, &s_sys, s_dyn);
-            __syncthreads();
-            ru1_sys_body<SP, true>(a, hop_items[k].x, cur, &s_sys);
         }
+        ru1_list_body<SP, true>(a, cur, blockIdx.x, gridDim.x, &s_sys);
         if (!grid_barrier(bar, nblk, &s_ok)) return;
         for (int k = blockIdx.x; k < nhop; k += gridDim.x) {
             __syncthreads();
             hop2_sys_body<GP, SP, NB, true>(a, hop_items[k].x, cur, &s_sys, s_dyn, s_red, s_tot, &s_mask);
-            __syncthreads();
-            ru2_sys_body<SP, true>(a, hop_items[k].x, cur, &s_sys, s_bs, &s_mask);
         }
+        ru2_list_body<SP, true>(a, cur, blockIdx.x, gridDim.x, &s_sys, s_bs, &s_mask);
         if (!grid_barrier(bar, nblk, &s_ok)) return;
         for (int k = blockIdx.x; k < nupd; k += gridDim.x) {
             __syncthreads();
@@ -1267,18 +1287,22 @@ struct Phase {
     int width;      // RHS width of the work items
     size_t smem;
     int slot;       // timing slot
+    bool list;      // walks the reliable-update lane list with a fixed grid
 };
 
 static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
 {
     int n = 0;
-    ph[n++] = {k.hop1, k.nb1, k.smem, PH_HOP1};
-    if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1};
-    ph[n++] = {k.hop2, k.nb2, k.smem, PH_HOP2};
-    if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2};
-    ph[n++] = {k.update, 1, 0, PH_UPDATE};
+    ph[n++] = {k.hop1, k.nb1, k.smem, PH_HOP1, false};
+    if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1, true};
+    ph[n++] = {k.hop2, k.nb2, k.smem, PH_HOP2, false};
+    if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2, true};
+    ph[n++] = {k.update, 1, 0, PH_UPDATE, false};
     return n;
 }
+
+// blocks of the lane-list kernels per SM
+constexpr int kListBlocksPerSm = 2;
 
 // work-item width of the system-blocked kernels: one item per tile, covering
 // every RHS of the system
@@ -1308,8 +1332,8 @@ static CgKernels pick_sys(int nb, bool persistent)
     }
     k.init = cg_init<SP, 2>;
     k.update = cg_update<SP>;
-    k.ru1 = cg_ru1_sys<SP>;
-    k.ru2 = cg_ru2_sys<SP>;
+    k.ru1 = cg_ru1_list<SP>;
+    k.ru2 = cg_ru2_list<SP>;
     k.nb1 = k.nb2 = kSysItems;
     k.smem = SysStage<GP, SP>::bytes;
     k.sys = true;
@@ -1417,6 +1441,7 @@ struct CgWorkspace {
     double* d_partial = nullptr;
     int* d_active = nullptr;
     GridBar* d_bar = nullptr;  // grid barrier of the persistent solve
+    int* d_rulist = nullptr;   // reliable-update lane lists [2][1 + nlanes]
     bool timed_out = false;    // the last persistent solve gave up at a barrier
     int num_sms = 0;
     std::vector<void*> allocs;
@@ -1458,7 +1483,7 @@ struct CgWorkspace {
         allocs.clear();
         item_cache.clear();
         d_sys = nullptr; d_rhs = nullptr; d_lanes = nullptr;
-        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr; d_bar = nullptr;
+        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr; d_bar = nullptr; d_rulist = nullptr;
     }
     cudaError_t alloc(void** p, size_t n)
     {
@@ -1542,6 +1567,12 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
     if ((e = w.alloc((void**)&w.d_tile_sys, sizeof(int) * std::max(1, w.ntiles))) != cudaSuccess) return e;
     if ((e = w.alloc((void**)&w.d_partial, sizeof(double) * std::max(1, poff))) != cudaSuccess) return e;
     if ((e = w.alloc((void**)&w.d_active, sizeof(int))) != cudaSuccess) return e;
+    if ((e = w.alloc((void**)&w.d_rulist, sizeof(int) * 2 * (w.nlanes + 1))) != cudaSuccess) return e;
+    {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&w.num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    }
     if ((e = cudaMemcpy(w.d_sys, w.sys.data(), sizeof(CgSys) * w.nsys, cudaMemcpyHostToDevice)) != cudaSuccess) return e;
     if (!w.rhs.empty())
         if ((e = cudaMemcpy(w.d_rhs, w.rhs.data(), sizeof(CgRhs) * w.rhs.size(), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
@@ -1608,6 +1639,7 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.restart = 0;  // restart only when an update shows little progress (finish_lane)
     a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
     a.tpi = tpi;
+    a.ru_list = nullptr;
     return a;
 }
 
@@ -1631,8 +1663,10 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
     const int2* items[kMaxPhases];
     int nitems[kMaxPhases];
     cudaError_t e;
-    for (int j = 0; j < nph; ++j)
+    for (int j = 0; j < nph; ++j) {
         if ((e = items_for(w, ph[j].width, a.tpi, &items[j], &nitems[j])) != cudaSuccess) return e;
+        if (ph[j].list) nitems[j] = kListBlocksPerSm * w.num_sms;
+    }
     e = cudaGraphCreate(&w.graph, 0);
     if (e != cudaSuccess) return e;
     cudaGraphNode_t prev = nullptr;
@@ -1769,6 +1803,10 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     // the system-blocked kernels serve one tile per block: one partial-sum
     // slot per tile, so every kernel of the iteration takes single tiles
     CgArgs a = make_args(w, tol, maxit, delta, k.sys ? 1 : (tpi > 0 ? tpi : 2));
+    if (k.ru1 || k.pers) {  // reliable updates by lane list: both lists start empty
+        a.ru_list = w.d_rulist;
+        if ((e = cudaMemsetAsync(w.d_rulist, 0, sizeof(int) * 2 * (w.nlanes + 1), stream)) != cudaSuccess) return e;
+    }
     k.init<<<w.ntiles, kTile, 0, stream>>>(a);
     w.launches = 1;
     w.timed_out = false;
@@ -1783,8 +1821,10 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     std::vector<cudaEvent_t> tev;
     const int per_chunk = nph * kChunk;
     if (timing) {
-        for (int j = 0; j < nph; ++j)
+        for (int j = 0; j < nph; ++j) {
             if ((e = items_for(w, ph[j].width, a.tpi, &items[j], &nitems[j])) != cudaSuccess) return e;
+            if (ph[j].list) nitems[j] = kListBlocksPerSm * w.num_sms;
+        }
         for (int r = 0; r < kTimedPhases; ++r) {
             timing->ms[r] = 0.0;
             timing->n[r] = 0;

@@ -56,6 +56,9 @@ struct CgArgs {
     int maxit, maxloop, mixed;
     int restart;  // restart the Krylov space after every residual update
     int tpi;      // tiles per work item of the iteration kernels
+    // lanes due for a reliable update, per iteration parity: [2][1 + nlanes],
+    // a count then lane ids (null: the hop kernels do the reliable updates)
+    int* ru_list;
 };
 
 namespace {

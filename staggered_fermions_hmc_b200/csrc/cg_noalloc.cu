@@ -565,6 +565,7 @@ extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* 
     a.tile_sys = reinterpret_cast<const int*>(base + kOffTiles);
     a.partial = reinterpret_cast<double*>(base + kOffPartial);
     a.n_active = reinterpret_cast<int*>(base + kOffActive);
+    a.ru_list = nullptr;
     a.tol2 = tol * tol;
     a.delta = 0.1;
     a.maxit = maxit;
