@@ -315,7 +315,7 @@ void* sfh_batch_get_stream(sfh_batch* batch);
 int sfh_batch_set_rhs_block(sfh_batch* batch, int width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
  * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
- * (0 to 3 as below; FP64: 0) on the batch's current inputs and keep the
+ * (0 to 5 as below; FP64: 0) on the batch's current inputs and keep the
  * fastest.
  * The schedule never changes the results.  No counterpart in the reference
  * (its solver has no schedule). */
@@ -331,8 +331,10 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * solve, its phases separated by a grid barrier whose waits are bounded (a
  * wait that gives up fails the solve with SFH_ERR_TIMEOUT); the solutions
  * equal those of 2 bit for bit.  2 and 3 serve FP16, BF16 and FP32 12-real
- * storage (FP32 18-real takes 1).  Staging applies to the reduced precisions
- * only.  And its current values. */
+ * storage (FP32 18-real takes 1).  4 and 5: 0 and 1 with the FP64
+ * reliable-update hops taken out of the hop kernels into two kernels that
+ * walk a device list of the lanes due for one (as 2 and 3 always do).
+ * Staging applies to the reduced precisions only.  And its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Reliable-update threshold of the mixed precisions (default 0.1 for
  * the 16-bit storages, 0.01 for the FP32 ones): an FP64

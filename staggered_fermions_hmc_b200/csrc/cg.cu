@@ -519,7 +519,7 @@ __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const C
 
 // t = K p for the active lanes of one work item (tpi tiles of output parity
 // q, one RHS group); thi for lanes in a reliable update
-template <int GP, int SP, int NB, bool STG>
+template <int GP, int SP, int NB, bool STG, bool RUI>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
 {
@@ -536,8 +536,9 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
     const int q = ir.q, Vh = S.g.Vh;
     LanePass<NB> P;
     // the FP64 hop of lanes in a reliable update (mixed precisions only: FP64
-    // vectors belong to the plain FP64 CG, which has no reliable updates)
-    constexpr bool ru_here = SP != SP_F64;
+    // vectors belong to the plain FP64 CG, which has no reliable updates;
+    // RUI false: the lane-list kernels do it)
+    constexpr bool ru_here = RUI && SP != SP_F64;
     gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
     if (!(P.anyA || (ru_here && P.anyR))) return;
     const void* pin[NB];
@@ -661,7 +662,7 @@ __device__ __forceinline__ double site_dot(const Vec3<R>& a, const Vec3<R>& b)
 
 // own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
 // the four sums; reliable-update residuals
-template <int GP, int SP, int NB, bool STG>
+template <int GP, int SP, int NB, bool STG, bool RUI>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
 {
@@ -683,7 +684,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     // than a kernel of their own, and the compiler keeps the FP64 hop's
     // registers better with them here
     gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
-    if (!(P.anyA || P.anyR)) return;  // uniform across the block
+    if (!(P.anyA || (RUI && P.anyR))) return;  // uniform across the block
     bool part[NB], on[NB];
     double sums[NB * kSums];
     // this thread's partial sums across the item's tiles, in shared memory
@@ -694,7 +695,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
         on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
-        part[l] = on[l] || P.mode[l] == LM_RU;
+        part[l] = on[l] || (RUI && P.mode[l] == LM_RU);
         tin[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
 #pragma unroll
         for (int f = 0; f < kSums; ++f) s_part[l * kSums + f][threadIdx.x] = 0.0;
@@ -739,7 +740,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
     }
 #pragma unroll
     for (int f = 0; f < NB * kSums; ++f) sums[f] = s_part[f][threadIdx.x];
-    if (P.anyR) {
+    if (RUI && P.anyR) {
         for (int t = ir.first; t < ir.end; ++t) {
             const TileInfo ti = decode_tile(S, t);
             if (!ti.valid) break;
@@ -1340,38 +1341,45 @@ static CgKernels pick_sys(int nb, bool persistent)
     return k;
 }
 
-template <int GP, int SP, bool STG>
+template <int GP, int SP, bool STG, bool RUI>
 static HopKernel pick_hop1(int nb, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 8) { *nb_eff = 8; return cg_hop1<GP, SP, 8, STG>; }
-        if (nb >= 4) { *nb_eff = 4; return cg_hop1<GP, SP, 4, STG>; }
+        if (nb >= 8) { *nb_eff = 8; return cg_hop1<GP, SP, 8, STG, RUI>; }
+        if (nb >= 4) { *nb_eff = 4; return cg_hop1<GP, SP, 4, STG, RUI>; }
     }
-    if (nb >= 2) { *nb_eff = 2; return cg_hop1<GP, SP, 2, STG>; }
+    if (nb >= 2) { *nb_eff = 2; return cg_hop1<GP, SP, 2, STG, RUI>; }
     *nb_eff = 1;
-    return cg_hop1<GP, SP, 1, STG>;
+    return cg_hop1<GP, SP, 1, STG, RUI>;
 }
 
-template <int GP, int SP, bool STG>
+template <int GP, int SP, bool STG, bool RUI>
 static void pick_hop2(int nb, HopKernel* hop2, InitKernel* init, int* nb_eff)
 {
     if constexpr (SP != SP_F64) {
-        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4, STG>; *init = cg_init<SP, 4>; *nb_eff = 4; return; }
+        if (nb >= 4) { *hop2 = cg_hop2<GP, SP, 4, STG, RUI>; *init = cg_init<SP, 4>; *nb_eff = 4; return; }
     }
-    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2, STG>; *init = cg_init<SP, 2>; *nb_eff = 2; return; }
-    *hop2 = cg_hop2<GP, SP, 1, STG>;
+    if (nb >= 2) { *hop2 = cg_hop2<GP, SP, 2, STG, RUI>; *init = cg_init<SP, 2>; *nb_eff = 2; return; }
+    *hop2 = cg_hop2<GP, SP, 1, STG, RUI>;
     *init = cg_init<SP, 1>;
     *nb_eff = 1;
 }
 
-template <int GP, int SP, bool STG>
+// RUI: the hop kernels do the reliable-update hops of their lanes (inline);
+// otherwise the lane-list kernels cg_ru1_list / cg_ru2_list follow them
+template <int GP, int SP, bool STG, bool RUI>
 static CgKernels pick_typed(int nb1, int nb2)
 {
     CgKernels k;
-    k.hop1 = pick_hop1<GP, SP, STG>(nb1, &k.nb1);
-    pick_hop2<GP, SP, STG>(nb2, &k.hop2, &k.init, &k.nb2);
+    k.hop1 = pick_hop1<GP, SP, STG, RUI>(nb1, &k.nb1);
+    pick_hop2<GP, SP, STG, RUI>(nb2, &k.hop2, &k.init, &k.nb2);
     k.update = cg_update<SP>;
-    k.ru1 = k.ru2 = nullptr;  // the reliable-update hops run inside hop1 / hop2
+    if constexpr (RUI || SP == SP_F64) {
+        k.ru1 = k.ru2 = nullptr;
+    } else {
+        k.ru1 = cg_ru1_list<SP>;
+        k.ru2 = cg_ru2_list<SP>;
+    }
     k.smem = STG ? StageBytes<GP>::v : 0;
     k.sys = false;
     k.pers = nullptr;
@@ -1379,30 +1387,33 @@ static CgKernels pick_typed(int nb1, int nb2)
 }
 
 template <int GP, int SP>
-static CgKernels pick_staged(int nb1, int nb2, bool stage)
+static CgKernels pick_staged(int nb1, int nb2, bool stage, bool list)
 {
     if constexpr (GP == GP_F64_18) {
-        return pick_typed<GP, SP, false>(nb1, nb2);
+        return pick_typed<GP, SP, false, true>(nb1, nb2);
     } else {
-        return stage ? pick_typed<GP, SP, true>(nb1, nb2) : pick_typed<GP, SP, false>(nb1, nb2);
+        if (list) return stage ? pick_typed<GP, SP, true, false>(nb1, nb2) : pick_typed<GP, SP, false, false>(nb1, nb2);
+        return stage ? pick_typed<GP, SP, true, true>(nb1, nb2) : pick_typed<GP, SP, false, true>(nb1, nb2);
     }
 }
 
 // stage: 0 links read directly, 1 staged per work item, 2 system-blocked
 // kernels, 3 the system-blocked bodies in one persistent cooperative launch
 // (2 and 3: FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
+// stage 4, 5: 0, 1 with the reliable updates in the lane-list kernels
 static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
 {
     CgKernels k;
-    const bool sys = stage >= 2, pers = stage == 3;
-    if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false);
+    const bool sys = stage == 2 || stage == 3, pers = stage == 3, list = stage >= 4;
+    const bool stg = stage == 1 || stage == 5 || (sys && prec == SFH_PREC_F32_18);
+    if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false, false);
     else if (sys && prec == SFH_PREC_F16) k = pick_sys<GP_F16_12, SP_F16>(nb1, pers);
     else if (sys && prec == SFH_PREC_BF16) k = pick_sys<GP_BF16_12, SP_BF16>(nb1, pers);
     else if (sys && prec == SFH_PREC_F32) k = pick_sys<GP_F32_12, SP_F32>(nb1, pers);
-    else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stage != 0);
-    else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stage != 0);
-    else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stage != 0);
-    else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stage != 0);
+    else if (prec == SFH_PREC_F32) k = pick_staged<GP_F32_12, SP_F32>(nb1, nb2, stg, list);
+    else if (prec == SFH_PREC_F32_18) k = pick_staged<GP_F32_18, SP_F32>(nb1, nb2, stg, list);
+    else if (prec == SFH_PREC_BF16) k = pick_staged<GP_BF16_12, SP_BF16>(nb1, nb2, stg, list);
+    else k = pick_staged<GP_F16_12, SP_F16>(nb1, nb2, stg, list);
     if (k.smem) {  // opt in to the staged kernels' shared memory (idempotent)
         cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
         cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem);
@@ -2463,11 +2474,11 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
     int bw = 1, bt = 2, bs = 0;
-    const int nstage = f64 ? 1 : (b->prec == SFH_PREC_F32_18 ? 2 : 4);
-    for (int stage = 0; stage < nstage; ++stage)
+    for (int stage = 0; stage < (f64 ? 1 : 6); ++stage)
         for (int c = 0; c < ncand; ++c)
             for (int tp : tiles) {
-                if (stage >= 2 && tp != 1) continue;  // system-blocked: one tile per block
+                if ((stage == 2 || stage == 3) && (tp != 1 || b->prec == SFH_PREC_F32_18))
+                    continue;  // system-blocked: one tile per block; not for FP32 18-real links
                 double t = 0.0;
                 for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
                     auto t0 = std::chrono::steady_clock::now();
@@ -2495,7 +2506,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
-    if (stage_links < 0 || stage_links > 3) return SFH_ERR_INVALID;
+    if (stage_links < 0 || stage_links > 5) return SFH_ERR_INVALID;
     b->stage_links = stage_links;
     return SFH_OK;
 }
@@ -2503,7 +2514,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
 extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int stage_links)
 {
     if (!c || width < 0 || width > 8 || tiles_per_block < 0 || tiles_per_block > 64 || stage_links < 0 ||
-        stage_links > 3)
+        stage_links > 5)
         return SFH_ERR_INVALID;
     c->sched_nb = width;
     c->sched_tpi = tiles_per_block;

@@ -182,12 +182,15 @@ def test_batch_full_lattice_matches_single(sfh, orc):
 
 
 def test_batch_rhs_block_widths_agree(sfh, orc):
-    """The RHS-block width, the tiles per block and link staging change
-    scheduling only, not results (bit-identical solutions)."""
+    """The RHS-block width, the tiles per block, link staging and where the
+    reliable updates run (inside the hop kernels or in the lane-list kernels,
+    stages 4 and 5) change scheduling only, not results (bit-identical
+    solutions)."""
     systems = [((4, 4, 4, 8), 0.1, 6)]
     U = orc.random_gauge(systems[0][0], 0.5, 7)
     out = []
-    for w, tiles, stage in ((1, 1, False), (2, 2, True), (4, 3, False), (8, 4, True), (2, 1, True)):
+    for w, tiles, stage in ((1, 1, False), (2, 2, True), (4, 3, False), (8, 4, True), (2, 1, True), (2, 4, 4),
+                            (4, 2, 5)):
         B = sfh.Batch(systems, precision="f32")
         B.set_schedule(w, tiles, stage)
         assert B.schedule() == (w, tiles, stage)
