@@ -665,6 +665,21 @@ def run_c5(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_hmc(args):
+    """A short launch of every HMC kernel on an L^4 lattice (eps = 0.3 links,
+    random momenta, one launch each after the untimed ones of
+    sfh_kernel_timing): the case for kernel profiling; prints one line."""
+    import staggered_fermions_hmc_b200 as sfh
+    sfh.load_library()
+    L = args.profile_hmc
+    lat = sfh.Lattice((L, L, L, L), 0.02, 4.2)
+    lat.random_gauge(0.3, 5)
+    lat.generate_conjugate_field_configuration(6)
+    ms = {name: lat.kernel_timing(name, nrep=1) for name in lat.HMC_KERNELS}
+    lat.close()
+    print(json.dumps({"profile_hmc": True, "dims": [L] * 4, "ms": ms}), flush=True)
+
+
 def run_profile_case(args, spec):
     import staggered_fermions_hmc_b200 as sfh
     sfh.load_library()
@@ -704,6 +719,8 @@ def main():
                     help="build the batch, run --warmup solves, then one solve capped at --maxit "
                          "iterations (a short launch for kernel profiling); prints one line")
     ap.add_argument("--maxit", type=int, default=MAXIT)
+    ap.add_argument("--profile-hmc", type=int, default=0, metavar="L",
+                    help="launch every HMC kernel once on an L^4 lattice (a case for kernel profiling)")
     ap.add_argument("--workload", default="batch", choices=["batch", "c5"],
                     help="batch: the headline uneven-batch CG (default); c5: full HMC on 24^4, its own JSON line")
     ap.add_argument("--c5-traj", type=int, default=50)
@@ -713,6 +730,9 @@ def main():
     spec = batch_spec(nsys=args.nsys)
     if args.workload == "c5":
         run_c5(args)
+        return
+    if args.profile_hmc:
+        run_profile_hmc(args)
         return
     if args.profile_case:
         run_profile_case(args, spec)
