@@ -1067,28 +1067,40 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
 
 // The FP64 reliable updates of the lanes on this iteration's list (the
 // lanes whose recurrence asked for one in the last iteration), walked by a
-// small fixed grid: blk / nblk split each lane's work items among the blocks.
+// small fixed grid of nblk blocks.
 // ru1: thi = K (x_hi + x_lo) on the tiles of the other parity; ru2: x_hi +=
 // x_lo, r = b - M x_hi and |r|^2 on the lane's own tiles, in work items of
 // tpi tiles whose sums complete the lane's partial-sum slots and ticket (the
 // same order of additions as the hop kernels' own reliable-update loops).
+// The listed lanes' work items (tpi tiles of a lane's tiles) are numbered in
+// list order and dealt to the blocks round robin: pair k goes to block
+// k mod nblk.  Every block walks the list (block-uniform) and takes its pairs.
 template <int SP, bool COH>
 __device__ __forceinline__ void ru1_list_body(const CgArgs& a, int cur, int blk, int nblk, CgSys* s_sys)
 {
     constexpr int XP = XFmt<SP>::v;
     const int* lst = a.ru_list + cur * (a.nlanes + 1);
     const int n = ld_int(lst);
+    int off = 0;  // pairs of the lanes before this one
     for (int u = 0; u < n; ++u) {
         const int lane = ld_int(lst + 1 + u);
         const CgLane* L = a.lanes + lane;  // sys, rhs and parity are fixed for the solve
+        const int ntq = a.sys[L->sys].ntq;
+        const int nsq = (ntq + a.tpi - 1) / a.tpi;
+        int g = ((blk - off) % nblk + nblk) % nblk;  // this block's first item of the lane
+        off += nsq;
+        if (g >= nsq) continue;  // uniform in the block
         __syncthreads();
         if (threadIdx.x == 0) *s_sys = a.sys[L->sys];
         __syncthreads();
         const CgSys& S = *s_sys;
         const int q = 1 - L->parity, rid = L->rhs;
-        for (int j = blk; j < S.ntq; j += nblk) {
-            const int i = j * kTile + (int)threadIdx.x;
-            if (i < S.g.Vh) ru_hop1<XP, COH>(a, S, eo_coords(S.g, q, i), q, i, rid);
+        for (; g < nsq; g += nblk) {
+            const int j1 = min((g + 1) * a.tpi, S.ntq);
+            for (int j = g * a.tpi; j < j1; ++j) {
+                const int i = j * kTile + (int)threadIdx.x;
+                if (i < S.g.Vh) ru_hop1<XP, COH>(a, S, eo_coords(S.g, q, i), q, i, rid);
+            }
         }
     }
 }
@@ -1100,15 +1112,20 @@ __device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk,
     constexpr int XP = XFmt<SP>::v;
     const int* lst = a.ru_list + cur * (a.nlanes + 1);
     const int n = ld_int(lst);
+    int off = 0;
     for (int u = 0; u < n; ++u) {
         const int lane = ld_int(lst + 1 + u);
         const CgLane* L = a.lanes + lane;
+        const int ntq = a.sys[L->sys].ntq;
+        const int nsq = (ntq + a.tpi - 1) / a.tpi;
+        int g = ((blk - off) % nblk + nblk) % nblk;
+        off += nsq;
+        if (g >= nsq) continue;  // uniform in the block
         __syncthreads();
         if (threadIdx.x == 0) *s_sys = a.sys[L->sys];
         __syncthreads();
         const CgSys& S = *s_sys;
         const int p = L->parity, rid = L->rhs;
-        const int nsq = item_groups(a, S);
         LanePass<1> P;
         P.lane[0] = lane;
         P.mode[0] = LM_RU;
@@ -1116,7 +1133,7 @@ __device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk,
         P.alpha[0] = P.beta[0] = 0.0;
         P.anyA = false;
         P.anyR = true;
-        for (int g = blk; g < nsq; g += nblk) {
+        for (; g < nsq; g += nblk) {
             double sums[kSums] = {0.0, 0.0, 0.0, 0.0};
             const int j1 = min((g + 1) * a.tpi, S.ntq);
             for (int j = g * a.tpi; j < j1; ++j) {
