@@ -178,12 +178,12 @@ def solve_bytes(spec, infos, precision):
 
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
 # algorithmic byte of cg_hop2 for one launch of the first 8 systems of the
-# batch with every lane active, RHS groups of 2, 4 tiles per block (the ncu
-# captures of the three iteration kernels kept under profiles/): f32 553.2 MB
-# for 491.0 MB, f16 (packed-half products, links read directly) 247.3 MB for
-# 291.9 MB.  The bench scales it to its own launches by their algorithmic
-# bytes.
-HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 247.3 / 291.9}
+# batch with every lane active, RHS groups of 2, 4 tiles per work item, links
+# read directly (the headline schedule): f16 251.3 MB for 291.9 MB (a
+# single-kernel ncu capture, summarised under profiles/), f32 553.2 MB for
+# 491.0 MB (the FP32 capture summarised there).
+# The bench scales it to its own launches by their algorithmic bytes.
+HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 251.3 / 291.9}
 
 
 def build_batch(sfh, spec, precision, device):
