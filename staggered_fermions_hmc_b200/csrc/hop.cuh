@@ -157,6 +157,25 @@ __device__ __forceinline__ void hlink_load(const uint2* s, int tile, const void*
     hlink_unpack(w, e);
 }
 
+// f broadcast to both halves of a packed FP32 pair
+__device__ __forceinline__ unsigned long long f32x2_bcast(float f)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(f));
+    return r;
+}
+
+// (acc.re, acc.im) += f2 * (y.x, y.y) as one packed FP32 FMA (fma.rn.f32x2,
+// sm_100 and later): each half rounds as fmaf does
+__device__ __forceinline__ void acc_f32x2(Cx<float>& acc, unsigned long long f2, float2 y)
+{
+    unsigned long long b, c, d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(y.x), "f"(y.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(c) : "f"(acc.re), "f"(acc.im));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2), "l"(b), "l"(c));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(acc.re), "=f"(acc.im) : "l"(d));
+}
+
 // acc += f (U v) (ADJ false) or acc += f (U^dag v) (ADJ true) for a stored
 // FP16 vector v with site scale sc: f = s sc, products in half2
 template <bool ADJ, bool COH = false>
@@ -165,7 +184,7 @@ __device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9]
 {
     const uint4 w = ld_vec<COH>((const uint4*)in + (size_t)nq * Vh + j);
     const __half2 v[3] = {h2_bits(w.x), h2_bits(w.y), h2_bits(w.z)};
-    f *= __uint_as_float(w.w);
+    const unsigned long long f2 = f32x2_bcast(f * __uint_as_float(w.w));
     __half2 vp[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) vp[k] = ADJ ? __hneg2(h2_perp(v[k])) : h2_perp(v[k]);
@@ -180,9 +199,7 @@ __device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9]
             y = __hfma2(__low2half2(u), v[k], y);
             y = __hfma2(__high2half2(u), vp[k], y);
         }
-        const float2 yf = __half22float2(y);
-        acc.c[r].re = fmaf(f, yf.x, acc.c[r].re);
-        acc.c[r].im = fmaf(f, yf.y, acc.c[r].im);
+        acc_f32x2(acc.c[r], f2, __half22float2(y));
     }
 }
 
