@@ -53,8 +53,13 @@ constexpr int kSums = 4;  // <p,v>, <r,v>, |v|^2, |r|^2
 // hold a link in nine registers; measured 6 % faster on the uneven batch than
 // three, despite a few spilled words); wider RHS groups and FP64 take 128
 // registers and two
-template <int GP, int SP, int NB, bool SUMS> struct HopOcc {
-    static constexpr int v = (SP == SP_F64 || NB > 2) ? 2 : ((GP == GP_F16_12 && SP == SP_F16) ? 4 : 3);
+template <int GP, int SP, int NB, bool SUMS, bool RUI = true> struct HopOcc {
+    // without the inline FP64 reliable-update hop the kernels need fewer
+    // registers: FP16 fits in 48 (five blocks), the FP32-arithmetic ones with
+    // 12-real links in 64 (four); 18-real FP32 links keep three
+    static constexpr int v = (SP == SP_F64 || NB > 2) ? 2
+                             : ((GP == GP_F16_12 && SP == SP_F16) ? (RUI ? 4 : 5)
+                                                                   : ((RUI || GP == GP_F32_18) ? 3 : 4));
 };
 
 // one RHS pass of a tile: the lanes and their scalars
@@ -520,7 +525,7 @@ __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const C
 // t = K p for the active lanes of one work item (tpi tiles of output parity
 // q, one RHS group); thi for lanes in a reliable update
 template <int GP, int SP, int NB, bool STG, bool RUI>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false>::v))
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
     cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -663,7 +668,7 @@ __device__ __forceinline__ double site_dot(const Vec3<R>& a, const Vec3<R>& b)
 // own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
 // the four sums; reliable-update residuals
 template <int GP, int SP, int NB, bool STG, bool RUI>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true>::v))
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
     cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -1065,6 +1070,9 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
     }
 }
 
+// blocks of the lane-list kernels per SM (their grid, and their launch bounds)
+constexpr int kListBlocksPerSm = 3;
+
 // The FP64 reliable updates of the lanes on this iteration's list (the
 // lanes whose recurrence asked for one in the last iteration), walked by a
 // small fixed grid of nblk blocks.
@@ -1150,14 +1158,14 @@ __device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk,
 }
 
 template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru1_list(CgArgs a, const int2* __restrict__, int cur)
+__global__ void __launch_bounds__(kTile, kListBlocksPerSm) cg_ru1_list(CgArgs a, const int2* __restrict__, int cur)
 {
     __shared__ CgSys s_sys;
     ru1_list_body<SP, false>(a, cur, blockIdx.x, gridDim.x, &s_sys);
 }
 
 template <int SP>
-__global__ void __launch_bounds__(kTile) cg_ru2_list(CgArgs a, const int2* __restrict__, int cur)
+__global__ void __launch_bounds__(kTile, kListBlocksPerSm) cg_ru2_list(CgArgs a, const int2* __restrict__, int cur)
 {
     __shared__ CgSys s_sys;
     __shared__ double s_bs[32];
@@ -1319,8 +1327,7 @@ static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
     return n;
 }
 
-// blocks of the lane-list kernels per SM
-constexpr int kListBlocksPerSm = 2;
+
 
 // work-item width of the system-blocked kernels: one item per tile, covering
 // every RHS of the system
