@@ -602,6 +602,8 @@ def run_c5(args):
 
     def new_lattice():
         lat = sfh.Lattice(dims, 0.02, 4.2)
+        if args.c5_schedule:
+            lat.set_schedule(*[int(x) for x in args.c5_schedule.split(",")])
         lat.random_gauge(0.3, 5)
         lat.set_fermion_smearing(0.125, 4)
         lat.set_hasenbusch(0.2)
@@ -654,7 +656,8 @@ def run_c5(args):
         "workload": "24^4, Symanzik beta 4.2, Hasenbusch pair m 0.02 / 0.2 on 4-level stout (rho 0.125) fermion "
                     f"links, leapfrog tau = 1 with {N} steps, {ntraj} trajectories from an eps = 0.3 start "
                     "(seed 5), no heatbath",
-        "precision": {"mixed": args.c5_precision, "arithmetic": ARITHMETIC[args.c5_precision]},
+        "precision": {"mixed": args.c5_precision, "arithmetic": ARITHMETIC[args.c5_precision],
+                      "schedule": args.c5_schedule or "default"},
         "mixed": summary(mixed, pmix), "fp64": summary(f64, p64),
         "accept_decisions_equal": float(np.mean(same)),
         "dH_mixed_minus_fp64_max": float(max(abs(a["dH"] - b["dH"]) for a, b in zip(mixed, f64))),
@@ -726,6 +729,8 @@ def main():
     ap.add_argument("--c5-traj", type=int, default=50)
     ap.add_argument("--c5-steps", type=int, default=20)
     ap.add_argument("--c5-precision", default="f32", choices=["f32", "f16", "bf16", "f32_18"])
+    ap.add_argument("--c5-schedule", default="",
+                    help="W,T,S: schedule of the trajectory's mixed-precision solves (sfh_set_schedule)")
     args = ap.parse_args()
     spec = batch_spec(nsys=args.nsys)
     if args.workload == "c5":
