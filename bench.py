@@ -920,7 +920,7 @@ def main():
         "kernels": kernels,
         "solve_roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                            "alg_bytes_per_step": alg_bytes,
-                           "what": "all three iteration kernels, graph replay, per timed step"},
+                           "what": "every iteration kernel, graph replay, per timed step"},
         "other_mixed_precisions": other,
         "solver_config": {"precision": args.precision, "arithmetic": ARITHMETIC[args.precision],
                           "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
