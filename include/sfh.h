@@ -336,6 +336,11 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * walk a device list of the lanes due for one (as 2 and 3 always do).
  * Staging applies to the reduced precisions only.  And its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
+/* Bound on each grid-barrier wait of the persistent schedule (3), in polls
+ * of about 128 ns (0 = the default, about 4 s): a wait that runs out fails
+ * the solve with SFH_ERR_TIMEOUT and leaves the batch usable.  No
+ * counterpart in the reference. */
+int sfh_batch_set_barrier_polls(sfh_batch* batch, long long polls);
 /* Reliable-update threshold of the mixed precisions (default 0.1 for
  * the 16-bit storages, 0.01 for the FP32 ones): an FP64
  * update (x_hi += x_lo, r = b - M x_hi) when the iterated residual has dropped

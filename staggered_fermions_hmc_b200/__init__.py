@@ -145,6 +145,7 @@ SIGNATURES = {
     "sfh_hex_staples": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
     "sfh_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_set_barrier_polls": (ctypes.c_int, [_VP, ctypes.c_longlong]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -579,6 +580,11 @@ class Batch:
         one persistent cooperative launch."""
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
+
+    def set_barrier_polls(self, polls):
+        """Bound on each grid-barrier wait of the persistent schedule (0: the
+        default, about 4 s)."""
+        self._check(self.lib.sfh_batch_set_barrier_polls(self.h, int(polls)), "set_barrier_polls")
 
     def set_reliable_delta(self, delta):
         """Reliable-update threshold of the mixed precisions (default 0.1 for

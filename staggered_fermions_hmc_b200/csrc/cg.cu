@@ -1210,9 +1210,10 @@ struct GridBar {
     unsigned count, gen;
     int err;  // set when a wait gave up
     unsigned pad;
+    long long polls;  // bound on each wait
 };
 
-constexpr long long kBarrierPolls = 1ll << 25;  // about 4 s at the 128 ns back-off
+constexpr long long kBarrierPolls = 1ll << 25;  // about 4 s at the 128 ns back-off (the default bound)
 
 __device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblocks, int* s_ok)
 {
@@ -1230,8 +1231,9 @@ __device__ __forceinline__ bool grid_barrier(GridBar* b, unsigned nblocks, int* 
                 atomicAdd(&b->gen, 1u);
             } else {
                 long long polls = 0;
+                const long long limit = b->polls;
                 while (*vgen == g) {
-                    if (*verr != 0 || ++polls > kBarrierPolls) {
+                    if (*verr != 0 || ++polls > limit) {
                         atomicOr(&b->err, 1);
                         ok = 0;
                         break;
@@ -1478,6 +1480,7 @@ struct CgWorkspace {
     GridBar* d_bar = nullptr;  // grid barrier of the persistent solve
     int* d_rulist = nullptr;   // reliable-update lane lists [2][1 + nlanes]
     bool timed_out = false;    // the last persistent solve gave up at a barrier
+    long long barrier_polls = 0;  // bound on each barrier wait (0: the default)
     int num_sms = 0;
     std::vector<void*> allocs;
     size_t bytes = 0;
@@ -1765,7 +1768,11 @@ static cudaError_t persistent_solve(CgWorkspace& w, const CgKernels& k, CgArgs a
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.pers, kTile, k.smem)) != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
     const int grid = std::max(1, std::min(per_sm * w.num_sms, std::max(nhop, nupd)));
-    if ((e = cudaMemsetAsync(w.d_bar, 0, sizeof(GridBar), stream)) != cudaSuccess) return e;
+    GridBar bar0;
+    std::memset(&bar0, 0, sizeof(bar0));
+    bar0.polls = w.barrier_polls > 0 ? w.barrier_polls : kBarrierPolls;
+    if ((e = cudaMemcpyAsync(w.d_bar, &bar0, sizeof(GridBar), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     if (timing) {
         for (int r = 0; r < kTimedPhases; ++r) {
@@ -2543,6 +2550,13 @@ extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int 
     c->sched_nb = width;
     c->sched_tpi = tiles_per_block;
     c->sched_stage = stage_links;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_set_barrier_polls(sfh_batch* b, long long polls)
+{
+    if (!b || polls < 0) return SFH_ERR_INVALID;
+    b->ws.barrier_polls = polls;
     return SFH_OK;
 }
 

@@ -361,3 +361,26 @@ def test_lattice_solve_persistent_schedule(sfh, orc, precision):
         assert np.array_equal(out[0], out[1])
     finally:
         lat.close()
+
+
+def test_persistent_barrier_wait_runs_out_and_the_batch_stays_usable(sfh, orc):
+    """The persistent schedule's grid barrier waits a bounded number of polls.
+    With the bound cut to one poll the first wait of a multi-block launch runs
+    out: every block leaves at its next wait, the solve returns
+    SFH_ERR_TIMEOUT, and the next solve with the default bound on the same
+    batch (same context) is correct."""
+    tol = 1e-10
+    B, data = _sys_batch(sfh, orc, "f16", (2, 1, 3))
+    try:
+        B.set_barrier_polls(1)
+        with pytest.raises(sfh.SfhError) as e:
+            B.solve(tol=tol, max_iter=20000)
+        assert e.value.status == sfh.SFH_ERR_TIMEOUT
+        B.set_barrier_polls(0)
+        B.solve(tol=tol, max_iter=20000)
+        for k, (dims, mass, nrhs) in enumerate(SYS_SYSTEMS):
+            U, bs = data[k]
+            for j in range(nrhs):
+                assert true_resid(orc, dims, mass, U, bs[j], B.solution(k, j)) < 1.05 * tol
+    finally:
+        B.close()
