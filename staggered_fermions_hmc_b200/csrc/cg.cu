@@ -1,5 +1,6 @@
-// cg.cu — batched conjugate-gradient solver for D D^dag x = b (three kernels
-// per iteration, replayed as CUDA-graph chunks).
+// cg.cu — batched conjugate-gradient solver for D D^dag x = b (three to five
+// kernels per iteration, replayed as CUDA-graph chunks, or one persistent
+// launch per solve).
 //
 // Restates solve_CG_DDdagger (Fermions.cpp:553-617) for the GPU.  D D^dag =
 // m^2 - K^2 and K couples only even and odd sites, so D D^dag is block
@@ -22,8 +23,14 @@
 // convergence test (Fermions.cpp:569).  One reduction point per iteration.
 //
 // Work is split into tiles of 256 sites of one system and one output parity.
-// A tile processes all lanes of its system that are active in the phase, so a
-// link loaded once serves every right-hand side (RHS blocking).
+// A work item is a range of tiles and a group of the system's RHS, so a link
+// loaded once serves every RHS of the group (RHS blocking).  Schedules (the
+// autotuner times them; results never depend on the choice): links read
+// directly or staged per work item; the FP64 reliable-update hops inside the
+// hop kernels or in two kernels walking a device list of the lanes due for
+// one; system-blocked kernels (one tile per block, every RHS of the system,
+// the tile's links staged once); and the system-blocked work in one
+// cooperative launch with a bounded grid barrier.
 //
 // Mixed precision (FP32 or FP16+scale vectors with FP32 / FP16 12-real links):
 // x is accumulated in FP32 between reliable updates.  When |r| has dropped by
