@@ -179,11 +179,13 @@ def solve_bytes(spec, infos, precision):
 # DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
 # algorithmic byte of cg_hop2 for one launch of the first 8 systems of the
 # batch with every lane active, RHS groups of 2, 4 tiles per work item, links
-# read directly (the headline schedule): f16 251.3 MB for 291.9 MB (a
-# single-kernel ncu capture, summarised under profiles/), f32 553.2 MB for
-# 491.0 MB (the FP32 capture summarised there).
-# The bench scales it to its own launches by their algorithmic bytes.
-HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 251.3 / 291.9}
+# read directly, reliable updates in the lane-list kernels (the headline
+# schedule): f16 284.0 MB for 291.9 MB (a single-kernel ncu capture,
+# summarised under profiles/); f32 553.2 MB for 491.0 MB (the FP32 capture
+# summarised there, of the same work items with the updates inside the hop
+# kernels).  The bench scales it to its own launches by their algorithmic
+# bytes.
+HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 284.0 / 291.9}
 
 
 def build_batch(sfh, spec, precision, device):
