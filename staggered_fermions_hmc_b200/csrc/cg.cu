@@ -73,7 +73,7 @@ template <int GP, int SP, int NB, bool SUMS, bool RUI = true> struct HopOcc {
 template <int NB>
 struct LanePass {
     int lane[NB], mode[NB], rid[NB];
-    double alpha[NB], beta[NB];
+    double alpha[NB], beta[NB], m2[NB];
     bool anyA, anyR;
 };
 
@@ -90,11 +90,13 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
         P.rid[l] = 0;
         P.alpha[l] = 0.0;
         P.beta[l] = 0.0;
+        P.m2[l] = 0.0;
         if (l < cnt) {
             P.lane[l] = lane_of(S, base + l, q, hop1);
             const CgLane* L = a.lanes + P.lane[l];
             P.mode[l] = ld_int(&L->mode[cur]);
             P.rid[l] = __ldg(&L->rhs);
+            P.m2[l] = __ldg(&L->m2);  // fixed for the solve
             if (scalars && P.mode[l] == LM_ACTIVE) {
                 P.alpha[l] = ld_dbl(&L->alpha);
                 P.beta[l] = ld_dbl(&L->beta);
@@ -600,7 +602,8 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
 // reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
 // r = b - M x_hi; returns the |r|^2 contribution (FP64)
 template <int SP, int XP, bool COH = false>
-__device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const Coord& c, int q, int i, int rid)
+__device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const Coord& c, int q, int i, int rid,
+                                          double m2)
 {
     typedef typename SpinorFmt<SP>::R RS;
     const int nq = 1 - q, Vh = S.g.Vh;
@@ -630,8 +633,8 @@ __device__ __forceinline__ double ru_hop2(const CgRhs* a, const CgSys& S, const 
     Vec3<double> res;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        res.c[k].re = b.c[k].re - (S.m2 * xn.c[k].re - 0.5 * acc.c[k].re);
-        res.c[k].im = b.c[k].im - (S.m2 * xn.c[k].im - 0.5 * acc.c[k].im);
+        res.c[k].re = b.c[k].re - (m2 * xn.c[k].re - 0.5 * acc.c[k].re);
+        res.c[k].im = b.c[k].im - (m2 * xn.c[k].im - 0.5 * acc.c[k].im);
     }
     // The search direction of the previous update, p = r_iter + beta p_old,
     // was built from the iterated residual; give it the true one instead,
@@ -725,10 +728,10 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
             hop_lanes<GP, SP, NB, STG>(S.Ulo, sl, n, q, ti.i, Vh, tin, on, acc);
-            const R m2 = (R)S.m2;
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
                 if (!on[l]) continue;
+                const R m2 = (R)P.m2[l];
                 Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
                 Vec3<RS> p = r;
                 if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
@@ -759,7 +762,8 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
             const Coord c = eo_coords(S.g, q, ti.i);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (P.mode[l] == LM_RU) sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l]);
+                if (P.mode[l] == LM_RU)
+                    sums[l * kSums + 3] += ru_hop2<SP, XP>(a.rhs, S, c, q, ti.i, P.rid[l], P.m2[l]);
         }
     }
     block_sum<NB * kSums>(sums, smem);
@@ -1020,7 +1024,6 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
         n = neighbours(S.g, eo_coords(S.g, q, ti.i));
         stage_tile_links<GP, SP>(stage, S.Ulo, n, q, ti.i, Vh);
     }
-    const R m2 = (R)S.m2;
     for (int base = 0; base < S.nrhs; base += NB) {
         LanePass<NB> P;
         gather_pass<NB>(a, S, base, q, false, cur, false, P);
@@ -1043,6 +1046,7 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
 #pragma unroll
             for (int l = 0; l < NB; ++l) {
                 if (!on[l]) continue;
+                const R m2 = (R)P.m2[l];
                 Vec3<RS> r = SpinorFmt<SP>::template load<COH>(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
                 Vec3<RS> p = r;
                 if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
@@ -1146,6 +1150,7 @@ __device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk,
         P.mode[0] = LM_RU;
         P.rid[0] = rid;
         P.alpha[0] = P.beta[0] = 0.0;
+        P.m2[0] = L->m2;
         P.anyA = false;
         P.anyR = true;
         for (; g < nsq; g += nblk) {
@@ -1153,7 +1158,7 @@ __device__ __forceinline__ void ru2_list_body(const CgArgs& a, int cur, int blk,
             const int j1 = min((g + 1) * a.tpi, S.ntq);
             for (int j = g * a.tpi; j < j1; ++j) {
                 const int i = j * kTile + (int)threadIdx.x;
-                if (i < S.g.Vh) sums[3] += ru_hop2<SP, XP, COH>(a.rhs, S, eo_coords(S.g, p, i), p, i, rid);
+                if (i < S.g.Vh) sums[3] += ru_hop2<SP, XP, COH>(a.rhs, S, eo_coords(S.g, p, i), p, i, rid, P.m2[0]);
             }
             block_sum<kSums>(sums, s_bs);
             const bool part[1] = {true};
@@ -1593,6 +1598,7 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
                 std::memset(&L, 0, sizeof(L));
                 L.sys = k;
                 L.rhs = rid;
+                L.m2 = S.m2;
                 L.parity = both ? 2 : lp;
                 L.poff = poff;  // slots indexed by the tile's local index (both parities)
                 poff += kSums * 2 * S.ntq;
@@ -2274,6 +2280,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     if (!w) return cuda_check(c, e, "cg workspace");
     if (c->ws_mass[prec] != c->mass) {  // the mass lives in the device system table
         w->sys[0].m2 = c->mass * c->mass;
+        for (CgLane& L : w->lanes_h) L.m2 = w->sys[0].m2;  // uploaded with the lanes at the solve
         e = cudaMemcpyAsync(w->d_sys, w->sys.data(), sizeof(CgSys), cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg mass");
         c->ws_mass[prec] = c->mass;
@@ -2311,10 +2318,10 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
 }
 
 // Two solves on the context's links at two masses (a Hasenbusch pair) as one
-// batch of two systems sharing the links: their lanes iterate together and
-// the heavy system's retire first, instead of two solves one after the
-// other.  FP64 runs full-lattice lanes (the reference's CG), as
-// ctx_solve_device does.
+// system with two right-hand sides, each lane carrying its own mass: the
+// work items serve both RHS, so a link read once serves both masses, the
+// lanes iterate together and the heavy mass's retire first.  FP64 runs
+// full-lattice lanes (the reference's CG), as ctx_solve_device does.
 int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_eo[2], const double mass[2],
                           double tol, int maxit, int prec, sfh_cg_info info[2])
 {
@@ -2328,34 +2335,28 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
     if (!w) {
         w = new CgWorkspace();
         const void* const lo[5] = {c->U64, c->U32, c->U16, c->U32_18, c->Ubf16};
-        std::vector<SolverSystemHost> hs(2);
-        for (int k = 0; k < 2; ++k) {
-            hs[k].g = c->g;
-            hs[k].mass = mass[k];
-            hs[k].nrhs = 1;
-            hs[k].U64 = c->U64;
-            hs[k].Ulo = lo[prec];
-        }
+        std::vector<SolverSystemHost> hs(1);
+        hs[0].g = c->g;
+        hs[0].mass = mass[0];
+        hs[0].nrhs = 2;
+        hs[0].U64 = c->U64;
+        hs[0].Ulo = lo[prec];
         e = workspace_build(*w, hs, prec, prec == SFH_PREC_F64 ? 1 : 0);
         if (e != cudaSuccess) {
             delete w;
             return cuda_check(c, e, "cg pair workspace");
         }
         c->ws_pair[prec] = w;
+        c->ws_pair_mass[prec][0] = c->ws_pair_mass[prec][1] = -1.0;  // set below
+    }
+    if (c->ws_pair_mass[prec][0] != mass[0] || c->ws_pair_mass[prec][1] != mass[1]) {
+        for (CgLane& L : w->lanes_h) L.m2 = mass[L.rhs] * mass[L.rhs];  // uploaded with the lanes
         c->ws_pair_mass[prec][0] = mass[0];
         c->ws_pair_mass[prec][1] = mass[1];
     }
-    if (c->ws_pair_mass[prec][0] != mass[0] || c->ws_pair_mass[prec][1] != mass[1]) {
-        for (int k = 0; k < 2; ++k) {
-            w->sys[k].m2 = mass[k] * mass[k];
-            c->ws_pair_mass[prec][k] = mass[k];
-        }
-        e = cudaMemcpyAsync(w->d_sys, w->sys.data(), 2 * sizeof(CgSys), cudaMemcpyHostToDevice, c->stream);
-        if (e != cudaSuccess) return cuda_check(c, e, "cg pair masses");
-    }
     const size_t fs = (size_t)c->g.V * 6 * sizeof(double);
     for (int k = 0; k < 2; ++k) {
-        e = cudaMemcpyAsync(w->rhs[w->rhs0[k]].b, b_eo[k], fs, cudaMemcpyDeviceToDevice, c->stream);
+        e = cudaMemcpyAsync(w->rhs[k].b, b_eo[k], fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair rhs");
     }
     const bool lowp = prec != SFH_PREC_F64;
@@ -2364,7 +2365,7 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
     if (e != cudaSuccess) return cuda_check(c, e, "cg pair solve");
     if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
     for (int k = 0; k < 2; ++k) {
-        e = cudaMemcpyAsync(x_eo[k], w->rhs[w->rhs0[k]].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
+        e = cudaMemcpyAsync(x_eo[k], w->rhs[k].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair solution");
     }
     int status = SFH_OK;
@@ -2373,7 +2374,7 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
         std::memset(&inf, 0, sizeof(inf));
         double rr = 0, bb = 0;
         for (const CgLane& L : w->lanes_h) {
-            if (L.sys != k) continue;
+            if (L.rhs != k) continue;
             if (L.status != SFH_OK && inf.status == SFH_OK) inf.status = L.status;
             inf.iters = std::max(inf.iters, L.iters);
             if (L.parity < 2) inf.iters_parity[L.parity] = L.iters;

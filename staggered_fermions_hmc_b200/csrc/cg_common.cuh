@@ -38,6 +38,7 @@ struct CgRhs {
 
 struct CgLane {
     int sys, rhs, parity, poff;
+    double m2;  // the lane's mass squared (the system's, or its own for RHS at several masses)
     double bb, target, rr, rr_old, pAp, alpha, beta, rmax, rr_next;
     int mode[2];
     int iters, nru, status, pad;

@@ -441,9 +441,12 @@ def test_heatbath_rejects_extents_not_multiple_of_four(sfh, orc):
 
 
 # --- Hasenbusch pair (no counterpart in the reference) --------------------
-def test_hasenbusch_force_vs_oracle(sfh, orc):
+@pytest.mark.parametrize("precision,tol,bound", [("f64", 1e-13, 1e-10), ("f16", 1e-11, 1e-7)])
+def test_hasenbusch_force_vs_oracle(sfh, orc, precision, tol, bound):
     """P -= dt F with F = F_f(X_h, Y_h) + (m_h^2 - m^2) F_f(X, Y), X_h solved at
-    the heavy mass, X at the light one."""
+    the heavy mass, X at the light one: the two solves run as one system with
+    two right-hand sides, each lane at its own mass (FP64, and FP16 with FP64
+    reliable updates, whose solutions sit within cond(M) tol of the oracle's)."""
     dims, m, mh, beta, dt = (4, 4, 4, 8), 0.1, 0.4, 4.2, 0.05
     U = orc.random_gauge(dims, 0.4, 201)
     phi = orc.random_spinor(dims, 202)
@@ -452,12 +455,12 @@ def test_hasenbusch_force_vs_oracle(sfh, orc):
     lat.upload_gauge(U)
     lat.upload_momenta(np.zeros(72 * int(np.prod(dims))))
     lat.set_hasenbusch(mh, phih)
-    lat.momentum_kick(dt, phi, forces="fermion", tol=1e-13)
+    lat.momentum_kick(dt, phi, forces="fermion", tol=tol, precision=precision)
     Xh, _, _, _ = orc.cg(dims, mh, U, phih, 1e-13)
     Xr, _, _, _ = orc.cg(dims, m, U, phi, 1e-13)
     F = orc.fermion_force(dims, U, Xh, orc.dirac(dims, mh, U, Xh, dagger=True)) + \
         (mh * mh - m * m) * orc.fermion_force(dims, U, Xr, orc.dirac(dims, m, U, Xr, dagger=True))
-    assert rel(lat.download_momenta(), -dt * F) < 1e-10
+    assert rel(lat.download_momenta(), -dt * F) < bound
 
 
 @pytest.mark.parametrize("smear", [0, 2])
