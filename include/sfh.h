@@ -350,6 +350,11 @@ int sfh_batch_set_reliable_delta(sfh_batch* batch, double delta);
 int sfh_batch_get_schedule(sfh_batch* batch, int* width, int* tiles_per_block, int* stage_links);
 int sfh_batch_set_gauge(sfh_batch* batch, int sys, const double* links);
 int sfh_batch_set_rhs(sfh_batch* batch, int sys, int rhs, const double* phi);
+/* The mass of one right-hand side (default: its system's), so that the RHS of
+ * a system can be solves at several masses on the same links (a Hasenbusch
+ * pair, a multi-mass set): they share the system's link loads.  No
+ * counterpart in the reference (one mass per program, Parameters.h:18). */
+int sfh_batch_set_rhs_mass(sfh_batch* batch, int sys, int rhs, double mass);
 int sfh_batch_solve(sfh_batch* batch, double tol, int maxit);
 int sfh_batch_get_solution(sfh_batch* batch, int sys, int rhs, double* X);
 int sfh_batch_get_info(sfh_batch* batch, int sys, int rhs, sfh_cg_info* info);

@@ -146,6 +146,7 @@ SIGNATURES = {
     "sfh_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sfh_batch_set_barrier_polls": (ctypes.c_int, [_VP, ctypes.c_longlong]),
+    "sfh_batch_set_rhs_mass": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "sfh_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(SystemDesc),
                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]),
     "sfh_batch_destroy": (ctypes.c_int, [_VP]),
@@ -580,6 +581,10 @@ class Batch:
         one persistent cooperative launch."""
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
+
+    def set_rhs_mass(self, k, j, mass):
+        """Mass of right-hand side j of system k (default: the system's)."""
+        self._check(self.lib.sfh_batch_set_rhs_mass(self.h, k, j, mass), "set_rhs_mass")
 
     def set_barrier_polls(self, polls):
         """Bound on each grid-barrier wait of the persistent schedule (0: the

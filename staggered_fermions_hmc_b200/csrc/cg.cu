@@ -2212,6 +2212,8 @@ extern "C" int sfh_batch_true_residual(sfh_batch* b, int k, int j, double* rel)
     const sfh::Geom& g = b->geoms[k];
     const sfh::CgRhs& R = b->ws.rhs[b->ws.rhs0[k] + j];
     double m = b->desc[k].mass;
+    for (const sfh::CgLane& L : b->ws.lanes_h)  // the RHS's own mass, if it has one
+        if (L.rhs == b->ws.rhs0[k] + j) m = std::sqrt(L.m2);
     char* s = (char*)b->scratch;
     size_t fs = (size_t)g.V * 6 * sizeof(double);
     void *t = s, *mx = s + fs;
@@ -2558,6 +2560,16 @@ extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int 
     c->sched_nb = width;
     c->sched_tpi = tiles_per_block;
     c->sched_stage = stage_links;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_set_rhs_mass(sfh_batch* b, int k, int j, double mass)
+{
+    if (!b || k < 0 || k >= (int)b->desc.size() || j < 0 || j >= b->desc[k].nrhs || !(mass >= 0.0))
+        return SFH_ERR_INVALID;
+    const int rid = b->ws.rhs0[k] + j;
+    for (sfh::CgLane& L : b->ws.lanes_h)  // uploaded with the lanes at the next solve
+        if (L.rhs == rid) L.m2 = mass * mass;
     return SFH_OK;
 }
 

@@ -384,3 +384,31 @@ def test_persistent_barrier_wait_runs_out_and_the_batch_stays_usable(sfh, orc):
                 assert true_resid(orc, dims, mass, U, bs[j], B.solution(k, j)) < 1.05 * tol
     finally:
         B.close()
+
+
+@pytest.mark.parametrize("precision", ["f64", "f16"])
+def test_batch_rhs_at_their_own_masses(sfh, orc, precision):
+    """The RHS of one system solved at three masses on the same links: each
+    solution reaches the true residual of D(m) D(m)^dag at its own mass (by
+    the oracle), and the batch's own residual check uses that mass."""
+    dims, tol = (8, 8, 8, 8), 1e-10
+    masses = [0.05, 0.2, 0.8]
+    U = orc.random_gauge(dims, 1.0, 301)
+    B = sfh.Batch([(dims, 0.5, 3)], precision=precision)
+    try:
+        B.set_gauge(0, U)
+        bs = [orc.random_spinor(dims, 302 + j) for j in range(3)]
+        for j, (b, m) in enumerate(zip(bs, masses)):
+            B.set_rhs(0, j, b)
+            B.set_rhs_mass(0, j, m)
+        B.solve(tol=tol, max_iter=20000)
+        iters = []
+        for j, (b, m) in enumerate(zip(bs, masses)):
+            X = B.solution(0, j)
+            r = true_resid(orc, dims, m, U, b, X)
+            assert r < (2.0 if precision == "f64" else 1.05) * tol, (j, r)
+            assert abs(B.true_residual(0, j) - r) < 1e-3 * tol + 1e-3 * r
+            iters.append(B.info(0, j)["iters"])
+        assert iters[0] > iters[1] > iters[2]  # lighter masses need more iterations
+    finally:
+        B.close()
