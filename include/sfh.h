@@ -351,7 +351,7 @@ int sfh_batch_get_schedule(sfh_batch* batch, int* width, int* tiles_per_block, i
 int sfh_batch_set_gauge(sfh_batch* batch, int sys, const double* links);
 int sfh_batch_set_rhs(sfh_batch* batch, int sys, int rhs, const double* phi);
 /* The mass of one right-hand side (default: its system's), so that the RHS of
- * a system can be solves at several masses on the same links (a Hasenbusch
+ * a system can be solved at several masses on the same links (a Hasenbusch
  * pair, a multi-mass set): they share the system's link loads.  No
  * counterpart in the reference (one mass per program, Parameters.h:18). */
 int sfh_batch_set_rhs_mass(sfh_batch* batch, int sys, int rhs, double mass);
