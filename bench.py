@@ -136,6 +136,9 @@ ARITHMETIC = {
 }
 SPINOR_BYTES = {"f64": 48, "f32": 24, "f16": 16, "f32_18": 24, "bf16": 16}
 LINK_BYTES = {"f64": 144, "f32": 48, "f16": 24, "f32_18": 72, "bf16": 24}
+# the solution increment x_lo between reliable updates: FP32 for every mixed
+# precision (the FP64 solve updates x_hi directly)
+X_BYTES = {"f64": 48, "f32": 24, "f16": 24, "f32_18": 24, "bf16": 24}
 KERNELS = ("cg_hop1", "cg_hop2", "cg_update")
 
 
@@ -144,7 +147,7 @@ def kernel_bytes(spec, infos, precision, ru_separate=False):
     and reliable-update counts.  ru_separate: the reliable-update hops run in
     kernels of their own (cg_ru1, cg_ru2; the system-blocked schedule)."""
     s = SPINOR_BYTES[precision]
-    sx = 48 if precision == "f64" else 24
+    sx = X_BYTES[precision]
     lb = LINK_BYTES[precision]
     out = dict.fromkeys(KERNELS + (("cg_ru1", "cg_ru2") if ru_separate else ()), 0.0)
     ru1, ru2 = ("cg_ru1", "cg_ru2") if ru_separate else ("cg_hop1", "cg_hop2")
@@ -163,8 +166,8 @@ def kernel_bytes(spec, infos, precision, ru_separate=False):
                     # FP64 hop of x (links, x_hi + x_lo in, t_hi out); FP64
                     # hop of t_hi, x_hi, x_lo, b in, x_hi, x_lo, r out, and
                     # the search direction rebuilt (r, p in, p out)
-                    out[ru1] += nru * Vh * (8 * 144 + 48 + 24 + 48)
-                    out[ru2] += nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s + 3 * s)
+                    out[ru1] += nru * Vh * (8 * 144 + 48 + sx + 48)
+                    out[ru2] += nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * sx + 48 + s + 3 * s)
                 group_iters[par] = max(group_iters[par], it)
         for par in (0, 1):
             out["cg_hop1"] += group_iters[par] * 8 * lb * Vh

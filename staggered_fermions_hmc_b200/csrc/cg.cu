@@ -2320,10 +2320,10 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
 }
 
 // Two solves on the context's links at two masses (a Hasenbusch pair) as one
-// system with two right-hand sides, each lane carrying its own mass: the
-// work items serve both RHS, so a link read once serves both masses, the
-// lanes iterate together and the heavy mass's retire first.  FP64 runs
-// full-lattice lanes (the reference's CG), as ctx_solve_device does.
+// system with two right-hand sides, each lane carrying its own mass, in one
+// sequence of launches; the heavy mass's lanes retire first.  FP64 runs
+// full-lattice lanes (the reference's CG), as ctx_solve_device does, with
+// both RHS in each work item (a link read once serves both masses).
 int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_eo[2], const double mass[2],
                           double tol, int maxit, int prec, sfh_cg_info info[2])
 {
@@ -2361,9 +2361,15 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
         e = cudaMemcpyAsync(w->rhs[k].b, b_eo[k], fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair rhs");
     }
+    // the mixed precisions take one RHS per work item unless the context's
+    // schedule says otherwise: the heavy mass retires after a fifth of the
+    // light one's iterations, and a two-RHS item with one lane left runs its
+    // hops slower than a one-RHS item (24^4, FP32 storage: 62.2 ms for the
+    // pair at width 1 against 74.4 ms at width 2 and 64.5 ms for two solves)
     const bool lowp = prec != SFH_PREC_F64;
-    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), lowp ? c->sched_nb : 0, lowp ? c->sched_nb : 0,
-                        lowp ? c->sched_tpi : 0, lowp ? c->sched_stage : 0, c->stream);
+    const int nb = lowp ? (c->sched_nb > 0 ? c->sched_nb : 1) : 0;
+    e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), nb, nb, lowp ? c->sched_tpi : 0,
+                        lowp ? c->sched_stage : 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg pair solve");
     if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
     for (int k = 0; k < 2; ++k) {

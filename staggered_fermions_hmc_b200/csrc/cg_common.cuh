@@ -64,6 +64,11 @@ struct CgArgs {
 
 namespace {
 
+// storage of the low-precision solution x_lo, which sums alpha p between two
+// reliable updates and is then added to the FP64 x_hi and cleared: FP32 for
+// every mixed precision.  FP16 with a per-site scale for the 16-bit storages
+// cut the update kernel's time by 8 % on the uneven batch but its rounding
+// cost 6 % more iterations (mean 360 against 341): 401 against 417 solves/s.
 template <int SP> struct XFmt { static constexpr int v = SP_F32; };
 template <> struct XFmt<SP_F64> { static constexpr int v = SP_F64; };
 

@@ -157,7 +157,8 @@ int pf_terms(sfh_ctx* c, const void* phi, void* X, PfTerm (&t)[2])
 }
 
 // X_k = M(m_k)^-1 phi_k for the pseudofermion terms: a Hasenbusch pair as
-// one batch of two systems on the same links, a single term alone
+// one system with two right-hand sides at their own masses on the same
+// links, a single term alone
 int solve_terms(sfh_ctx* c, const PfTerm* t, int n, double tol, int maxit, int prec, long* iters, int* solves)
 {
     if (n == 2) {

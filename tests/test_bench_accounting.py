@@ -36,7 +36,7 @@ def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
     parity, iteration) with the longer lane's count, spinors per RHS; each
     reliable update adds an FP64 hop to both hop kernels (or to the two
     reliable-update kernels of the system-blocked schedule), the second with
-    the search direction rebuilt."""
+    the search direction rebuilt.  The increment x_lo is FP32."""
     import bench
     dims = (4, 4, 4, 8)
     Vh = 256
@@ -46,8 +46,8 @@ def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
     s, sx, lb = 16, 24, 24
     its = 12 + 20
     nru = (2 + 4) / 2.0  # per parity
-    ru1 = nru * Vh * (8 * 144 + 48 + 24 + 48)
-    ru2 = nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * 24 + 48 + s + 3 * s)
+    ru1 = nru * Vh * (8 * 144 + 48 + sx + 48)
+    ru2 = nru * Vh * (8 * 144 + 48 + 2 * 48 + 2 * sx + 48 + s + 3 * s)
     hop1 = its * Vh * 2 * s + 20 * 8 * lb * Vh
     hop2 = its * Vh * 4 * s + 20 * 8 * lb * Vh
     upd = its * Vh * (5 * s + 2 * sx)
