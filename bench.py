@@ -721,6 +721,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--rhs-block", type=int, default=0,
                     help="RHS-block width of the hop kernels (0: time the schedules and keep the fastest)")
+    ap.add_argument("--hop2-width", type=int, default=0,
+                    help="with --rhs-block: the second hop's RHS-block width (the first hop takes --rhs-block)")
     ap.add_argument("--tiles", type=int, default=2, help="tiles per block with --rhs-block")
     ap.add_argument("--stage", type=int, default=0, help="stage links in shared memory with --rhs-block (0/1)")
     ap.add_argument("--profile-case", action="store_true",
@@ -766,9 +768,12 @@ def main():
     B = build_batch(sfh, spec, args.precision, local)
     if args.rhs_block:
         B.set_schedule(args.rhs_block, args.tiles, args.stage)
+        if args.hop2_width:
+            B.set_hop_widths(args.rhs_block, args.hop2_width)
     else:
         B.autotune()
     schedule = B.schedule()
+    hop_widths = B.hop_widths()
 
     def solve():
         B.solve(tol=TOL, max_iter=MAXIT)
@@ -929,7 +934,7 @@ def main():
         "other_mixed_precisions": other,
         "solver_config": {"precision": args.precision, "arithmetic": ARITHMETIC[args.precision],
                           "schedule": {"rhs_block": schedule[0], "tiles_per_block": schedule[1],
-                                       "staged_links": schedule[2]}},
+                                       "staged_links": schedule[2], "hop_widths": list(hop_widths)}},
         "c4_oracle_check": c4_check,
         "solver": {"iters_mean": float(np.mean(iters)), "iters_max": int(max(iters)),
                    "reliable_updates_mean": float(np.mean(nru)), "worst_true_resid": worst},

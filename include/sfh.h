@@ -313,10 +313,17 @@ int sfh_batch_set_stream(sfh_batch* batch, void* cuda_stream);
 void* sfh_batch_get_stream(sfh_batch* batch);
 /* RHS-block width for the fused hop (0 = automatic); the autotuner sets it */
 int sfh_batch_set_rhs_block(sfh_batch* batch, int width);
+/* RHS-block widths of the two hop kernels separately (0 = automatic; 1, 2,
+ * 4, 8): the first hop (t = K p) can serve wider groups than the second,
+ * whose CG sums take registers.  sfh_batch_set_rhs_block and
+ * sfh_batch_set_schedule set both to one width.  No counterpart in the
+ * reference. */
+int sfh_batch_set_hop_widths(sfh_batch* batch, int hop1_width, int hop2_width);
+int sfh_batch_get_hop_widths(sfh_batch* batch, int* hop1_width, int* hop2_width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
  * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
- * (0 to 5 as below; FP64: 0) on the batch's current inputs and keep the
- * fastest.
+ * (0 to 5 as below; FP64: 0), and for the lane-list stages (4, 5) also hop
+ * widths 4 and 2, on the batch's current inputs and keep the fastest.
  * The schedule never changes the results.  No counterpart in the reference
  * (its solver has no schedule). */
 int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);

@@ -154,6 +154,8 @@ SIGNATURES = {
     "sfh_batch_set_stream": (ctypes.c_int, [_VP, _VP]),
     "sfh_batch_get_stream": (_VP, [_VP]),
     "sfh_batch_set_rhs_block": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sfh_batch_set_hop_widths": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
+    "sfh_batch_get_hop_widths": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_autotune": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "sfh_batch_set_schedule": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sfh_batch_set_reliable_delta": (ctypes.c_int, [_VP, ctypes.c_double]),
@@ -555,6 +557,17 @@ class Batch:
 
     def set_rhs_block(self, width):
         self._check(self.lib.sfh_batch_set_rhs_block(self.h, width), "set_rhs_block")
+
+    def set_hop_widths(self, hop1_width, hop2_width):
+        """RHS-block widths of the first and second hop kernels separately
+        (after set_schedule, which sets both)."""
+        self._check(self.lib.sfh_batch_set_hop_widths(self.h, hop1_width, hop2_width), "set_hop_widths")
+
+    def hop_widths(self):
+        """(first hop's, second hop's) RHS-block widths the next solve uses."""
+        a, b = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.sfh_batch_get_hop_widths(self.h, ctypes.byref(a), ctypes.byref(b)), "hop_widths")
+        return a.value, b.value
 
     def autotune(self, probe_iters=48):
         """Pick the fastest RHS-block width and tiles per block for this batch

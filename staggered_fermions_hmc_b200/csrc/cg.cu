@@ -63,8 +63,11 @@ constexpr int kSums = 4;  // <p,v>, <r,v>, |v|^2, |r|^2
 template <int GP, int SP, int NB, bool SUMS, bool RUI = true> struct HopOcc {
     // without the inline FP64 reliable-update hop the kernels need fewer
     // registers: FP16 fits in 48 (five blocks), the FP32-arithmetic ones with
-    // 12-real links in 64 (four); 18-real FP32 links keep three
-    static constexpr int v = (SP == SP_F64 || NB > 2) ? 2
+    // 12-real links in 64 (four); 18-real FP32 links keep three.  FP16 in
+    // groups of four RHS: the first hop fits in 64 registers (four blocks,
+    // no spills), the second, with its sums, in 80 (three)
+    static constexpr int v = (NB == 4 && GP == GP_F16_12 && SP == SP_F16 && !RUI) ? (SUMS ? 3 : 4)
+                             : (SP == SP_F64 || NB > 2) ? 2
                              : ((GP == GP_F16_12 && SP == SP_F16) ? (RUI ? 4 : 5)
                                                                    : ((RUI || GP == GP_F32_18) ? 3 : 4));
 };
@@ -95,7 +98,7 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
             P.lane[l] = lane_of(S, base + l, q, hop1);
             const CgLane* L = a.lanes + P.lane[l];
             P.mode[l] = ld_int(&L->mode[cur]);
-            P.rid[l] = __ldg(&L->rhs);
+            P.rid[l] = S.rhs0 + base + l;  // == L->rhs, without waiting for the lane
             P.m2[l] = __ldg(&L->m2);  // fixed for the solve
             if (scalars && P.mode[l] == LM_ACTIVE) {
                 P.alpha[l] = ld_dbl(&L->alpha);
@@ -111,6 +114,19 @@ __device__ __forceinline__ void gather_pass(const CgArgs& a, const CgSys& S, int
 __device__ __forceinline__ void stage_sys(const CgArgs& a, int tile, CgSys* s_sys)
 {
     if (threadIdx.x == 0) *s_sys = a.sys[__ldg(a.tile_sys + tile)];
+    __syncthreads();
+}
+
+// A work item of the per-phase kernels: x its first tile, y its first RHS
+// (below 64) and its system index above bit kItemSysShift, so that a block
+// reaches its system descriptor in one dependent load rather than through
+// the tile table, and its vectors' addresses without waiting for its lanes
+constexpr int kItemSysShift = 8;
+__device__ __forceinline__ int item_rhs(int2 it) { return it.y & ((1 << kItemSysShift) - 1); }
+
+__device__ __forceinline__ void stage_item_sys(const CgArgs& a, int2 it, CgSys* s_sys)
+{
+    if (threadIdx.x == 0) *s_sys = a.sys[it.y >> kItemSysShift];
     __syncthreads();
 }
 
@@ -346,8 +362,7 @@ __device__ __forceinline__ void finish_lane(const CgArgs& a, const CgSys& S, int
     const double* base = a.partial + L->poff + (S.both ? 0 : L->parity * nsq);
     const int n = S.both ? 2 * nsq : nsq;
     double s[kSums];
-#pragma unroll
-    for (int f = 0; f < kSums; ++f) s[f] = warp_sum_slots(base + f * nslot, n);
+    warp_sum_slots_n<kSums>(base, nslot, n, s);
     if (threadIdx.x != 0) return;
     const int nxt = cur ^ 1;
     if (mode == LM_ACTIVE || mode == LM_RESTART) {
@@ -544,7 +559,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
     constexpr int XP = XFmt<SP>::v;
     const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
-    stage_sys(a, it.x, &s_sys);
+    stage_item_sys(a, it, &s_sys);
     const CgSys& S = s_sys;
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
@@ -553,16 +568,25 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
     // vectors belong to the plain FP64 CG, which has no reliable updates;
     // RUI false: the lane-list kernels do it)
     constexpr bool ru_here = RUI && SP != SP_F64;
-    gather_pass<NB>(a, S, it.y, q, true, cur, false, P);
+    const int base = item_rhs(it), cnt = min(NB, S.nrhs - base);
+    // the vectors' addresses, loaded alongside the lanes' modes
+    const void* pr[NB];
+    const void* pp[NB];
+    const void* tout[NB];
+#pragma unroll
+    for (int l = 0; l < NB; ++l) {
+        pr[l] = l < cnt ? rhs_ptr(a, S.rhs0 + base + l, F_R) : nullptr;
+        pp[l] = l < cnt ? rhs_ptr(a, S.rhs0 + base + l, F_P) : nullptr;
+        tout[l] = l < cnt ? rhs_ptr(a, S.rhs0 + base + l, F_T) : nullptr;
+    }
+    gather_pass<NB>(a, S, base, q, true, cur, false, P);
     if (!(P.anyA || (ru_here && P.anyR))) return;
     const void* pin[NB];
-    const void* tout[NB];
     bool on[NB];
 #pragma unroll
     for (int l = 0; l < NB; ++l) {
         on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
-        pin[l] = on[l] ? rhs_ptr(a, P.rid[l], P.mode[l] == LM_RESTART ? F_R : F_P) : nullptr;
-        tout[l] = on[l] ? rhs_ptr(a, P.rid[l], F_T) : nullptr;
+        pin[l] = on[l] ? (P.mode[l] == LM_RESTART ? pr[l] : pp[l]) : nullptr;
     }
     if (P.anyA) {
         for (int t = ir.first; t < ir.end; ++t) {
@@ -690,7 +714,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
     __shared__ CgSys s_sys;
     __shared__ double smem[32 * NB * kSums];
     __shared__ unsigned s_mask;
-    stage_sys(a, it.x, &s_sys);
+    stage_item_sys(a, it, &s_sys);
     const CgSys& S = s_sys;
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
@@ -698,7 +722,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
     // the reliable-update residuals are computed here too: measured faster
     // than a kernel of their own, and the compiler keeps the FP64 hop's
     // registers better with them here
-    gather_pass<NB>(a, S, it.y, q, false, cur, false, P);
+    gather_pass<NB>(a, S, item_rhs(it), q, false, cur, false, P);
     if (!(P.anyA || (RUI && P.anyR))) return;  // uniform across the block
     bool part[NB], on[NB];
     double sums[NB * kSums];
@@ -787,11 +811,16 @@ __device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, C
     // this iteration's reliable-update list was read by the kernels before
     // this one: empty it for the iteration after next
     if (a.ru_list && blockIdx.x == 0 && threadIdx.x == 0) a.ru_list[cur * (a.nlanes + 1)] = 0;
-    stage_sys(a, it.x, s_sys);
+    stage_item_sys(a, it, s_sys);
     const CgSys& S = *s_sys;
     const ItemRange ir = item_range(a, S, it.x);
     const int q = ir.q, Vh = S.g.Vh;
-    CgLane* L = a.lanes + lane_of(S, it.y, q, false);
+    const int rid = S.rhs0 + item_rhs(it);
+    void* pp = rhs_ptr(a, rid, F_P);
+    void* rp = rhs_ptr(a, rid, F_R);
+    void* xp = rhs_ptr(a, rid, F_XLO);
+    const void* vp = rhs_ptr(a, rid, F_V);
+    CgLane* L = a.lanes + lane_of(S, item_rhs(it), q, false);
     const int mode = ld_int(&L->mode[cur]);
     if (mode != LM_ACTIVE && mode != LM_RESTART && mode != LM_LAST) return;
     if (mode == LM_LAST && threadIdx.x == 0) {  // the last item retires the lane
@@ -803,11 +832,6 @@ __device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, C
         }
     }
     const double alpha = ld_dbl(&L->alpha), beta = ld_dbl(&L->beta);
-    const int rid = __ldg(&L->rhs);
-    void* pp = rhs_ptr(a, rid, F_P);
-    void* rp = rhs_ptr(a, rid, F_R);
-    void* xp = rhs_ptr(a, rid, F_XLO);
-    const void* vp = rhs_ptr(a, rid, F_V);
     for (int t = ir.first; t < ir.end; ++t) {
         const TileInfo ti = decode_tile(S, t);
         if (!ti.valid) break;
@@ -1566,6 +1590,7 @@ static cudaError_t workspace_build(CgWorkspace& w, const std::vector<SolverSyste
         S.both = both;
         S.tile0 = tile;
         S.ntq = (h.g.Vh + kTile - 1) / kTile;
+        S.rhs0 = (int)w.rhs.size();
         for (int q = 0; q < 2; ++q)
             for (int j = 0; j < S.ntq; ++j) tile_sys.push_back(k);
         tile += 2 * S.ntq;
@@ -1656,10 +1681,13 @@ static cudaError_t items_for(CgWorkspace& w, int nb, int tpi, const int2** d, in
             return cudaSuccess;
         }
     std::vector<int2> h;
-    for (const CgSys& S : w.sys)
+    for (int k = 0; k < (int)w.sys.size(); ++k) {
+        const CgSys& S = w.sys[k];
         for (int q = 0; q < 2; ++q)
             for (int j = 0; j < S.ntq; j += tpi)
-                for (int b = 0; b < S.nrhs; b += nb) h.push_back(make_int2(S.tile0 + q * S.ntq + j, b));
+                for (int b = 0; b < S.nrhs; b += nb)
+                    h.push_back(make_int2(S.tile0 + q * S.ntq + j, b | (k << kItemSysShift)));
+    }
     int2* p = nullptr;
     cudaError_t e = w.alloc((void**)&p, sizeof(int2) * std::max<size_t>(1, h.size()));
     if (e != cudaSuccess) return e;
@@ -2026,6 +2054,7 @@ extern "C" int sfh_batch_create(int device, int nsys, const sfh_system_desc* sys
     for (int k = 0; k < nsys; ++k)
         if (!sfh::dims_ok(systems[k].dims) || systems[k].nrhs <= 0 || systems[k].nrhs > 64)
             return SFH_ERR_INVALID;
+    if (nsys >= (1 << (31 - sfh::kItemSysShift))) return SFH_ERR_INVALID;  // the work items' system field
     *out = nullptr;
     sfh_batch* b = new sfh_batch();
     b->device = device;
@@ -2125,6 +2154,14 @@ extern "C" int sfh_batch_set_rhs_block(sfh_batch* b, int width)
     if (!b || width < 0 || width > 8) return SFH_ERR_INVALID;
     b->nb = width;
     b->nb2 = width;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_set_hop_widths(sfh_batch* b, int hop1_width, int hop2_width)
+{
+    if (!b || hop1_width < 0 || hop1_width > 8 || hop2_width < 0 || hop2_width > 8) return SFH_ERR_INVALID;
+    b->nb = hop1_width;
+    b->nb2 = hop2_width;
     return SFH_OK;
 }
 
@@ -2520,28 +2557,34 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int* cand = f64 ? widths64 : widths;
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
-    int bw = 1, bt = 2, bs = 0;
+    int bw = 1, bw2 = 1, bt = 2, bs = 0;
     for (int stage = 0; stage < (f64 ? 1 : 6); ++stage)
-        for (int c = 0; c < ncand; ++c)
+        for (int c = 0; c < ncand + 1; ++c)
             for (int tp : tiles) {
                 if ((stage == 2 || stage == 3) && (tp != 1 || b->prec == SFH_PREC_F32_18))
                     continue;  // system-blocked: one tile per block; not for FP32 18-real links
+                // the last candidate: the first hop in groups of four, the
+                // second in groups of two (lane-list stages only)
+                const bool split = c == ncand;
+                if (split && (f64 || stage < 4)) continue;
+                const int w1 = split ? 4 : cand[c], w2 = split ? 2 : cand[c];
                 double t = 0.0;
                 for (int rep = 0; rep < 2; ++rep) {  // the first run builds the graph
                     auto t0 = std::chrono::steady_clock::now();
-                    cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, cand[c], cand[c], tp,
-                                                         stage, b->stream);
+                    cudaError_t e = sfh::workspace_solve(b->ws, 1e-30, probe_iters, 0.1, w1, w2, tp, stage, b->stream);
                     if (e != cudaSuccess) return batch_cuda(b, e, "autotune");
                     t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
                 }
                 if (t < best) {
                     best = t;
-                    bw = cand[c];
+                    bw = w1;
+                    bw2 = w2;
                     bt = tp;
                     bs = stage;
                 }
             }
-    b->nb = b->nb2 = bw;
+    b->nb = bw;
+    b->nb2 = bw2;
     b->tpi = bt;
     b->stage_links = bs;
     if (best_width) *best_width = bw;
@@ -2590,6 +2633,14 @@ extern "C" int sfh_batch_set_reliable_delta(sfh_batch* b, double delta)
 {
     if (!b || !(delta > 0.0) || !(delta < 1.0)) return SFH_ERR_INVALID;
     b->delta = delta;
+    return SFH_OK;
+}
+
+extern "C" int sfh_batch_get_hop_widths(sfh_batch* b, int* hop1_width, int* hop2_width)
+{
+    if (!b) return SFH_ERR_INVALID;
+    if (hop1_width) *hop1_width = b->nb;
+    if (hop2_width) *hop2_width = b->nb2;
     return SFH_OK;
 }
 

@@ -23,6 +23,7 @@ struct CgSys {
     const void* U64;
     const void* Ulo;
     int lane0, nrhs, both, tile0, ntq;
+    int rhs0;  // the system's first entry in the RHS table (its RHS are consecutive)
 };
 
 struct CgRhs {
@@ -150,15 +151,45 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* smem)
     __syncthreads();
 }
 
-// Sum of n partial slots by one warp in a fixed order (all lanes get it).
-__device__ __forceinline__ double warp_sum_slots(const double* slots, int n)
+// Sums of NF arrays of n partial slots (array f at slots + f * stride) by one
+// warp in a fixed order (all lanes get them): lane j adds slots j, j + 32,
+// j + 64, ... in turn, then the lanes combine by a fixed butterfly.  The
+// loads of four rounds are issued before their adds, so that a sum over n
+// slots waits about n / 128 memory latencies rather than n / 32 (the slots
+// were just written by other blocks and are read from L2); the order of the
+// adds is the same either way.
+template <int NF>
+__device__ __forceinline__ void warp_sum_slots_n(const double* slots, int stride, int n, double (&s)[NF])
 {
     const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int k = lane; k < n; k += 32) s += __ldcg(slots + k);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
+    for (int f = 0; f < NF; ++f) s[f] = 0.0;
+    int k = lane;
+    for (; k + 96 < n; k += 128) {
+        double v[NF][4];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[f][u] = __ldcg(slots + (size_t)f * stride + k + 32 * u);
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) s[f] += v[f][u];
+    }
+    for (; k < n; k += 32)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) s[f] += __ldcg(slots + (size_t)f * stride + k);
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[f] += __shfl_xor_sync(0xffffffffu, s[f], o);
+}
+
+__device__ __forceinline__ double warp_sum_slots(const double* slots, int n)
+{
+    double s[1];
+    warp_sum_slots_n<1>(slots, 0, n, s);
+    return s[0];
 }
 
 __device__ __forceinline__ void set_mode_final(CgLane* L, int mode, int status, int* n_active)

@@ -543,6 +543,7 @@ extern "C" int sfh_cg_solve_noalloc(const int dims[4], double mass, const void* 
     S.both = 1;
     S.tile0 = 0;
     S.ntq = (S.g.Vh + kTile - 1) / kTile;
+    S.rhs0 = 0;
     CgRhs R;
     R.b = const_cast<void*>(phi_eo);
     R.xhi = x_eo;

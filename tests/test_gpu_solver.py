@@ -203,6 +203,32 @@ def test_batch_rhs_block_widths_agree(sfh, orc):
         assert np.array_equal(o, out[0])
 
 
+def test_batch_split_hop_widths_agree(sfh, orc):
+    """FP16 storage: the two hop kernels in groups of different widths (the
+    first hop in fours, the second in twos) give the solutions of equal
+    widths bit for bit; the solution passes the oracle's true residual."""
+    systems = [((4, 4, 4, 8), 0.1, 5), ((6, 6, 6, 6), 0.05, 3)]
+    fields = [orc.random_gauge(d, 0.5, 40 + k) for k, (d, m, n) in enumerate(systems)]
+    out = []
+    for w1, w2, stage in ((2, 2, 4), (4, 2, 4), (4, 4, 4), (4, 2, 5), (1, 1, 0)):
+        B = sfh.Batch(systems, precision="f16")
+        B.set_schedule(w2, 2, stage)
+        B.set_hop_widths(w1, w2)
+        assert B.hop_widths() == (w1, w2)
+        for k, (d, m, n) in enumerate(systems):
+            B.set_gauge(k, fields[k])
+            for j in range(n):
+                B.set_rhs(k, j, orc.random_spinor(d, 600 + 10 * k + j))
+        B.solve(tol=1e-10)
+        out.append([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)])
+    for o in out[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(o, out[0]))
+    d, m, n = systems[1]
+    b = orc.random_spinor(d, 600 + 10 + 2)  # system 1, RHS 2: after system 0's five
+    r = b - orc.ddag(d, m, fields[1], out[1][5 + 2])
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.5e-10
+
+
 def test_batch_autotune_keeps_results(sfh, orc):
     """The autotuner only changes the schedule: solutions are bit-identical."""
     systems = [((4, 4, 4, 8), 0.1, 3), ((6, 6, 6, 6), 0.2, 2)]
