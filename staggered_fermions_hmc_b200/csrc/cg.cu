@@ -496,8 +496,7 @@ __global__ void __launch_bounds__(kTile) cg_init(CgArgs a)
             SpinorFmt<SP_F64>::store(rhs_ptr(a, P.rid[l], F_XHI), ti.q, ti.i, Vh, z);
             if (a.mixed)
                 SpinorFmt<XP>::store(rhs_ptr(a, P.rid[l], F_XLO), ti.q, ti.i, Vh, vcvt<typename SpinorFmt<XP>::R>(z));
-            Vec3<RS> bq = SpinorFmt<SP>::quantize(vcvt<RS>(b));
-            SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_R), ti.q, ti.i, Vh, bq);
+            const Vec3<RS> bq = SpinorFmt<SP>::store_q(rhs_ptr(a, P.rid[l], F_R), ti.q, ti.i, Vh, vcvt<RS>(b));
             SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), ti.q, ti.i, Vh, bq);
             sums[l * kSums + 3] = vdot_re(b, b);
         }
@@ -768,8 +767,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
                     w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
                     w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
                 }
-                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
-                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+                const Vec3<RS> vn = SpinorFmt<SP>::store_q(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vcvt<RS>(w));
                 s_part[l * kSums + 0][threadIdx.x] += site_dot(p, vn);
                 s_part[l * kSums + 1][threadIdx.x] += site_dot(r, vn);
                 s_part[l * kSums + 2][threadIdx.x] += site_dot(vn, vn);
@@ -840,8 +838,7 @@ __device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, C
         Vec3<RS> v = SpinorFmt<SP>::template load<COH>(vp, q, ti.i, Vh);
         Vec3<RX> x = SpinorFmt<XP>::template load<COH>(xp, q, ti.i, Vh);
         SpinorFmt<XP>::store(xp, q, ti.i, Vh, vaxpy(x, (RX)alpha, vcvt<RX>(p)));
-        Vec3<RS> rn = SpinorFmt<SP>::quantize(vaxpy(r, (RS)(-alpha), v));
-        SpinorFmt<SP>::store(rp, q, ti.i, Vh, rn);
+        const Vec3<RS> rn = SpinorFmt<SP>::store_q(rp, q, ti.i, Vh, vaxpy(r, (RS)(-alpha), v));
         SpinorFmt<SP>::store(pp, q, ti.i, Vh, vaxpy(rn, (RS)beta, p));
     }
 }
@@ -1083,8 +1080,7 @@ __device__ __forceinline__ void hop2_sys_body(const CgArgs& a, int tile, int cur
                     w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
                     w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
                 }
-                Vec3<RS> vn = SpinorFmt<SP>::quantize(vcvt<RS>(w));
-                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vn);
+                const Vec3<RS> vn = SpinorFmt<SP>::store_q(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vcvt<RS>(w));
                 v[l * kSums + 0] = (float)site_dot(p, vn);
                 v[l * kSums + 1] = (float)site_dot(r, vn);
                 v[l * kSums + 2] = (float)site_dot(vn, vn);

@@ -254,6 +254,12 @@ template <> struct SpinorFmt<SP_F64> {
 #pragma unroll
         for (int c = 0; c < 3; ++c) b[(size_t)c * Vh + i] = make_double2(v.c[c].re, v.c[c].im);
     }
+    // store v and return what was stored (v itself: no rounding)
+    __device__ static __forceinline__ Vec3<R> store_q(void* base, int p, int i, int Vh, const Vec3<R>& v)
+    {
+        store(base, p, i, Vh, v);
+        return v;
+    }
 };
 
 template <> struct SpinorFmt<SP_F32> {
@@ -289,6 +295,11 @@ template <> struct SpinorFmt<SP_F32> {
         float2* b = (float2*)base + (size_t)p * 3 * Vh;
 #pragma unroll
         for (int c = 0; c < 3; ++c) b[(size_t)c * Vh + i] = make_float2(v.c[c].re, v.c[c].im);
+    }
+    __device__ static __forceinline__ Vec3<R> store_q(void* base, int p, int i, int Vh, const Vec3<R>& v)
+    {
+        store(base, p, i, Vh, v);
+        return v;
     }
 };
 
@@ -381,6 +392,14 @@ template <int SP> struct ScaledSpinorFmt {
     {
         uint4* b = (uint4*)base + (size_t)p * Vh;
         b[i] = pack(v);
+    }
+    // store v and return the stored (rounded) value, packing once: equal to
+    // quantize(v), whose packing a later store would repeat bit for bit
+    __device__ static __forceinline__ Vec3<R> store_q(void* base, int p, int i, int Vh, const Vec3<R>& v)
+    {
+        const uint4 w = pack(v);
+        ((uint4*)base + (size_t)p * Vh)[i] = w;
+        return unpack(w);
     }
 };
 
