@@ -183,12 +183,12 @@ def solve_bytes(spec, infos, precision):
 # algorithmic byte of cg_hop2 for one launch of the first 8 systems of the
 # batch with every lane active, RHS groups of 2, 4 tiles per work item, links
 # read directly, reliable updates in the lane-list kernels (the headline
-# schedule): f16 284.0 MB for 291.9 MB (a single-kernel ncu capture,
+# schedule): f16 283.4 MB for 291.9 MB (an ncu capture of the hop kernels,
 # summarised under profiles/); f32 553.2 MB for 491.0 MB (the FP32 capture
 # summarised there, of the same work items with the updates inside the hop
 # kernels).  The bench scales it to its own launches by their algorithmic
 # bytes.
-HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 284.0 / 291.9}
+HOP2_TRAFFIC_PER_ALG_BYTE = {"f32": 553.2 / 491.0, "f16": 283.4 / 291.9}
 
 
 def build_batch(sfh, spec, precision, device):
