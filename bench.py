@@ -446,8 +446,11 @@ def c4_oracle_check(B, spec):
 # algorithmic bytes per output site of one hop: its 8 links (144 / 48 / 24 /
 # 72 / 24 / 96 B), one input vector (each is the neighbour of 8 sites but
 # leaves DRAM once) and one output vector (48 / 24 / 16 / 24 / 16 / 48 B)
-DSLASH_BYTES = {0: 1248, 1: 432, 2: 224, 3: 624, 4: 224, 5: 864}
-DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18", 4: "bf16_12", 5: "f64_12"}
+# (6 and 7: the storages of 2 and 4, time and z neighbours staged in shared
+# memory by one bulk asynchronous copy per block)
+DSLASH_BYTES = {0: 1248, 1: 432, 2: 224, 3: 624, 4: 224, 5: 864, 6: 224, 7: 224}
+DSLASH_NAMES = {0: "f64_18", 1: "f32_12", 2: "f16_12", 3: "f32_18", 4: "bf16_12", 5: "f64_12",
+                6: "f16_12_tstaged", 7: "bf16_12_tstaged"}
 
 
 def run_extras(sfh, hbm, quick=False):
@@ -463,7 +466,7 @@ def run_extras(sfh, hbm, quick=False):
     lat.random_gauge(1.0, 3)
     Vh = int(np.prod(dims)) // 2
     ds = {}
-    for st in (0, 5, 3, 1, 2, 4):
+    for st in (0, 5, 3, 1, 2, 6, 4, 7):
         ms = lat.dslash_timing(st, nrep=20)
         gbs = DSLASH_BYTES[st] * Vh / (ms * 1e-3) / 1e9
         ds[DSLASH_NAMES[st]] = {"ms_per_hop": ms, "GB/s": gbs, "frac": gbs / hbm,

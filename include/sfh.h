@@ -109,12 +109,15 @@ int sfh_ddag(sfh_ctx* ctx, const double* in, double* out);
 /* Device time of one even-odd hop (V/2 output sites, the hopping part of
  * Fermions.cpp:218-283) in a storage format: 0 FP64 18-real, 1 FP32 12-real,
  * 2 FP16 12-real with per-site spinor scale, 3 FP32 18-real, 4 BF16 12-real
- * with per-site spinor scale, 5 FP64 12-real.  Benchmark aid;
- * the input is all zeros, so the value of the output is meaningless. */
+ * with per-site spinor scale, 5 FP64 12-real; 6 and 7 the storages of 2 and 4
+ * with each block's time and z neighbours staged in shared memory by one
+ * bulk asynchronous (TMA) copy along the time direction (results identical
+ * to 2 and 4; SFH_ERR_INVALID for Lt above 2816).  Benchmark aid; the input
+ * is all zeros, so the value of the output is meaningless. */
 int sfh_dslash_timing(sfh_ctx* ctx, int storage, int nrep, double* ms_per_hop);
 /* out = K in (the hopping term of D = m + K, Fermions.cpp:218-247, both
  * parities, reference AoS layout) computed by the same Dslash kernel in a
- * storage format (0..5 as above): the input rounded to the format's vectors
+ * storage format (0..7 as above): the input rounded to the format's vectors
  * and the links to its links; the result returned in FP64.  The numerical
  * check of the kernels sfh_dslash_timing times. */
 int sfh_dslash_storage(sfh_ctx* ctx, int storage, const double* in, double* out);
@@ -322,8 +325,9 @@ int sfh_batch_set_hop_widths(sfh_batch* batch, int hop1_width, int hop2_width);
 int sfh_batch_get_hop_widths(sfh_batch* batch, int* hop1_width, int* hop2_width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
  * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
- * (0 to 5 as below; FP64: 0), and for the lane-list stages (4, 5) also hop
- * widths 4 and 2, on the batch's current inputs and keep the fastest.
+ * (0 to 6 as below; FP64: 0; 6 for FP16 only), and for the lane-list stages
+ * (4 to 6) also hop widths 4 and 2, on the batch's current inputs and keep
+ * the fastest.
  * The schedule never changes the results.  No counterpart in the reference
  * (its solver has no schedule). */
 int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
@@ -341,7 +345,13 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * storage (FP32 18-real takes 1).  4 and 5: 0 and 1 with the FP64
  * reliable-update hops taken out of the hop kernels into two kernels that
  * walk a device list of the lanes due for one (as 2 and 3 always do).
- * Staging applies to the reduced precisions only.  And its current values. */
+ * 6 (FP16; the other precisions run 4): 4 with each tile's time and z
+ * neighbour vectors staged in shared memory, one bulk asynchronous (TMA)
+ * copy per RHS of the tile's range [i0 - Lt/2, i0 + 256 + Lt/2) of the other
+ * parity, double-buffered across the work item's tiles (RHS groups of at
+ * most 4; a staging wait that gives up fails the solve with SFH_ERR_TIMEOUT,
+ * its solutions still exact).  Staging applies to the reduced precisions
+ * only.  And its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Bound on each grid-barrier wait of the persistent schedule (3), in polls
  * of about 128 ns (0 = the default, about 4 s): a wait that runs out fails

@@ -307,7 +307,9 @@ class Lattice:
     def dslash_storage(self, storage, psi):
         """K psi (the hopping term, both parities) by the standalone Dslash in
         a storage format (0 FP64-18, 1 FP32-12, 2 FP16-12, 3 FP32-18,
-        4 BF16-12, 5 FP64-12), returned in FP64."""
+        4 BF16-12, 5 FP64-12; 6 and 7 the storages of 2 and 4 with each
+        block's time and z neighbours staged in shared memory by one bulk
+        asynchronous copy), returned in FP64."""
         psi = _f64(psi).reshape(-1)
         out = np.empty_like(psi)
         self._check(self.lib.sfh_dslash_storage(self.h, storage, _dptr(psi), _dptr(out)), "dslash storage")
@@ -315,7 +317,8 @@ class Lattice:
 
     def dslash_timing(self, storage, nrep=20):
         """ms per even-odd hop (V/2 output sites); storage 0 FP64-18, 1 FP32-12,
-        2 FP16-12, 3 FP32-18, 4 BF16-12, 5 FP64-12."""
+        2 FP16-12, 3 FP32-18, 4 BF16-12, 5 FP64-12, 6 FP16-12 and 7 BF16-12
+        with the neighbours staged along the time direction."""
         ms = ctypes.c_double(0.0)
         self._check(self.lib.sfh_dslash_timing(self.h, storage, nrep, ctypes.byref(ms)), "dslash timing")
         return ms.value
@@ -591,7 +594,9 @@ class Batch:
         """stage_links: 0 (or False) links read directly, 1 (or True) staged per
         work item, 2 system-blocked (one tile per block serving every RHS of
         the system, links read once per tile), 3 the system-blocked work in
-        one persistent cooperative launch."""
+        one persistent cooperative launch, 4 and 5: 0 and 1 with the reliable
+        updates in lane-list kernels, 6 (FP16): 4 with each tile's time and z
+        neighbours staged in shared memory by bulk asynchronous copies."""
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
 

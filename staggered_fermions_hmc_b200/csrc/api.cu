@@ -310,10 +310,18 @@ extern "C" int sfh_download_momenta(sfh_ctx* c, double* P)
 // 0 FP64 18-real, 1 FP32 12-real, 2 FP16 12-real + scale, 3 FP32 18-real,
 // 4 BF16 12-real + scale, 5 FP64 12-real (derived from U64 on each call,
 // in a buffer allocated on first use).
+// storages 6 and 7: the links and vectors of 2 (FP16) and 4 (BF16), the
+// Dslash with its time and z neighbours staged in shared memory
+static bool storage_tstaged(int storage) { return storage == 6 || storage == 7; }
+
 static int storage_links(sfh_ctx* c, int storage, const void** U, int* gp, int* sp)
 {
     static const int gps[6] = {GP_F64_18, GP_F32_12, GP_F16_12, GP_F32_18, GP_BF16_12, GP_F64_12};
     static const int sps[6] = {SP_F64, SP_F32, SP_F16, SP_F32, SP_BF16, SP_F64};
+    if (storage_tstaged(storage)) {
+        if (!hop_tstaged_fits(c->g)) return set_error(c, SFH_ERR_INVALID, "time-staged Dslash: Lt above 2816");
+        storage = storage == 6 ? 2 : 4;
+    }
     if (storage < 0 || storage > 5) return SFH_ERR_INVALID;
     if (!c->lowp_valid) {
         launch_make_lowp_gauge(c->g, c->U64, c->U32, c->U16, c->stream, c->U32_18, c->Ubf16);
@@ -340,9 +348,20 @@ static int storage_links(sfh_ctx* c, int storage, const void** U, int* gp, int* 
     return SFH_OK;
 }
 
+// one standalone Dslash, out = K in over parities [q0, q0 + nq), in a
+// storage format (0..7)
+static void storage_hop(sfh_ctx* c, int storage, const void* U, int gp, int sp, const void* in, void* out, int q0,
+                        int nq)
+{
+    if (storage_tstaged(storage))
+        launch_hop_tstaged(c->g, gp, U, in, out, nullptr, 0.0, 1.0, q0, nq, c->derr, c->stream);
+    else
+        launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, q0, nq, c->stream);
+}
+
 // out = K in (the hopping term of D = m + K, Fermions.cpp:218-247, both
 // parities) computed by the standalone Dslash kernel in a storage format
-// (0..5 as storage_links): the input rounded to the format's vectors, the
+// (0..7 as storage_links): the input rounded to the format's vectors, the
 // links to its links, the result returned in FP64.  The check of the
 // kernels that sfh_dslash_timing times.
 extern "C" int sfh_dslash_storage(sfh_ctx* c, int storage, const double* in, double* out)
@@ -358,12 +377,14 @@ extern "C" int sfh_dslash_storage(sfh_ctx* c, int storage, const double* in, dou
     if (st) return st;
     launch_spinor_aos_to_eo(c->g, (const double*)c->stage, c->spin[0], c->stream);
     launch_spinor_convert(c->g, sp, true, c->spin[0], c->spin[1], c->stream);
-    launch_hop(c->g, gp, U, sp, c->spin[1], sp, c->spin[2], nullptr, 0.0, 1.0, 0, 2, c->stream);
+    storage_hop(c, storage, U, gp, sp, c->spin[1], c->spin[2], 0, 2);
     launch_spinor_convert(c->g, sp, false, c->spin[2], c->spin[3], c->stream);
     launch_spinor_eo_to_aos(c->g, c->spin[3], (double*)c->stage, c->stream);
     st = cuda_check(c, cudaMemcpyAsync(out, c->stage, n, cudaMemcpyDeviceToHost, c->stream), "dslash output");
     if (st) return st;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "dslash storage");
+    st = cuda_check(c, cudaStreamSynchronize(c->stream), "dslash storage");
+    if (st) return st;
+    return take_device_error(c, "dslash storage");
 }
 
 // Device time of one even-odd hop (V/2 output sites) in a storage format
@@ -386,9 +407,9 @@ extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_p
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int k = 0; k < 3; ++k) launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    for (int k = 0; k < 3; ++k) storage_hop(c, storage, U, gp, sp, in, out, 0, 1);
     cudaEventRecord(e0, c->stream);
-    for (int k = 0; k < nrep; ++k) launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, 0, 1, c->stream);
+    for (int k = 0; k < nrep; ++k) storage_hop(c, storage, U, gp, sp, in, out, 0, 1);
     cudaEventRecord(e1, c->stream);
     st = cuda_check(c, cudaEventSynchronize(e1), "dslash timing");
     float ms = 0.f;
@@ -397,5 +418,5 @@ extern "C" int sfh_dslash_timing(sfh_ctx* c, int storage, int nrep, double* ms_p
     cudaEventDestroy(e1);
     if (st) return st;
     *ms_per_hop = (double)ms / nrep;
-    return SFH_OK;
+    return take_device_error(c, "dslash timing");
 }

@@ -29,8 +29,10 @@
 // directly or staged per work item; the FP64 reliable-update hops inside the
 // hop kernels or in two kernels walking a device list of the lanes due for
 // one; system-blocked kernels (one tile per block, every RHS of the system,
-// the tile's links staged once); and the system-blocked work in one
-// cooperative launch with a bounded grid barrier.
+// the tile's links staged once); the system-blocked work in one
+// cooperative launch with a bounded grid barrier; and (FP16) each tile's time
+// and z neighbours staged in shared memory by bulk asynchronous copies,
+// double-buffered across the item's tiles (tstage.cuh).
 //
 // Mixed precision (FP32 or FP16+scale vectors with FP32 / FP16 12-real links):
 // x is accumulated in FP32 between reliable updates.  When |r| has dropped by
@@ -47,6 +49,7 @@
 #include <vector>
 
 #include "cg_common.cuh"
+#include "tstage.cuh"
 
 namespace sfh {
 
@@ -234,11 +237,15 @@ __device__ __forceinline__ Mat3<typename GaugeFmt<GP>::R> hop_link(const typenam
 // (the hopping term K, Fermions.cpp:218-247) for the lanes with on[l]; each
 // link is loaded once for all lanes of the block.  The time-wrap signs apply
 // to the input vectors of mu = 3, eta / 2 to the sum of both hops.
-template <int GP, int SP, int NB, bool STG, bool COH = false>
+// NST (FP16 only): the neighbour vectors of lane l from its staged range at
+// sn + l * W where it holds them (tstage.cuh), else from global memory.
+template <int GP, int SP, int NB, bool STG, bool COH = false, bool NST = false>
 __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeFmt<GP>::E* sl, const Nbr& n, int q,
                                           int i, int Vh, const void* const (&in)[NB], const bool (&on)[NB],
-                                          Vec3<typename GaugeFmt<GP>::R> (&acc)[NB])
+                                          Vec3<typename GaugeFmt<GP>::R> (&acc)[NB], const uint4* sn = nullptr,
+                                          int W = 0, TRange sr = {0, 0}, bool sok = false)
 {
+    static_assert(!NST || (GP == GP_F16_12 && SP == SP_F16 && !COH), "neighbour staging: FP16 graph kernels");
     typedef typename GaugeFmt<GP>::R R;
     const int nq = 1 - q;
     // FP16 links and vectors: products in packed half2, accumulated in FP32
@@ -256,11 +263,27 @@ __device__ __forceinline__ void hop_lanes(const void* Ulo, const typename GaugeF
             hlink_load<STG>(sl, kTile, Ulo, 2 * mu, q, mu, i, Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<false, COH>(acc[l], U, in[l], nq, n.up[mu], Vh, (n.wu && mu == 3) ? -s : s);
+                if (on[l]) {
+                    const float f = (n.wu && mu == 3) ? -s : s;
+                    if constexpr (NST)
+                        hop_half_word<false>(
+                            acc[l], U, nbr_word(sn + l * W, sr, sok, (const uint4*)in[l] + (size_t)nq * Vh, n.up[mu]),
+                            f);
+                    else
+                        hop_half<false, COH>(acc[l], U, in[l], nq, n.up[mu], Vh, f);
+                }
             hlink_load<STG>(sl, kTile, Ulo, 2 * mu + 1, nq, mu, n.dn[mu], Vh, U);
 #pragma unroll
             for (int l = 0; l < NB; ++l)
-                if (on[l]) hop_half<true, COH>(acc[l], U, in[l], nq, n.dn[mu], Vh, (n.wd && mu == 3) ? s : -s);
+                if (on[l]) {
+                    const float f = (n.wd && mu == 3) ? s : -s;
+                    if constexpr (NST)
+                        hop_half_word<true>(
+                            acc[l], U, nbr_word(sn + l * W, sr, sok, (const uint4*)in[l] + (size_t)nq * Vh, n.dn[mu]),
+                            f);
+                    else
+                        hop_half<true, COH>(acc[l], U, in[l], nq, n.dn[mu], Vh, f);
+                }
         }
         return;
     }
@@ -545,9 +568,80 @@ __device__ __forceinline__ void ru_hop1(const CgArgs& a, const CgSys& S, const C
     SpinorFmt<SP_F64>::store(rhs_ptr(a, rid, F_THI), q, i, Vh, acc);
 }
 
+// Neighbour staging of one work item's tiles (schedule 6, FP16): buffer
+// k & 1 of [2][NB][W] uint4 words holds tile k's range [i0 - Lt/2,
+// i0 + kTile + Lt/2) of each active lane's input (tstage.cuh), filled by
+// one thread's bulk copies completing on mbarrier k & 1; tile k + 1's copies
+// are issued before tile k is computed, and a __syncthreads guards each
+// buffer's reuse, so every thread walks every tile of the item.  The
+// arithmetic is the unstaged kernels', operand for operand.
+struct NstItem {
+    uint4* buf;                 // [2][NB][W]
+    unsigned long long* bar;    // [2]
+    int W, tile0, nt;           // words per lane and buffer; the item's first tile in its parity; tiles
+};
+
+// thread 0: tile k's ranges of the active lanes into buffer k & 1
+template <int NB>
+__device__ __forceinline__ void nst_issue(const NstItem& st, const CgSys& S, int q, const void* const (&in)[NB],
+                                          const bool (&on)[NB], int k)
+{
+    const TRange r = trange(S.g, (st.tile0 + k) * kTile, kTile);
+    unsigned bytes = 0;
+#pragma unroll
+    for (int l = 0; l < NB; ++l)
+        if (on[l]) bytes += (unsigned)r.cnt * 16u;
+    unsigned long long* bar = st.bar + (k & 1);
+    mbar_arrive_expect_tx(bar, bytes);
+#pragma unroll
+    for (int l = 0; l < NB; ++l)
+        if (on[l])
+            bulk_copy_g2s(st.buf + ((k & 1) * NB + l) * st.W, (const uint4*)in[l] + (size_t)(1 - q) * S.g.Vh + r.lo,
+                          (unsigned)r.cnt * 16u, bar);
+}
+
+// set up the item's staging and issue its first tile (every thread calls it)
+template <int NB>
+__device__ __forceinline__ NstItem nst_begin(const CgArgs& a, const CgSys& S, const ItemRange& ir, int q,
+                                             const void* const (&in)[NB], const bool (&on)[NB], void* dyn,
+                                             unsigned long long* bar)
+{
+    NstItem st;
+    st.buf = reinterpret_cast<uint4*>(dyn);
+    st.bar = bar;
+    st.W = a.nst_words;
+    st.tile0 = ir.first - S.tile0 - q * S.ntq;
+    st.nt = ir.end - ir.first;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) nst_issue<NB>(st, S, q, in, on, 0);
+    return st;
+}
+
+// before tile k: issue tile k + 1 once every thread is done with tile k - 1,
+// then wait (bounded) for tile k's copies; false: read tile k from global
+// memory (DEV_ERR_TIMEOUT raised)
+template <int NB>
+__device__ __forceinline__ bool nst_next(const CgArgs& a, const NstItem& st, const CgSys& S, int q,
+                                         const void* const (&in)[NB], const bool (&on)[NB], int k)
+{
+    if (k + 1 < st.nt) {
+        __syncthreads();
+        if (threadIdx.x == 0) nst_issue<NB>(st, S, q, in, on, k + 1);
+    }
+    const unsigned parity = (unsigned)(k >> 1) & 1u;
+    if (mbar_wait_bounded(st.bar + (k & 1), parity)) return true;
+    if (a.err) atomicOr(a.err, DEV_ERR_TIMEOUT);
+    mbar_wait_bounded(st.bar + (k & 1), parity);  // the copy in flight lands before the buffer is reused
+    return false;
+}
+
 // t = K p for the active lanes of one work item (tpi tiles of output parity
 // q, one RHS group); thi for lanes in a reliable update
-template <int GP, int SP, int NB, bool STG, bool RUI>
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
     cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
 {
@@ -587,7 +681,29 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
         on[l] = P.mode[l] == LM_ACTIVE || P.mode[l] == LM_RESTART;
         pin[l] = on[l] ? (P.mode[l] == LM_RESTART ? pr[l] : pp[l]) : nullptr;
     }
-    if (P.anyA) {
+    if constexpr (NST) {
+        if (P.anyA) {  // uniform across the block
+            __shared__ __align__(8) unsigned long long s_bar[2];
+            const NstItem st = nst_begin<NB>(a, S, ir, q, pin, on, s_dyn, s_bar);
+            for (int k = 0; k < st.nt; ++k) {
+                const bool ok = nst_next<NB>(a, st, S, q, pin, on, k);
+                const TileInfo ti = decode_tile(S, ir.first + k);
+                if (!ti.valid) continue;  // only the parity's last tile is partial
+                const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+                Vec3<R> acc[NB];
+#pragma unroll
+                for (int l = 0; l < NB; ++l) vzero(acc[l]);
+                hop_lanes<GP, SP, NB, false, false, true>(S.Ulo, nullptr, n, q, ti.i, Vh, pin, on, acc,
+                                                          st.buf + (k & 1) * NB * st.W, st.W,
+                                                          trange(S.g, (st.tile0 + k) * kTile, kTile), ok);
+#pragma unroll
+                for (int l = 0; l < NB; ++l) {
+                    if (!on[l]) continue;
+                    SpinorFmt<SP>::store(const_cast<void*>(tout[l]), q, ti.i, Vh, vcvt<RS>(acc[l]));
+                }
+            }
+        }
+    } else if (P.anyA) {
         for (int t = ir.first; t < ir.end; ++t) {
             const TileInfo ti = decode_tile(S, t);
             if (!ti.valid) break;  // only the parity's last tile is partial
@@ -700,7 +816,7 @@ __device__ __forceinline__ double site_dot(const Vec3<R>& a, const Vec3<R>& b)
 
 // own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
 // the four sums; reliable-update residuals
-template <int GP, int SP, int NB, bool STG, bool RUI>
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false>
 __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
     cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
 {
@@ -738,7 +854,50 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
 #pragma unroll
         for (int f = 0; f < kSums; ++f) s_part[l * kSums + f][threadIdx.x] = 0.0;
     }
-    if (P.anyA) {
+    // v = m^2 p - K t at the tile's sites and the lanes' partial sums
+    auto own_sites = [&](const TileInfo& ti, Vec3<R>(&acc)[NB]) {
+#pragma unroll
+        for (int l = 0; l < NB; ++l) {
+            if (!on[l]) continue;
+            const R m2 = (R)P.m2[l];
+            Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
+            Vec3<RS> p = r;
+            if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
+                SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
+            else
+                p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
+            Vec3<R> pr = vcvt<R>(p), w;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
+                w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
+            }
+            const Vec3<RS> vn = SpinorFmt<SP>::store_q(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vcvt<RS>(w));
+            s_part[l * kSums + 0][threadIdx.x] += site_dot(p, vn);
+            s_part[l * kSums + 1][threadIdx.x] += site_dot(r, vn);
+            s_part[l * kSums + 2][threadIdx.x] += site_dot(vn, vn);
+            s_part[l * kSums + 3][threadIdx.x] += site_dot(r, r);
+        }
+    };
+    if constexpr (NST) {
+        if (P.anyA) {  // uniform across the block
+            __shared__ __align__(8) unsigned long long s_bar[2];
+            const NstItem st = nst_begin<NB>(a, S, ir, q, tin, on, s_dyn, s_bar);
+            for (int k = 0; k < st.nt; ++k) {
+                const bool ok = nst_next<NB>(a, st, S, q, tin, on, k);
+                const TileInfo ti = decode_tile(S, ir.first + k);
+                if (!ti.valid) continue;  // only the parity's last tile is partial
+                const Nbr n = neighbours(S.g, eo_coords(S.g, q, ti.i));
+                Vec3<R> acc[NB];
+#pragma unroll
+                for (int l = 0; l < NB; ++l) vzero(acc[l]);
+                hop_lanes<GP, SP, NB, false, false, true>(S.Ulo, nullptr, n, q, ti.i, Vh, tin, on, acc,
+                                                          st.buf + (k & 1) * NB * st.W, st.W,
+                                                          trange(S.g, (st.tile0 + k) * kTile, kTile), ok);
+                own_sites(ti, acc);
+            }
+        }
+    } else if (P.anyA) {
         for (int t = ir.first; t < ir.end; ++t) {
             const TileInfo ti = decode_tile(S, t);
             if (!ti.valid) break;  // no barrier inside the loop
@@ -751,28 +910,7 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
 #pragma unroll
             for (int l = 0; l < NB; ++l) vzero(acc[l]);
             hop_lanes<GP, SP, NB, STG>(S.Ulo, sl, n, q, ti.i, Vh, tin, on, acc);
-#pragma unroll
-            for (int l = 0; l < NB; ++l) {
-                if (!on[l]) continue;
-                const R m2 = (R)P.m2[l];
-                Vec3<RS> r = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_R), q, ti.i, Vh);
-                Vec3<RS> p = r;
-                if (P.mode[l] == LM_RESTART)  // restart: the search direction becomes r
-                    SpinorFmt<SP>::store(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh, r);
-                else
-                    p = SpinorFmt<SP>::load(rhs_ptr(a, P.rid[l], F_P), q, ti.i, Vh);
-                Vec3<R> pr = vcvt<R>(p), w;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    w.c[k].re = fma(m2, pr.c[k].re, -acc[l].c[k].re);
-                    w.c[k].im = fma(m2, pr.c[k].im, -acc[l].c[k].im);
-                }
-                const Vec3<RS> vn = SpinorFmt<SP>::store_q(rhs_ptr(a, P.rid[l], F_V), q, ti.i, Vh, vcvt<RS>(w));
-                s_part[l * kSums + 0][threadIdx.x] += site_dot(p, vn);
-                s_part[l * kSums + 1][threadIdx.x] += site_dot(r, vn);
-                s_part[l * kSums + 2][threadIdx.x] += site_dot(vn, vn);
-                s_part[l * kSums + 3][threadIdx.x] += site_dot(r, r);
-            }
+            own_sites(ti, acc);
         }
     }
 #pragma unroll
@@ -1340,6 +1478,8 @@ struct CgKernels {
     size_t smem;    // dynamic shared memory of the hop kernels (staged links)
     bool sys;       // system-blocked hop kernels (one tile per block, every RHS)
     PersKernel pers;  // the whole solve in one cooperative launch (or null)
+    bool nst = false;  // hop kernels stage their neighbours (schedule 6)
+    size_t nst1 = 0, nst2 = 0;  // their staging buffers' bytes (set per workspace)
 };
 
 struct Phase {
@@ -1353,9 +1493,9 @@ struct Phase {
 static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
 {
     int n = 0;
-    ph[n++] = {k.hop1, k.nb1, k.smem, PH_HOP1, false};
+    ph[n++] = {k.hop1, k.nb1, k.smem + k.nst1, PH_HOP1, false};
     if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1, true};
-    ph[n++] = {k.hop2, k.nb2, k.smem, PH_HOP2, false};
+    ph[n++] = {k.hop2, k.nb2, k.smem + k.nst2, PH_HOP2, false};
     if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2, true};
     ph[n++] = {k.update, 1, 0, PH_UPDATE, false};
     return n;
@@ -1366,6 +1506,10 @@ static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
 // work-item width of the system-blocked kernels: one item per tile, covering
 // every RHS of the system
 constexpr int kSysItems = 1 << 20;
+
+// the largest neighbour-staging buffers of a hop kernel (schedule 6): two
+// buffers of four RHS at Lt up to 1024 fit
+constexpr size_t kMaxNstBytes = 160 * 1024;
 
 template <int GP, int SP>
 static CgKernels pick_sys(int nb, bool persistent)
@@ -1444,6 +1588,22 @@ static CgKernels pick_typed(int nb1, int nb2)
     return k;
 }
 
+// schedule 6 (FP16): schedule 4's kernels with each tile's time and z
+// neighbours staged in shared memory; RHS groups of at most four
+template <int GP, int SP>
+static CgKernels pick_nst(int nb1, int nb2)
+{
+    CgKernels k = pick_typed<GP, SP, false, false>(nb1, nb2);
+    if (nb1 >= 4) { k.hop1 = cg_hop1<GP, SP, 4, false, false, true>; k.nb1 = 4; }
+    else if (nb1 >= 2) { k.hop1 = cg_hop1<GP, SP, 2, false, false, true>; k.nb1 = 2; }
+    else { k.hop1 = cg_hop1<GP, SP, 1, false, false, true>; k.nb1 = 1; }
+    if (nb2 >= 4) { k.hop2 = cg_hop2<GP, SP, 4, false, false, true>; k.nb2 = 4; }
+    else if (nb2 >= 2) { k.hop2 = cg_hop2<GP, SP, 2, false, false, true>; k.nb2 = 2; }
+    else { k.hop2 = cg_hop2<GP, SP, 1, false, false, true>; k.nb2 = 1; }
+    k.nst = true;
+    return k;
+}
+
 template <int GP, int SP>
 static CgKernels pick_staged(int nb1, int nb2, bool stage, bool list)
 {
@@ -1459,9 +1619,12 @@ static CgKernels pick_staged(int nb1, int nb2, bool stage, bool list)
 // kernels, 3 the system-blocked bodies in one persistent cooperative launch
 // (2 and 3: FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
 // stage 4, 5: 0, 1 with the reliable updates in the lane-list kernels
+// stage 6: 4 with the neighbours staged along the time direction (FP16; the
+// other precisions run 4)
 static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
 {
     CgKernels k;
+    if (stage == 6 && prec == SFH_PREC_F16) return pick_nst<GP_F16_12, SP_F16>(nb1, nb2);
     const bool sys = stage == 2 || stage == 3, pers = stage == 3, list = stage >= 4;
     const bool stg = stage == 1 || stage == 5 || (sys && prec == SFH_PREC_F32_18);
     if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false, false);
@@ -1715,6 +1878,8 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.maxloop = a.mixed ? 2 * maxit + 64 : maxit + 1;
     a.tpi = tpi;
     a.ru_list = nullptr;
+    a.nst_words = 0;
+    a.err = nullptr;
     return a;
 }
 
@@ -1879,9 +2044,30 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
     if ((e = cudaMemcpyAsync(w.d_active, &w.h_active[0], sizeof(int), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
         return e;
     CgKernels k = pick_kernels(w.prec, nb1, nb2, stage);
+    int nst_words = 0;
+    if (k.nst) {  // staging buffers for the batch's largest Lt; schedule 4 where they do not fit
+        int max_lt = 2;
+        for (const CgSys& S : w.sys) max_lt = std::max(max_lt, S.g.L[3]);
+        nst_words = kTile + max_lt;
+        k.nst1 = (size_t)2 * k.nb1 * nst_words * sizeof(uint4);
+        k.nst2 = (size_t)2 * k.nb2 * nst_words * sizeof(uint4);
+        if (std::max(k.nst1, k.nst2) > kMaxNstBytes) {
+            k = pick_kernels(w.prec, nb1, nb2, 4);
+            nst_words = 0;
+        } else {
+            cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.nst1);
+            cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.nst2);
+            if (!w.d_bar && (e = w.alloc((void**)&w.d_bar, sizeof(GridBar))) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(&w.d_bar->err, 0, sizeof(int), stream)) != cudaSuccess) return e;
+        }
+    }
     // the system-blocked kernels serve one tile per block: one partial-sum
     // slot per tile, so every kernel of the iteration takes single tiles
     CgArgs a = make_args(w, tol, maxit, delta, k.sys ? 1 : (tpi > 0 ? tpi : 2));
+    if (k.nst) {
+        a.nst_words = nst_words;
+        a.err = &w.d_bar->err;
+    }
     if (k.ru1 || k.pers) {  // reliable updates by lane list: both lists start empty
         a.ru_list = w.d_rulist;
         if ((e = cudaMemsetAsync(w.d_rulist, 0, sizeof(int) * 2 * (w.nlanes + 1), stream)) != cudaSuccess) return e;
@@ -1962,7 +2148,13 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         }
     }
     destroy_events();
-    return finish_solve(w, stream);
+    int err = 0;
+    if (k.nst &&
+        (e = cudaMemcpyAsync(&err, &w.d_bar->err, sizeof(int), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        return e;
+    if ((e = finish_solve(w, stream)) != cudaSuccess) return e;
+    w.timed_out = err != 0;  // a staging wait gave up (the solution is still exact)
+    return cudaSuccess;
 }
 
 // the lanes' final state to the host; a lane that never stopped did not
@@ -2196,7 +2388,7 @@ extern "C" int sfh_batch_solve(sfh_batch* b, double tol, int maxit)
                         "batched CG");
     if (st) return st;
     if (b->ws.timed_out)
-        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a grid-barrier wait of the persistent solve gave up");
+        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a bounded device wait (grid barrier or neighbour staging) gave up");
     for (const sfh::CgLane& L : b->ws.lanes_h)
         if (L.status != SFH_OK) return L.status;
     return SFH_OK;
@@ -2327,7 +2519,7 @@ int ctx_solve_device(sfh_ctx* c, const void* b_eo, void* x_eo, double tol, int m
     e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), lowp ? c->sched_nb : 0, lowp ? c->sched_nb : 0,
                         lowp ? c->sched_tpi : 0, lowp ? c->sched_stage : 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solve");
-    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
+    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a bounded device wait (grid barrier or neighbour staging) gave up");
     e = cudaMemcpyAsync(x_eo, w->rhs[0].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg solution");
     int status = SFH_OK;
@@ -2404,7 +2596,7 @@ int ctx_solve_pair_device(sfh_ctx* c, const void* const b_eo[2], void* const x_e
     e = workspace_solve(*w, tol, maxit, default_reliable_delta(prec), nb, nb, lowp ? c->sched_tpi : 0,
                         lowp ? c->sched_stage : 0, c->stream);
     if (e != cudaSuccess) return cuda_check(c, e, "cg pair solve");
-    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a grid-barrier wait of the persistent solve gave up");
+    if (w->timed_out) return set_error(c, SFH_ERR_TIMEOUT, "CG: a bounded device wait (grid barrier or neighbour staging) gave up");
     for (int k = 0; k < 2; ++k) {
         e = cudaMemcpyAsync(x_eo[k], w->rhs[k].xhi, fs, cudaMemcpyDeviceToDevice, c->stream);
         if (e != cudaSuccess) return cuda_check(c, e, "cg pair solution");
@@ -2520,7 +2712,7 @@ extern "C" int sfh_batch_solve_timed(sfh_batch* b, double tol, int maxit, double
                         "timed batched CG");
     if (st) return st;
     if (b->ws.timed_out)
-        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a grid-barrier wait of the persistent solve gave up");
+        return batch_err(b, SFH_ERR_TIMEOUT, "batched CG: a bounded device wait (grid barrier or neighbour staging) gave up");
     static_assert(sfh::kTimedPhases == SFH_TIMED_KERNELS, "timing slots of include/sfh.h");
     for (int k = 0; k < sfh::kTimedPhases; ++k) {
         ms[k] = t.ms[k];
@@ -2554,9 +2746,10 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
     int bw = 1, bw2 = 1, bt = 2, bs = 0;
-    for (int stage = 0; stage < (f64 ? 1 : 6); ++stage)
+    for (int stage = 0; stage < (f64 ? 1 : 7); ++stage)
         for (int c = 0; c < ncand + 1; ++c)
             for (int tp : tiles) {
+                if (stage == 6 && b->prec != SFH_PREC_F16) continue;  // schedule 4 there
                 if ((stage == 2 || stage == 3) && (tp != 1 || b->prec == SFH_PREC_F32_18))
                     continue;  // system-blocked: one tile per block; not for FP32 18-real links
                 // the last candidate: the first hop in groups of four, the
@@ -2592,7 +2785,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
-    if (stage_links < 0 || stage_links > 5) return SFH_ERR_INVALID;
+    if (stage_links < 0 || stage_links > 6) return SFH_ERR_INVALID;
     b->stage_links = stage_links;
     return SFH_OK;
 }
@@ -2600,7 +2793,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
 extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int stage_links)
 {
     if (!c || width < 0 || width > 8 || tiles_per_block < 0 || tiles_per_block > 64 || stage_links < 0 ||
-        stage_links > 5)
+        stage_links > 6)
         return SFH_ERR_INVALID;
     c->sched_nb = width;
     c->sched_tpi = tiles_per_block;

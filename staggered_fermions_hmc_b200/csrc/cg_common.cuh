@@ -61,6 +61,11 @@ struct CgArgs {
     // lanes due for a reliable update, per iteration parity: [2][1 + nlanes],
     // a count then lane ids (null: the hop kernels do the reliable updates)
     int* ru_list;
+    // neighbour staging (schedule 6): shared-memory words of one RHS's staged
+    // range per buffer (kTile + the batch's largest Lt), and the device error
+    // word a staging wait that gives up sets DEV_ERR_TIMEOUT in (null: unused)
+    int nst_words;
+    int* err;
 };
 
 namespace {

@@ -19,6 +19,7 @@
 // vector.
 #include "hop.cuh"
 #include "sfh_internal.h"
+#include "tstage.cuh"
 
 namespace sfh {
 
@@ -144,6 +145,84 @@ __global__ void __launch_bounds__(256, HopMinBlocks<GP>::v) hop_kernel(Geom g, c
     SpinorFmt<SPO>::store(out, q, i, g.Vh, cvt<typename SpinorFmt<SPO>::R, R>(res));
 }
 
+// The 16-bit storages with the neighbour vectors staged along the time
+// direction (tstage.cuh): the block's 256 output sites take their time and z
+// neighbours from one bulk copy of [i0 - Lt/2, i0 + 256 + Lt/2) into shared
+// memory, the x and y neighbours and the links from global memory.  The
+// arithmetic is hop_site's, operand for operand, so the result is
+// bit-identical to hop_kernel's.
+template <int GP, int SP, bool SELF>
+__global__ void __launch_bounds__(256, HopMinBlocks<GP>::v)
+    hop_kernel_tstaged(Geom g, const void* __restrict__ gauge, const void* __restrict__ in, const void* self,
+                       void* out, double a, double b, int q0, int* err)
+{
+    static_assert(SpinorFmt<SP>::scaled, "staging covers the one-word-per-site storages");
+    extern __shared__ __align__(16) uint4 s_nb[];
+    __shared__ __align__(8) unsigned long long s_bar;
+    const int q = q0 + blockIdx.y, nq = 1 - q;
+    const int i0 = blockIdx.x * blockDim.x, i = i0 + threadIdx.x;
+    const uint4* src = (const uint4*)in + (size_t)nq * g.Vh;
+    const TRange r = trange(g, i0, blockDim.x);
+    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) bulk_g2s(s_nb, src + r.lo, (unsigned)r.cnt * 16u, &s_bar);
+    if (i >= g.Vh) return;  // every block has a site of its own, whose thread waits
+    const Coord c = eo_coords(g, q, i);
+    bool ok = mbar_wait_bounded(&s_bar, 0);
+    if (!ok) {
+        atomicOr(err, DEV_ERR_TIMEOUT);
+        mbar_wait_bounded(&s_bar, 0);  // the copy in flight, before the block may leave
+    }
+    Vec3<float> acc;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc.c[k] = {0.f, 0.f};
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        const float s = eta_sign(c, mu) < 0 ? -0.5f : 0.5f;
+        const uint4 wu = nbr_word(s_nb, r, ok, src, lex_up(g, c, mu) >> 1);
+        const int ld = lex_dn(g, c, mu) >> 1;
+        const uint4 wd = nbr_word(s_nb, r, ok, src, ld);
+        const bool wrap_up = (mu == 3) && (c.x[3] == g.L[3] - 1);
+        const bool wrap_dn = (mu == 3) && (c.x[3] == 0);
+        if constexpr (GP == GP_F16_12) {
+            __half2 U[9];
+            hlink_load<false>(nullptr, 0, gauge, 0, q, mu, i, g.Vh, U);
+            hop_half_word<false>(acc, U, wu, wrap_up ? -s : s);
+            hlink_load<false>(nullptr, 0, gauge, 0, nq, mu, ld, g.Vh, U);
+            hop_half_word<true>(acc, U, wd, wrap_dn ? s : -s);
+        } else {
+            mv_add<false>(acc, GaugeFmt<GP>::load(gauge, q, mu, i, g.Vh), hop_input_word<SP, float>(wu, wrap_up, s));
+            mdv_sub(acc, GaugeFmt<GP>::load(gauge, nq, mu, ld, g.Vh), hop_input_word<SP, float>(wd, wrap_dn, s));
+        }
+    }
+    const float hb = (float)b;
+    Vec3<float> res;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) res.c[k] = {hb * acc.c[k].re, hb * acc.c[k].im};
+    if (SELF) {
+        Vec3<float> sv = SpinorFmt<SP>::load(self, q, i, g.Vh);
+        const float ra = (float)a;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            res.c[k].re = ra * sv.c[k].re + res.c[k].re;
+            res.c[k].im = ra * sv.c[k].im + res.c[k].im;
+        }
+    }
+    SpinorFmt<SP>::store(out, q, i, g.Vh, res);
+}
+
+template <int GP, int SP>
+void launch_typed_tstaged(const Geom& g, const void* gauge, const void* in, void* out, const void* self, double a,
+                          double b, int q0, int nq, int* err, cudaStream_t s)
+{
+    dim3 grid((g.Vh + 255) / 256, nq);
+    const size_t smem = (size_t)tstage_words(256, g.L[3]) * sizeof(uint4);
+    if (self)
+        hop_kernel_tstaged<GP, SP, true><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err);
+    else
+        hop_kernel_tstaged<GP, SP, false><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err);
+}
+
 template <int GP, int SP>
 void launch_typed(const Geom& g, const void* gauge, const void* in, void* out, const void* self,
                   double a, double b, int q0, int nq, cudaStream_t s)
@@ -187,6 +266,20 @@ void launch_spinor_convert(const Geom& g, int sp, bool to_fmt, const void* src, 
     else if (sp == SP_F16) launch_convert<SP_F16>(g, to_fmt, src, dst, s);
     else if (sp == SP_BF16) launch_convert<SP_BF16>(g, to_fmt, src, dst, s);
     else launch_convert<SP_F64>(g, to_fmt, src, dst, s);
+}
+
+bool hop_tstaged_fits(const Geom& g)
+{
+    return (size_t)tstage_words(256, g.L[3]) * sizeof(uint4) <= 48 * 1024;
+}
+
+void launch_hop_tstaged(const Geom& g, int gauge_prec, const void* gauge, const void* in, void* out,
+                        const void* self, double a, double b, int q0, int nq, int* err, cudaStream_t s)
+{
+    if (gauge_prec == GP_F16_12)
+        launch_typed_tstaged<GP_F16_12, SP_F16>(g, gauge, in, out, self, a, b, q0, nq, err, s);
+    else if (gauge_prec == GP_BF16_12)
+        launch_typed_tstaged<GP_BF16_12, SP_BF16>(g, gauge, in, out, self, a, b, q0, nq, err, s);
 }
 
 void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,

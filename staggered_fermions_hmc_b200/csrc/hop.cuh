@@ -94,6 +94,15 @@ __device__ __forceinline__ Vec3<R> hop_input(const void* in, int nq, int j, int 
     }
 }
 
+// hop_input for a stored word of a scaled 16-bit vector format
+template <int SP, typename R>
+__device__ __forceinline__ Vec3<R> hop_input_word(const uint4 w, bool neg, R s)
+{
+    float sc;
+    const Vec3<R> v = SpinorFmt<SP>::unscaled(w, &sc);
+    return vneg_if(v, neg, s * sc);
+}
+
 // ---------------------------------------------------------------------------
 // FP16 links and vectors: the products in packed half2 arithmetic
 // ---------------------------------------------------------------------------
@@ -176,13 +185,12 @@ __device__ __forceinline__ void acc_f32x2(Cx<float>& acc, unsigned long long f2,
     asm("mov.b64 {%0, %1}, %2;" : "=f"(acc.re), "=f"(acc.im) : "l"(d));
 }
 
-// acc += f (U v) (ADJ false) or acc += f (U^dag v) (ADJ true) for a stored
-// FP16 vector v with site scale sc: f = s sc, products in half2
-template <bool ADJ, bool COH = false>
-__device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9], const void* in, int nq, int j,
-                                         int Vh, float f)
+// acc += f (U v) (ADJ false) or acc += f (U^dag v) (ADJ true) for the
+// stored FP16 vector word w (three half2 pairs and the site scale sc):
+// f = s sc, products in half2
+template <bool ADJ>
+__device__ __forceinline__ void hop_half_word(Vec3<float>& acc, const __half2 (&U)[9], const uint4 w, float f)
 {
-    const uint4 w = ld_vec<COH>((const uint4*)in + (size_t)nq * Vh + j);
     const __half2 v[3] = {h2_bits(w.x), h2_bits(w.y), h2_bits(w.z)};
     const unsigned long long f2 = f32x2_bcast(f * __uint_as_float(w.w));
     __half2 vp[3];
@@ -201,6 +209,14 @@ __device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9]
         }
         acc_f32x2(acc.c[r], f2, __half22float2(y));
     }
+}
+
+// hop_half_word for the vector of site j of parity nq in global memory
+template <bool ADJ, bool COH = false>
+__device__ __forceinline__ void hop_half(Vec3<float>& acc, const __half2 (&U)[9], const void* in, int nq, int j,
+                                         int Vh, float f)
+{
+    hop_half_word<ADJ>(acc, U, ld_vec<COH>((const uint4*)in + (size_t)nq * Vh + j), f);
 }
 
 }  // namespace

@@ -371,7 +371,11 @@ template <int SP> struct ScaledSpinorFmt {
     __device__ static __forceinline__ Vec3<R> load_unscaled(const void* base, int p, int i, int Vh, float* scale)
     {
         const uint4* b = (const uint4*)base + (size_t)p * Vh;
-        uint4 w = ld_vec<COH>(b + i);
+        return unscaled(ld_vec<COH>(b + i), scale);
+    }
+    // the pairs of a stored word converted, without the scale (in *scale)
+    __device__ static __forceinline__ Vec3<R> unscaled(uint4 w, float* scale)
+    {
         *scale = __uint_as_float(w.w);
         Vec3<R> v;
         uint32_t words[3] = {w.x, w.y, w.z};

@@ -81,6 +81,15 @@ void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, c
                 int out_prec, void* out, const void* self, double a, double b, int q0, int nq,
                 cudaStream_t s);
 
+// launch_hop for the 16-bit storages (gauge_prec GP_F16_12 or GP_BF16_12,
+// vectors of the matching format) with the neighbours staged along the time
+// direction; a bounded staging wait that gives up sets DEV_ERR_TIMEOUT in
+// *err (the result is the same).  hop_tstaged_fits: the staged range of a
+// 256-site tile fits the default 48 KB of shared memory (Lt <= 2816).
+bool hop_tstaged_fits(const Geom& g);
+void launch_hop_tstaged(const Geom& g, int gauge_prec, const void* gauge, const void* in, void* out,
+                        const void* self, double a, double b, int q0, int nq, int* err, cudaStream_t s);
+
 cudaError_t launch_random_gauge(const Geom& g, double eps, unsigned long long seed, void* U, int* d_err,
                                 cudaStream_t s);
 cudaError_t launch_random_spinor(const Geom& g, double sigma, unsigned long long seed, void* out,

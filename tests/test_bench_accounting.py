@@ -64,8 +64,8 @@ def test_kernel_bytes_links_shared_by_rhs_and_reliable_updates():
 def test_dslash_bytes_table():
     """Per output site of one hop: 8 links, one input and one output vector."""
     import bench
-    link = {0: 144, 1: 48, 2: 24, 3: 72, 4: 24, 5: 96}
-    vec = {0: 48, 1: 24, 2: 16, 3: 24, 4: 16, 5: 48}
+    link = {0: 144, 1: 48, 2: 24, 3: 72, 4: 24, 5: 96, 6: 24, 7: 24}
+    vec = {0: 48, 1: 24, 2: 16, 3: 24, 4: 16, 5: 48, 6: 16, 7: 16}
     for st in link:
         assert bench.DSLASH_BYTES[st] == 8 * link[st] + 2 * vec[st], bench.DSLASH_NAMES[st]
 

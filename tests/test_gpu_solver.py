@@ -71,7 +71,8 @@ def test_operators_vs_oracle(sfh, orc, dims, mass, geps):
     assert rel(lat.apply_DDdagger(psi), orc.ddag(dims, mass, U, psi)) < 1e-12
 
 
-@pytest.mark.parametrize("storage,tol", [(0, 1e-14), (5, 1e-14), (1, 1e-6), (3, 1e-6), (2, 2e-3), (4, 1.5e-2)])
+@pytest.mark.parametrize("storage,tol", [(0, 1e-14), (5, 1e-14), (1, 1e-6), (3, 1e-6), (2, 2e-3), (4, 1.5e-2),
+                                         (6, 2e-3), (7, 1.5e-2)])
 def test_dslash_storage_formats_vs_oracle(sfh, orc, storage, tol):
     """The standalone Dslash in each storage format (the kernels the bench's
     Dslash GB/s times) against the oracle's hopping term K = D - m, within
@@ -86,6 +87,28 @@ def test_dslash_storage_formats_vs_oracle(sfh, orc, storage, tol):
         K = orc.dirac(dims, mass, U, psi) - mass * psi
         out = lat.dslash_storage(storage, psi)
         assert np.linalg.norm(out - K) / np.linalg.norm(K) < tol
+    finally:
+        lat.close()
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8, 12), (4, 6, 8, 10), (6, 4, 4, 2), (16, 16, 16, 32), (12, 6, 10, 64)])
+def test_dslash_time_staged_bit_identical(sfh, orc, dims):
+    """The 16-bit Dslash with each block's time and z neighbours staged in
+    shared memory by one bulk copy (storages 6, 7) gives exactly the result
+    of the unstaged kernel (2, 4): same operands in the same order.  The
+    shapes cover tiles whose staged range is clipped at both ends of the
+    parity (Vh not a multiple of 256), Lt = 2 (a time hop that wraps onto
+    the same line), Lt = 64, and z wraps that fall back to global loads."""
+    mass = 0.1
+    U = orc.random_gauge(dims, 1.0, 61)
+    psi = orc.random_spinor(dims, 62)
+    lat = sfh.Lattice(dims, mass)
+    try:
+        lat.upload_gauge(U)
+        for plain, staged in ((2, 6), (4, 7)):
+            a = lat.dslash_storage(plain, psi)
+            b = lat.dslash_storage(staged, psi)
+            assert np.array_equal(a, b), (plain, staged)
     finally:
         lat.close()
 
@@ -226,6 +249,45 @@ def test_batch_split_hop_widths_agree(sfh, orc):
     d, m, n = systems[1]
     b = orc.random_spinor(d, 600 + 10 + 2)  # system 1, RHS 2: after system 0's five
     r = b - orc.ddag(d, m, fields[1], out[1][5 + 2])
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.5e-10
+
+
+def test_batch_neighbour_staging_bit_identical(sfh, orc):
+    """Schedule 6 (FP16: schedule 4 with each tile's time and z neighbours
+    staged in shared memory by bulk copies, double-buffered over the work
+    item's tiles) gives schedule 4's solutions bit for bit, for hop widths
+    1 to 4 and 1, 2 or 4 tiles per item, in the graph solve and the timed
+    solve.  The systems cover a partial last tile (Vh not a multiple of
+    256), Lt = 2, and Lt = 64 (the widest staged range of the batch); FP32
+    storage with schedule 6 runs schedule 4."""
+    systems = [((4, 4, 4, 8), 0.1, 5), ((6, 6, 6, 6), 0.05, 3), ((4, 6, 8, 2), 0.2, 2), ((6, 4, 4, 64), 0.1, 2)]
+    fields = [orc.random_gauge(d, 0.5 + 0.25 * (k % 2), 80 + k) for k, (d, m, n) in enumerate(systems)]
+
+    def run(prec, w1, w2, tiles, stage, timed=False):
+        B = sfh.Batch(systems, precision=prec)
+        B.set_schedule(w2, tiles, stage)
+        B.set_hop_widths(w1, w2)
+        for k, (d, m, n) in enumerate(systems):
+            B.set_gauge(k, fields[k])
+            for j in range(n):
+                B.set_rhs(k, j, orc.random_spinor(d, 900 + 10 * k + j))
+        times = B.solve_timed(tol=1e-10) if timed else B.solve(tol=1e-10)
+        return [B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)], times
+
+    for w1, w2, tiles in ((4, 2, 4), (2, 2, 2), (1, 1, 1), (4, 4, 4), (8, 2, 2)):
+        ref, _ = run("f16", w1, w2, tiles, 4)
+        got, _ = run("f16", w1, w2, tiles, 6)
+        assert all(np.array_equal(a, b) for a, b in zip(ref, got)), (w1, w2, tiles)
+    ref, _ = run("f16", 4, 2, 4, 4)
+    got, times = run("f16", 4, 2, 4, 6, timed=True)
+    assert all(np.array_equal(a, b) for a, b in zip(ref, got))
+    assert times["cg_hop1"][1] == times["cg_hop2"][1] > 0
+    ref32, _ = run("f32", 2, 2, 2, 4)
+    got32, _ = run("f32", 2, 2, 2, 6)
+    assert all(np.array_equal(a, b) for a, b in zip(ref32, got32))
+    d, m, n = systems[3]
+    b = orc.random_spinor(d, 900 + 30 + 1)
+    r = b - orc.ddag(d, m, fields[3], got[5 + 3 + 2 + 1])
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1.5e-10
 
 
