@@ -133,9 +133,9 @@ int sfh_cg_solve(sfh_ctx* ctx, const double* phi, double* X, double tol, int max
 
 /* The schedule of the context's mixed-precision solves (sfh_cg_solve, the
  * trajectory's solves), as sfh_batch_set_schedule: RHS-block width, tiles per
- * block, link staging 0..3 (3: the whole solve in one persistent launch).
- * Default 0, 0, 0; the FP64 CG keeps its own.  No counterpart in the
- * reference. */
+ * block, link staging 0..6 (3: the whole solve in one persistent launch).
+ * Default 0, 0, 0; the FP64 CG keeps its own (default tiles per block).  No
+ * counterpart in the reference. */
 int sfh_set_schedule(sfh_ctx* ctx, int width, int tiles_per_block, int stage_links);
 
 /* ---- forces, link update, observables (context's device fields) --------- */
@@ -332,7 +332,8 @@ int sfh_batch_get_hop_widths(sfh_batch* batch, int* hop1_width, int* hop2_width)
  * (its solver has no schedule). */
 int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
 /* The schedule directly: RHS-block width (0 = automatic), 256-site tiles per
- * block of the iteration kernels (0 = 2), and the hop kernels' link staging:
+ * block of the iteration kernels (0 = 2, or 1 where two would give the first
+ * hop fewer than four work items per SM), and the hop kernels' link staging:
  * 0 links read directly per RHS group; 1 staged in shared memory per work
  * item with asynchronous copies; 2 system-blocked: one block per tile serves
  * every RHS of its system in groups of the RHS-block width, the tile's links
