@@ -218,6 +218,53 @@ def time_steps(torch, stream_ptr, fn, steps, warmup):
     return [a.elapsed_time(b) for a, b in ev]
 
 
+def e2e_pipelined(torch, pair, upload, download, steps):
+    """ms per step of `steps` end-to-end steps through the public API, the
+    two batches of `pair` taking turns: step n uploads its inputs, solves and
+    downloads its solutions on batch n % 2, and its uploads and downloads run
+    (from a second host thread; the library's calls release the GIL) while
+    the other batch solves.  CUDA events on the first batch's stream bracket
+    every step's copies and solve, the first upload and the last download
+    included."""
+    import threading
+    for X in pair:  # warm-up: builds each batch's graph
+        upload(X)
+        X.solve(tol=TOL, max_iter=MAXIT)
+        download(X)
+    torch.cuda.synchronize()
+    s0 = torch.cuda.ExternalStream(pair[0].stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s0)
+    upload(pair[0])
+    for n in range(steps):
+        jobs = []
+        if n >= 1:
+            jobs.append((download, pair[(n - 1) % 2]))
+        if n + 1 < steps:
+            jobs.append((upload, pair[(n + 1) % 2]))
+        errors = []
+
+        def side():
+            try:
+                for fn, X in jobs:
+                    fn(X)
+            except Exception as e:  # re-raised on the main thread
+                errors.append(e)
+
+        t = threading.Thread(target=side)
+        t.start()
+        pair[n % 2].solve(tol=TOL, max_iter=MAXIT)
+        t.join()
+        if errors:
+            raise errors[0]
+    download(pair[(steps - 1) % 2])
+    torch.cuda.synchronize()
+    e1.record(s0)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
 # ---------------------------------------------------------------------------
 # CPU baselines: the reference's own CG on a sample stratified over the
 # batch's (lattice, mass, eps) classes
@@ -721,6 +768,8 @@ def main():
                     help="seconds of reference CPU solves for the cpu_baseline of the GPU arm")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-serial", action="store_true",
+                    help="end-to-end steps one after another only (no second batch alternating)")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--rhs-block", type=int, default=0,
                     help="RHS-block width of the hop kernels (0: time the schedules and keep the fastest)")
@@ -873,20 +922,42 @@ def main():
         h2d = sum(u.nbytes for u in host_U) + sum(x.nbytes for bs in host_b for x in bs)
         d2h = sum(x.nbytes for xs in host_x for x in xs)
 
+        def upload(X):
+            for k, s in enumerate(spec):
+                X.set_gauge(k, host_U[k])
+                for j in range(s["nrhs"]):
+                    X.set_rhs(k, j, host_b[k][j])
+
+        def download(X):
+            for k, s in enumerate(spec):
+                for j in range(s["nrhs"]):
+                    X.solution(k, j, out=host_x[k][j])
+
         def e2e_step():
-            for k, s in enumerate(spec):
-                B.set_gauge(k, host_U[k])
-                for j in range(s["nrhs"]):
-                    B.set_rhs(k, j, host_b[k][j])
+            upload(B)
             B.solve(tol=TOL, max_iter=MAXIT)
-            for k, s in enumerate(spec):
-                for j in range(s["nrhs"]):
-                    B.solution(k, j, out=host_x[k][j])
+            download(B)
 
         te = time_steps(torch, B.stream, e2e_step, max(2, args.steps // 2), 1)
-        mse = max_over_ranks(statistics.mean(te), world)
-        e2e = {"value": replica_value(world, total_rhs, mse), "unit": "solves/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        mse_serial = max_over_ranks(statistics.mean(te), world)
+        e2e = {"value": replica_value(world, total_rhs, mse_serial), "unit": "solves/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "mode": "serial"}
+        if not args.e2e_serial:
+            # two batches alternate: while one solves, a second host thread
+            # downloads the other's solutions and uploads its next inputs
+            B2 = sfh.Batch([(s["dims"], s["mass"], s["nrhs"]) for s in spec], precision=args.precision,
+                           device=local)
+            B2.set_schedule(*schedule)
+            B2.set_hop_widths(*hop_widths)
+            mse = max_over_ranks(e2e_pipelined(torch, (B, B2), upload, download, max(4, args.steps)), world)
+            B2.close()
+            e2e = {"value": replica_value(world, total_rhs, mse), "unit": "solves/s",
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "mode": ("pipelined: two batches on two streams alternate; each step uploads its gauge fields "
+                            "and sources from pinned host memory, solves and downloads every solution, its copies "
+                            "overlapping the other batch's solve (CUDA events around all steps)"),
+                   "serial": {"value": replica_value(world, total_rhs, mse_serial), "unit": "solves/s",
+                              "ms_per_step": mse_serial}, "ms_per_step": mse}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -133,3 +133,62 @@ def test_reference_arm_is_cpu_only_and_reports_the_same_workload(monkeypatch, ca
     assert line["cpu_baseline"]["kind"] in ("reference", "port", "mixed")
     assert line["reference_sample"]["solves_timed"] >= 2
     assert line["value"] > 0 and 0 < line["ms_per_step"] < 60000
+
+
+def test_e2e_pipeline_order():
+    """The pipelined end-to-end measurement: every step uploads, solves and
+    downloads on its own batch (n % 2); a batch's solutions are downloaded
+    before its next inputs are uploaded, and a step's upload happens before
+    its solve."""
+    import threading
+    import types
+
+    import bench
+
+    log, lock = [], threading.Lock()
+
+    class FakeBatch:
+        def __init__(self, name):
+            self.name, self.stream = name, 0
+
+        def solve(self, tol, max_iter):
+            with lock:
+                log.append(("solve", self.name))
+
+    class Ev:
+        def __init__(self, enable_timing=False):
+            pass
+
+        def record(self, s):
+            pass
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, other):
+            return 100.0
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(
+        synchronize=lambda: None, ExternalStream=lambda p: p, Event=Ev))
+
+    def upload(X):
+        with lock:
+            log.append(("up", X.name))
+
+    def download(X):
+        with lock:
+            log.append(("down", X.name))
+
+    pair = (FakeBatch("A"), FakeBatch("B"))
+    steps = 5
+    ms = bench.e2e_pipelined(fake_torch, pair, upload, download, steps)
+    assert ms == 100.0 / steps
+    timed = log[6:]  # after the warm-up: up, solve, down for each batch
+    assert log[:6] == [("up", "A"), ("solve", "A"), ("down", "A"), ("up", "B"), ("solve", "B"), ("down", "B")]
+    for op in ("up", "solve", "down"):
+        assert sum(1 for o, _ in timed if o == op) == steps
+    # per batch, the operations come in the order up, solve, down, up, ...
+    for name in ("A", "B"):
+        seq = [o for o, n in timed if n == name]
+        assert seq == ["up", "solve", "down"] * (len(seq) // 3), seq
+    assert [n for o, n in timed if o == "solve"] == ["A", "B", "A", "B", "A"]
