@@ -121,6 +121,15 @@ int sfh_dslash_timing(sfh_ctx* ctx, int storage, int nrep, double* ms_per_hop);
  * and the links to its links; the result returned in FP64.  The numerical
  * check of the kernels sfh_dslash_timing times. */
 int sfh_dslash_storage(sfh_ctx* ctx, int storage, const double* in, double* out);
+/* Test hook of the time-staged Dslash (storages 6 and 7), for checking its
+ * bounded waits without a GPU fault: each block announces extra_bytes (a
+ * multiple of 16, at most 65536) more on its barrier than its bulk copy
+ * delivers, so the copy lands but the barrier never completes, every
+ * staging wait runs out after its bound (about 0.1 s, twice per block), the
+ * blocks read their neighbours from global memory (same result) and the
+ * call returns SFH_ERR_TIMEOUT.  0, the default, turns it off.  No
+ * counterpart in the reference. */
+int sfh_set_staging_fault(sfh_ctx* ctx, int extra_bytes);
 
 /* ---- solver --------------------------------------------------------------- */
 /* X = (D D^dag)^{-1} phi to |r| < tol |phi|: solve_CG_DDdagger / solve_X_field

@@ -113,6 +113,7 @@ SIGNATURES = {
     "sfh_ddag": (ctypes.c_int, [_VP, _D, _D]),
     "sfh_dslash_timing": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _D]),
     "sfh_dslash_storage": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D]),
+    "sfh_set_staging_fault": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sfh_cg_solve": (ctypes.c_int, [_VP, _D, _D, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(CgInfo)]),
     "sfh_staples": (ctypes.c_int, [_VP, _D, _D]),
@@ -314,6 +315,12 @@ class Lattice:
         out = np.empty_like(psi)
         self._check(self.lib.sfh_dslash_storage(self.h, storage, _dptr(psi), _dptr(out)), "dslash storage")
         return out
+
+    def set_staging_fault(self, extra_bytes):
+        """Test hook of the time-staged Dslash (storages 6, 7): announce
+        extra_bytes more per block than its bulk copy delivers, so every
+        staging wait runs out (SFH_ERR_TIMEOUT, same result); 0 turns it off."""
+        self._check(self.lib.sfh_set_staging_fault(self.h, int(extra_bytes)), "set_staging_fault")
 
     def dslash_timing(self, storage, nrep=20):
         """ms per even-odd hop (V/2 output sites); storage 0 FP64-18, 1 FP32-12,

@@ -354,7 +354,7 @@ static void storage_hop(sfh_ctx* c, int storage, const void* U, int gp, int sp, 
                         int nq)
 {
     if (storage_tstaged(storage))
-        launch_hop_tstaged(c->g, gp, U, in, out, nullptr, 0.0, 1.0, q0, nq, c->derr, c->stream);
+        launch_hop_tstaged(c->g, gp, U, in, out, nullptr, 0.0, 1.0, q0, nq, c->derr, c->stage_extra_tx, c->stream);
     else
         launch_hop(c->g, gp, U, sp, in, sp, out, nullptr, 0.0, 1.0, q0, nq, c->stream);
 }
@@ -385,6 +385,18 @@ extern "C" int sfh_dslash_storage(sfh_ctx* c, int storage, const double* in, dou
     st = cuda_check(c, cudaStreamSynchronize(c->stream), "dslash storage");
     if (st) return st;
     return take_device_error(c, "dslash storage");
+}
+
+// Test hook of the time-staged Dslash (storages 6, 7): each block announces
+// extra_bytes more on its barrier than its bulk copy delivers, so the copy
+// lands but the barrier's phase never completes, every staging wait runs out
+// after its bound, the blocks read their neighbours from global memory, and
+// the call reports SFH_ERR_TIMEOUT.  0 (the default) turns it off.
+extern "C" int sfh_set_staging_fault(sfh_ctx* c, int extra_bytes)
+{
+    if (!c || extra_bytes < 0 || (extra_bytes & 15) || extra_bytes > (1 << 16)) return SFH_ERR_INVALID;
+    c->stage_extra_tx = (unsigned)extra_bytes;
+    return SFH_OK;
 }
 
 // Device time of one even-odd hop (V/2 output sites) in a storage format

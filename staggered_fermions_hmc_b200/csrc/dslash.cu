@@ -151,10 +151,12 @@ __global__ void __launch_bounds__(256, HopMinBlocks<GP>::v) hop_kernel(Geom g, c
 // memory, the x and y neighbours and the links from global memory.  The
 // arithmetic is hop_site's, operand for operand, so the result is
 // bit-identical to hop_kernel's.
+// extra_tx (a test hook, normally 0): bytes announced on the barrier beyond
+// the copy's, so that its phase never completes and every wait runs out.
 template <int GP, int SP, bool SELF>
 __global__ void __launch_bounds__(256, HopMinBlocks<GP>::v)
     hop_kernel_tstaged(Geom g, const void* __restrict__ gauge, const void* __restrict__ in, const void* self,
-                       void* out, double a, double b, int q0, int* err)
+                       void* out, double a, double b, int q0, int* err, unsigned extra_tx)
 {
     static_assert(SpinorFmt<SP>::scaled, "staging covers the one-word-per-site storages");
     extern __shared__ __align__(16) uint4 s_nb[];
@@ -165,7 +167,10 @@ __global__ void __launch_bounds__(256, HopMinBlocks<GP>::v)
     const TRange r = trange(g, i0, blockDim.x);
     if (threadIdx.x == 0) mbar_init(&s_bar, 1);
     __syncthreads();
-    if (threadIdx.x == 0) bulk_g2s(s_nb, src + r.lo, (unsigned)r.cnt * 16u, &s_bar);
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&s_bar, (unsigned)r.cnt * 16u + extra_tx);
+        bulk_copy_g2s(s_nb, src + r.lo, (unsigned)r.cnt * 16u, &s_bar);
+    }
     if (i >= g.Vh) return;  // every block has a site of its own, whose thread waits
     const Coord c = eo_coords(g, q, i);
     bool ok = mbar_wait_bounded(&s_bar, 0);
@@ -213,14 +218,14 @@ __global__ void __launch_bounds__(256, HopMinBlocks<GP>::v)
 
 template <int GP, int SP>
 void launch_typed_tstaged(const Geom& g, const void* gauge, const void* in, void* out, const void* self, double a,
-                          double b, int q0, int nq, int* err, cudaStream_t s)
+                          double b, int q0, int nq, int* err, unsigned extra_tx, cudaStream_t s)
 {
     dim3 grid((g.Vh + 255) / 256, nq);
     const size_t smem = (size_t)tstage_words(256, g.L[3]) * sizeof(uint4);
     if (self)
-        hop_kernel_tstaged<GP, SP, true><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err);
+        hop_kernel_tstaged<GP, SP, true><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err, extra_tx);
     else
-        hop_kernel_tstaged<GP, SP, false><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err);
+        hop_kernel_tstaged<GP, SP, false><<<grid, 256, smem, s>>>(g, gauge, in, self, out, a, b, q0, err, extra_tx);
 }
 
 template <int GP, int SP>
@@ -274,12 +279,13 @@ bool hop_tstaged_fits(const Geom& g)
 }
 
 void launch_hop_tstaged(const Geom& g, int gauge_prec, const void* gauge, const void* in, void* out,
-                        const void* self, double a, double b, int q0, int nq, int* err, cudaStream_t s)
+                        const void* self, double a, double b, int q0, int nq, int* err, unsigned extra_tx,
+                        cudaStream_t s)
 {
     if (gauge_prec == GP_F16_12)
-        launch_typed_tstaged<GP_F16_12, SP_F16>(g, gauge, in, out, self, a, b, q0, nq, err, s);
+        launch_typed_tstaged<GP_F16_12, SP_F16>(g, gauge, in, out, self, a, b, q0, nq, err, extra_tx, s);
     else if (gauge_prec == GP_BF16_12)
-        launch_typed_tstaged<GP_BF16_12, SP_BF16>(g, gauge, in, out, self, a, b, q0, nq, err, s);
+        launch_typed_tstaged<GP_BF16_12, SP_BF16>(g, gauge, in, out, self, a, b, q0, nq, err, extra_tx, s);
 }
 
 void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, const void* in,

@@ -43,6 +43,7 @@ struct sfh_ctx {
     sfh::CgWorkspace* ws[sfh::kNumPrecisions] = {};  // cached solver workspaces per precision
     double ws_mass[sfh::kNumPrecisions] = {};
     int sched_nb = 0, sched_tpi = 0, sched_stage = 0;  // schedule of the context's mixed-precision solves
+    unsigned stage_extra_tx = 0;  // test hook of the time-staged Dslash (sfh_set_staging_fault)
     sfh::CgWorkspace* ws_pair[sfh::kNumPrecisions] = {};  // two systems on the links (Hasenbusch pair)
     double ws_pair_mass[sfh::kNumPrecisions][2] = {};
     void* Utrial = nullptr;        // gauge backup for the Metropolis step
@@ -84,11 +85,14 @@ void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, c
 // launch_hop for the 16-bit storages (gauge_prec GP_F16_12 or GP_BF16_12,
 // vectors of the matching format) with the neighbours staged along the time
 // direction; a bounded staging wait that gives up sets DEV_ERR_TIMEOUT in
-// *err (the result is the same).  hop_tstaged_fits: the staged range of a
-// 256-site tile fits the default 48 KB of shared memory (Lt <= 2816).
+// *err (the result is the same).  extra_tx: a test hook, normally 0 (bytes
+// announced beyond each copy's, so that every staging wait runs out).
+// hop_tstaged_fits: the staged range of a 256-site tile fits the default
+// 48 KB of shared memory (Lt <= 2816).
 bool hop_tstaged_fits(const Geom& g);
 void launch_hop_tstaged(const Geom& g, int gauge_prec, const void* gauge, const void* in, void* out,
-                        const void* self, double a, double b, int q0, int nq, int* err, cudaStream_t s);
+                        const void* self, double a, double b, int q0, int nq, int* err, unsigned extra_tx,
+                        cudaStream_t s);
 
 cudaError_t launch_random_gauge(const Geom& g, double eps, unsigned long long seed, void* U, int* d_err,
                                 cudaStream_t s);

@@ -113,6 +113,29 @@ def test_dslash_time_staged_bit_identical(sfh, orc, dims):
         lat.close()
 
 
+def test_dslash_staging_wait_runs_out_and_the_context_stays_usable(sfh, orc):
+    """The staged Dslash's waits are bounded.  With the test hook on, every
+    block announces 16 bytes more on its barrier than its bulk copy
+    delivers: the copy lands, the barrier never completes, each wait gives
+    up after its bound, and the call reports SFH_ERR_TIMEOUT (no GPU fault:
+    no copy is left in flight).  With the hook off the next call succeeds
+    and equals the unstaged kernel's result."""
+    dims, mass = (4, 4, 4, 8), 0.1  # two blocks: one 256-site tile per parity
+    U = orc.random_gauge(dims, 1.0, 71)
+    psi = orc.random_spinor(dims, 72)
+    lat = sfh.Lattice(dims, mass)
+    try:
+        lat.upload_gauge(U)
+        with pytest.raises(sfh.SfhError) as e:
+            lat.set_staging_fault(16)
+            lat.dslash_storage(6, psi)
+        assert e.value.status == sfh.SFH_ERR_TIMEOUT
+        lat.set_staging_fault(0)
+        assert np.array_equal(lat.dslash_storage(6, psi), lat.dslash_storage(2, psi))
+    finally:
+        lat.close()
+
+
 def true_resid(orc, dims, mass, U, b, x):
     r = b - orc.ddag(dims, mass, U, x)
     return float(np.linalg.norm(r) / np.linalg.norm(b))
