@@ -142,7 +142,7 @@ int sfh_cg_solve(sfh_ctx* ctx, const double* phi, double* X, double tol, int max
 
 /* The schedule of the context's mixed-precision solves (sfh_cg_solve, the
  * trajectory's solves), as sfh_batch_set_schedule: RHS-block width, tiles per
- * block, link staging 0..6 (3: the whole solve in one persistent launch).
+ * block, link staging 0..7 (3: the whole solve in one persistent launch).
  * Default 0, 0, 0; the FP64 CG keeps its own (default tiles per block).  No
  * counterpart in the reference. */
 int sfh_set_schedule(sfh_ctx* ctx, int width, int tiles_per_block, int stage_links);
@@ -334,8 +334,8 @@ int sfh_batch_set_hop_widths(sfh_batch* batch, int hop1_width, int hop2_width);
 int sfh_batch_get_hop_widths(sfh_batch* batch, int* hop1_width, int* hop2_width);
 /* Autotuner: time probe_iters capped iterations for every RHS-block width
  * (1, 2, 4, 8; FP64: 1, 2), tiles-per-block count (1, 2, 4) and link staging
- * (0 to 6 as below; FP64: 0; 6 for FP16 only), and for the lane-list stages
- * (4 to 6) also hop widths 4 and 2, on the batch's current inputs and keep
+ * (0 to 7 as below; FP64: 0; 6 for FP16 only), and for the lane-list stages
+ * (4 to 7) also hop widths 4 and 2, on the batch's current inputs and keep
  * the fastest.
  * The schedule never changes the results.  No counterpart in the reference
  * (its solver has no schedule). */
@@ -360,8 +360,10 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * copy per RHS of the tile's range [i0 - Lt/2, i0 + 256 + Lt/2) of the other
  * parity, double-buffered across the work item's tiles (RHS groups of at
  * most 4; a staging wait that gives up fails the solve with SFH_ERR_TIMEOUT,
- * its solutions still exact).  Staging applies to the reduced precisions
- * only.  And its current values. */
+ * its solutions still exact).  7: 4 with the two hop kernels on grids of
+ * as many blocks as fit on the GPU at once, each block taking work items in
+ * turn from a device counter (no partial last wave; FP64 runs 0).  Staging
+ * applies to the reduced precisions only.  And its current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Bound on each grid-barrier wait of the persistent schedule (3), in polls
  * of about 128 ns (0 = the default, about 4 s): a wait that runs out fails

@@ -603,7 +603,9 @@ class Batch:
         the system, links read once per tile), 3 the system-blocked work in
         one persistent cooperative launch, 4 and 5: 0 and 1 with the reliable
         updates in lane-list kernels, 6 (FP16): 4 with each tile's time and z
-        neighbours staged in shared memory by bulk asynchronous copies."""
+        neighbours staged in shared memory by bulk asynchronous copies, 7: 4
+        with the hop kernels on resident grids taking their work items from
+        a device counter."""
         self._check(self.lib.sfh_batch_set_schedule(self.h, width, tiles_per_block, int(stage_links)),
                     "set_schedule")
 

@@ -641,16 +641,14 @@ __device__ __forceinline__ bool nst_next(const CgArgs& a, const NstItem& st, con
 
 // t = K p for the active lanes of one work item (tpi tiles of output parity
 // q, one RHS group); thi for lanes in a reliable update
-template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
-    cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST>
+__device__ __forceinline__ void hop1_item(const CgArgs& a, const int2 it, int cur)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     typename GaugeFmt<GP>::E* sl = reinterpret_cast<typename GaugeFmt<GP>::E*>(s_dyn);
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
     stage_item_sys(a, it, &s_sys);
     const CgSys& S = s_sys;
@@ -738,6 +736,29 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
     }
 }
 
+// DYN: a grid of resident blocks takes the work items in turn from a
+// device counter (a.qctr, zeroed by the iteration's update kernel), so no
+// partial last wave idles the SMs and uneven items balance; otherwise one
+// block per item
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false, bool DYN = false>
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, false, RUI>::v))
+    cg_hop1(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    if constexpr (DYN) {
+        __shared__ int s_next;
+        for (;;) {
+            if (threadIdx.x == 0) s_next = atomicAdd(a.qctr + 2 * cur + 0, 1);
+            __syncthreads();
+            const int idx = s_next;
+            if (idx >= a.nitems1) break;  // uniform across the block
+            hop1_item<GP, SP, NB, STG, RUI, NST>(a, items[idx], cur);
+            __syncthreads();  // the item's shared memory and s_next are free again
+        }
+    } else {
+        hop1_item<GP, SP, NB, STG, RUI, NST>(a, items[blockIdx.x], cur);
+    }
+}
+
 // reliable update at the lane's own site: x_hi += x_lo, x_lo = 0,
 // r = b - M x_hi; returns the |r|^2 contribution (FP64)
 template <int SP, int XP, bool COH = false>
@@ -816,16 +837,14 @@ __device__ __forceinline__ double site_dot(const Vec3<R>& a, const Vec3<R>& b)
 
 // own sites of one work item (tpi tiles, one RHS group): v = m^2 p - K t and
 // the four sums; reliable-update residuals
-template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false>
-__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
-    cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST>
+__device__ __forceinline__ void hop2_item(const CgArgs& a, const int2 it, int cur)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     typename GaugeFmt<GP>::E* sl = reinterpret_cast<typename GaugeFmt<GP>::E*>(s_dyn);
     typedef typename GaugeFmt<GP>::R R;
     typedef typename SpinorFmt<SP>::R RS;
     constexpr int XP = XFmt<SP>::v;
-    const int2 it = items[blockIdx.x];
     __shared__ CgSys s_sys;
     __shared__ double smem[32 * NB * kSums];
     __shared__ unsigned s_mask;
@@ -936,6 +955,29 @@ __global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
     }
 }
 
+// DYN: a grid of resident blocks takes the work items in turn from a
+// device counter (a.qctr, zeroed by the iteration's update kernel), so no
+// partial last wave idles the SMs and uneven items balance; otherwise one
+// block per item
+template <int GP, int SP, int NB, bool STG, bool RUI, bool NST = false, bool DYN = false>
+__global__ void __launch_bounds__(kTile, (HopOcc<GP, SP, NB, true, RUI>::v))
+    cg_hop2(CgArgs a, const int2* __restrict__ items, int cur)
+{
+    if constexpr (DYN) {
+        __shared__ int s_next;
+        for (;;) {
+            if (threadIdx.x == 0) s_next = atomicAdd(a.qctr + 2 * cur + 1, 1);
+            __syncthreads();
+            const int idx = s_next;
+            if (idx >= a.nitems2) break;  // uniform across the block
+            hop2_item<GP, SP, NB, STG, RUI, NST>(a, items[idx], cur);
+            __syncthreads();  // the item's shared memory and s_next are free again
+        }
+    } else {
+        hop2_item<GP, SP, NB, STG, RUI, NST>(a, items[blockIdx.x], cur);
+    }
+}
+
 // own sites of one lane (work item: tpi tiles, one RHS) if ACTIVE:
 // x += alpha p, r -= alpha v, p = r + beta p
 template <int SP, bool COH>
@@ -947,6 +989,12 @@ __device__ __forceinline__ void update_body(const CgArgs& a, int2 it, int cur, C
     // this iteration's reliable-update list was read by the kernels before
     // this one: empty it for the iteration after next
     if (a.ru_list && blockIdx.x == 0 && threadIdx.x == 0) a.ru_list[cur * (a.nlanes + 1)] = 0;
+    // this iteration's hop kernels have taken their work items: their
+    // counters start from zero again two iterations on
+    if (a.qctr && blockIdx.x == 0 && threadIdx.x == 0) {
+        a.qctr[2 * cur] = 0;
+        a.qctr[2 * cur + 1] = 0;
+    }
     stage_item_sys(a, it, s_sys);
     const CgSys& S = *s_sys;
     const ItemRange ir = item_range(a, S, it.x);
@@ -1480,6 +1528,8 @@ struct CgKernels {
     PersKernel pers;  // the whole solve in one cooperative launch (or null)
     bool nst = false;  // hop kernels stage their neighbours (schedule 6)
     size_t nst1 = 0, nst2 = 0;  // their staging buffers' bytes (set per workspace)
+    bool dyn = false;  // hop kernels take their work items from a counter (schedule 7)
+    int grid1 = 0, grid2 = 0;  // their resident grids (set per solve; 0: one block per item)
 };
 
 struct Phase {
@@ -1488,16 +1538,20 @@ struct Phase {
     size_t smem;
     int slot;       // timing slot
     bool list;      // walks the reliable-update lane list with a fixed grid
+    int grid;       // blocks of a resident grid taking items from a counter (0: one per item)
 };
+
+// blocks a phase launches for nitems work items
+static int phase_grid(const Phase& p, int nitems) { return p.grid > 0 ? std::min(p.grid, nitems) : nitems; }
 
 static int phases_of(const CgKernels& k, Phase (&ph)[kMaxPhases])
 {
     int n = 0;
-    ph[n++] = {k.hop1, k.nb1, k.smem + k.nst1, PH_HOP1, false};
-    if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1, true};
-    ph[n++] = {k.hop2, k.nb2, k.smem + k.nst2, PH_HOP2, false};
-    if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2, true};
-    ph[n++] = {k.update, 1, 0, PH_UPDATE, false};
+    ph[n++] = {k.hop1, k.nb1, k.smem + k.nst1, PH_HOP1, false, k.grid1};
+    if (k.ru1) ph[n++] = {k.ru1, k.nb1, 0, PH_RU1, true, 0};
+    ph[n++] = {k.hop2, k.nb2, k.smem + k.nst2, PH_HOP2, false, k.grid2};
+    if (k.ru2) ph[n++] = {k.ru2, k.nb2, 0, PH_RU2, true, 0};
+    ph[n++] = {k.update, 1, 0, PH_UPDATE, false, 0};
     return n;
 }
 
@@ -1604,6 +1658,25 @@ static CgKernels pick_nst(int nb1, int nb2)
     return k;
 }
 
+// schedule 7: schedule 4's kernels on resident grids taking their work
+// items from a counter
+template <int GP, int SP>
+static CgKernels pick_dyn(int nb1, int nb2)
+{
+    CgKernels k = pick_typed<GP, SP, false, false>(nb1, nb2);
+    if constexpr (SP != SP_F64) {
+        if (nb1 >= 8) { k.hop1 = cg_hop1<GP, SP, 8, false, false, false, true>; k.nb1 = 8; }
+        else if (nb1 >= 4) { k.hop1 = cg_hop1<GP, SP, 4, false, false, false, true>; k.nb1 = 4; }
+        else if (nb1 >= 2) { k.hop1 = cg_hop1<GP, SP, 2, false, false, false, true>; k.nb1 = 2; }
+        else { k.hop1 = cg_hop1<GP, SP, 1, false, false, false, true>; k.nb1 = 1; }
+        if (nb2 >= 4) { k.hop2 = cg_hop2<GP, SP, 4, false, false, false, true>; k.nb2 = 4; }
+        else if (nb2 >= 2) { k.hop2 = cg_hop2<GP, SP, 2, false, false, false, true>; k.nb2 = 2; }
+        else { k.hop2 = cg_hop2<GP, SP, 1, false, false, false, true>; k.nb2 = 1; }
+        k.dyn = true;
+    }
+    return k;
+}
+
 template <int GP, int SP>
 static CgKernels pick_staged(int nb1, int nb2, bool stage, bool list)
 {
@@ -1620,11 +1693,19 @@ static CgKernels pick_staged(int nb1, int nb2, bool stage, bool list)
 // (2 and 3: FP16, BF16 and FP32 12-real storage; FP32-18 takes 1)
 // stage 4, 5: 0, 1 with the reliable updates in the lane-list kernels
 // stage 6: 4 with the neighbours staged along the time direction (FP16; the
-// other precisions run 4)
+// other precisions run 4); stage 7: 4 with the hop kernels on resident grids
+// taking their work items from a counter (FP64 runs 0)
 static CgKernels pick_kernels(int prec, int nb1, int nb2, int stage)
 {
     CgKernels k;
     if (stage == 6 && prec == SFH_PREC_F16) return pick_nst<GP_F16_12, SP_F16>(nb1, nb2);
+    if (stage == 7) {
+        if (prec == SFH_PREC_F16) return pick_dyn<GP_F16_12, SP_F16>(nb1, nb2);
+        if (prec == SFH_PREC_F32) return pick_dyn<GP_F32_12, SP_F32>(nb1, nb2);
+        if (prec == SFH_PREC_BF16) return pick_dyn<GP_BF16_12, SP_BF16>(nb1, nb2);
+        if (prec == SFH_PREC_F32_18) return pick_dyn<GP_F32_18, SP_F32>(nb1, nb2);
+        stage = 0;  // FP64: schedule 0
+    }
     const bool sys = stage == 2 || stage == 3, pers = stage == 3, list = stage >= 4;
     const bool stg = stage == 1 || stage == 5 || (sys && prec == SFH_PREC_F32_18);
     if (prec == SFH_PREC_F64) k = pick_staged<GP_F64_18, SP_F64>(nb1, nb2, false, false);
@@ -1674,6 +1755,7 @@ struct CgWorkspace {
     int* d_active = nullptr;
     GridBar* d_bar = nullptr;  // grid barrier of the persistent solve
     int* d_rulist = nullptr;   // reliable-update lane lists [2][1 + nlanes]
+    int* d_qctr = nullptr;     // work-item counters of schedule 7 [2][2]
     bool timed_out = false;    // the last persistent solve gave up at a barrier
     long long barrier_polls = 0;  // bound on each barrier wait (0: the default)
     int num_sms = 0;
@@ -1716,7 +1798,7 @@ struct CgWorkspace {
         allocs.clear();
         item_cache.clear();
         d_sys = nullptr; d_rhs = nullptr; d_lanes = nullptr;
-        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr; d_bar = nullptr; d_rulist = nullptr;
+        d_tile_sys = nullptr; d_partial = nullptr; d_active = nullptr; d_bar = nullptr; d_rulist = nullptr; d_qctr = nullptr;
     }
     cudaError_t alloc(void** p, size_t n)
     {
@@ -1880,6 +1962,8 @@ static CgArgs make_args(const CgWorkspace& w, double tol, int maxit, double delt
     a.ru_list = nullptr;
     a.nst_words = 0;
     a.err = nullptr;
+    a.qctr = nullptr;
+    a.nitems1 = a.nitems2 = 0;
     return a;
 }
 
@@ -1916,7 +2000,7 @@ static cudaError_t ensure_graph(CgWorkspace& w, const CgKernels& k, CgArgs a, do
             cudaKernelNodeParams p;
             std::memset(&p, 0, sizeof(p));
             p.func = (void*)ph[j].fn;
-            p.gridDim = dim3(nitems[j]);
+            p.gridDim = dim3(phase_grid(ph[j], nitems[j]));
             p.blockDim = dim3(kTile);
             p.sharedMemBytes = (unsigned)ph[j].smem;
             void* args[] = {&a, (void*)&items[j], &cur};
@@ -2079,6 +2163,19 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         a.nst_words = nst_words;
         a.err = &w.d_bar->err;
     }
+    if (k.dyn) {  // resident grids: as many blocks as fit at once, at most one per item
+        if (!w.d_qctr && (e = w.alloc((void**)&w.d_qctr, 4 * sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(w.d_qctr, 0, 4 * sizeof(int), stream)) != cudaSuccess) return e;
+        const int2* it;
+        if ((e = items_for(w, k.nb1, a.tpi, &it, &a.nitems1)) != cudaSuccess) return e;
+        if ((e = items_for(w, k.nb2, a.tpi, &it, &a.nitems2)) != cudaSuccess) return e;
+        int b1 = 0, b2 = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k.hop1, kTile, k.smem)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k.hop2, kTile, k.smem)) != cudaSuccess) return e;
+        k.grid1 = std::max(1, b1) * w.num_sms;
+        k.grid2 = std::max(1, b2) * w.num_sms;
+        a.qctr = w.d_qctr;
+    }
     if (k.ru1 || k.pers) {  // reliable updates by lane list: both lists start empty
         a.ru_list = w.d_rulist;
         if ((e = cudaMemsetAsync(w.d_rulist, 0, sizeof(int) * 2 * (w.nlanes + 1), stream)) != cudaSuccess) return e;
@@ -2132,7 +2229,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
             if ((e = cudaEventRecord(ev[0], stream)) != cudaSuccess) { destroy_events(); return e; }
             for (int it = 0; it < kChunk; ++it)
                 for (int j = 0; j < nph; ++j) {
-                    ph[j].fn<<<nitems[j], kTile, ph[j].smem, stream>>>(a, items[j], it & 1);
+                    ph[j].fn<<<phase_grid(ph[j], nitems[j]), kTile, ph[j].smem, stream>>>(a, items[j], it & 1);
                     if ((e = cudaEventRecord(ev[nph * it + j + 1], stream)) != cudaSuccess) {
                         destroy_events();
                         return e;
@@ -2757,7 +2854,7 @@ extern "C" int sfh_batch_autotune(sfh_batch* b, int probe_iters, int* best_width
     const int ncand = f64 ? 2 : 4;
     double best = 1e300;
     int bw = 1, bw2 = 1, bt = 2, bs = 0;
-    for (int stage = 0; stage < (f64 ? 1 : 7); ++stage)
+    for (int stage = 0; stage < (f64 ? 1 : 8); ++stage)
         for (int c = 0; c < ncand + 1; ++c)
             for (int tp : tiles) {
                 if (stage == 6 && b->prec != SFH_PREC_F16) continue;  // schedule 4 there
@@ -2796,7 +2893,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
     if (!b || width < 0 || tiles_per_block < 0 || tiles_per_block > 64) return SFH_ERR_INVALID;
     b->nb = b->nb2 = width;
     b->tpi = tiles_per_block;
-    if (stage_links < 0 || stage_links > 6) return SFH_ERR_INVALID;
+    if (stage_links < 0 || stage_links > 7) return SFH_ERR_INVALID;
     b->stage_links = stage_links;
     return SFH_OK;
 }
@@ -2804,7 +2901,7 @@ extern "C" int sfh_batch_set_schedule(sfh_batch* b, int width, int tiles_per_blo
 extern "C" int sfh_set_schedule(sfh_ctx* c, int width, int tiles_per_block, int stage_links)
 {
     if (!c || width < 0 || width > 8 || tiles_per_block < 0 || tiles_per_block > 64 || stage_links < 0 ||
-        stage_links > 6)
+        stage_links > 7)
         return SFH_ERR_INVALID;
     c->sched_nb = width;
     c->sched_tpi = tiles_per_block;

@@ -66,6 +66,11 @@ struct CgArgs {
     // word a staging wait that gives up sets DEV_ERR_TIMEOUT in (null: unused)
     int nst_words;
     int* err;
+    // work-item counters of the hop kernels with a resident grid (schedule
+    // 7): [iteration parity][hop1, hop2], zeroed by the update kernel of the
+    // same iteration; the item counts of the two hops (null / 0: unused)
+    int* qctr;
+    int nitems1, nitems2;
 };
 
 namespace {

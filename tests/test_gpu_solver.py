@@ -314,6 +314,46 @@ def test_batch_neighbour_staging_bit_identical(sfh, orc):
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1.5e-10
 
 
+@pytest.mark.parametrize("precision", ["f16", "f32", "bf16", "f32_18", "f64"])
+def test_batch_resident_grid_schedule_bit_identical(sfh, orc, precision):
+    """Schedule 7 (the hop kernels on grids of resident blocks, each taking
+    work items in turn from a device counter that the update kernel zeroes)
+    gives schedule 4's solutions bit for bit, over several solves of the
+    same batch (the counters start from zero each time) and in the timed
+    solve; FP64 runs schedule 0 for both."""
+    systems = [((4, 4, 4, 8), 0.1, 5), ((6, 6, 6, 6), 0.05, 3), ((8, 8, 8, 8), 0.2, 2)]
+    fields = [orc.random_gauge(d, 0.5 + 0.25 * (k % 2), 120 + k) for k, (d, m, n) in enumerate(systems)]
+
+    def run(stage, w1, w2, tiles, timed=False):
+        B = sfh.Batch(systems, precision=precision)
+        B.set_schedule(w2, tiles, stage)
+        B.set_hop_widths(w1, w2)
+        for k, (d, m, n) in enumerate(systems):
+            B.set_gauge(k, fields[k])
+            for j in range(n):
+                B.set_rhs(k, j, orc.random_spinor(d, 1300 + 10 * k + j))
+        out = []
+        for _ in range(2):
+            if timed:
+                B.solve_timed(tol=1e-10)
+            else:
+                B.solve(tol=1e-10)
+            out.append([B.solution(k, j) for k, (d, m, n) in enumerate(systems) for j in range(n)])
+        return out
+
+    for w1, w2, tiles in ((4, 2, 4), (2, 2, 1), (1, 1, 2)):
+        ref = run(4, w1, w2, tiles)
+        got = run(7, w1, w2, tiles)
+        for a, b in zip(ref, got):
+            assert all(np.array_equal(x, y) for x, y in zip(a, b)), (w1, w2, tiles)
+    got = run(7, 4, 2, 4, timed=True)
+    assert all(np.array_equal(x, y) for x, y in zip(run(4, 4, 2, 4)[0], got[1]))
+    d, m, n = systems[2]
+    b = orc.random_spinor(d, 1300 + 20 + 1)
+    r = b - orc.ddag(d, m, fields[2], got[1][5 + 3 + 1])
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.5e-10
+
+
 def test_batch_autotune_keeps_results(sfh, orc):
     """The autotuner only changes the schedule: solutions are bit-identical."""
     systems = [((4, 4, 4, 8), 0.1, 3), ((6, 6, 6, 6), 0.2, 2)]
