@@ -360,10 +360,11 @@ int sfh_batch_autotune(sfh_batch* batch, int probe_iters, int* best_width);
  * copy per RHS of the tile's range [i0 - Lt/2, i0 + 256 + Lt/2) of the other
  * parity, double-buffered across the work item's tiles (RHS groups of at
  * most 4; a staging wait that gives up fails the solve with SFH_ERR_TIMEOUT,
- * its solutions still exact).  7: 4 with the two hop kernels on grids of
- * as many blocks as fit on the GPU at once, each block taking work items in
- * turn from a device counter (no partial last wave; FP64 runs 0).  Staging
- * applies to the reduced precisions only.  And its current values. */
+ * the thread reading that tile from global memory).  7: 4 with the two hop
+ * kernels on grids of as many blocks as fit on the GPU at once, each block
+ * taking work items in turn from a device counter (no partial last wave;
+ * FP64 runs 0).  Staging applies to the reduced precisions only.  And its
+ * current values. */
 int sfh_batch_set_schedule(sfh_batch* batch, int width, int tiles_per_block, int stage_links);
 /* Bound on each grid-barrier wait of the persistent schedule (3), in polls
  * of about 128 ns (0 = the default, about 4 s): a wait that runs out fails

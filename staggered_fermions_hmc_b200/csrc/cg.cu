@@ -2261,7 +2261,7 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
         (e = cudaMemcpyAsync(&err, &w.d_bar->err, sizeof(int), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
         return e;
     if ((e = finish_solve(w, stream)) != cudaSuccess) return e;
-    w.timed_out = err != 0;  // a staging wait gave up (the solution is still exact)
+    w.timed_out = err != 0;  // a staging wait gave up: the solve reports SFH_ERR_TIMEOUT
     return cudaSuccess;
 }
 

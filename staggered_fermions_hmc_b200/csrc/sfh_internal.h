@@ -85,8 +85,9 @@ void launch_hop(const Geom& g, int gauge_prec, const void* gauge, int in_prec, c
 // launch_hop for the 16-bit storages (gauge_prec GP_F16_12 or GP_BF16_12,
 // vectors of the matching format) with the neighbours staged along the time
 // direction; a bounded staging wait that gives up sets DEV_ERR_TIMEOUT in
-// *err (the result is the same).  extra_tx: a test hook, normally 0 (bytes
-// announced beyond each copy's, so that every staging wait runs out).
+// *err, and the thread reads its neighbours from global memory instead.
+// extra_tx: a test hook, normally 0 (bytes announced beyond each copy's, so
+// that every staging wait runs out).
 // hop_tstaged_fits: the staged range of a 256-site tile fits the default
 // 48 KB of shared memory (Lt <= 2816).
 bool hop_tstaged_fits(const Geom& g);
