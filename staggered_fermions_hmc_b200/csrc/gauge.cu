@@ -39,7 +39,9 @@ __device__ __forceinline__ M3 path(const void* U, const Geom& g, Walker w, const
     return m;
 }
 
-// A1 (plaquette staples) and A2 (rectangle staples) of link (x, mu)
+// A1 (plaquette staples) and A2 (rectangle staples) of link (x, mu); RECT
+// false: A1 alone (the same paths in the same order, A2 left zero)
+template <bool RECT = true>
 __device__ void staples(const void* U, const Geom& g, const Walker& x, int mu, M3& A1, M3& A2)
 {
     Walker xp = x;
@@ -55,6 +57,7 @@ __device__ void staples(const void* U, const Geom& g, const Walker& x, int mu, M
         const int bot[3] = {-N, -M, +N};
         m3_acc(A1, path(U, g, xp, top));
         m3_acc(A1, path(U, g, xp, bot));
+        if constexpr (!RECT) continue;
         const int r1[5] = {-N, -N, -M, +N, +N};
         const int r2[5] = {+N, +N, -M, -N, -N};
         const int r3[5] = {+M, -N, -M, -M, +N};
@@ -265,7 +268,10 @@ __global__ void __launch_bounds__(kRedThreads) reduce_kernel(Geom g, int kind, c
             } else {
                 Walker x = link_coords(g, p, i);
                 M3 A1, A2;
-                staples(A, g, x, mu, A1, A2);
+                if (kind == RED_PLAQ)
+                    staples<false>(A, g, x, mu, A1, A2);  // the plaquette staples only
+                else
+                    staples(A, g, x, mu, A1, A2);
                 M3 Ux = link_at(A, g, x, mu);
                 double plaq = m3_tr(m3_mul(Ux, A1)).re;
                 if (kind == RED_PLAQ) {
