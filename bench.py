@@ -254,8 +254,10 @@ def e2e_pipelined(torch, pair, upload, download, steps):
 
         t = threading.Thread(target=side)
         t.start()
-        pair[n % 2].solve(tol=TOL, max_iter=MAXIT)
-        t.join()
+        try:
+            pair[n % 2].solve(tol=TOL, max_iter=MAXIT)
+        finally:
+            t.join()
         if errors:
             raise errors[0]
     download(pair[(steps - 1) % 2])

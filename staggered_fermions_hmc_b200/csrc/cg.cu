@@ -2150,8 +2150,12 @@ static cudaError_t workspace_solve(CgWorkspace& w, double tol, int maxit, double
             k = pick_kernels(w.prec, nb1, nb2, 4);
             nst_words = 0;
         } else {
-            cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.nst1);
-            cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.nst2);
+            if ((e = cudaFuncSetAttribute((const void*)k.hop1, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)k.nst1)) != cudaSuccess)
+                return e;
+            if ((e = cudaFuncSetAttribute((const void*)k.hop2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)k.nst2)) != cudaSuccess)
+                return e;
             if (!w.d_bar && (e = w.alloc((void**)&w.d_bar, sizeof(GridBar))) != cudaSuccess) return e;
             if ((e = cudaMemsetAsync(&w.d_bar->err, 0, sizeof(int), stream)) != cudaSuccess) return e;
         }
