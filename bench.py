@@ -519,7 +519,7 @@ def run_extras(sfh, hbm, quick=False):
         ms = lat.dslash_timing(st, nrep=20)
         gbs = DSLASH_BYTES[st] * Vh / (ms * 1e-3) / 1e9
         ds[DSLASH_NAMES[st]] = {"ms_per_hop": ms, "GB/s": gbs, "frac": gbs / hbm,
-                                "bytes_per_site": DSLASH_BYTES[st]}
+                                "frac_of_spec": gbs / HBM_SPEC_GBS, "bytes_per_site": DSLASH_BYTES[st]}
     ex["dslash_32x32x32x64"] = ds
     # ill-conditioned single solve: 32^3x64, eps = 1.0, m = 0.01; each
     # solution's true residual by the oracle's D D^dag on the host
@@ -625,6 +625,7 @@ HMC_KERNEL_COST = {  # (bytes, flops) per link
     "plaquette": (144, 13 * 198),
 }
 FP64_TFLOPS_NOMINAL = 40.0  # B200 datasheet FP64 (no measured FP64 peak on this pool)
+HBM_SPEC_GBS = 8000.0  # B200 datasheet HBM3e bandwidth; fractions of it are reported beside the measured ones
 
 
 def hmc_kernel_table(lat, hbm):
@@ -997,7 +998,8 @@ def main():
         "data": "synthetic (seeded exp(i eps H) links, N(0,1) sources)",
         "config": workload_config(spec, world),
         "roofline": {"bound": "hbm", "achieved": top_gbs, "peak": hbm, "unit": "GB/s",
-                     "frac": top_gbs / hbm, "traffic": top_traffic, "peak_kind": peak_kind,
+                     "frac": top_gbs / hbm, "frac_of_spec": top_gbs / HBM_SPEC_GBS, "spec_gbs": HBM_SPEC_GBS,
+                     "traffic": top_traffic, "peak_kind": peak_kind,
                      "kernel": top, "alg_bytes_per_launch": kbytes[top] / top_n,
                      "ms_per_launch": kernels[top]["ms_total"] / top_n},
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
@@ -1005,6 +1007,7 @@ def main():
         "extras": extras,
         "kernels": kernels,
         "solve_roofline": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                           "frac_of_spec": achieved / HBM_SPEC_GBS,
                            "alg_bytes_per_step": alg_bytes,
                            "what": "every iteration kernel, graph replay, per timed step"},
         "other_mixed_precisions": other,
