@@ -109,3 +109,17 @@ def test_python_constants_match_header():
         py = name if name.startswith(("SFH_OK", "SFH_ERR_")) else name[len("SFH_"):]
         assert getattr(sfh, py) == value, (name, py)
     assert sorted(sfh.PRECISIONS.values()) == sorted(v for k, v in defines.items() if k.startswith("SFH_PREC_"))
+
+
+def test_null_handles_rejected_without_a_gpu():
+    """Entry points check their handle before any CUDA call: a null context
+    or batch gives SFH_ERR_INVALID (the staged Dslash storages, its test
+    hook and the schedules among them)."""
+    import staggered_fermions_hmc_b200 as sfh
+    lib = sfh.load_library()
+    buf = (ctypes.c_double * 8)()
+    assert lib.sfh_set_staging_fault(None, 0) == sfh.SFH_ERR_INVALID
+    assert lib.sfh_dslash_storage(None, 6, buf, buf) == sfh.SFH_ERR_INVALID
+    assert lib.sfh_set_schedule(None, 2, 4, 7) == sfh.SFH_ERR_INVALID
+    assert lib.sfh_batch_set_schedule(None, 2, 4, 6) == sfh.SFH_ERR_INVALID
+    assert lib.sfh_batch_set_hop_widths(None, 4, 2) == sfh.SFH_ERR_INVALID

@@ -192,3 +192,46 @@ def test_e2e_pipeline_order():
         seq = [o for o, n in timed if n == name]
         assert seq == ["up", "solve", "down"] * (len(seq) // 3), seq
     assert [n for o, n in timed if o == "solve"] == ["A", "B", "A", "B", "A"]
+
+
+def test_e2e_pipeline_reraises_a_side_thread_error():
+    """An upload that fails on the side thread is raised on the main thread
+    once the step's solve has returned (the side thread is joined first)."""
+    import types
+
+    import bench
+
+    class Ev:
+        def __init__(self, enable_timing=False):
+            pass
+
+        def record(self, s):
+            pass
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, other):
+            return 1.0
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(
+        synchronize=lambda: None, ExternalStream=lambda p: p, Event=Ev))
+    solves = []
+
+    class FakeBatch:
+        def __init__(self, name):
+            self.name, self.stream = name, 0
+
+        def solve(self, tol, max_iter):
+            solves.append(self.name)
+
+    uploads = []
+
+    def upload(X):
+        uploads.append(X.name)
+        if len(uploads) > 3:  # the warm-up's two and the first timed one succeed
+            raise RuntimeError("upload failed")
+
+    with pytest.raises(RuntimeError, match="upload failed"):
+        bench.e2e_pipelined(fake_torch, (FakeBatch("A"), FakeBatch("B")), upload, lambda X: None, 4)
+    assert solves == ["A", "B", "A"]  # the step whose side thread failed still finished its solve
